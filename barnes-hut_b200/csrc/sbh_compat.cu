@@ -1,0 +1,946 @@
+// Reference-compatible ("compat") entry points: the softened direct sums,
+// the dense Morton octree8 build and its classic and stochastic Barnes-Hut
+// traversals, all on the reference's byte layouts.
+//
+// This translation unit is compiled with --use_fast_math, the flag the
+// reference's sbh_ffi target uses (CMakeLists.txt:39), so that the Morton
+// quantisation (v - min) / span runs the same division instruction and
+// produces the same codes, and the opening tests round the same way.
+//
+// Differences from the reference that are deliberate (and invisible at the
+// byte level except where noted):
+//  * no cudaMalloc/cudaFree, no D2H copy and no stream synchronisation: the
+//    bounding span is computed on the device and temporaries live in a
+//    caller-provided workspace (the reference syncs the stream and allocates
+//    4*depth+12 buffers per build, src/sbh_ffi.cu:1111-1370);
+//  * leaves are ordered by a stable radix sort of (Morton code, input index),
+//    so the order inside one leaf cell is the input order (the reference's
+//    atomic cursor makes it nondeterministic, src/sbh_ffi.cu:1732);
+//  * the upward pass sums in FP64 (prefix sums over the sorted leaves), the
+//    reference accumulates FP32 atomics;
+//  * parameters travel by value, not through __constant__ globals, so calls
+//    on concurrent streams do not race (src/sbh_ffi.cu:2536-2561);
+//  * a traversal whose stack would exceed 128 entries records
+//    SBH_DEV_STACK_OVERFLOW instead of writing past the array.
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+
+#include <cstdint>
+#include <string>
+
+#include "sbh_common.cuh"
+#include "sbh_primitives.cuh"
+
+namespace sbh {
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+  float y = v - c;
+  float t = s + y;
+  c = (t - s) - y;
+  s = t;
+}
+
+// ---------------------------------------------------------------------------
+// Direct sums (src/sbh_ffi.cu:399-546), shared-memory tiled, one query per
+// thread, Kahan-compensated across tiles.
+// ---------------------------------------------------------------------------
+constexpr int kDirectThreads = 256;
+
+template <int VJP>
+__global__ void __launch_bounds__(kDirectThreads)
+    direct_soft_kernel(const float* __restrict__ pts, const float* __restrict__ masses, int64_t n,
+                       const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq,
+                       float* __restrict__ out, Soft s, Periodic per) {
+  __shared__ float4 tile[kDirectThreads];
+  int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  bool active = qi < nq;
+  float qx = 0.f, qy = 0.f, qz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+  if (active) {
+    qx = queries[3 * qi];
+    qy = queries[3 * qi + 1];
+    qz = queries[3 * qi + 2];
+    if (VJP) {
+      gx = cot[3 * qi];
+      gy = cot[3 * qi + 1];
+      gz = cot[3 * qi + 2];
+    }
+  }
+  float inv_l = (per.on && per.box > 0.0f) ? 1.0f / per.box : 0.0f;
+  float sx = 0.f, sy = 0.f, sz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+  for (int64_t base = 0; base < n; base += kDirectThreads) {
+    int64_t j = base + threadIdx.x;
+    tile[threadIdx.x] =
+        j < n ? make_float4(pts[3 * j], pts[3 * j + 1], pts[3 * j + 2], masses[j]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    int cnt = static_cast<int>(n - base < kDirectThreads ? n - base : kDirectThreads);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for (int k = 0; k < cnt; k++) {
+      float4 p = tile[k];
+      float rx = min_image_rint(qx - p.x, inv_l, per);
+      float ry = min_image_rint(qy - p.y, inv_l, per);
+      float rz = min_image_rint(qz - p.z, inv_l, per);
+      if (VJP) {
+        soft_vjp_accum(rx, ry, rz, p.w, gx, gy, gz, s, ax, ay, az);
+      } else {
+        float c = soft_coeff(rx * rx + ry * ry + rz * rz, p.w, s);
+        ax += c * rx;
+        ay += c * ry;
+        az += c * rz;
+      }
+    }
+    kahan_add(sx, cx, ax);
+    kahan_add(sy, cy, ay);
+    kahan_add(sz, cz, az);
+    __syncthreads();
+  }
+  if (active) {
+    out[3 * qi] = sx;
+    out[3 * qi + 1] = sy;
+    out[3 * qi + 2] = sz;
+  }
+}
+
+__global__ void __launch_bounds__(kDirectThreads)
+    bruteforce_gravity_kernel(const float* __restrict__ pts, const float* __restrict__ masses, int64_t n,
+                              int dim, const float* __restrict__ queries, int64_t nq,
+                              float* __restrict__ out, Periodic per) {
+  __shared__ float4 tile[kDirectThreads];
+  int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  bool active = qi < nq;
+  float q0 = 0.f, q1 = 0.f, q2 = 0.f;
+  if (active) {
+    q0 = queries[dim * qi];
+    q1 = queries[dim * qi + 1];
+    q2 = dim == 3 ? queries[dim * qi + 2] : 0.f;
+  }
+  float s = 0.f, c = 0.f;
+  for (int64_t base = 0; base < n; base += kDirectThreads) {
+    int64_t j = base + threadIdx.x;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (j < n) v = make_float4(pts[dim * j], pts[dim * j + 1], dim == 3 ? pts[dim * j + 2] : 0.f, masses[j]);
+    tile[threadIdx.x] = v;
+    __syncthreads();
+    int cnt = static_cast<int>(n - base < kDirectThreads ? n - base : kDirectThreads);
+    float a = 0.f;
+    for (int k = 0; k < cnt; k++) {
+      float4 p = tile[k];
+      // src/sbh_ffi.cu:414-426: diff = p - q, wrapped with nearbyint(diff / L)
+      float d0 = p.x - q0, d1 = p.y - q1, d2 = p.z - q2;
+      if (per.on && per.box > 0.0f) {
+        d0 -= per.box * nearbyintf(d0 / per.box);
+        d1 -= per.box * nearbyintf(d1 / per.box);
+        if (dim == 3) d2 -= per.box * nearbyintf(d2 / per.box);
+      }
+      float dsq = d0 * d0 + d1 * d1;
+      if (dim == 3) dsq += d2 * d2;
+      a += -p.w / (sqrtf(dsq) + 1e-1f);
+    }
+    kahan_add(s, c, a);
+    __syncthreads();
+  }
+  if (active) out[qi] = s;
+}
+
+// ---------------------------------------------------------------------------
+// octree8 build (src/sbh_ffi.cu:1039-1420)
+// ---------------------------------------------------------------------------
+struct O8Params {
+  float min[3];
+  float span;
+  float cx, cy, cz, half;
+  int valid;
+};
+
+// span = max axis extent, root centre = min + span/2 (src/sbh_ffi.cu:1128-1133,1395-1398).
+__global__ void o8_setup_kernel(const float* min_corner, const float* max_corner, O8Params* prm,
+                                uint32_t* status) {
+  float mn0 = min_corner[0], mn1 = min_corner[1], mn2 = min_corner[2];
+  float span = fmaxf(fmaxf(max_corner[0] - mn0, max_corner[1] - mn1), max_corner[2] - mn2);
+  O8Params p;
+  p.min[0] = mn0;
+  p.min[1] = mn1;
+  p.min[2] = mn2;
+  p.span = span;
+  p.cx = mn0 + span * 0.5f;
+  p.cy = mn1 + span * 0.5f;
+  p.cz = mn2 + span * 0.5f;
+  p.half = span * 0.5f;
+  p.valid = span > 0.0f ? 1 : 0;
+  if (!p.valid) raise_status(status, SBH_DEV_BAD_BOUNDS);
+  *prm = p;
+}
+
+// quantize_axis (src/sbh_ffi.cu:173-179); fast-math division like the reference.
+__device__ __forceinline__ uint32_t o8_quantize(float v, float min_v, float span, int bits) {
+  float t = (v - min_v) / span;
+  t = fminf(fmaxf(t, 0.0f), 0.999999f);
+  uint32_t max_bin = (1u << bits) - 1u;
+  return static_cast<uint32_t>(t * static_cast<float>(max_bin + 1));
+}
+
+__device__ __forceinline__ uint32_t o8_morton(uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint32_t code = 0;
+  for (int i = 0; i < bits; i++) {
+    code |= ((x >> i) & 1u) << (3 * i);
+    code |= ((y >> i) & 1u) << (3 * i + 1);
+    code |= ((z >> i) & 1u) << (3 * i + 2);
+  }
+  return code;
+}
+
+__global__ void o8_codes_kernel(const float* __restrict__ pts, int64_t n, const O8Params* __restrict__ prm,
+                                int depth, uint32_t* __restrict__ codes, uint32_t* __restrict__ counts) {
+  if (!prm->valid) return;
+  float mn0 = prm->min[0], mn1 = prm->min[1], mn2 = prm->min[2], span = prm->span;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t qx = o8_quantize(pts[3 * i], mn0, span, depth);
+    uint32_t qy = o8_quantize(pts[3 * i + 1], mn1, span, depth);
+    uint32_t qz = o8_quantize(pts[3 * i + 2], mn2, span, depth);
+    uint32_t c = o8_morton(qx, qy, qz, depth);
+    codes[i] = c;
+    atomicAdd(&counts[c], 1u);
+  }
+}
+
+// Leaf records in sorted order (src/sbh_ffi.cu:1723-1743 writes the same record).
+__global__ void o8_gather_kernel(const float* __restrict__ pts, const float* __restrict__ nrm,
+                                 const float* __restrict__ masses, int64_t n,
+                                 const uint32_t* __restrict__ perm, const O8Params* __restrict__ prm,
+                                 Leaf3* __restrict__ leaf) {
+  if (prm && !prm->valid) return;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t s = perm[i];
+    float4 a = make_float4(pts[3 * s], pts[3 * s + 1], pts[3 * s + 2], nrm ? nrm[3 * s] : 0.f);
+    float4 b = make_float4(nrm ? nrm[3 * s + 1] : 0.f, nrm ? nrm[3 * s + 2] : 0.f, masses[s], 1.0f);
+    float4* dst = reinterpret_cast<float4*>(leaf + i);
+    dst[0] = a;
+    dst[1] = b;
+  }
+}
+
+// FP64 moment vector of a leaf record: (m, m x, m y, m z, m nx, m ny, m nz).
+struct LeafMomentLoad {
+  const Leaf3* leaf;
+  __device__ DVec<7> operator()(int64_t i) const {
+    const float4* p = reinterpret_cast<const float4*>(leaf + i);
+    float4 a = p[0], b = p[1];
+    double m = b.z;
+    DVec<7> r;
+    r.v[0] = m;
+    r.v[1] = m * a.x;
+    r.v[2] = m * a.y;
+    r.v[3] = m * a.z;
+    r.v[4] = m * a.w;
+    r.v[5] = m * b.x;
+    r.v[6] = m * b.y;
+    return r;
+  }
+};
+
+// One thread per dense node, all levels (src/sbh_ffi.cu:1788-1876).
+__global__ void o8_nodes_kernel(OctreeNode8* __restrict__ nodes, Leaf3* __restrict__ contrib,
+                                const uint32_t* __restrict__ off, const DVec<7>* __restrict__ P,
+                                int depth, uint64_t total, const O8Params* __restrict__ prm) {
+  if (!prm->valid) return;
+  float cx0 = prm->cx, cy0 = prm->cy, cz0 = prm->cz, half0 = prm->half;
+  for (uint64_t node_idx = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; node_idx < total;
+       node_idx += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    int level = 0;
+    uint64_t level_off = 0, level_n = 1;
+    while (node_idx >= level_off + level_n) {
+      level_off += level_n;
+      level_n <<= 3;
+      level++;
+    }
+    uint32_t idx = static_cast<uint32_t>(node_idx - level_off);
+    int shift = 3 * (depth - level);
+    uint64_t first_leaf = static_cast<uint64_t>(idx) << shift;
+    uint64_t last_leaf = static_cast<uint64_t>(idx + 1) << shift;
+    OctreeNode8 nd;
+    nd.start = off[first_leaf];
+    nd.end = off[last_leaf];
+    nd.depth = static_cast<uint8_t>(level);
+    nd.parent = level == 0 ? static_cast<uint32_t>(node_idx)
+                           : static_cast<uint32_t>(level_off - (level_n >> 3) + (idx >> 3));
+    nd.is_leaf = level == depth ? 1 : 0;
+    nd.first_child = 0xFFFFFFFFu;
+    nd.child_mask = 0;
+    nd.pad0 = 0;
+    int grid = 1 << level;
+    int ix = 0, iy = 0, iz = 0;
+    for (int b = 0; b < level; b++) {
+      ix |= ((idx >> (3 * b + 0)) & 1) << b;
+      iy |= ((idx >> (3 * b + 1)) & 1) << b;
+      iz |= ((idx >> (3 * b + 2)) & 1) << b;
+    }
+    float step = half0 * 2.0f / static_cast<float>(grid);
+    nd.cx = fmaf(static_cast<float>(ix) + 0.5f, step, cx0 - half0);
+    nd.cy = fmaf(static_cast<float>(iy) + 0.5f, step, cy0 - half0);
+    nd.cz = fmaf(static_cast<float>(iz) + 0.5f, step, cz0 - half0);
+    nd.half_size = step * 0.5f;
+    nd.diameter = step * sqrtf(3.0f);
+    if (level < depth) {
+      uint32_t child_base = static_cast<uint32_t>(level_off + level_n) + (idx << 3);
+      int cshift = 3 * (depth - level - 1);
+      uint8_t mask = 0;
+      for (uint32_t c = 0; c < 8; c++) {
+        nd.child[c] = child_base + c;
+        uint64_t cl = static_cast<uint64_t>((idx << 3) + c) << cshift;
+        uint64_t ch = static_cast<uint64_t>((idx << 3) + c + 1) << cshift;
+        if (off[ch] > off[cl]) {
+          mask |= static_cast<uint8_t>(1u << c);
+          if (nd.first_child == 0xFFFFFFFFu) nd.first_child = child_base + c;
+        }
+      }
+      nd.child_mask = mask;
+      if (mask == 0) nd.is_leaf = 1;
+    } else {
+      for (int c = 0; c < 8; c++) nd.child[c] = 0xFFFFFFFFu;
+    }
+    DVec<7> hi = P[nd.end], lo = P[nd.start];
+    double M = hi.v[0] - lo.v[0];
+    float mass = static_cast<float>(M);
+    nd.contrib.alpha = 1.0f;
+    nd.contrib.mass = mass;
+    if (mass > 0.0f) {
+      for (int d = 0; d < 3; d++) {
+        nd.contrib.pos[d] = static_cast<float>((hi.v[1 + d] - lo.v[1 + d]) / M);
+        nd.contrib.nrm[d] = static_cast<float>((hi.v[4 + d] - lo.v[4 + d]) / M);
+      }
+    } else {
+      for (int d = 0; d < 3; d++) {
+        nd.contrib.pos[d] = 0.0f;
+        nd.contrib.nrm[d] = 0.0f;
+      }
+    }
+    // 8-byte stores: node_idx * 104 is 8-byte aligned.
+    const uint2* src = reinterpret_cast<const uint2*>(&nd);
+    uint2* dst = reinterpret_cast<uint2*>(nodes + node_idx);
+#pragma unroll
+    for (int k = 0; k < 13; k++) dst[k] = src[k];
+    const float4* cs = reinterpret_cast<const float4*>(&nd.contrib);
+    float4* cd = reinterpret_cast<float4*>(contrib + node_idx);
+    cd[0] = cs[0];
+    cd[1] = cs[1];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// octree8 classic BH traversal (src/sbh_ffi.cu:1878-2144)
+// ---------------------------------------------------------------------------
+constexpr int kO8Stack = 128;
+
+struct O8Node {
+  float cx, cy, cz, half, diam;
+  uint32_t start, end;
+  uint8_t mask, is_leaf;
+};
+
+__device__ __forceinline__ float o8_mass(const OctreeNode8* nodes, int idx) {
+  return __ldg(&nodes[idx].contrib.mass);
+}
+
+__device__ __forceinline__ bool o8_far(const OctreeNode8& nd, float qx, float qy, float qz, float beta,
+                                       const Periodic& per) {
+  if (nd.is_leaf) return true;
+  float dx = min_image_floor(qx - nd.cx, per);
+  float dy = min_image_floor(qy - nd.cy, per);
+  float dz = min_image_floor(qz - nd.cz, per);
+  float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+  return dist / nd.diameter >= beta;
+}
+
+__device__ __forceinline__ float axis_gap(float q, float lo, float hi) {
+  if (q < lo) return lo - q;
+  if (q > hi) return q - hi;
+  return 0.0f;
+}
+
+__device__ __forceinline__ bool o8_prune(const OctreeNode8& nd, float qx, float qy, float qz,
+                                         int prune_on, float r_cut_sq, const Periodic& per) {
+  if (!prune_on) return false;
+  if (per.on && per.box > 0.0f) {
+    float inv_l = 1.0f / per.box;
+    qx -= per.box * nearbyintf((qx - nd.cx) * inv_l);
+    qy -= per.box * nearbyintf((qy - nd.cy) * inv_l);
+    qz -= per.box * nearbyintf((qz - nd.cz) * inv_l);
+  }
+  float dx = axis_gap(qx, nd.cx - nd.half_size, nd.cx + nd.half_size);
+  float dy = axis_gap(qy, nd.cy - nd.half_size, nd.cy + nd.half_size);
+  float dz = axis_gap(qz, nd.cz - nd.half_size, nd.cz + nd.half_size);
+  return dx * dx + dy * dy + dz * dz > r_cut_sq;
+}
+
+enum O8Kernel { O8_GRAV_GRAD = 0, O8_SOFT = 1, O8_SOFT_VJP = 2, O8_GRAV_GRAD_VJP = 3 };
+
+template <int KERNEL>
+__device__ __forceinline__ void o8_pair(float qx, float qy, float qz, float px, float py, float pz, float m,
+                                        float gx, float gy, float gz, const Soft& s, const Periodic& per,
+                                        float& ax, float& ay, float& az) {
+  float rx = min_image_floor(qx - px, per);
+  float ry = min_image_floor(qy - py, per);
+  float rz = min_image_floor(qz - pz, per);
+  if (KERNEL == O8_GRAV_GRAD) {
+    float c = grav_grad_coeff(rx * rx + ry * ry + rz * rz, m);
+    ax += c * rx;
+    ay += c * ry;
+    az += c * rz;
+  } else if (KERNEL == O8_SOFT) {
+    float c = soft_coeff(rx * rx + ry * ry + rz * rz, m, s);
+    ax += c * rx;
+    ay += c * ry;
+    az += c * rz;
+  } else if (KERNEL == O8_SOFT_VJP) {
+    soft_vjp_accum(rx, ry, rz, m, gx, gy, gz, s, ax, ay, az);
+  } else {
+    grav_grad_vjp_accum(rx, ry, rz, m, gx, gy, gz, ax, ay, az);
+  }
+}
+
+template <int KERNEL>
+__device__ __forceinline__ void o8_leaf_sum(const Leaf3* __restrict__ leaf, uint32_t start, uint32_t end,
+                                            float qx, float qy, float qz, float gx, float gy, float gz,
+                                            const Soft& s, const Periodic& per, float& ax, float& ay,
+                                            float& az) {
+  for (uint32_t i = start; i < end; i++) {
+    const float4* p = reinterpret_cast<const float4*>(leaf + i);
+    float4 a = __ldg(p);
+    float m = __ldg(&leaf[i].mass);
+    o8_pair<KERNEL>(qx, qy, qz, a.x, a.y, a.z, m, gx, gy, gz, s, per, ax, ay, az);
+  }
+}
+
+// Buffers come from the caller: child indices and leaf ranges are checked
+// against the buffer sizes and a violation sets SBH_DEV_BAD_BOUNDS instead of
+// reading out of bounds.
+struct O8Bounds {
+  uint32_t num_nodes;
+  uint32_t num_leaves;
+};
+
+__device__ __forceinline__ bool o8_node_ok(uint32_t idx, const O8Bounds& bd, uint32_t* status) {
+  if (idx < bd.num_nodes) return true;
+  raise_status(status, SBH_DEV_BAD_BOUNDS);
+  return false;
+}
+
+__device__ __forceinline__ uint32_t o8_leaf_end(uint32_t start, uint32_t end, const O8Bounds& bd,
+                                                uint32_t* status) {
+  if (end <= bd.num_leaves && start <= end) return end;
+  raise_status(status, SBH_DEV_BAD_BOUNDS);
+  return start <= bd.num_leaves ? (end < bd.num_leaves ? end : bd.num_leaves) : start;
+}
+
+template <int KERNEL>
+__global__ void __launch_bounds__(256)
+    o8_bh_kernel(const Leaf3* __restrict__ leaf, const OctreeNode8* __restrict__ nodes,
+                 const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq, float beta,
+                 Soft s, int prune_on, float r_cut_sq, Periodic per, float* __restrict__ out,
+                 uint32_t* status, O8Bounds bd) {
+  int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (qi >= nq) return;
+  float qx = queries[3 * qi], qy = queries[3 * qi + 1], qz = queries[3 * qi + 2];
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  if (KERNEL == O8_SOFT_VJP || KERNEL == O8_GRAV_GRAD_VJP) {
+    gx = cot[3 * qi];
+    gy = cot[3 * qi + 1];
+    gz = cot[3 * qi + 2];
+  }
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  int stack[kO8Stack];
+  int top = 0;
+  stack[top++] = 0;
+  bool overflow = false;
+  while (top > 0) {
+    int idx = stack[--top];
+    if (o8_mass(nodes, idx) == 0.0f) continue;
+    const OctreeNode8& nd = nodes[idx];
+    if (KERNEL != O8_GRAV_GRAD && KERNEL != O8_GRAV_GRAD_VJP &&
+        o8_prune(nd, qx, qy, qz, prune_on, r_cut_sq, per))
+      continue;
+    if (o8_far(nd, qx, qy, qz, beta, per)) {
+      if (nd.is_leaf) {
+        o8_leaf_sum<KERNEL>(leaf, nd.start, o8_leaf_end(nd.start, nd.end, bd, status), qx, qy, qz, gx, gy, gz, s,
+                            per, ax, ay, az);
+      } else {
+        o8_pair<KERNEL>(qx, qy, qz, nd.contrib.pos[0], nd.contrib.pos[1], nd.contrib.pos[2], nd.contrib.mass,
+                        gx, gy, gz, s, per, ax, ay, az);
+      }
+    } else {
+      uint8_t mask = nd.child_mask;
+      for (int c = 0; c < 8; c++) {
+        if (mask & (1u << c)) {
+          if (!o8_node_ok(nd.child[c], bd, status)) continue;
+          if (top < kO8Stack) {
+            stack[top++] = static_cast<int>(nd.child[c]);
+          } else {
+            overflow = true;
+          }
+        }
+      }
+    }
+  }
+  if (overflow) raise_status(status, SBH_DEV_STACK_OVERFLOW);
+  out[3 * qi] = ax;
+  out[3 * qi + 1] = ay;
+  out[3 * qi + 2] = az;
+}
+
+// ---------------------------------------------------------------------------
+// octree8 stochastic BH, the multi-level prefix control variate
+// (src/sbh_ffi.cu:2146-2442). Same curand calls as the reference, so a
+// fixed seed gives the reference's sample paths.
+// ---------------------------------------------------------------------------
+constexpr int kControlDepth = 3;
+constexpr int kMaxSubdomains = 512;
+
+template <int KERNEL>
+__device__ __forceinline__ void o8_contrib_pair(const OctreeNode8& nd, float qx, float qy, float qz, float gx,
+                                                float gy, float gz, const Soft& s, const Periodic& per,
+                                                float& ax, float& ay, float& az) {
+  o8_pair<KERNEL>(qx, qy, qz, nd.contrib.pos[0], nd.contrib.pos[1], nd.contrib.pos[2], nd.contrib.mass, gx,
+                  gy, gz, s, per, ax, ay, az);
+}
+
+__device__ __forceinline__ uint32_t o8_child_slot(const OctreeNode8& nd, float px, float py, float pz) {
+  uint32_t ix = px >= nd.cx ? 1u : 0u;
+  uint32_t iy = py >= nd.cy ? 1u : 0u;
+  uint32_t iz = pz >= nd.cz ? 1u : 0u;
+  return ix | (iy << 1) | (iz << 2);
+}
+
+template <int KERNEL, bool SOFTENED>
+__global__ void __launch_bounds__(256)
+    o8_stochastic_kernel(const Leaf3* __restrict__ leaf, const OctreeNode8* __restrict__ nodes,
+                         const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq,
+                         int samples, int seed, float beta, Soft s, int prune_on, float r_cut_sq,
+                         Periodic per, float* __restrict__ out, uint32_t* status, O8Bounds bd) {
+  int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (qi >= nq) return;
+  float qx = queries[3 * qi], qy = queries[3 * qi + 1], qz = queries[3 * qi + 2];
+  float gx = 0.f, gy = 0.f, gz = 0.f;
+  if (KERNEL == O8_SOFT_VJP || KERNEL == O8_GRAV_GRAD_VJP) {
+    gx = cot[3 * qi];
+    gy = cot[3 * qi + 1];
+    gz = cot[3 * qi + 2];
+  }
+  // curand_init(seed + q, 0, 0) and curand_init(seed + q + 0x9e3779b9, 0, 0):
+  // int addition, then sign extension (first) or u32 wraparound (second).
+  int sq = seed + static_cast<int>(qi);
+  curandState st, st2;
+  curand_init(static_cast<unsigned long long>(static_cast<long long>(sq)), 0, 0, &st);
+  curand_init(static_cast<unsigned long long>(static_cast<unsigned>(sq) + 0x9e3779b9u), 0, 0, &st2);
+
+  float tx = 0.f, ty = 0.f, tz = 0.f;
+  int stack[kO8Stack];
+  int top = 0;
+  stack[top++] = 0;
+  uint32_t subs[kMaxSubdomains];
+  int nsub = 0;
+  bool overflow = false;
+  while (top > 0) {
+    int idx = stack[--top];
+    const OctreeNode8& nd = nodes[idx];
+    if (nd.contrib.mass == 0.0f) continue;
+    if (nd.is_leaf || nd.depth >= kControlDepth) {
+      if (nsub < kMaxSubdomains) subs[nsub++] = static_cast<uint32_t>(idx);
+      continue;
+    }
+    uint8_t mask = nd.child_mask;
+    for (int c = 0; c < 8; c++) {
+      if (mask & (1u << c)) {
+        if (!o8_node_ok(nd.child[c], bd, status)) continue;
+        if (top < kO8Stack)
+          stack[top++] = static_cast<int>(nd.child[c]);
+        else
+          overflow = true;
+      }
+    }
+  }
+  for (int sd = 0; sd < nsub; sd++) {
+    const OctreeNode8& sub = nodes[subs[sd]];
+    if (SOFTENED && o8_prune(sub, qx, qy, qz, prune_on, r_cut_sq, per)) continue;
+    uint32_t sub_end = o8_leaf_end(sub.start, sub.end, bd, status);
+    if (sub.is_leaf) {
+      o8_leaf_sum<KERNEL>(leaf, sub.start, sub_end, qx, qy, qz, gx, gy, gz, s, per, tx, ty, tz);
+    } else {
+      o8_contrib_pair<KERNEL>(sub, qx, qy, qz, gx, gy, gz, s, per, tx, ty, tz);
+    }
+    if (sub_end <= sub.start) continue;
+    uint32_t num_el = sub.end - sub.start;
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    for (int ss = 0; ss < samples; ss++) {
+      uint32_t pick = min(static_cast<uint32_t>(num_el * curand_uniform(&st2)) + sub.start, sub_end - 1);
+      float spx = leaf[pick].pos[0], spy = leaf[pick].pos[1], spz = leaf[pick].pos[2];
+      const OctreeNode8* prev = &sub;
+      const OctreeNode8* cur = &sub;
+      float event_prob = 1.0f;
+      float wx = 0.f, wy = 0.f, wz = 0.f;
+      float dx = min_image_floor(qx - cur->cx, per);
+      float dy = min_image_floor(qy - cur->cy, per);
+      float dz = min_image_floor(qz - cur->cz, per);
+      float cur_beta = fmaxf(beta, sqrtf(dx * dx + dy * dy + dz * dz) / cur->diameter);
+      while (!cur->is_leaf) {
+        if (SOFTENED && o8_prune(*cur, qx, qy, qz, prune_on, r_cut_sq, per)) break;
+        float ex = min_image_floor(qx - cur->cx, per);
+        float ey = min_image_floor(qy - cur->cy, per);
+        float ez = min_image_floor(qz - cur->cz, per);
+        float dist = sqrtf(ex * ex + ey * ey + ez * ez);
+        float ffr = dist / cur->diameter;
+        float tp = fminf(cur_beta / ffr, 1.0f);
+        float p = curand_uniform(&st);
+        if (p > tp) {
+          event_prob *= 1.0f - tp;
+          break;
+        }
+        event_prob *= tp;
+        prev = cur;
+        uint32_t slot = o8_child_slot(*cur, spx, spy, spz);
+        if (!(cur->child_mask & (1u << slot))) break;
+        if (!o8_node_ok(cur->child[slot], bd, status)) break;
+        cur = &nodes[cur->child[slot]];
+        cur_beta = fmaxf(cur_beta, ffr);
+        float px_ = 0.f, py_ = 0.f, pz_ = 0.f;
+        o8_contrib_pair<KERNEL>(*prev, qx, qy, qz, gx, gy, gz, s, per, px_, py_, pz_);
+        float cx_ = 0.f, cy_ = 0.f, cz_ = 0.f;
+        uint8_t mask = prev->child_mask;
+        for (int cc = 0; cc < 8; cc++) {
+          if (!(mask & (1u << cc))) continue;
+          if (!o8_node_ok(prev->child[cc], bd, status)) continue;
+          const OctreeNode8& ch = nodes[prev->child[cc]];
+          if (SOFTENED && o8_prune(ch, qx, qy, qz, prune_on, r_cut_sq, per)) continue;
+          if (ch.is_leaf) {
+            o8_leaf_sum<KERNEL>(leaf, ch.start, o8_leaf_end(ch.start, ch.end, bd, status), qx, qy, qz, gx, gy, gz, s,
+                                per, cx_, cy_, cz_);
+          } else {
+            o8_contrib_pair<KERNEL>(ch, qx, qy, qz, gx, gy, gz, s, per, cx_, cy_, cz_);
+          }
+        }
+        float pinv = static_cast<float>(num_el) / (event_prob * static_cast<float>(prev->end - prev->start));
+        wx += pinv * (cx_ - px_);
+        wy += pinv * (cy_ - py_);
+        wz += pinv * (cz_ - pz_);
+      }
+      sx += wx;
+      sy += wy;
+      sz += wz;
+    }
+    if (samples > 0) {
+      float inv = static_cast<float>(samples);
+      tx += sx / inv;
+      ty += sy / inv;
+      tz += sz / inv;
+    }
+  }
+  if (overflow) raise_status(status, SBH_DEV_STACK_OVERFLOW);
+  out[3 * qi] = tx;
+  out[3 * qi + 1] = ty;
+  out[3 * qi + 2] = tz;
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+static int check_threads(int threads) {
+  if (threads <= 0 || threads > 1024) return invalid("threads must be in [1, 1024]");
+  return SBH_OK;
+}
+
+static unsigned grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  return static_cast<unsigned>(b < 1 ? 1 : b);
+}
+
+static unsigned grid_stride(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b > 148 * 64) b = 148 * 64;
+  return static_cast<unsigned>(b < 1 ? 1 : b);
+}
+
+static bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+template <typename Body>
+static int o8_layout_checks(const void* leaf, size_t leaf_bytes, const void* nodes, size_t node_bytes,
+                            const float* queries, int64_t nq, Body) {
+  if (leaf_bytes % sizeof(Leaf3) != 0) return invalid("leaf_bytes size mismatch");
+  if (node_bytes % sizeof(OctreeNode8) != 0) return invalid("node_bytes size mismatch");
+  if (node_bytes == 0) return invalid("node_bytes must hold at least the root");
+  if (nq < 0) return invalid("num_queries must be >= 0");
+  if (nq > 0 && !queries) return invalid("queries must be non-null");
+  if ((leaf_bytes > 0 && !aligned16(leaf)) || !aligned16(nodes)) return invalid("leaf/node buffers must be 16-byte aligned");
+  return SBH_OK;
+}
+
+template <typename C>
+static void o8_carve(C& c, int64_t n, int depth, O8Params** prm, uint32_t** k0, uint32_t** v0,
+                     uint32_t** k1, uint32_t** v1, uint32_t** counts, uint32_t** hist, uint32_t** scan_tmp,
+                     DVec<7>** P, DVec<7>** ptmp) {
+  uint64_t cells = 1ull << (3 * depth);
+  int64_t nn = n > 0 ? n : 1;
+  *prm = c.template take<O8Params>(1);
+  *k0 = c.template take<uint32_t>(nn);
+  *v0 = c.template take<uint32_t>(nn);
+  *k1 = c.template take<uint32_t>(nn);
+  *v1 = c.template take<uint32_t>(nn);
+  *counts = c.template take<uint32_t>(cells + 1);
+  int64_t hist_n = radix_hist_elems(nn);
+  *hist = c.template take<uint32_t>(hist_n);
+  int64_t st = scan_tiles(static_cast<int64_t>(cells) + 1);
+  int64_t st2 = scan_tiles(hist_n);
+  *scan_tmp = c.template take<uint32_t>(st > st2 ? st : st2);
+  *P = c.template take<DVec<7>>(nn + 1);
+  *ptmp = c.template take<DVec<7>>(scan_tiles(nn));
+}
+
+}  // namespace sbh
+
+using namespace sbh;
+
+extern "C" {
+
+int sbh_bruteforce_gravity(cudaStream_t stream, const float* points, const float* masses, int64_t n, int dim,
+                           const float* queries, int64_t nq, float* out, int periodic, float box_length,
+                           int threads) {
+  if (n < 0 || nq < 0) return invalid("sizes must be >= 0");
+  if (dim != 2 && dim != 3) return invalid("only dim=2 or dim=3 supported");
+  if (int rc = check_threads(threads)) return rc;
+  if (nq == 0) return SBH_OK;
+  bruteforce_gravity_kernel<<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(
+      points, masses, n, dim, queries, nq, out, Periodic{periodic, box_length});
+  return check_launch("bruteforce_gravity");
+}
+
+int sbh_direct_force_soft(cudaStream_t stream, const float* points, const float* masses, int64_t n,
+                          const float* queries, int64_t nq, float* out, float softening_scale,
+                          float cutoff_scale, int periodic, float box_length, int threads) {
+  if (n < 0 || nq < 0) return invalid("sizes must be >= 0");
+  if (softening_scale < 0.0f) return invalid("softening_scale must be >= 0");
+  if (!(cutoff_scale > 0.0f)) return invalid("cutoff_scale must be > 0");
+  if (int rc = check_threads(threads)) return rc;
+  if (nq == 0) return SBH_OK;
+  direct_soft_kernel<0><<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(
+      points, masses, n, queries, nullptr, nq, out, Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
+      Periodic{periodic, box_length});
+  return check_launch("direct_force_soft");
+}
+
+int sbh_direct_force_soft_vjp(cudaStream_t stream, const float* points, const float* masses, int64_t n,
+                              const float* queries, int64_t nq, const float* cotangent, float* out,
+                              float softening_scale, float cutoff_scale, int periodic, float box_length,
+                              int threads) {
+  if (n < 0 || nq < 0) return invalid("sizes must be >= 0");
+  if (softening_scale < 0.0f) return invalid("softening_scale must be >= 0");
+  if (!(cutoff_scale > 0.0f)) return invalid("cutoff_scale must be > 0");
+  if (int rc = check_threads(threads)) return rc;
+  if (nq == 0) return SBH_OK;
+  direct_soft_kernel<1><<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(
+      points, masses, n, queries, cotangent, nq, out, Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
+      Periodic{periodic, box_length});
+  return check_launch("direct_force_soft_vjp");
+}
+
+size_t sbh_build_octree8_workspace_bytes(int64_t n, int max_depth) {
+  if (max_depth < 1 || max_depth > 10 || n < 0) return 0;
+  Sizer s;
+  O8Params* prm;
+  uint32_t *k0, *v0, *k1, *v1, *counts, *hist, *scan_tmp;
+  DVec<7>*P, *ptmp;
+  o8_carve(s, n, max_depth, &prm, &k0, &v0, &k1, &v1, &counts, &hist, &scan_tmp, &P, &ptmp);
+  return s.off;
+}
+
+int sbh_build_octree8(cudaStream_t stream, const float* points, const float* normals, const float* masses,
+                      int64_t n, const float* min_corner, const float* max_corner, int max_depth, void* leaf_out,
+                      size_t leaf_bytes, void* node_out, size_t node_bytes, void* contrib_out,
+                      size_t contrib_bytes, void* workspace, size_t workspace_bytes) {
+  if (max_depth < 1 || max_depth > 10) return invalid("max_depth must be in [1, 10]");
+  if (n < 0 || n > 0xFFFFFFFFll) return invalid("number of points must be in [0, 2^32)");
+  uint64_t total = sbh_octree8_total_nodes(max_depth);
+  if (leaf_bytes != static_cast<size_t>(n) * sizeof(Leaf3)) return invalid("leaf_out size mismatch");
+  if (node_bytes != total * sizeof(OctreeNode8)) return invalid("node_out size mismatch");
+  if (contrib_bytes != total * sizeof(Leaf3)) return invalid("contrib_out size mismatch");
+  if (!min_corner || !max_corner) return invalid("min_corner/max_corner must be non-null");
+  if ((n > 0 && !aligned16(leaf_out)) || !aligned16(node_out) || !aligned16(contrib_out))
+    return invalid("output buffers must be 16-byte aligned");
+  size_t need = sbh_build_octree8_workspace_bytes(n, max_depth);
+  if (!workspace || workspace_bytes < need)
+    return fail(SBH_ERR_WORKSPACE, "workspace too small: need " + std::to_string(need) + " bytes");
+  Carver c(workspace, workspace_bytes);
+  O8Params* prm;
+  uint32_t *k0, *v0, *k1, *v1, *counts, *hist, *scan_tmp;
+  DVec<7>*P, *ptmp;
+  o8_carve(c, n, max_depth, &prm, &k0, &v0, &k1, &v1, &counts, &hist, &scan_tmp, &P, &ptmp);
+  uint32_t* status = static_cast<uint32_t*>(workspace);
+  uint64_t cells = 1ull << (3 * max_depth);
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(counts, 0, (cells + 1) * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  o8_setup_kernel<<<1, 1, 0, stream>>>(min_corner, max_corner, prm, status);
+  if (n > 0) {
+    o8_codes_kernel<<<grid_stride(n, 256), 256, 0, stream>>>(points, n, prm, max_depth, k0, counts);
+    int which = 0;
+    e = radix_sort<uint32_t>(stream, k0, v0, k1, v1, n, 3 * max_depth, false, hist, scan_tmp, &which);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    const uint32_t* perm = which == 0 ? v0 : v1;
+    o8_gather_kernel<<<grid_stride(n, 256), 256, 0, stream>>>(points, normals, masses, n, perm, prm,
+                                                              static_cast<Leaf3*>(leaf_out));
+  }
+  e = exclusive_scan<uint32_t>(stream, ArrayLoad<uint32_t>{counts}, static_cast<int64_t>(cells), counts, scan_tmp,
+                               true);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  e = exclusive_scan<DVec<7>>(stream, LeafMomentLoad{static_cast<const Leaf3*>(leaf_out)}, n, P, ptmp, true);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  o8_nodes_kernel<<<grid_stride(static_cast<int64_t>(total), 256), 256, 0, stream>>>(
+      static_cast<OctreeNode8*>(node_out), static_cast<Leaf3*>(contrib_out), counts, P, max_depth, total, prm);
+  return check_launch("build_octree8");
+}
+
+// --------------------------- octree8 traversals -----------------------------
+static int o8_launch_bh(int kernel, cudaStream_t stream, const void* leaf, size_t leaf_bytes, const void* nodes,
+                        size_t node_bytes, const float* queries, int64_t nq, const float* cot, float* out,
+                        float beta, Soft s, int prune_on, float r_cut_sq, Periodic per, int threads,
+                        void* workspace, size_t workspace_bytes) {
+  if (int rc = o8_layout_checks(leaf, leaf_bytes, nodes, node_bytes, queries, nq, 0)) return rc;
+  if (int rc = check_threads(threads)) return rc;
+  if (!workspace || workspace_bytes < kStatusBytes) return fail(SBH_ERR_WORKSPACE, "workspace too small");
+  uint32_t* status = static_cast<uint32_t*>(workspace);
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  if (nq == 0) return SBH_OK;
+  const Leaf3* L = static_cast<const Leaf3*>(leaf);
+  const OctreeNode8* N = static_cast<const OctreeNode8*>(nodes);
+  O8Bounds bd{static_cast<uint32_t>(node_bytes / sizeof(OctreeNode8)), static_cast<uint32_t>(leaf_bytes / sizeof(Leaf3))};
+  unsigned g = grid_for(nq, 256);
+  switch (kernel) {
+    case O8_GRAV_GRAD:
+      o8_bh_kernel<O8_GRAV_GRAD><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out, status, bd);
+      break;
+    case O8_SOFT:
+      o8_bh_kernel<O8_SOFT><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per, out,
+                                                   status, bd);
+      break;
+    default:
+      o8_bh_kernel<O8_SOFT_VJP><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per,
+                                                       out, status, bd);
+      break;
+  }
+  return check_launch("barnes_hut_force_octree8");
+}
+
+// prune_on / r_cut exactly as the reference handler derives them (src/sbh_ffi.cu:3235-3237).
+static void o8_prune_params(int prune_enabled, float prune_r_cut_mult, float cutoff_scale, int* on, float* rsq) {
+  *on = (prune_enabled != 0 && cutoff_scale > 0.0f) ? 1 : 0;
+  float r_cut = *on ? prune_r_cut_mult * cutoff_scale : 0.0f;
+  *rsq = r_cut * r_cut;
+}
+
+int sbh_barnes_hut_force_octree8(cudaStream_t stream, const void* leaf, size_t leaf_bytes, const void* nodes,
+                                 size_t node_bytes, const float* queries, int64_t nq, float* out, float beta,
+                                 int periodic, float box_length, int threads, void* workspace,
+                                 size_t workspace_bytes) {
+  return o8_launch_bh(O8_GRAV_GRAD, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, nullptr, out, beta,
+                      Soft{0.f, 0.f}, 0, 0.f, Periodic{periodic, box_length}, threads, workspace, workspace_bytes);
+}
+
+int sbh_barnes_hut_force_octree8_soft(cudaStream_t stream, const void* leaf, size_t leaf_bytes, const void* nodes,
+                                      size_t node_bytes, const float* queries, int64_t nq, float* out, float beta,
+                                      float softening_scale, float cutoff_scale, int prune_enabled,
+                                      float prune_r_cut_mult, int periodic, float box_length, int threads,
+                                      void* workspace, size_t workspace_bytes) {
+  if (prune_enabled != 0 && prune_r_cut_mult <= 0.0f)
+    return invalid("prune_r_cut_mult must be > 0 when prune_enabled is set");
+  int on;
+  float rsq;
+  o8_prune_params(prune_enabled, prune_r_cut_mult, cutoff_scale, &on, &rsq);
+  return o8_launch_bh(O8_SOFT, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, nullptr, out, beta,
+                      Soft{fmaxf(softening_scale, 0.0f), cutoff_scale}, on, rsq, Periodic{periodic, box_length},
+                      threads, workspace, workspace_bytes);
+}
+
+int sbh_barnes_hut_force_octree8_soft_vjp(cudaStream_t stream, const void* leaf, size_t leaf_bytes,
+                                          const void* nodes, size_t node_bytes, const float* queries, int64_t nq,
+                                          const float* cotangent, float* out, float beta, float softening_scale,
+                                          float cutoff_scale, int prune_enabled, float prune_r_cut_mult,
+                                          int periodic, float box_length, int threads, void* workspace,
+                                          size_t workspace_bytes) {
+  if (prune_enabled != 0 && prune_r_cut_mult <= 0.0f)
+    return invalid("prune_r_cut_mult must be > 0 when prune_enabled is set");
+  if (nq > 0 && !cotangent) return invalid("cotangent must be non-null");
+  int on;
+  float rsq;
+  o8_prune_params(prune_enabled, prune_r_cut_mult, cutoff_scale, &on, &rsq);
+  return o8_launch_bh(O8_SOFT_VJP, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, cotangent, out, beta,
+                      Soft{fmaxf(softening_scale, 0.0f), cutoff_scale}, on, rsq, Periodic{periodic, box_length},
+                      threads, workspace, workspace_bytes);
+}
+
+static int o8_launch_stochastic(bool vjp, int softened, cudaStream_t stream, const void* leaf, size_t leaf_bytes,
+                                const void* nodes, size_t node_bytes, const float* queries, int64_t nq,
+                                const float* cot, float* out, int samples, int seed, float beta,
+                                float softening_scale, float cutoff_scale, int prune_enabled,
+                                float prune_r_cut_mult, int periodic, float box_length, int threads,
+                                void* workspace, size_t workspace_bytes) {
+  if (int rc = o8_layout_checks(leaf, leaf_bytes, nodes, node_bytes, queries, nq, 0)) return rc;
+  if (int rc = check_threads(threads)) return rc;
+  if (softened && prune_enabled != 0 && prune_r_cut_mult <= 0.0f)
+    return invalid("prune_r_cut_mult must be > 0 when prune_enabled is set");
+  if (vjp && nq > 0 && !cot) return invalid("cotangent must be non-null");
+  if (!workspace || workspace_bytes < kStatusBytes) return fail(SBH_ERR_WORKSPACE, "workspace too small");
+  uint32_t* status = static_cast<uint32_t*>(workspace);
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  if (nq == 0) return SBH_OK;
+  int on = 0;
+  float rsq = 0.f;
+  if (softened) o8_prune_params(prune_enabled, prune_r_cut_mult, cutoff_scale, &on, &rsq);
+  Soft s{fmaxf(softening_scale, 0.0f), cutoff_scale};
+  Periodic per{periodic, box_length};
+  const Leaf3* L = static_cast<const Leaf3*>(leaf);
+  const OctreeNode8* N = static_cast<const OctreeNode8*>(nodes);
+  O8Bounds bd{static_cast<uint32_t>(node_bytes / sizeof(OctreeNode8)), static_cast<uint32_t>(leaf_bytes / sizeof(Leaf3))};
+  // The reference's kernel reads a curand state per query, independent of
+  // the block size, so any launch shape gives the same numbers.
+  unsigned g = grid_for(nq, 128);
+  if (!vjp) {
+    if (softened)
+      o8_stochastic_kernel<O8_SOFT, true><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed, beta, s, on,
+                                                                 rsq, per, out, status, bd);
+    else
+      o8_stochastic_kernel<O8_GRAV_GRAD, false><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed, beta,
+                                                                       s, 0, 0.f, per, out, status, bd);
+  } else {
+    if (softened)
+      o8_stochastic_kernel<O8_SOFT_VJP, true><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed, beta, s,
+                                                                     on, rsq, per, out, status, bd);
+    else
+      o8_stochastic_kernel<O8_GRAV_GRAD_VJP, false><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed,
+                                                                           beta, s, 0, 0.f, per, out, status, bd);
+  }
+  return check_launch("stochastic_bh_force_octree8");
+}
+
+int sbh_stochastic_bh_force_octree8(cudaStream_t stream, int softened, const void* leaf, size_t leaf_bytes,
+                                    const void* nodes, size_t node_bytes, const float* queries, int64_t nq,
+                                    float* out, int samples_per_subdomain, int seed, float beta,
+                                    float softening_scale, float cutoff_scale, int prune_enabled,
+                                    float prune_r_cut_mult, int periodic, float box_length, int threads,
+                                    void* workspace, size_t workspace_bytes) {
+  return o8_launch_stochastic(false, softened, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, nullptr,
+                              out, samples_per_subdomain, seed, beta, softening_scale, cutoff_scale, prune_enabled,
+                              prune_r_cut_mult, periodic, box_length, threads, workspace, workspace_bytes);
+}
+
+int sbh_stochastic_bh_force_octree8_vjp(cudaStream_t stream, int softened, const void* leaf, size_t leaf_bytes,
+                                        const void* nodes, size_t node_bytes, const float* queries, int64_t nq,
+                                        const float* cotangent, float* out, int samples_per_subdomain, int seed,
+                                        float beta, float softening_scale, float cutoff_scale, int prune_enabled,
+                                        float prune_r_cut_mult, int periodic, float box_length, int threads,
+                                        void* workspace, size_t workspace_bytes) {
+  return o8_launch_stochastic(true, softened, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, cotangent,
+                              out, samples_per_subdomain, seed, beta, softening_scale, cutoff_scale, prune_enabled,
+                              prune_r_cut_mult, periodic, box_length, threads, workspace, workspace_bytes);
+}
+
+}  // extern "C"

@@ -1,0 +1,606 @@
+"""Host side of the sbh_b200 library: ctypes bindings of the C ABI
+(``include/sbh_b200.h``) and a torch-tensor mirror of the reference's
+``python/jax_sbh_ffi.py`` surface (same function names, keyword defaults,
+validation messages and ``custom_vjp`` semantics).
+
+Device memory, streams and autograd come from PyTorch; all arithmetic runs in
+the hand-written CUDA kernels of ``libsbh_b200.so``. There is no CPU fallback:
+without the built library or without a CUDA device every compute function
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import threading
+from typing import Optional
+
+import numpy as np
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsbh_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "sbh_b200.h")
+
+# Target names of the reference FFI (python/jax_sbh_ffi.py:10-34).
+TARGETS = {
+    "bruteforce_gravity": "sbh_bruteforce_gravity",
+    "direct_force_soft": "sbh_direct_force_soft",
+    "direct_force_soft_vjp": "sbh_direct_force_soft_vjp",
+    "barnes_hut_gravity": "sbh_barnes_hut_gravity",
+    "barnes_hut_force": "sbh_barnes_hut_force",
+    "barnes_hut_gravity_3d": "sbh_barnes_hut_gravity_3d",
+    "barnes_hut_force_3d": "sbh_barnes_hut_force_3d",
+    "barnes_hut_force_soft": "sbh_barnes_hut_force_soft",
+    "barnes_hut_force_soft_3d": "sbh_barnes_hut_force_soft_3d",
+    "stochastic_bh_gravity": "sbh_stochastic_bh_gravity",
+    "stochastic_bh_gravity_3d": "sbh_stochastic_bh_gravity_3d",
+    "stochastic_bh_force": "sbh_stochastic_bh_force",
+    "stochastic_bh_force_3d": "sbh_stochastic_bh_force_3d",
+    "stochastic_bh_force_soft": "sbh_stochastic_bh_force_soft",
+    "stochastic_bh_force_soft_3d": "sbh_stochastic_bh_force_soft_3d",
+    "build_octree_level3_buffers": "sbh_build_octree_level3_buffers",
+    "build_octree8_buffers": "sbh_build_octree8_buffers",
+    "barnes_hut_force_octree8": "sbh_barnes_hut_force_octree8",
+    "barnes_hut_force_octree8_soft": "sbh_barnes_hut_force_octree8_soft",
+    "barnes_hut_force_octree8_soft_vjp": "sbh_barnes_hut_force_octree8_soft_vjp",
+    "stochastic_bh_force_octree8": "sbh_stochastic_bh_force_octree8",
+    "stochastic_bh_force_octree8_soft": "sbh_stochastic_bh_force_octree8_soft",
+    "stochastic_bh_force_octree8_vjp": "sbh_stochastic_bh_force_octree8_vjp",
+    "stochastic_bh_force_octree8_soft_vjp": "sbh_stochastic_bh_force_octree8_soft_vjp",
+}
+
+SBH_OK = 0
+SBH_ERR_INVALID_ARGUMENT = 1
+SBH_ERR_CUDA = 2
+SBH_ERR_WORKSPACE = 3
+SBH_ERR_LIMIT = 4
+DEV_STACK_OVERFLOW = 0x1
+DEV_BAD_BOUNDS = 0x2
+DEV_ITER_LIMIT = 0x4
+
+
+class SbhError(RuntimeError):
+    """A CUDA-side failure reported by libsbh_b200 (SBH_ERR_CUDA / _LIMIT)."""
+
+
+_c_p = ctypes.c_void_p
+_c_sz = ctypes.c_size_t
+_c_i = ctypes.c_int
+_c_i64 = ctypes.c_int64
+_c_f = ctypes.c_float
+_c_u64 = ctypes.c_uint64
+
+# argtypes of every entry point, keyed by symbol (checked against the header
+# by the CPU tests).
+_SIGS = {
+    "sbh_last_error": ([], ctypes.c_char_p),
+    "sbh_version": ([], ctypes.c_char_p),
+    "sbh_read_device_status": ([_c_p, _c_p, _c_p], _c_i),
+    "sbh_leaf3_size": ([], _c_sz),
+    "sbh_node3_size": ([], _c_sz),
+    "sbh_octree_level3_max_nodes": ([], _c_sz),
+    "sbh_octree8_node_size": ([], _c_sz),
+    "sbh_leaf2_size": ([], _c_sz),
+    "sbh_node2_size": ([], _c_sz),
+    "sbh_octree8_total_nodes": ([_c_i], _c_u64),
+    "sbh_traversal_workspace_bytes": ([], _c_sz),
+    "sbh_bruteforce_gravity": ([_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_i64, _c_p, _c_i, _c_f, _c_i], _c_i),
+    "sbh_direct_force_soft": ([_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_i, _c_f, _c_i], _c_i),
+    "sbh_direct_force_soft_vjp": ([_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f, _c_i, _c_f, _c_i],
+                                  _c_i),
+    "sbh_build_octree8_workspace_bytes": ([_c_i64, _c_i], _c_sz),
+    "sbh_build_octree8": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz,
+                           _c_p, _c_sz], _c_i),
+    "sbh_barnes_hut_force_octree8": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_f, _c_i, _c_f, _c_i,
+                                      _c_p, _c_sz], _c_i),
+    "sbh_barnes_hut_force_octree8_soft": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_f,
+                                           _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_barnes_hut_force_octree8_soft_vjp": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f,
+                                               _c_f, _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_stochastic_bh_force_octree8": ([_c_p, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_i, _c_i, _c_f,
+                                         _c_f, _c_f, _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_stochastic_bh_force_octree8_vjp": ([_c_p, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p, _c_i,
+                                             _c_i, _c_f, _c_f, _c_f, _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+}
+
+_lib_handle = None
+_lib_lock = threading.Lock()
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded libsbh_b200.so (raises if it was not built)."""
+    global _lib_handle
+    with _lib_lock:
+        if _lib_handle is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"{LIB_PATH} is not built; run `python barnes-hut_b200/sbh_build.py` "
+                                   "(or __graft_entry__.build()) first")
+            h = ctypes.CDLL(LIB_PATH)
+            for name, (args, res) in _SIGS.items():
+                fn = getattr(h, name, None)
+                if fn is None:
+                    continue
+                fn.argtypes = args
+                fn.restype = res
+            _lib_handle = h
+    return _lib_handle
+
+
+def header_symbols() -> list[str]:
+    """Function names declared in include/sbh_b200.h."""
+    text = open(HEADER_PATH).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sbh_[a-z0-9_]+)\s*\(", text)))
+
+
+def last_error() -> str:
+    return lib().sbh_last_error().decode()
+
+
+def _check(rc: int, what: str) -> None:
+    if rc == SBH_OK:
+        return
+    msg = last_error()
+    if rc == SBH_ERR_INVALID_ARGUMENT:
+        raise ValueError(f"{what}: {msg}")
+    raise SbhError(f"{what}: {msg} (status {rc})")
+
+
+# ---------------------------------------------------------------------------
+# device plumbing
+# ---------------------------------------------------------------------------
+def _device() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("sbh_b200 needs a CUDA device (no CPU fallback)")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+_ws_cache: dict = {}
+
+
+def workspace(nbytes: int, device: Optional[torch.device] = None) -> torch.Tensor:
+    """A uint8 device buffer of at least nbytes, reused per (device, stream)."""
+    device = device or _device()
+    key = (device.index, _stream_ptr(device))
+    buf = _ws_cache.get(key)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+        _ws_cache[key] = buf
+    return buf
+
+
+def read_device_status(ws: torch.Tensor) -> int:
+    out = ctypes.c_uint32(0)
+    _check(lib().sbh_read_device_status(_stream_ptr(ws.device), ws.data_ptr(), ctypes.byref(out)),
+           "read_device_status")
+    return int(out.value)
+
+
+def _f32(x, device) -> torch.Tensor:
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=torch.float32).contiguous()
+    return torch.as_tensor(np.asarray(x, dtype=np.float32), device=device).contiguous()
+
+
+def _u8(x, device) -> torch.Tensor:
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=torch.uint8).contiguous()
+    return torch.as_tensor(np.asarray(x, dtype=np.uint8), device=device).contiguous()
+
+
+def _p(t: Optional[torch.Tensor]):
+    return None if t is None else t.data_ptr()
+
+
+# ---------------------------------------------------------------------------
+# layout queries (python/jax_sbh_ffi.py:62-96)
+# ---------------------------------------------------------------------------
+def leaf3_size() -> int:
+    return int(lib().sbh_leaf3_size())
+
+
+def node3_size() -> int:
+    return int(lib().sbh_node3_size())
+
+
+def octree_level3_max_nodes() -> int:
+    return int(lib().sbh_octree_level3_max_nodes())
+
+
+def octree8_node_size() -> int:
+    return int(lib().sbh_octree8_node_size())
+
+
+def _octree8_total_nodes(max_depth: int) -> int:
+    return int(lib().sbh_octree8_total_nodes(int(max_depth)))
+
+
+# ---------------------------------------------------------------------------
+# direct sums (python/jax_sbh_ffi.py:341-480)
+# ---------------------------------------------------------------------------
+def brute_force_gravity(points, masses, queries, *, periodic: bool = False, box_length: float = 1.0,
+                        threads: int = 64) -> torch.Tensor:
+    dev = _device()
+    points, masses, queries = _f32(points, dev), _f32(masses, dev), _f32(queries, dev)
+    if points.ndim != 2 or queries.ndim != 2:
+        raise ValueError("points and queries must be rank-2")
+    if masses.ndim != 1:
+        raise ValueError("masses must be rank-1")
+    if points.shape[0] != masses.shape[0]:
+        raise ValueError("masses length mismatch")
+    if points.shape[1] != queries.shape[1]:
+        raise ValueError("dim mismatch")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    out = torch.empty(queries.shape[0], dtype=torch.float32, device=dev)
+    _check(lib().sbh_bruteforce_gravity(_stream_ptr(dev), _p(points), _p(masses), points.shape[0], points.shape[1],
+                                        _p(queries), queries.shape[0], _p(out), int(bool(periodic)),
+                                        float(box_length), int(threads)), "brute_force_gravity")
+    return out
+
+
+def _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads):
+    if softening_scale < 0:
+        raise ValueError("softening_scale must be >= 0")
+    if cutoff_scale <= 0:
+        raise ValueError("cutoff_scale must be > 0")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+
+
+def softened_direct_force(points, masses, queries, *, softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                          periodic: bool = False, box_length: float = 1.0, threads: int = 256) -> torch.Tensor:
+    dev = _device()
+    points, masses, queries = _f32(points, dev), _f32(masses, dev), _f32(queries, dev)
+    if points.ndim != 2 or points.shape[1] != 3:
+        raise ValueError("points must be (N, 3)")
+    if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
+        raise ValueError("masses must have shape (N,)")
+    if queries.ndim != 2 or queries.shape[1] != 3:
+        raise ValueError("queries must be (M, 3)")
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
+    _check(lib().sbh_direct_force_soft(_stream_ptr(dev), _p(points), _p(masses), points.shape[0], _p(queries),
+                                       queries.shape[0], _p(out), float(softening_scale), float(cutoff_scale),
+                                       int(bool(periodic)), float(box_length), int(threads)), "softened_direct_force")
+    return out
+
+
+def softened_direct_force_vjp(points, masses, queries, cotangent, *, softening_scale: float = 1e-2,
+                              cutoff_scale: float = 1.0, periodic: bool = False, box_length: float = 1.0,
+                              threads: int = 256) -> torch.Tensor:
+    dev = _device()
+    points, masses = _f32(points, dev), _f32(masses, dev)
+    queries, cotangent = _f32(queries, dev), _f32(cotangent, dev)
+    if points.ndim != 2 or points.shape[1] != 3:
+        raise ValueError("points must be (N, 3)")
+    if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
+        raise ValueError("masses must have shape (N,)")
+    if queries.ndim != 2 or queries.shape[1] != 3:
+        raise ValueError("queries must be (M, 3)")
+    if cotangent.shape != queries.shape:
+        raise ValueError("cotangent must have same shape as queries")
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
+    _check(lib().sbh_direct_force_soft_vjp(_stream_ptr(dev), _p(points), _p(masses), points.shape[0], _p(queries),
+                                           queries.shape[0], _p(cotangent), _p(out), float(softening_scale),
+                                           float(cutoff_scale), int(bool(periodic)), float(box_length),
+                                           int(threads)), "softened_direct_force_vjp")
+    return out
+
+
+class _SoftenedDirectForceRecompute(torch.autograd.Function):
+    """custom_vjp of python/jax_sbh_ffi.py:482-594: forward = self-gravity
+    direct force, backward = query-side VJP only, grad_masses = 0."""
+
+    @staticmethod
+    def forward(ctx, points, masses, softening_scale, cutoff_scale, periodic, box_length, threads):
+        ctx.save_for_backward(points, masses)
+        ctx.cfg = (softening_scale, cutoff_scale, periodic, box_length, threads)
+        return softened_direct_force(points, masses, points, softening_scale=softening_scale,
+                                     cutoff_scale=cutoff_scale, periodic=periodic, box_length=box_length,
+                                     threads=threads)
+
+    @staticmethod
+    def backward(ctx, cot):
+        points, masses = ctx.saved_tensors
+        s, c, per, box, thr = ctx.cfg
+        gp = softened_direct_force_vjp(points, masses, points, cot.contiguous(), softening_scale=s, cutoff_scale=c,
+                                       periodic=per, box_length=box, threads=thr)
+        return gp, torch.zeros_like(masses), None, None, None, None, None
+
+
+def softened_direct_force_recompute_vjp(points, masses, *, softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                                        periodic: bool = False, box_length: float = 1.0,
+                                        threads: int = 256) -> torch.Tensor:
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    dev = _device()
+    points = points if isinstance(points, torch.Tensor) else _f32(points, dev)
+    masses = masses if isinstance(masses, torch.Tensor) else _f32(masses, dev)
+    return _SoftenedDirectForceRecompute.apply(points, masses, float(softening_scale), float(cutoff_scale),
+                                               bool(periodic), float(box_length), int(threads))
+
+
+# ---------------------------------------------------------------------------
+# octree8 (python/jax_sbh_ffi.py:864-961, 1336-1897)
+# ---------------------------------------------------------------------------
+def _default_corners(points: torch.Tensor, min_corner, max_corner, dev):
+    if min_corner is None:
+        min_corner = points.min(dim=0).values - 1e-3
+    if max_corner is None:
+        max_corner = points.max(dim=0).values + 1e-3
+    return _f32(min_corner, dev), _f32(max_corner, dev)
+
+
+def build_octree8_buffers_with_contrib(points, normals, masses, min_corner=None, max_corner=None, *,
+                                       max_depth: int = 7, check_status: bool = True):
+    """(leaf_bytes, node_bytes, contrib_bytes) as uint8 device tensors."""
+    dev = _device()
+    points, normals, masses = _f32(points, dev), _f32(normals, dev), _f32(masses, dev)
+    if points.ndim != 2 or points.shape[1] != 3:
+        raise ValueError("points must have shape (N, 3)")
+    if normals.shape != points.shape:
+        raise ValueError("normals shape mismatch")
+    if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
+        raise ValueError("masses must have shape (N,)")
+    if max_depth < 1 or max_depth > 10:
+        raise ValueError("max_depth must be in [1, 10]")
+    if points.shape[0] == 0 and (min_corner is None or max_corner is None):
+        raise ValueError("empty point set needs explicit min_corner/max_corner")
+    mn, mx = _default_corners(points, min_corner, max_corner, dev)
+    if mn.shape != (3,) or mx.shape != (3,):
+        raise ValueError("min_corner/max_corner must have shape (3,)")
+    n = points.shape[0]
+    total = _octree8_total_nodes(max_depth)
+    leaf = torch.empty(n * 32, dtype=torch.uint8, device=dev)
+    node = torch.empty(total * 104, dtype=torch.uint8, device=dev)
+    contrib = torch.empty(total * 32, dtype=torch.uint8, device=dev)
+    need = int(lib().sbh_build_octree8_workspace_bytes(n, int(max_depth)))
+    ws = workspace(need, dev)
+    _check(lib().sbh_build_octree8(_stream_ptr(dev), _p(points), _p(normals), _p(masses), n, _p(mn), _p(mx),
+                                   int(max_depth), _p(leaf), leaf.numel(), _p(node), node.numel(), _p(contrib),
+                                   contrib.numel(), _p(ws), ws.numel()), "build_octree8_buffers")
+    if check_status:
+        st = read_device_status(ws)
+        if st & DEV_BAD_BOUNDS:
+            raise ValueError("invalid bounds span")
+    return leaf, node, contrib
+
+
+def build_octree8_buffers(points, normals, masses, min_corner=None, max_corner=None, *, max_depth: int = 7):
+    leaf, node, _ = build_octree8_buffers_with_contrib(points, normals, masses, min_corner, max_corner,
+                                                       max_depth=max_depth)
+    return leaf, node
+
+
+def _check_traversal(queries, periodic, box_length, threads):
+    if queries.ndim != 2 or queries.shape[1] != 3:
+        raise ValueError("queries must be (M, 3)")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+
+
+def _status_after(ws, what, check_status):
+    if check_status:
+        st = read_device_status(ws)
+        if st & (DEV_STACK_OVERFLOW | DEV_ITER_LIMIT):
+            raise SbhError(f"{what}: device traversal limit reached (status 0x{st:x})")
+
+
+def barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: float = 2.0, periodic: bool = False,
+                             box_length: float = 1.0, threads: int = 256, check_status: bool = False):
+    dev = _device()
+    leaf, node, queries = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
+    _check_traversal(queries, periodic, box_length, threads)
+    out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_barnes_hut_force_octree8(_stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(),
+                                              _p(queries), queries.shape[0], _p(out), float(beta), int(bool(periodic)),
+                                              float(box_length), int(threads), _p(ws), ws.numel()),
+           "barnes_hut_force_octree8")
+    _status_after(ws, "barnes_hut_force_octree8", check_status)
+    return out
+
+
+def softened_barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: float = 2.0,
+                                      softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                                      prune_enabled: bool = True, prune_r_cut_mult: float = 4.0,
+                                      periodic: bool = False, box_length: float = 1.0, threads: int = 256,
+                                      check_status: bool = False):
+    dev = _device()
+    leaf, node, queries = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
+    _check_traversal(queries, periodic, box_length, threads)
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    if prune_enabled and prune_r_cut_mult <= 0:
+        raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
+    out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_barnes_hut_force_octree8_soft(
+        _stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(), _p(queries), queries.shape[0], _p(out),
+        float(beta), float(softening_scale), float(cutoff_scale), int(bool(prune_enabled)), float(prune_r_cut_mult),
+        int(bool(periodic)), float(box_length), int(threads), _p(ws), ws.numel()), "softened_barnes_hut_force_octree8")
+    _status_after(ws, "softened_barnes_hut_force_octree8", check_status)
+    return out
+
+
+def softened_barnes_hut_force_octree8_vjp(leaf_bytes, node_bytes, queries, cotangent, *, beta: float = 2.0,
+                                          softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                                          prune_enabled: bool = True, prune_r_cut_mult: float = 4.0,
+                                          periodic: bool = False, box_length: float = 1.0, threads: int = 256,
+                                          check_status: bool = False):
+    dev = _device()
+    leaf, node = _u8(leaf_bytes, dev), _u8(node_bytes, dev)
+    queries, cotangent = _f32(queries, dev), _f32(cotangent, dev)
+    _check_traversal(queries, periodic, box_length, threads)
+    if cotangent.shape != queries.shape:
+        raise ValueError("cotangent must have same shape as queries")
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    if prune_enabled and prune_r_cut_mult <= 0:
+        raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
+    out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_barnes_hut_force_octree8_soft_vjp(
+        _stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(), _p(queries), queries.shape[0],
+        _p(cotangent), _p(out), float(beta), float(softening_scale), float(cutoff_scale), int(bool(prune_enabled)),
+        float(prune_r_cut_mult), int(bool(periodic)), float(box_length), int(threads), _p(ws), ws.numel()),
+        "softened_barnes_hut_force_octree8_vjp")
+    _status_after(ws, "softened_barnes_hut_force_octree8_vjp", check_status)
+    return out
+
+
+def _stochastic_octree8(vjp, softened, leaf_bytes, node_bytes, queries, cotangent, beta, samples_per_subdomain,
+                        seed, softening_scale, cutoff_scale, prune_enabled, prune_r_cut_mult, periodic, box_length,
+                        threads, check_status):
+    dev = _device()
+    leaf, node, queries = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
+    _check_traversal(queries, periodic, box_length, threads)
+    if softened:
+        _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+        if prune_enabled and prune_r_cut_mult <= 0:
+            raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
+    out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    common = (float(beta), float(softening_scale), float(cutoff_scale), int(bool(prune_enabled)),
+              float(prune_r_cut_mult), int(bool(periodic)), float(box_length), int(threads), _p(ws), ws.numel())
+    if vjp:
+        cot = _f32(cotangent, dev)
+        if cot.shape != queries.shape:
+            raise ValueError("cotangent must have same shape as queries")
+        rc = lib().sbh_stochastic_bh_force_octree8_vjp(_stream_ptr(dev), int(softened), _p(leaf), leaf.numel(),
+                                                       _p(node), node.numel(), _p(queries), queries.shape[0], _p(cot),
+                                                       _p(out), int(samples_per_subdomain), int(seed), *common)
+    else:
+        rc = lib().sbh_stochastic_bh_force_octree8(_stream_ptr(dev), int(softened), _p(leaf), leaf.numel(), _p(node),
+                                                   node.numel(), _p(queries), queries.shape[0], _p(out),
+                                                   int(samples_per_subdomain), int(seed), *common)
+    _check(rc, "stochastic_barnes_hut_force_octree8")
+    _status_after(ws, "stochastic_barnes_hut_force_octree8", check_status)
+    return out
+
+
+def stochastic_barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: float = 1.0,
+                                        samples_per_subdomain: int = 1, seed: int = 0, periodic: bool = False,
+                                        box_length: float = 1.0, threads: int = 256, check_status: bool = False):
+    return _stochastic_octree8(False, False, leaf_bytes, node_bytes, queries, None, beta, samples_per_subdomain,
+                               seed, 0.0, 1.0, False, 4.0, periodic, box_length, threads, check_status)
+
+
+def stochastic_barnes_hut_force_octree8_vjp(leaf_bytes, node_bytes, queries, cotangent, *, beta: float = 1.0,
+                                            samples_per_subdomain: int = 1, seed: int = 0, periodic: bool = False,
+                                            box_length: float = 1.0, threads: int = 256,
+                                            check_status: bool = False):
+    """Analytic query-side VJP kernel (the reference's Python wrapper of the same
+    name differentiates by finite differences, python/jax_sbh_ffi.py:1490-1535)."""
+    return _stochastic_octree8(True, False, leaf_bytes, node_bytes, queries, cotangent, beta, samples_per_subdomain,
+                               seed, 0.0, 1.0, False, 4.0, periodic, box_length, threads, check_status)
+
+
+def softened_stochastic_barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: float = 1.0,
+                                                 samples_per_subdomain: int = 1, seed: int = 0,
+                                                 softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                                                 prune_enabled: bool = True, prune_r_cut_mult: float = 4.0,
+                                                 periodic: bool = False, box_length: float = 1.0, threads: int = 256,
+                                                 check_status: bool = False):
+    return _stochastic_octree8(False, True, leaf_bytes, node_bytes, queries, None, beta, samples_per_subdomain, seed,
+                               softening_scale, cutoff_scale, prune_enabled, prune_r_cut_mult, periodic, box_length,
+                               threads, check_status)
+
+
+def softened_stochastic_barnes_hut_force_octree8_vjp(leaf_bytes, node_bytes, queries, cotangent, *,
+                                                     beta: float = 1.0, samples_per_subdomain: int = 1, seed: int = 0,
+                                                     softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                                                     prune_enabled: bool = True, prune_r_cut_mult: float = 4.0,
+                                                     periodic: bool = False, box_length: float = 1.0,
+                                                     threads: int = 256, use_ffi: bool = True,
+                                                     check_status: bool = False):
+    """Analytic query-side VJP. The reference defaults to use_ffi=False, an
+    element-wise finite difference with 6*M forward calls
+    (python/jax_sbh_ffi.py:1591-1628); here both settings run the kernel."""
+    del use_ffi
+    return _stochastic_octree8(True, True, leaf_bytes, node_bytes, queries, cotangent, beta, samples_per_subdomain,
+                               seed, softening_scale, cutoff_scale, prune_enabled, prune_r_cut_mult, periodic,
+                               box_length, threads, check_status)
+
+
+class _SoftenedOctree8Recompute(torch.autograd.Function):
+    """custom_vjp of python/jax_sbh_ffi.py:1731-1897: forward builds the tree
+    and evaluates self-gravity; backward rebuilds the tree from the saved
+    inputs and applies the query-side VJP; grad_masses = 0."""
+
+    @staticmethod
+    def forward(ctx, points, masses, cfg):
+        ctx.save_for_backward(points, masses)
+        ctx.cfg = cfg
+        return _octree8_self_force(points, masses, cfg)
+
+    @staticmethod
+    def backward(ctx, cot):
+        points, masses = ctx.saved_tensors
+        beta, s, c, depth, prune, mult, per, box, thr = ctx.cfg
+        leaf, node = build_octree8_buffers(points, torch.zeros_like(points), masses, max_depth=depth)
+        gp = softened_barnes_hut_force_octree8_vjp(leaf, node, points, cot.contiguous(), beta=beta,
+                                                   softening_scale=s, cutoff_scale=c, prune_enabled=prune,
+                                                   prune_r_cut_mult=mult, periodic=per, box_length=box,
+                                                   threads=thr)
+        return gp, torch.zeros_like(masses), None
+
+
+def _octree8_self_force(points, masses, cfg):
+    beta, s, c, depth, prune, mult, per, box, thr = cfg
+    leaf, node = build_octree8_buffers(points, torch.zeros_like(points), masses, max_depth=depth)
+    return softened_barnes_hut_force_octree8(leaf, node, points, beta=beta, softening_scale=s, cutoff_scale=c,
+                                             prune_enabled=prune, prune_r_cut_mult=mult, periodic=per,
+                                             box_length=box, threads=thr)
+
+
+def softened_barnes_hut_force_octree8_recompute_vjp(points, masses, *, beta: float = 2.0,
+                                                    softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                                                    max_depth: int = 7, prune_enabled: bool = True,
+                                                    prune_r_cut_mult: float = 4.0, periodic: bool = False,
+                                                    box_length: float = 1.0, threads: int = 256) -> torch.Tensor:
+    if prune_enabled and prune_r_cut_mult <= 0:
+        raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    dev = _device()
+    points = points if isinstance(points, torch.Tensor) else _f32(points, dev)
+    masses = masses if isinstance(masses, torch.Tensor) else _f32(masses, dev)
+    cfg = (float(beta), float(softening_scale), float(cutoff_scale), int(max_depth), bool(prune_enabled),
+           float(prune_r_cut_mult), bool(periodic), float(box_length), int(threads))
+    return _SoftenedOctree8Recompute.apply(points, masses, cfg)
+
+
+# register_* exist in the reference to hand handler capsules to XLA; with
+# torch there is nothing to register, so they only load the library.
+def _register(*_a, **_k) -> None:
+    lib()
+
+
+for _name in ("register_bruteforce_gravity", "register_softened_direct_force", "register_softened_direct_force_vjp",
+              "register_build_octree_level3_buffers", "register_build_octree8_buffers",
+              "register_barnes_hut_gravity", "register_stochastic_barnes_hut_gravity",
+              "register_stochastic_barnes_hut_force", "register_softened_stochastic_barnes_hut_force",
+              "register_barnes_hut_force", "register_softened_barnes_hut_force", "register_barnes_hut_force_octree8",
+              "register_softened_barnes_hut_force_octree8", "register_softened_barnes_hut_force_octree8_vjp",
+              "register_stochastic_barnes_hut_force_octree8", "register_softened_stochastic_barnes_hut_force_octree8",
+              "register_stochastic_barnes_hut_force_octree8_vjp",
+              "register_softened_stochastic_barnes_hut_force_octree8_vjp"):
+    globals()[_name] = _register

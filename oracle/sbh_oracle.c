@@ -1,0 +1,1182 @@
+/*
+ * CPU oracle for the Barnes-Hut summation path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the reference's algorithms (bhorowitz/barnes-hut,
+ * src/sbh_ffi.cu and include/kernel.h), used by tests/, by the smoke check
+ * and by bench.py's CPU-baseline leg as the checker. The product library
+ * never calls, links or loads this file.
+ *
+ * Conventions:
+ *  - Opening decisions, quantisation and node geometry are computed in float
+ *    in the same operation order as the reference, so that the oracle takes
+ *    the same traversal decisions; every kernel contribution and every sum is
+ *    then evaluated in double. The result is "the reference's algorithm with
+ *    exact arithmetic", the right yardstick for an FP32 GPU implementation.
+ *  - The reference compiles with --use_fast_math, so its float divisions are
+ *    approximate; decisions and Morton codes that sit exactly on a boundary
+ *    can differ from this IEEE oracle. Tests count such cases instead of
+ *    requiring them to be zero.
+ *  - The reference scatters leaves with an atomic cursor (src/sbh_ffi.cu:1732),
+ *    so its order inside one leaf cell is nondeterministic; the oracle keeps
+ *    input order inside a cell (a stable counting sort).
+ *
+ * Native-tree section (orc_native_*): the CPU restatement of this project's
+ * own adaptive Morton octree and group traversal, used to pin the GPU build
+ * bit-exactly (keys, permutation, topology) and the GPU sums within FP32
+ * tolerance.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORC_SQRT_PI 1.772453850905516
+#define ORC_PI 3.14159265358979323846
+
+/* ------------------------------------------------------------------------ */
+/* Byte layouts of the reference (src/sbh_ffi.cu:47-63, include/leaf_data.h) */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  float pos[3];
+  float nrm[3];
+  float mass;
+  float alpha;
+} Leaf3; /* LeafData<3>, 32 bytes */
+
+typedef struct {
+  uint32_t start, end, parent, first_child;
+  uint32_t child[8];
+  uint8_t child_mask, depth, is_leaf, pad0;
+  float cx, cy, cz, half_size, diameter;
+  Leaf3 contrib;
+} OctreeNode8; /* 104 bytes */
+
+_Static_assert(sizeof(Leaf3) == 32, "Leaf3 size");
+_Static_assert(sizeof(OctreeNode8) == 104, "OctreeNode8 size");
+
+size_t orc_leaf3_size(void) { return sizeof(Leaf3); }
+size_t orc_octree8_node_size(void) { return sizeof(OctreeNode8); }
+
+uint32_t orc_octree8_total_nodes(int max_depth) {
+  uint32_t total = 0, level = 1;
+  for (int l = 0; l <= max_depth; l++) {
+    total += level;
+    level <<= 3;
+  }
+  return total;
+}
+
+/* morton3d, src/sbh_ffi.cu:162-171 */
+static uint32_t morton3d(uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint32_t code = 0;
+  for (int i = 0; i < bits; i++) {
+    code |= ((x >> i) & 1u) << (3 * i);
+    code |= ((y >> i) & 1u) << (3 * i + 1);
+    code |= ((z >> i) & 1u) << (3 * i + 2);
+  }
+  return code;
+}
+
+/* quantize_axis, src/sbh_ffi.cu:173-179 (IEEE division here) */
+static uint32_t quantize_axis(float v, float min_v, float span, int bits) {
+  float t = (v - min_v) / span;
+  t = fminf(fmaxf(t, 0.0f), 0.999999f);
+  uint32_t max_bin = (1u << bits) - 1u;
+  return (uint32_t)(t * (float)(max_bin + 1));
+}
+
+/* ------------------------------------------------------------------------ */
+/* Softened force and its query-side VJP (src/sbh_ffi.cu:142-160, 431-501,  */
+/* 2062-2090), in double. cutoff <= 0 disables the erfc attenuation.        */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  double eps, cutoff;
+  int periodic;
+  double box;
+} SoftParams;
+
+static void min_image(double* r, const SoftParams* sp, int use_floor) {
+  if (sp->periodic && sp->box > 0.0) {
+    for (int d = 0; d < 3; d++) {
+      double q = r[d] / sp->box;
+      r[d] -= sp->box * (use_floor ? floor(q + 0.5) : nearbyint(q));
+    }
+  }
+}
+
+static void soft_force_pair(const double* r, double m, const SoftParams* sp, double* acc) {
+  double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  double eps = sp->eps > 0 ? sp->eps : 0.0;
+  double inv_r = 1.0 / sqrt(r2 + eps * eps + 1e-12);
+  double inv_r3 = inv_r * inv_r * inv_r;
+  double att = 1.0;
+  if (sp->cutoff > 0.0) {
+    double dist = sqrt(r2 + 1e-12);
+    double u = dist / (2.0 * sp->cutoff);
+    att = erfc(u) + (2.0 / ORC_SQRT_PI) * u * exp(-(u * u));
+  }
+  double c = -m * att * inv_r3;
+  acc[0] += c * r[0];
+  acc[1] += c * r[1];
+  acc[2] += c * r[2];
+}
+
+static void soft_force_pair_vjp(const double* r, double m, const double* g,
+                                const SoftParams* sp, double* acc) {
+  double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  double eps = sp->eps > 0 ? sp->eps : 0.0;
+  double inv_r = 1.0 / sqrt(r2 + eps * eps + 1e-12);
+  double inv_r3 = inv_r * inv_r * inv_r;
+  double inv_r5 = inv_r3 * inv_r * inv_r;
+  double att = 1.0, cc = 0.0;
+  if (sp->cutoff > 0.0) {
+    double dist = sqrt(r2 + 1e-12);
+    double u = dist / (2.0 * sp->cutoff);
+    double e = exp(-(u * u));
+    att = erfc(u) + (2.0 / ORC_SQRT_PI) * u * e;
+    cc = inv_r3 * dist * e / (2.0 * ORC_SQRT_PI * sp->cutoff * sp->cutoff * sp->cutoff);
+  }
+  double rg = r[0] * g[0] + r[1] * g[1] + r[2] * g[2];
+  double lin = att * inv_r3;
+  double rad = rg * (3.0 * att * inv_r5 + cc);
+  for (int d = 0; d < 3; d++) acc[d] += -m * (lin * g[d] - rad * r[d]);
+}
+
+/* gravityGrad (include/kernel.h:89-94): -m (q-p) / (|q-p| + 0.1)^3 */
+static void grav_grad_pair(const double* r, double m, double* acc) {
+  double dist = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+  double den = dist + 0.1;
+  double c = -m / (den * den * den);
+  acc[0] += c * r[0];
+  acc[1] += c * r[1];
+  acc[2] += c * r[2];
+}
+
+/* gravityGradVjp (src/sbh_ffi.cu:2044-2060) */
+static void grav_grad_pair_vjp(const double* r, double m, const double* g, double* acc) {
+  double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+  double dist = sqrt(r2 + 1e-12);
+  double den = dist + 0.1;
+  double id3 = 1.0 / (den * den * den);
+  double id4 = id3 / den;
+  double rg = r[0] * g[0] + r[1] * g[1] + r[2] * g[2];
+  double dinv = 1.0 / (dist + 1e-12);
+  for (int d = 0; d < 3; d++) acc[d] += -m * (id3 * g[d] - 3.0 * rg * dinv * id4 * r[d]);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Direct sums (src/sbh_ffi.cu:399-546), double precision                   */
+/* ------------------------------------------------------------------------ */
+
+/* softened_direct_force: out[q] = sum_i f(q - p_i), nearbyint min-image */
+void orc_direct_force_soft(const float* pts, const float* masses, int64_t n,
+                           const float* queries, int64_t nq, double eps, double cutoff,
+                           int periodic, double box, double* out) {
+  SoftParams sp = {eps, cutoff, periodic, box};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t q = 0; q < nq; q++) {
+    double acc[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; i++) {
+      double r[3] = {(double)queries[3 * q] - pts[3 * i], (double)queries[3 * q + 1] - pts[3 * i + 1],
+                     (double)queries[3 * q + 2] - pts[3 * i + 2]};
+      min_image(r, &sp, 0);
+      soft_force_pair(r, masses[i], &sp, acc);
+    }
+    out[3 * q] = acc[0];
+    out[3 * q + 1] = acc[1];
+    out[3 * q + 2] = acc[2];
+  }
+}
+
+void orc_direct_force_soft_vjp(const float* pts, const float* masses, int64_t n,
+                               const float* queries, int64_t nq, const float* cot,
+                               double eps, double cutoff, int periodic, double box,
+                               double* out) {
+  SoftParams sp = {eps, cutoff, periodic, box};
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t q = 0; q < nq; q++) {
+    double acc[3] = {0, 0, 0};
+    double g[3] = {cot[3 * q], cot[3 * q + 1], cot[3 * q + 2]};
+    for (int64_t i = 0; i < n; i++) {
+      double r[3] = {(double)queries[3 * q] - pts[3 * i], (double)queries[3 * q + 1] - pts[3 * i + 1],
+                     (double)queries[3 * q + 2] - pts[3 * i + 2]};
+      min_image(r, &sp, 0);
+      soft_force_pair_vjp(r, masses[i], g, &sp, acc);
+    }
+    out[3 * q] = acc[0];
+    out[3 * q + 1] = acc[1];
+    out[3 * q + 2] = acc[2];
+  }
+}
+
+/*
+ * Exact full gradient of L = sum_i w_i . a_i for self-gravity (queries ==
+ * sources, a_i = sum_j m_j phi(x_i - x_j), softened, cutoff <= 0 or > 0):
+ *   dL/dx_k = sum_j J(x_k - x_j) (m_j w_k - m_k w_j)       (J = d phi/dr, symmetric, even)
+ *   dL/dm_k = sum_i w_i . phi(x_i - x_k)
+ * A subset of k can be requested (idx); out_dx is (nk, 3), out_dm is (nk,).
+ * This is the exact adjoint the north star's "gradient w.r.t. positions and
+ * masses" asks for; the reference itself only has the query-side term.
+ */
+void orc_direct_full_adjoint(const float* pts, const float* masses, int64_t n,
+                             const float* w, double eps, double cutoff, const int64_t* idx,
+                             int64_t nk, double* out_dx, double* out_dm) {
+  SoftParams sp = {eps, cutoff, 0, 1.0};
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t t = 0; t < nk; t++) {
+    int64_t k = idx ? idx[t] : t;
+    double gx[3] = {0, 0, 0};
+    double gm = 0.0;
+    double wk[3] = {w[3 * k], w[3 * k + 1], w[3 * k + 2]};
+    double mk = masses[k];
+    for (int64_t j = 0; j < n; j++) {
+      double r[3] = {(double)pts[3 * k] - pts[3 * j], (double)pts[3 * k + 1] - pts[3 * j + 1],
+                     (double)pts[3 * k + 2] - pts[3 * j + 2]};
+      /* J(r) v via the VJP formula with unit mass: acc = -(J v) ... sign:
+       * soft_force_pair_vjp gives acc += -m*(lin g - rad r) = (d/dq of f)^T g
+       * where f(q) = m phi(q - p). So J(r)^T g with m=1 is exactly that. */
+      double v[3];
+      for (int d = 0; d < 3; d++) v[d] = masses[j] * wk[d] - mk * (double)w[3 * j + d];
+      soft_force_pair_vjp(r, 1.0, v, &sp, gx);
+      /* dL/dm_k: w_j . phi(x_j - x_k) = -w_j . phi(x_k - x_j) */
+      double f[3] = {0, 0, 0};
+      soft_force_pair(r, 1.0, &sp, f);
+      gm -= (double)w[3 * j] * f[0] + (double)w[3 * j + 1] * f[1] + (double)w[3 * j + 2] * f[2];
+    }
+    out_dx[3 * t] = gx[0];
+    out_dx[3 * t + 1] = gx[1];
+    out_dx[3 * t + 2] = gx[2];
+    out_dm[t] = gm;
+  }
+}
+
+/* brute_force_gravity (src/sbh_ffi.cu:399-429): -sum m/(|p-q| + 0.1), dim 2 or 3 */
+void orc_bruteforce_gravity(const float* pts, const float* masses, int64_t n, int dim,
+                            const float* queries, int64_t nq, int periodic, double box,
+                            double* out) {
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t q = 0; q < nq; q++) {
+    double acc = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+      double d2 = 0.0;
+      for (int d = 0; d < dim; d++) {
+        double diff = (double)pts[dim * i + d] - queries[dim * q + d];
+        if (periodic && box > 0.0) diff -= box * nearbyint(diff / box);
+        d2 += diff * diff;
+      }
+      acc += -(double)masses[i] / (sqrt(d2) + 0.1);
+    }
+    out[q] = acc;
+  }
+}
+
+/* signedSolidAngle<3> (include/kernel.h:73-80), direct sum in double:
+ * w(q) = sum m n.(p-q) / (4 pi (|p-q|^3 + 1e-5)) */
+void orc_direct_winding_number(const float* pts, const float* normals, const float* masses,
+                               int64_t n, const float* queries, int64_t nq, double* out) {
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t q = 0; q < nq; q++) {
+    double acc = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+      double d[3] = {(double)pts[3 * i] - queries[3 * q], (double)pts[3 * i + 1] - queries[3 * q + 1],
+                     (double)pts[3 * i + 2] - queries[3 * q + 2]};
+      double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      double nd = normals[3 * i] * d[0] + normals[3 * i + 1] * d[1] + normals[3 * i + 2] * d[2];
+      acc += (double)masses[i] * nd / (4.0 * ORC_PI * (dist * dist * dist + 1e-5));
+    }
+    out[q] = acc;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* octree8 build (src/sbh_ffi.cu:1039-1420, kernels :1682-1876)             */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Outputs, exactly sized as the reference's handler requires:
+ *   leaf_out    n * 32 bytes, Leaf3 in Morton-cell order (stable inside a cell)
+ *   node_out    T(d) * 104 bytes, dense levels 0..d, level l at offset (8^l-1)/7
+ *   contrib_out T(d) * 32 bytes, node.contrib copied out
+ *   codes_out   (optional) n Morton codes in input order
+ *   perm_out    (optional) n input indices in leaf order
+ * Returns 0, or 1 for invalid arguments (depth out of [1,10], span <= 0).
+ */
+int orc_build_octree8(const float* pts, const float* normals, const float* masses, int64_t n,
+                      const float* min_corner, const float* max_corner, int max_depth,
+                      void* leaf_out, void* node_out, void* contrib_out, uint32_t* codes_out,
+                      int64_t* perm_out) {
+  if (max_depth < 1 || max_depth > 10) return 1;
+  float span = fmaxf(fmaxf(max_corner[0] - min_corner[0], max_corner[1] - min_corner[1]),
+                     max_corner[2] - min_corner[2]);
+  if (!(span > 0.0f)) return 1;
+  uint32_t leaf_count = 1u << (3 * max_depth);
+  uint32_t total = orc_octree8_total_nodes(max_depth);
+
+  uint32_t* codes = (uint32_t*)malloc(sizeof(uint32_t) * (n > 0 ? n : 1));
+  uint32_t* cnt = (uint32_t*)calloc(leaf_count, sizeof(uint32_t));
+  uint32_t* off = (uint32_t*)calloc((size_t)leaf_count + 1, sizeof(uint32_t));
+  /* level sums in double: count, mass, m*pos, m*normal */
+  uint32_t** lcnt = (uint32_t**)calloc(max_depth + 1, sizeof(uint32_t*));
+  double** lsum = (double**)calloc(max_depth + 1, sizeof(double*));
+  for (int l = 0; l <= max_depth; l++) {
+    lcnt[l] = (uint32_t*)calloc((size_t)1 << (3 * l), sizeof(uint32_t));
+    lsum[l] = (double*)calloc(((size_t)1 << (3 * l)) * 7, sizeof(double));
+  }
+  for (int64_t i = 0; i < n; i++) {
+    uint32_t qx = quantize_axis(pts[3 * i], min_corner[0], span, max_depth);
+    uint32_t qy = quantize_axis(pts[3 * i + 1], min_corner[1], span, max_depth);
+    uint32_t qz = quantize_axis(pts[3 * i + 2], min_corner[2], span, max_depth);
+    uint32_t c = morton3d(qx, qy, qz, max_depth);
+    codes[i] = c;
+    cnt[c]++;
+    double m = masses[i];
+    double* s = &lsum[max_depth][7 * (size_t)c];
+    s[0] += m;
+    for (int d = 0; d < 3; d++) {
+      s[1 + d] += m * (double)pts[3 * i + d];
+      s[4 + d] += m * (double)(normals ? normals[3 * i + d] : 0.0f);
+    }
+  }
+  memcpy(lcnt[max_depth], cnt, sizeof(uint32_t) * leaf_count);
+  for (uint32_t c = 0; c < leaf_count; c++) off[c + 1] = off[c] + cnt[c];
+  /* stable scatter */
+  uint32_t* cur = (uint32_t*)calloc(leaf_count, sizeof(uint32_t));
+  Leaf3* leaf = (Leaf3*)leaf_out;
+  for (int64_t i = 0; i < n; i++) {
+    uint32_t c = codes[i];
+    uint32_t dst = off[c] + cur[c]++;
+    Leaf3 L;
+    for (int d = 0; d < 3; d++) {
+      L.pos[d] = pts[3 * i + d];
+      L.nrm[d] = normals ? normals[3 * i + d] : 0.0f;
+    }
+    L.mass = masses[i];
+    L.alpha = 1.0f;
+    leaf[dst] = L;
+    if (perm_out) perm_out[dst] = i;
+  }
+  /* reduce levels (src/sbh_ffi.cu:1745-1786) */
+  for (int l = max_depth - 1; l >= 0; l--) {
+    size_t cntl = (size_t)1 << (3 * l);
+    for (size_t p = 0; p < cntl; p++) {
+      uint32_t cc = 0;
+      double s[7] = {0, 0, 0, 0, 0, 0, 0};
+      for (int c = 0; c < 8; c++) {
+        size_t ch = p * 8 + c;
+        if (lcnt[l + 1][ch] == 0) continue;
+        cc += lcnt[l + 1][ch];
+        for (int k = 0; k < 7; k++) s[k] += lsum[l + 1][7 * ch + k];
+      }
+      lcnt[l][p] = cc;
+      for (int k = 0; k < 7; k++) lsum[l][7 * p + k] = s[k];
+    }
+  }
+  /* nodes (src/sbh_ffi.cu:1788-1876) */
+  float cx = min_corner[0] + span * 0.5f;
+  float cy = min_corner[1] + span * 0.5f;
+  float cz = min_corner[2] + span * 0.5f;
+  float half_size = span * 0.5f;
+  OctreeNode8* nodes = (OctreeNode8*)node_out;
+  Leaf3* contrib = (Leaf3*)contrib_out;
+  uint32_t level_off = 0;
+  for (int l = 0; l <= max_depth; l++) {
+    uint32_t level_nodes = 1u << (3 * l);
+    uint32_t parent_off = l == 0 ? 0u : level_off - (1u << (3 * (l - 1)));
+    uint32_t child_off = level_off + level_nodes;
+    int grid = 1 << l;
+    float step = half_size * 2.0f / (float)grid;
+    for (uint32_t idx = 0; idx < level_nodes; idx++) {
+      OctreeNode8 nd;
+      memset(&nd, 0, sizeof(nd));
+      uint32_t node_idx = level_off + idx;
+      nd.depth = (uint8_t)l;
+      nd.parent = l == 0 ? node_idx : parent_off + (idx >> 3);
+      nd.is_leaf = l == max_depth ? 1 : 0;
+      nd.child_mask = 0;
+      nd.first_child = 0xFFFFFFFFu;
+      uint32_t first_leaf = idx << (3 * (max_depth - l));
+      nd.start = off[first_leaf];
+      nd.end = nd.start + lcnt[l][idx];
+      int ix = 0, iy = 0, iz = 0;
+      for (int b = 0; b < l; b++) {
+        ix |= ((idx >> (3 * b + 0)) & 1) << b;
+        iy |= ((idx >> (3 * b + 1)) & 1) << b;
+        iz |= ((idx >> (3 * b + 2)) & 1) << b;
+      }
+      /* the GPU contracts (a + b*c) into one fma */
+      nd.cx = fmaf((float)ix + 0.5f, step, cx - half_size);
+      nd.cy = fmaf((float)iy + 0.5f, step, cy - half_size);
+      nd.cz = fmaf((float)iz + 0.5f, step, cz - half_size);
+      nd.half_size = step * 0.5f;
+      nd.diameter = step * sqrtf(3.0f);
+      if (l < max_depth) {
+        uint32_t child_base = child_off + (idx << 3);
+        uint8_t mask = 0;
+        for (uint32_t c = 0; c < 8; c++) {
+          nd.child[c] = child_base + c;
+          if (lcnt[l + 1][(idx << 3) + c] > 0) {
+            mask |= (uint8_t)(1u << c);
+            if (nd.first_child == 0xFFFFFFFFu) nd.first_child = child_base + c;
+          }
+        }
+        nd.child_mask = mask;
+        if (mask == 0) nd.is_leaf = 1;
+      } else {
+        for (int c = 0; c < 8; c++) nd.child[c] = 0xFFFFFFFFu;
+      }
+      double* s = &lsum[l][7 * (size_t)idx];
+      nd.contrib.alpha = 1.0f;
+      nd.contrib.mass = (float)s[0];
+      if ((float)s[0] > 0.0f) {
+        for (int d = 0; d < 3; d++) {
+          nd.contrib.pos[d] = (float)(s[1 + d] / s[0]);
+          nd.contrib.nrm[d] = (float)(s[4 + d] / s[0]);
+        }
+      }
+      nodes[node_idx] = nd;
+      contrib[node_idx] = nd.contrib;
+    }
+    level_off += level_nodes;
+  }
+  if (codes_out) memcpy(codes_out, codes, sizeof(uint32_t) * (size_t)n);
+  free(codes);
+  free(cnt);
+  free(off);
+  free(cur);
+  for (int l = 0; l <= max_depth; l++) {
+    free(lcnt[l]);
+    free(lsum[l]);
+  }
+  free(lcnt);
+  free(lsum);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* octree8 classic BH traversal (src/sbh_ffi.cu:1878-2144)                  */
+/* ------------------------------------------------------------------------ */
+
+/* minImageDisplacement (include/kernel.h:27-39), float, floor(x + 0.5) */
+static void min_image_f(float* d, int periodic, float box) {
+  if (periodic && box > 0.0f) {
+    float inv_l = 1.0f / box;
+    for (int k = 0; k < 3; k++) d[k] = d[k] - box * floorf(d[k] * inv_l + 0.5f);
+  }
+}
+
+/* octree8_use_far_field, :1878-1893 */
+static int use_far_field(const OctreeNode8* nd, const float* q, float beta, int periodic,
+                         float box) {
+  if (nd->is_leaf) return 1;
+  float dc[3] = {q[0] - nd->cx, q[1] - nd->cy, q[2] - nd->cz};
+  min_image_f(dc, periodic, box);
+  float dist = sqrtf(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]);
+  return dist / nd->diameter >= beta;
+}
+
+static float axis_dist(float q, float lo, float hi) {
+  if (q < lo) return lo - q;
+  if (q > hi) return q - hi;
+  return 0.0f;
+}
+
+/* octree8_should_prune, :1903-1948 */
+static int should_prune(const OctreeNode8* nd, const float* q, int prune_on, float r_cut_sq,
+                        int periodic, float box) {
+  if (!prune_on) return 0;
+  float qx = q[0], qy = q[1], qz = q[2];
+  if (periodic && box > 0.0f) {
+    float inv_l = 1.0f / box;
+    qx -= box * nearbyintf((qx - nd->cx) * inv_l);
+    qy -= box * nearbyintf((qy - nd->cy) * inv_l);
+    qz -= box * nearbyintf((qz - nd->cz) * inv_l);
+  }
+  float dx = axis_dist(qx, nd->cx - nd->half_size, nd->cx + nd->half_size);
+  float dy = axis_dist(qy, nd->cy - nd->half_size, nd->cy + nd->half_size);
+  float dz = axis_dist(qz, nd->cz - nd->half_size, nd->cz + nd->half_size);
+  return dx * dx + dy * dy + dz * dz > r_cut_sq;
+}
+
+/* kernel ids for the octree8 evaluators */
+enum { ORC_K_GRAV_GRAD = 0, ORC_K_SOFT = 1, ORC_K_SOFT_VJP = 2, ORC_K_GRAV_GRAD_VJP = 3 };
+
+static void eval_source(int kernel, const float* q, const Leaf3* src, const double* g,
+                        const SoftParams* sp, double* acc) {
+  double r[3] = {(double)q[0] - src->pos[0], (double)q[1] - src->pos[1],
+                 (double)q[2] - src->pos[2]};
+  min_image(r, sp, 1);
+  switch (kernel) {
+    case ORC_K_GRAV_GRAD:
+      grav_grad_pair(r, src->mass, acc);
+      break;
+    case ORC_K_SOFT:
+      soft_force_pair(r, src->mass, sp, acc);
+      break;
+    case ORC_K_SOFT_VJP:
+      soft_force_pair_vjp(r, src->mass, g, sp, acc);
+      break;
+    default:
+      grav_grad_pair_vjp(r, src->mass, g, acc);
+      break;
+  }
+}
+
+/*
+ * barnes_hut_force_octree8{,_soft,_soft_vjp}_kernel (:1950-2144).
+ * kernel: 0 gravityGrad, 1 softened force, 2 softened query-side VJP (cot).
+ * prune_on / r_cut_sq exactly as the handler derives them (:3235-3237).
+ * counts (optional): interactions per query. Returns 0, or 2 if a query's
+ * stack would exceed the reference's 128 entries.
+ */
+int orc_bh_octree8(const void* leaf_bytes, const void* node_bytes, const float* queries,
+                   int64_t nq, const float* cot, float beta, int kernel, double eps,
+                   double cutoff, int prune_on, float r_cut_sq, int periodic, float box,
+                   double* out, int32_t* counts) {
+  const Leaf3* leaf = (const Leaf3*)leaf_bytes;
+  const OctreeNode8* nodes = (const OctreeNode8*)node_bytes;
+  SoftParams sp = {eps, cutoff, periodic, box};
+  int status = 0;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int64_t qi = 0; qi < nq; qi++) {
+    const float* q = &queries[3 * qi];
+    double g[3] = {0, 0, 0};
+    if (cot) {
+      g[0] = cot[3 * qi];
+      g[1] = cot[3 * qi + 1];
+      g[2] = cot[3 * qi + 2];
+    }
+    double acc[3] = {0, 0, 0};
+    int32_t nint = 0;
+    int stack[128];
+    int top = 0;
+    stack[top++] = 0;
+    while (top > 0) {
+      int idx = stack[--top];
+      const OctreeNode8* nd = &nodes[idx];
+      if (nd->contrib.mass == 0.0f) continue;
+      if (kernel != ORC_K_GRAV_GRAD && should_prune(nd, q, prune_on, r_cut_sq, periodic, box))
+        continue;
+      if (use_far_field(nd, q, beta, periodic, box)) {
+        if (nd->is_leaf) {
+          for (uint32_t i = nd->start; i < nd->end; i++) {
+            eval_source(kernel, q, &leaf[i], g, &sp, acc);
+            nint++;
+          }
+        } else {
+          eval_source(kernel, q, &nd->contrib, g, &sp, acc);
+          nint++;
+        }
+      } else {
+        for (int c = 0; c < 8; c++) {
+          if (nd->child_mask & (1u << c)) {
+            if (top >= 128) {
+              status = 2;
+              break;
+            }
+            stack[top++] = (int)nd->child[c];
+          }
+        }
+      }
+    }
+    out[3 * qi] = acc[0];
+    out[3 * qi + 1] = acc[1];
+    out[3 * qi + 2] = acc[2];
+    if (counts) counts[qi] = nint;
+  }
+  return status;
+}
+
+/* ======================================================================== */
+/* Native adaptive Morton octree (this project's own tree)                  */
+/* ======================================================================== */
+/*
+ * Definition (the GPU build must reproduce every integer field bit-exactly):
+ *  1. lo = per-axis min of the points, hi = per-axis max; span = max(hi - lo)
+ *     over axes, replaced by 1 when it is 0. All in float, exact.
+ *  2. scale = 2097152.0 / (double)span; q_a = floor(((double)x_a - (double)lo_a)
+ *     * scale) clamped to [0, 2^21 - 1] (double, no fused operations).
+ *  3. key = 63-bit Morton interleave, x in bit 3i, y in 3i+1, z in 3i+2.
+ *  4. perm = stable sort of input indices by key.
+ *  5. level-l cell of a key = its top 3l bits (l = 0..21). A cell is a node
+ *     when l == 0 or its parent cell holds more than leaf_size particles. A
+ *     node is a leaf when it holds <= leaf_size particles or l == 21.
+ *  6. Nodes are numbered in DFS pre-order (parent before children, children
+ *     in Morton order). skip[n] = pre-order index after n's subtree; a node's
+ *     particles are the sorted range [start, end).
+ */
+static int common_levels(uint64_t a, uint64_t b) {
+  uint64_t x = a ^ b;
+  if (x == 0) return 21;
+  int lz = __builtin_clzll(x) - 1; /* 63-bit keys: bit 63 is always 0 */
+  return lz / 3;
+}
+
+static int cmp_key_idx(const void* a, const void* b) {
+  const uint64_t* x = (const uint64_t*)a;
+  const uint64_t* y = (const uint64_t*)b;
+  if (x[0] < y[0]) return -1;
+  if (x[0] > y[0]) return 1;
+  if (x[1] < y[1]) return -1;
+  if (x[1] > y[1]) return 1;
+  return 0;
+}
+
+/* Quantisation + keys + stable sort. keys_out[i] is the key of sorted slot i,
+ * perm_out[i] the input index stored there. box_out = {lo[3], span}. */
+void orc_native_sort(const float* pts, int64_t n, uint64_t* keys_out, int64_t* perm_out,
+                     float* box_out) {
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t i = 0; i < n; i++)
+    for (int d = 0; d < 3; d++) {
+      lo[d] = fminf(lo[d], pts[3 * i + d]);
+      hi[d] = fmaxf(hi[d], pts[3 * i + d]);
+    }
+  float span = 0.0f;
+  for (int d = 0; d < 3; d++) span = fmaxf(span, hi[d] - lo[d]);
+  if (!(span > 0.0f)) span = 1.0f;
+  double scale = 2097152.0 / (double)span;
+  uint64_t* kv = (uint64_t*)malloc(sizeof(uint64_t) * 2 * (n > 0 ? n : 1));
+  for (int64_t i = 0; i < n; i++) {
+    uint64_t key = 0;
+    for (int d = 0; d < 3; d++) {
+      double t = ((double)pts[3 * i + d] - (double)lo[d]) * scale;
+      double f = floor(t);
+      uint64_t qv = f < 0.0 ? 0 : (f > 2097151.0 ? 2097151u : (uint64_t)f);
+      for (int b = 0; b < 21; b++) key |= ((qv >> b) & 1ull) << (3 * b + d);
+    }
+    kv[2 * i] = key;
+    kv[2 * i + 1] = (uint64_t)i;
+  }
+  qsort(kv, (size_t)n, 2 * sizeof(uint64_t), cmp_key_idx);
+  for (int64_t i = 0; i < n; i++) {
+    keys_out[i] = kv[2 * i];
+    perm_out[i] = (int64_t)kv[2 * i + 1];
+  }
+  free(kv);
+  box_out[0] = lo[0];
+  box_out[1] = lo[1];
+  box_out[2] = lo[2];
+  box_out[3] = span;
+}
+
+/*
+ * Topology from sorted keys. Returns the node count; when the output arrays
+ * are non-NULL they receive (pre-order) start, end, skip and level per node.
+ * Every slot count is computed from per-position quantities only:
+ *   d(i)  = common levels of key[i-1] and key[i] (cells i starts: levels > d(i))
+ *   L(i)  = leaf level of position i = min(21, 1 + max_{a} cl(key[a], key[a+S]))
+ *           over windows a in [i-S, i] with a+S < n (S = leaf_size),
+ *           or 0 if n <= S.
+ *   position i starts internal nodes at levels [lo(i), L(i) - 1] where
+ *   lo(i) = 0 for i == 0 else d(i) + 1, and a leaf at level L(i) when
+ *   i == 0 or d(i) < L(i).
+ */
+int64_t orc_native_topology(const uint64_t* keys, int64_t n, int leaf_size, int32_t* start,
+                            int32_t* end, int32_t* skip, int8_t* level) {
+  if (n <= 0) return 0;
+  int S = leaf_size;
+  int* cl = (int*)malloc(sizeof(int) * (size_t)n);
+  int* Lv = (int*)malloc(sizeof(int) * (size_t)n);
+  int64_t* base = (int64_t*)malloc(sizeof(int64_t) * ((size_t)n + 1));
+  for (int64_t a = 0; a < n; a++) cl[a] = (a + S < n) ? common_levels(keys[a], keys[a + S]) : -1;
+  for (int64_t i = 0; i < n; i++) {
+    if (n <= S) {
+      Lv[i] = 0;
+      continue;
+    }
+    int mx = -1;
+    int64_t a0 = i - S < 0 ? 0 : i - S;
+    for (int64_t a = a0; a <= i; a++)
+      if (cl[a] > mx) mx = cl[a];
+    int L = mx + 1;
+    Lv[i] = L > 21 ? 21 : L;
+  }
+  base[0] = 0;
+  for (int64_t i = 0; i < n; i++) {
+    int lo = i == 0 ? 0 : common_levels(keys[i - 1], keys[i]) + 1;
+    int d = i == 0 ? -1 : common_levels(keys[i - 1], keys[i]);
+    int nint = Lv[i] - lo;
+    if (nint < 0) nint = 0;
+    int nleaf = (i == 0 || d < Lv[i]) ? 1 : 0;
+    base[i + 1] = base[i] + nint + nleaf;
+  }
+  int64_t total = base[n];
+  if (start) {
+    for (int64_t i = 0; i < n; i++) {
+      int lo = i == 0 ? 0 : common_levels(keys[i - 1], keys[i]) + 1;
+      int d = i == 0 ? -1 : common_levels(keys[i - 1], keys[i]);
+      int64_t slot = base[i];
+      int top = (i == 0 || d < Lv[i]) ? Lv[i] : Lv[i] - 1;
+      for (int l = lo; l <= top; l++) {
+        /* end: first j > i whose key leaves the level-l cell of key[i] */
+        int64_t e = i + 1;
+        int64_t lo_s = i + 1, hi_s = n;
+        uint64_t pref = l == 0 ? 0 : keys[i] >> (63 - 3 * l);
+        while (lo_s < hi_s) {
+          int64_t mid = (lo_s + hi_s) >> 1;
+          uint64_t pm = l == 0 ? 0 : keys[mid] >> (63 - 3 * l);
+          if (pm == pref)
+            lo_s = mid + 1;
+          else
+            hi_s = mid;
+        }
+        e = lo_s;
+        start[slot] = (int32_t)i;
+        end[slot] = (int32_t)e;
+        level[slot] = (int8_t)l;
+        skip[slot] = (int32_t)(e < n ? base[e] : total);
+        slot++;
+      }
+    }
+  }
+  free(cl);
+  free(Lv);
+  free(base);
+  return total;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Native tree handle: sorted order, topology, geometry, and a traversal     */
+/* plan (per target group: accepted nodes and near-field leaves).            */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  int64_t n, nn;
+  int leaf_size;
+  float lo[3], span;
+  uint64_t* keys;
+  int64_t* perm;
+  int32_t *start, *end, *skip;
+  int8_t* level;
+  float* center; /* nn x 3, cell centre */
+  float* side;   /* nn, cell side */
+  /* plan */
+  int group_size;
+  int64_t ngroups;
+  int64_t* far_off; /* ngroups + 1 */
+  int32_t* far_idx;
+  int64_t* near_off;
+  int32_t* near_idx; /* near-field leaf node ids */
+} NativeTree;
+
+static void cell_geometry(const NativeTree* t, int64_t nd, uint64_t key) {
+  int l = t->level[nd];
+  uint64_t p = l == 0 ? 0 : key >> (63 - 3 * l);
+  uint32_t c[3] = {0, 0, 0};
+  for (int b = 0; b < l; b++)
+    for (int d = 0; d < 3; d++) c[d] |= (uint32_t)((p >> (3 * b + d)) & 1u) << b;
+  float side = ldexpf(t->span, -l);
+  t->side[nd] = side;
+  for (int d = 0; d < 3; d++)
+    t->center[3 * nd + d] = (float)((double)t->lo[d] + ((double)c[d] + 0.5) * (double)side);
+}
+
+void* orc_native_build(const float* pts, int64_t n, int leaf_size) {
+  NativeTree* t = (NativeTree*)calloc(1, sizeof(NativeTree));
+  t->n = n;
+  t->leaf_size = leaf_size;
+  t->keys = (uint64_t*)malloc(sizeof(uint64_t) * (n > 0 ? n : 1));
+  t->perm = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  float box[4];
+  orc_native_sort(pts, n, t->keys, t->perm, box);
+  memcpy(t->lo, box, 3 * sizeof(float));
+  t->span = box[3];
+  int64_t nn = orc_native_topology(t->keys, n, leaf_size, NULL, NULL, NULL, NULL);
+  t->nn = nn;
+  size_t cap = nn > 0 ? (size_t)nn : 1;
+  t->start = (int32_t*)malloc(sizeof(int32_t) * cap);
+  t->end = (int32_t*)malloc(sizeof(int32_t) * cap);
+  t->skip = (int32_t*)malloc(sizeof(int32_t) * cap);
+  t->level = (int8_t*)malloc(cap);
+  t->center = (float*)malloc(sizeof(float) * 3 * cap);
+  t->side = (float*)malloc(sizeof(float) * cap);
+  orc_native_topology(t->keys, n, leaf_size, t->start, t->end, t->skip, t->level);
+  for (int64_t k = 0; k < nn; k++) cell_geometry(t, k, t->keys[t->start[k]]);
+  return t;
+}
+
+void orc_native_free(void* h) {
+  NativeTree* t = (NativeTree*)h;
+  if (!t) return;
+  free(t->keys);
+  free(t->perm);
+  free(t->start);
+  free(t->end);
+  free(t->skip);
+  free(t->level);
+  free(t->center);
+  free(t->side);
+  free(t->far_off);
+  free(t->far_idx);
+  free(t->near_off);
+  free(t->near_idx);
+  free(t);
+}
+
+int64_t orc_native_num_nodes(void* h) { return ((NativeTree*)h)->nn; }
+
+void orc_native_get(void* h, uint64_t* keys, int64_t* perm, int32_t* start, int32_t* end,
+                    int32_t* skip, int8_t* level, float* center, float* side, float* box) {
+  NativeTree* t = (NativeTree*)h;
+  if (keys) memcpy(keys, t->keys, sizeof(uint64_t) * t->n);
+  if (perm) memcpy(perm, t->perm, sizeof(int64_t) * t->n);
+  if (start) memcpy(start, t->start, sizeof(int32_t) * t->nn);
+  if (end) memcpy(end, t->end, sizeof(int32_t) * t->nn);
+  if (skip) memcpy(skip, t->skip, sizeof(int32_t) * t->nn);
+  if (level) memcpy(level, t->level, t->nn);
+  if (center) memcpy(center, t->center, sizeof(float) * 3 * t->nn);
+  if (side) memcpy(side, t->side, sizeof(float) * t->nn);
+  if (box) {
+    memcpy(box, t->lo, 3 * sizeof(float));
+    box[3] = t->span;
+  }
+}
+
+/* Node monopoles in double from the sorted particles: mass, mass-weighted
+ * centroid, and the float COM the GPU stores. mom: nn x 4 (M, X, Y, Z). */
+#define MOM 10
+static void native_moments(const NativeTree* t, const float* pts, const float* masses,
+                           double* mom) {
+  int64_t n = t->n;
+  /* prefix sums of m, m y, m y y^T with y = x - box centre (smaller magnitudes) */
+  double c0[3];
+  for (int d = 0; d < 3; d++) c0[d] = (double)t->lo[d] + 0.5 * (double)t->span;
+  double* P = (double*)calloc(((size_t)n + 1) * MOM, sizeof(double));
+  for (int64_t i = 0; i < n; i++) {
+    int64_t s = t->perm[i];
+    double m = masses[s];
+    double y[3] = {(double)pts[3 * s] - c0[0], (double)pts[3 * s + 1] - c0[1], (double)pts[3 * s + 2] - c0[2]};
+    double v[MOM] = {m, m * y[0], m * y[1], m * y[2], m * y[0] * y[0], m * y[1] * y[1], m * y[2] * y[2],
+                     m * y[0] * y[1], m * y[0] * y[2], m * y[1] * y[2]};
+    for (int c = 0; c < MOM; c++) P[MOM * (i + 1) + c] = P[MOM * i + c] + v[c];
+  }
+  for (int64_t k = 0; k < t->nn; k++) {
+    double v[MOM];
+    for (int c = 0; c < MOM; c++) v[c] = P[MOM * t->end[k] + c] - P[MOM * t->start[k] + c];
+    double M = v[0];
+    double* o = &mom[MOM * k];
+    o[0] = M;
+    if (M != 0.0) {
+      double Y[3] = {v[1] / M, v[2] / M, v[3] / M};
+      for (int d = 0; d < 3; d++) o[1 + d] = Y[d] + c0[d];
+      o[4] = v[4] - M * Y[0] * Y[0];
+      o[5] = v[5] - M * Y[1] * Y[1];
+      o[6] = v[6] - M * Y[2] * Y[2];
+      o[7] = v[7] - M * Y[0] * Y[1];
+      o[8] = v[8] - M * Y[0] * Y[2];
+      o[9] = v[9] - M * Y[1] * Y[2];
+    } else {
+      for (int d = 0; d < 3; d++) o[1 + d] = (double)t->center[3 * k + d];
+      for (int c = 4; c < MOM; c++) o[c] = 0.0;
+    }
+  }
+  free(P);
+}
+
+/* S x for the packed symmetric S = (xx, yy, zz, xy, xz, yz) */
+static void sym_mul(const double* S, const double* x, double* o) {
+  o[0] = S[0] * x[0] + S[3] * x[1] + S[4] * x[2];
+  o[1] = S[3] * x[0] + S[1] * x[1] + S[5] * x[2];
+  o[2] = S[4] * x[0] + S[5] * x[1] + S[2] * x[2];
+}
+
+/*
+ * Quadrupole correction of the softened far field about the COM, the exact
+ * second-order Taylor term of sum_k m_k phi(x + X - x_k) with
+ * phi(r) = -r (r^2 + eps^2)^{-3/2}:
+ *   a_q = h^{-5/2} (3 S x + 1.5 tr(S) x) - 7.5 (x^T S x) h^{-7/2} x,  h = |x|^2 + eps^2
+ * (x = q - X). Plummer softening only (no cutoff attenuation).
+ */
+static void quad_force(const double* x, const double* S, double eps, double* acc) {
+  double h = x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + eps * eps + 1e-12;
+  double ih = 1.0 / h;
+  double ir = 1.0 / sqrt(h);
+  double ir5 = ir * ih * ih;
+  double Sx[3];
+  sym_mul(S, x, Sx);
+  double tr = S[0] + S[1] + S[2];
+  double xSx = x[0] * Sx[0] + x[1] * Sx[1] + x[2] * Sx[2];
+  for (int d = 0; d < 3; d++) acc[d] += ir5 * (3.0 * Sx[d] + 1.5 * tr * x[d]) - 7.5 * xSx * ir5 * ih * x[d];
+}
+
+/* J w for the quadrupole term (J symmetric), and G = sym(d(w . a_q)/dS), the
+ * symmetric part of the gradient w.r.t. the full matrix S, packed
+ * (G00, G11, G22, G01, G02, G12): for S = sum m y y^T, dL/dy = 2 m G y and
+ * dL/dm = y^T G y. */
+static void quad_vjp(const double* x, const double* S, const double* w, double eps, double* jw,
+                     double* gS) {
+  double h = x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + eps * eps + 1e-12;
+  double ih = 1.0 / h;
+  double ir = 1.0 / sqrt(h);
+  double ir5 = ir * ih * ih, ir7 = ir5 * ih, ir9 = ir7 * ih;
+  double Sx[3], Sw[3];
+  sym_mul(S, x, Sx);
+  sym_mul(S, w, Sw);
+  double tr = S[0] + S[1] + S[2];
+  double xSx = x[0] * Sx[0] + x[1] * Sx[1] + x[2] * Sx[2];
+  double xw = x[0] * w[0] + x[1] * w[1] + x[2] * w[2];
+  double Sxw = Sx[0] * w[0] + Sx[1] * w[1] + Sx[2] * w[2];
+  for (int d = 0; d < 3; d++) {
+    jw[d] += ir5 * (3.0 * Sw[d] + 1.5 * tr * w[d]) - 5.0 * ir7 * xw * (3.0 * Sx[d] + 1.5 * tr * x[d]) -
+             7.5 * ir7 * xSx * w[d] - 7.5 * x[d] * (2.0 * ir7 * Sxw - 7.0 * ir9 * xSx * xw);
+  }
+  if (gS) {
+    /* d(w.a_q)/dS_ij = 1.5 h^-5/2 (w_i x_j + x_i w_j) + 1.5 h^-5/2 (x.w) delta_ij - 7.5 h^-7/2 (x.w) x_i x_j */
+    double a = 1.5 * ir5, b = 1.5 * ir5 * xw, c = 7.5 * ir7 * xw;
+    gS[0] += a * 2.0 * w[0] * x[0] + b - c * x[0] * x[0];
+    gS[1] += a * 2.0 * w[1] * x[1] + b - c * x[1] * x[1];
+    gS[2] += a * 2.0 * w[2] * x[2] + b - c * x[2] * x[2];
+    gS[3] += a * (w[0] * x[1] + x[0] * w[1]) - c * x[0] * x[1];
+    gS[4] += a * (w[0] * x[2] + x[0] * w[2]) - c * x[0] * x[2];
+    gS[5] += a * (w[1] * x[2] + x[1] * w[2]) - c * x[1] * x[2];
+  }
+}
+
+/* The GPU's float COM for node k from double moments. */
+static void com_float(const double* mom, int64_t k, float* X, float* M) {
+  *M = (float)mom[MOM * k];
+  for (int d = 0; d < 3; d++) X[d] = (float)mom[MOM * k + 1 + d];
+}
+
+/*
+ * Multipole acceptance for target group box [gmin, gmax] (float, no fused
+ * operations), in the reference's convention (src/sbh_ffi.cu:1878-1893:
+ * distance / cell diagonal >= beta, beta = 1/theta) made conservative for a
+ * group and for the offset of the COM from the cell centre:
+ *   accept node k iff dist^2(box, COM) > (side * sqrt(3) * beta + delta)^2,
+ *   delta = |COM - cell centre|.
+ */
+static int native_accept(const NativeTree* t, int64_t k, const float* X, const float* gmin,
+                         const float* gmax, float beta) {
+  float dcx = X[0] - t->center[3 * k], dcy = X[1] - t->center[3 * k + 1],
+        dcz = X[2] - t->center[3 * k + 2];
+  float delta = sqrtf(dcx * dcx + dcy * dcy + dcz * dcz);
+  float diag = t->side[k] * 1.7320508f;
+  float rc = diag * beta + delta;
+  float tt[3];
+  for (int d = 0; d < 3; d++) {
+    float a = gmin[d] - X[d], b = X[d] - gmax[d];
+    float m = a > b ? a : b;
+    tt[d] = m > 0.0f ? m : 0.0f;
+  }
+  float d2 = tt[0] * tt[0] + tt[1] * tt[1] + tt[2] * tt[2];
+  return d2 > rc * rc;
+}
+
+/*
+ * Record the traversal plan for beta: targets are consecutive runs of
+ * group_size sorted particles; each group walks the pre-order tree,
+ * accepting nodes by native_accept and summing near-field leaves directly.
+ * Mass-zero nodes are skipped. Returns the total interaction count
+ * (sum over groups of active targets x (accepted nodes + near particles)).
+ */
+int64_t orc_native_plan(void* h, const float* pts, const float* masses, double beta,
+                        int group_size) {
+  NativeTree* t = (NativeTree*)h;
+  int64_t n = t->n;
+  free(t->far_off);
+  free(t->far_idx);
+  free(t->near_off);
+  free(t->near_idx);
+  t->group_size = group_size;
+  int64_t ng = (n + group_size - 1) / group_size;
+  t->ngroups = ng;
+  double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
+  native_moments(t, pts, masses, mom);
+  float fbeta = (float)beta;
+  int64_t fcap = 1 << 20, ncap = 1 << 18;
+  t->far_idx = (int32_t*)malloc(sizeof(int32_t) * fcap);
+  t->near_idx = (int32_t*)malloc(sizeof(int32_t) * ncap);
+  t->far_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
+  t->near_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
+  int64_t nf = 0, nr = 0, total = 0;
+  for (int64_t g = 0; g < ng; g++) {
+    t->far_off[g] = nf;
+    t->near_off[g] = nr;
+    int64_t s0 = g * group_size, s1 = s0 + group_size < n ? s0 + group_size : n;
+    float gmin[3] = {INFINITY, INFINITY, INFINITY}, gmax[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = s0; i < s1; i++)
+      for (int d = 0; d < 3; d++) {
+        float v = pts[3 * t->perm[i] + d];
+        gmin[d] = fminf(gmin[d], v);
+        gmax[d] = fmaxf(gmax[d], v);
+      }
+    int64_t k = 0, cnt_int = 0;
+    while (k < t->nn) {
+      float X[3], M;
+      com_float(mom, k, X, &M);
+      if (M == 0.0f) {
+        k = t->skip[k];
+        continue;
+      }
+      int is_leaf = (k + 1 >= t->nn) || (t->skip[k] == k + 1);
+      if (native_accept(t, k, X, gmin, gmax, fbeta)) {
+        if (nf == fcap) {
+          fcap *= 2;
+          t->far_idx = (int32_t*)realloc(t->far_idx, sizeof(int32_t) * fcap);
+        }
+        t->far_idx[nf++] = (int32_t)k;
+        cnt_int += 1;
+        k = t->skip[k];
+      } else if (is_leaf) {
+        if (nr == ncap) {
+          ncap *= 2;
+          t->near_idx = (int32_t*)realloc(t->near_idx, sizeof(int32_t) * ncap);
+        }
+        t->near_idx[nr++] = (int32_t)k;
+        cnt_int += t->end[k] - t->start[k];
+        k = t->skip[k];
+      } else {
+        k = k + 1;
+      }
+    }
+    total += cnt_int * (s1 - s0);
+  }
+  t->far_off[ng] = nf;
+  t->near_off[ng] = nr;
+  free(mom);
+  return total;
+}
+
+/*
+ * Evaluate the planned sums with the given (possibly perturbed) positions
+ * and masses: topology, sorted order and decisions stay frozen, node
+ * moments are recomputed. out_force: n x 3 in input order. If w is given,
+ * *loss = sum_i w_i . a_i. quad != 0 adds the quadrupole term of accepted
+ * nodes (Plummer softening, cutoff must be <= 0).
+ */
+void orc_native_eval(void* h, const float* pts, const float* masses, double eps, double cutoff,
+                     int quad, double* out_force, const float* w, double* loss) {
+  NativeTree* t = (NativeTree*)h;
+  int64_t n = t->n;
+  SoftParams sp = {eps, cutoff, 0, 1.0};
+  double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
+  native_moments(t, pts, masses, mom);
+  double L = 0.0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : L)
+  for (int64_t g = 0; g < t->ngroups; g++) {
+    int64_t s0 = g * t->group_size, s1 = s0 + t->group_size < n ? s0 + t->group_size : n;
+    for (int64_t i = s0; i < s1; i++) {
+      int64_t qi = t->perm[i];
+      double q[3] = {pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]};
+      double acc[3] = {0, 0, 0};
+      for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) {
+        int32_t k = t->far_idx[e];
+        const double* o = &mom[MOM * k];
+        double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
+        soft_force_pair(r, o[0], &sp, acc);
+        if (quad) quad_force(r, o + 4, eps, acc);
+      }
+      for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
+        int32_t k = t->near_idx[e];
+        for (int32_t j = t->start[k]; j < t->end[k]; j++) {
+          int64_t sj = t->perm[j];
+          double r[3] = {q[0] - pts[3 * sj], q[1] - pts[3 * sj + 1], q[2] - pts[3 * sj + 2]};
+          soft_force_pair(r, masses[sj], &sp, acc);
+        }
+      }
+      if (out_force) {
+        out_force[3 * qi] = acc[0];
+        out_force[3 * qi + 1] = acc[1];
+        out_force[3 * qi + 2] = acc[2];
+      }
+      if (w) L += w[3 * qi] * acc[0] + w[3 * qi + 1] * acc[1] + w[3 * qi + 2] * acc[2];
+    }
+  }
+  if (loss) *loss = L;
+  free(mom);
+}
+
+/*
+ * Exact adjoint of orc_native_eval's loss w.r.t. positions and masses, with
+ * the plan frozen:
+ *   query side       dL/dx_i += sum_src J_src(x_i)^T w_i
+ *   direct sources   dL/dx_j -= m_j J(x_i - x_j)^T w_i,  dL/dm_j += w_i . phi(x_i - x_j)
+ *   node moments     A_X[k] = -sum_i J_k(x_i - X_k)^T w_i   (monopole + quadrupole)
+ *                    A_M[k] = sum_i w_i . phi(x_i - X_k)
+ *                    G_S[k] = sum_i d(w_i . a_q)/dS
+ *                    dL/dx_p += (m_p / M_k) A_X[k] + 2 m_p G_S[k] (x_p - X_k)
+ *                    dL/dm_p += A_M[k] + A_X[k] . (x_p - X_k) / M_k + (x_p - X_k)^T G_S[k] (x_p - X_k)
+ *   for every particle p of node k (S = sum m y y^T about X has zero derivative
+ *   through X because sum m y = 0).
+ * dx: n x 3, dm: n, input order.
+ */
+void orc_native_adjoint(void* h, const float* pts, const float* masses, const float* w,
+                        double eps, double cutoff, int quad, double* dx, double* dm) {
+  NativeTree* t = (NativeTree*)h;
+  int64_t n = t->n;
+  SoftParams sp = {eps, cutoff, 0, 1.0};
+  double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
+  native_moments(t, pts, masses, mom);
+  double* AX = (double*)calloc((size_t)(t->nn > 0 ? t->nn : 1) * MOM, sizeof(double));
+  memset(dx, 0, sizeof(double) * 3 * n);
+  memset(dm, 0, sizeof(double) * n);
+  for (int64_t g = 0; g < t->ngroups; g++) {
+    int64_t s0 = g * t->group_size, s1 = s0 + t->group_size < n ? s0 + t->group_size : n;
+    for (int64_t i = s0; i < s1; i++) {
+      int64_t qi = t->perm[i];
+      double q[3] = {pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]};
+      double wi[3] = {w[3 * qi], w[3 * qi + 1], w[3 * qi + 2]};
+      double gq[3] = {0, 0, 0};
+      for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) {
+        int32_t k = t->far_idx[e];
+        const double* o = &mom[MOM * k];
+        double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
+        double jt[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+        soft_force_pair_vjp(r, o[0], wi, &sp, jt);
+        soft_force_pair(r, 1.0, &sp, f);
+        if (quad) quad_vjp(r, o + 4, wi, eps, jt, &AX[MOM * k + 4]);
+        for (int d = 0; d < 3; d++) {
+          gq[d] += jt[d];
+          AX[MOM * k + 1 + d] -= jt[d];
+        }
+        AX[MOM * k] += wi[0] * f[0] + wi[1] * f[1] + wi[2] * f[2];
+      }
+      for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
+        int32_t k = t->near_idx[e];
+        for (int32_t j = t->start[k]; j < t->end[k]; j++) {
+          int64_t sj = t->perm[j];
+          double r[3] = {q[0] - pts[3 * sj], q[1] - pts[3 * sj + 1], q[2] - pts[3 * sj + 2]};
+          double jt[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+          soft_force_pair_vjp(r, 1.0, wi, &sp, jt);
+          soft_force_pair(r, 1.0, &sp, f);
+          for (int d = 0; d < 3; d++) {
+            gq[d] += masses[sj] * jt[d];
+            dx[3 * sj + d] -= masses[sj] * jt[d];
+          }
+          dm[sj] += wi[0] * f[0] + wi[1] * f[1] + wi[2] * f[2];
+        }
+      }
+      for (int d = 0; d < 3; d++) dx[3 * qi + d] += gq[d];
+    }
+  }
+  /* push node adjoints down to the particles of each node */
+  for (int64_t k = 0; k < t->nn; k++) {
+    const double* o = &mom[MOM * k];
+    double M = o[0];
+    if (M == 0.0) continue;
+    const double* A = &AX[MOM * k];
+    int any = 0;
+    for (int c = 0; c < MOM; c++) any |= A[c] != 0.0;
+    if (!any) continue;
+    for (int32_t j = t->start[k]; j < t->end[k]; j++) {
+      int64_t sj = t->perm[j];
+      double mj = masses[sj];
+      double y[3] = {(double)pts[3 * sj] - o[1], (double)pts[3 * sj + 1] - o[2], (double)pts[3 * sj + 2] - o[3]};
+      double Gy[3];
+      sym_mul(A + 4, y, Gy);
+      double proj = A[1] * y[0] + A[2] * y[1] + A[3] * y[2];
+      for (int d = 0; d < 3; d++) dx[3 * sj + d] += mj / M * A[1 + d] + 2.0 * mj * Gy[d];
+      dm[sj] += A[0] + proj / M + (y[0] * Gy[0] + y[1] * Gy[1] + y[2] * Gy[2]);
+    }
+  }
+  free(AX);
+  free(mom);
+}
+
+/* Plan statistics: number of groups and list lengths. */
+void orc_native_plan_stats(void* h, int64_t* ngroups, int64_t* nfar, int64_t* nnear) {
+  NativeTree* t = (NativeTree*)h;
+  *ngroups = t->ngroups;
+  *nfar = t->far_off ? t->far_off[t->ngroups] : 0;
+  *nnear = t->near_off ? t->near_off[t->ngroups] : 0;
+}

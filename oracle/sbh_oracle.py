@@ -1,0 +1,476 @@
+"""ctypes bindings for the oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loads the project's C restatement (``_ref/libsbh_oracle.so``, built from
+``sbh_oracle.c``) and, when present, the reference's own code compiled by
+``Makefile``'s ``ref`` target:
+
+* ``_ref/libsbh_ref_cpu.so`` / ``libsbh_ref_cpu64.so``: the reference's CPU
+  ``Tree3D``/``Tree2D`` build and ``evaluateBarnesHut_stackless`` driven like
+  ``src/sbh.cpp:49-88`` (FP32 and ``-DUSE_DOUBLE`` builds);
+* ``_ref/libsbh_ref_gpu.so``: the reference's ``src/sbh_ffi.cu`` handlers,
+  callable with device pointers (GPU box only).
+
+Only tests, the smoke check and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REF = os.path.join(_HERE, "_ref")
+
+_c_f = ctypes.c_float
+_c_d = ctypes.c_double
+_c_i = ctypes.c_int
+_c_i64 = ctypes.c_int64
+_c_p = ctypes.c_void_p
+_c_u32 = ctypes.c_uint32
+_c_sz = ctypes.c_size_t
+
+_LIBS: dict = {}
+
+
+def _ptr(a: Optional[np.ndarray]):
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be C-contiguous"
+    return a.ctypes.data_as(_c_p)
+
+
+def lib_path(name: str) -> str:
+    return os.path.join(_REF, name)
+
+
+def available(name: str) -> bool:
+    return os.path.exists(lib_path(name))
+
+
+def _load(name: str) -> ctypes.CDLL:
+    if name not in _LIBS:
+        path = lib_path(name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"oracle library {path} is missing; run `make -C oracle` (and `make -C oracle ref`)")
+        _LIBS[name] = ctypes.CDLL(path)
+    return _LIBS[name]
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+# ---------------------------------------------------------------------------
+# project restatement (libsbh_oracle.so)
+# ---------------------------------------------------------------------------
+def _orc() -> ctypes.CDLL:
+    lib = _load("libsbh_oracle.so")
+    if not getattr(lib, "_typed", False):
+        lib.orc_octree8_total_nodes.restype = _c_u32
+        lib.orc_octree8_total_nodes.argtypes = [_c_i]
+        lib.orc_leaf3_size.restype = _c_sz
+        lib.orc_octree8_node_size.restype = _c_sz
+        lib.orc_direct_force_soft.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_d, _c_d, _c_i, _c_d, _c_p]
+        lib.orc_direct_force_soft_vjp.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_d, _c_d, _c_i, _c_d, _c_p]
+        lib.orc_direct_full_adjoint.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_d, _c_d, _c_p, _c_i64, _c_p, _c_p]
+        lib.orc_bruteforce_gravity.argtypes = [_c_p, _c_p, _c_i64, _c_i, _c_p, _c_i64, _c_i, _c_d, _c_p]
+        lib.orc_direct_winding_number.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p]
+        lib.orc_build_octree8.restype = _c_i
+        lib.orc_build_octree8.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_i, _c_p, _c_p, _c_p, _c_p, _c_p]
+        lib.orc_bh_octree8.restype = _c_i
+        lib.orc_bh_octree8.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_f, _c_i, _c_d, _c_d, _c_i, _c_f, _c_i, _c_f, _c_p, _c_p]
+        lib.orc_native_sort.argtypes = [_c_p, _c_i64, _c_p, _c_p, _c_p]
+        lib.orc_native_topology.restype = _c_i64
+        lib.orc_native_topology.argtypes = [_c_p, _c_i64, _c_i, _c_p, _c_p, _c_p, _c_p]
+        lib.orc_native_build.restype = _c_p
+        lib.orc_native_build.argtypes = [_c_p, _c_i64, _c_i]
+        lib.orc_native_free.argtypes = [_c_p]
+        lib.orc_native_num_nodes.restype = _c_i64
+        lib.orc_native_num_nodes.argtypes = [_c_p]
+        lib.orc_native_get.argtypes = [_c_p] + [_c_p] * 9
+        lib.orc_native_plan.restype = _c_i64
+        lib.orc_native_plan.argtypes = [_c_p, _c_p, _c_p, _c_d, _c_i]
+        lib.orc_native_eval.argtypes = [_c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p, _c_p]
+        lib.orc_native_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p]
+        lib.orc_native_plan_stats.argtypes = [_c_p, _c_p, _c_p, _c_p]
+        lib._typed = True
+    return lib
+
+
+def octree8_total_nodes(max_depth: int) -> int:
+    return int(_orc().orc_octree8_total_nodes(int(max_depth)))
+
+
+def direct_force_soft(points, masses, queries, eps, cutoff=0.0, periodic=False, box=1.0):
+    """Softened direct force in double (src/sbh_ffi.cu:431-522); cutoff <= 0 is off."""
+    p, m, q = _f32(points), _f32(masses), _f32(queries)
+    out = np.zeros((q.shape[0], 3), np.float64)
+    _orc().orc_direct_force_soft(_ptr(p), _ptr(m), p.shape[0], _ptr(q), q.shape[0], eps, cutoff,
+                                 int(periodic), box, _ptr(out))
+    return out
+
+
+def direct_force_soft_vjp(points, masses, queries, cot, eps, cutoff=0.0, periodic=False, box=1.0):
+    p, m, q, g = _f32(points), _f32(masses), _f32(queries), _f32(cot)
+    out = np.zeros((q.shape[0], 3), np.float64)
+    _orc().orc_direct_force_soft_vjp(_ptr(p), _ptr(m), p.shape[0], _ptr(q), q.shape[0], _ptr(g), eps,
+                                     cutoff, int(periodic), box, _ptr(out))
+    return out
+
+
+def direct_full_adjoint(points, masses, w, eps, cutoff=0.0, idx=None):
+    """Exact d/d(x, m) of sum_i w_i . a_i for self-gravity (double)."""
+    p, m, ww = _f32(points), _f32(masses), _f32(w)
+    if idx is None:
+        nk = p.shape[0]
+        ip = None
+    else:
+        ip = np.ascontiguousarray(np.asarray(idx, np.int64))
+        nk = ip.shape[0]
+    dx = np.zeros((nk, 3), np.float64)
+    dm = np.zeros(nk, np.float64)
+    _orc().orc_direct_full_adjoint(_ptr(p), _ptr(m), p.shape[0], _ptr(ww), eps, cutoff, _ptr(ip), nk,
+                                   _ptr(dx), _ptr(dm))
+    return dx, dm
+
+
+def bruteforce_gravity(points, masses, queries, periodic=False, box=1.0):
+    p, m, q = _f32(points), _f32(masses), _f32(queries)
+    out = np.zeros(q.shape[0], np.float64)
+    _orc().orc_bruteforce_gravity(_ptr(p), _ptr(m), p.shape[0], p.shape[1], _ptr(q), q.shape[0],
+                                  int(periodic), box, _ptr(out))
+    return out
+
+
+def direct_winding_number(points, normals, masses, queries):
+    p, nr, m, q = _f32(points), _f32(normals), _f32(masses), _f32(queries)
+    out = np.zeros(q.shape[0], np.float64)
+    _orc().orc_direct_winding_number(_ptr(p), _ptr(nr), _ptr(m), p.shape[0], _ptr(q), q.shape[0], _ptr(out))
+    return out
+
+
+def build_octree8(points, normals, masses, min_corner, max_corner, max_depth):
+    """Reference-layout octree8 buffers (leaf, node, contrib bytes) + codes + perm."""
+    p, nr, m = _f32(points), _f32(normals), _f32(masses)
+    mn, mx = _f32(min_corner), _f32(max_corner)
+    n = p.shape[0]
+    total = octree8_total_nodes(max_depth)
+    leaf = np.zeros(n * 32, np.uint8)
+    node = np.zeros(total * 104, np.uint8)
+    contrib = np.zeros(total * 32, np.uint8)
+    codes = np.zeros(n, np.uint32)
+    perm = np.zeros(n, np.int64)
+    rc = _orc().orc_build_octree8(_ptr(p), _ptr(nr), _ptr(m), n, _ptr(mn), _ptr(mx), int(max_depth),
+                                  _ptr(leaf), _ptr(node), _ptr(contrib), _ptr(codes), _ptr(perm))
+    if rc != 0:
+        raise ValueError("oracle octree8 build rejected its arguments")
+    return leaf, node, contrib, codes, perm
+
+
+KERNEL_GRAV_GRAD = 0
+KERNEL_SOFT = 1
+KERNEL_SOFT_VJP = 2
+
+
+def bh_octree8(leaf, node, queries, beta, kernel, eps=0.0, cutoff=0.0, prune_enabled=False,
+               prune_r_cut_mult=4.0, periodic=False, box=1.0, cot=None):
+    """Classic BH on octree8 bytes (src/sbh_ffi.cu:1950-2144), double sums."""
+    q = _f32(queries)
+    leaf = np.ascontiguousarray(np.asarray(leaf, np.uint8))
+    node = np.ascontiguousarray(np.asarray(node, np.uint8))
+    g = _f32(cot) if cot is not None else None
+    prune_on = 1 if (prune_enabled and cutoff > 0.0) else 0
+    r_cut = np.float32(prune_r_cut_mult) * np.float32(cutoff) if prune_on else np.float32(0.0)
+    r_cut_sq = float(np.float32(r_cut) * np.float32(r_cut))
+    out = np.zeros((q.shape[0], 3), np.float64)
+    counts = np.zeros(q.shape[0], np.int32)
+    rc = _orc().orc_bh_octree8(_ptr(leaf), _ptr(node), _ptr(q), q.shape[0], _ptr(g), float(beta), int(kernel),
+                               float(eps), float(cutoff), prune_on, r_cut_sq, int(periodic), float(box),
+                               _ptr(out), _ptr(counts))
+    if rc != 0:
+        raise RuntimeError("oracle octree8 traversal overflowed its 128-entry stack")
+    return out, counts
+
+
+# ----------------------------- native tree -----------------------------------
+def native_sort(points):
+    p = _f32(points)
+    n = p.shape[0]
+    keys = np.zeros(n, np.uint64)
+    perm = np.zeros(n, np.int64)
+    box = np.zeros(4, np.float32)
+    _orc().orc_native_sort(_ptr(p), n, _ptr(keys), _ptr(perm), _ptr(box))
+    return keys, perm, box
+
+
+class NativeTree:
+    """The project's adaptive Morton octree, restated on the CPU."""
+
+    def __init__(self, points, masses, leaf_size=16):
+        self.points = _f32(points)
+        self.masses = _f32(masses)
+        self.leaf_size = int(leaf_size)
+        self._lib = _orc()
+        self._h = self._lib.orc_native_build(_ptr(self.points), self.points.shape[0], self.leaf_size)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.orc_native_free(self._h)
+            self._h = None
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self._lib.orc_native_num_nodes(self._h))
+
+    def arrays(self) -> dict:
+        n, nn = self.points.shape[0], self.num_nodes
+        a = dict(keys=np.zeros(n, np.uint64), perm=np.zeros(n, np.int64), start=np.zeros(nn, np.int32),
+                 end=np.zeros(nn, np.int32), skip=np.zeros(nn, np.int32), level=np.zeros(nn, np.int8),
+                 center=np.zeros((nn, 3), np.float32), side=np.zeros(nn, np.float32),
+                 box=np.zeros(4, np.float32))
+        self._lib.orc_native_get(self._h, *[_ptr(a[k]) for k in
+                                            ("keys", "perm", "start", "end", "skip", "level", "center", "side", "box")])
+        return a
+
+    def plan(self, beta, group_size=32) -> int:
+        """Record the traversal plan (beta = 1/theta); returns the interaction count."""
+        return int(self._lib.orc_native_plan(self._h, _ptr(self.points), _ptr(self.masses), float(beta),
+                                             int(group_size)))
+
+    def plan_stats(self):
+        a, b, c = _c_i64(), _c_i64(), _c_i64()
+        self._lib.orc_native_plan_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return a.value, b.value, c.value
+
+    def force(self, eps, cutoff=0.0, points=None, masses=None, w=None, quad=False):
+        p = self.points if points is None else _f32(points)
+        m = self.masses if masses is None else _f32(masses)
+        out = np.zeros((p.shape[0], 3), np.float64)
+        loss = ctypes.c_double(0.0)
+        ww = _f32(w) if w is not None else None
+        self._lib.orc_native_eval(self._h, _ptr(p), _ptr(m), float(eps), float(cutoff), int(quad), _ptr(out), _ptr(ww),
+                                  ctypes.byref(loss))
+        return out, loss.value
+
+    def adjoint(self, w, eps, cutoff=0.0, points=None, masses=None, quad=False):
+        p = self.points if points is None else _f32(points)
+        m = self.masses if masses is None else _f32(masses)
+        dx = np.zeros((p.shape[0], 3), np.float64)
+        dm = np.zeros(p.shape[0], np.float64)
+        self._lib.orc_native_adjoint(self._h, _ptr(p), _ptr(m), _ptr(_f32(w)), float(eps), float(cutoff), int(quad),
+                                     _ptr(dx), _ptr(dm))
+        return dx, dm
+
+
+# ---------------------------------------------------------------------------
+# reference CPU code (libsbh_ref_cpu.so / libsbh_ref_cpu64.so)
+# ---------------------------------------------------------------------------
+REF_K_POTENTIAL, REF_K_WINDING, REF_K_SMOOTHDIST, REF_K_SOFT_FORCE, REF_K_SOFT_FORCE_VJP, REF_K_GRAVITY_GRAD = range(6)
+
+
+def _refcpu(double: bool = False) -> ctypes.CDLL:
+    lib = _load("libsbh_ref_cpu64.so" if double else "libsbh_ref_cpu.so")
+    if not getattr(lib, "_typed", False):
+        lib.ref_set_softening.argtypes = [_c_d, _c_d]
+        lib.ref_tree3d_build.restype = _c_p
+        lib.ref_tree3d_build.argtypes = [_c_i, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_i]
+        lib.ref_tree3d_free.argtypes = [_c_p]
+        lib.ref_tree3d_num_nodes.restype = _c_i64
+        lib.ref_tree3d_num_nodes.argtypes = [_c_p]
+        lib.ref_tree3d_max_depth.restype = _c_i
+        lib.ref_tree3d_max_depth.argtypes = [_c_p]
+        lib.ref_tree3d_node_size.restype = _c_sz
+        lib.ref_tree3d_node_size.argtypes = [_c_i]
+        lib.ref_leaf3_size.restype = _c_sz
+        lib.ref_leaf2_size.restype = _c_sz
+        lib.ref_tree3d_copy_leaf.argtypes = [_c_p, _c_p]
+        lib.ref_tree3d_copy_nodes.argtypes = [_c_p, _c_p]
+        lib.ref_tree3d_copy_contrib.argtypes = [_c_p, _c_p]
+        lib.ref_tree3d_eval.restype = _c_i
+        lib.ref_tree3d_eval.argtypes = [_c_p, _c_p, _c_i64, _c_f, _c_i, _c_p, _c_p, _c_p, _c_i]
+        lib.ref_tree3d_mlpcv.restype = _c_i
+        lib.ref_tree3d_mlpcv.argtypes = [_c_p, _c_p, _c_i64, _c_i, _c_i, _c_u32, _c_p, _c_p, _c_i]
+        lib.ref_tree2d_build.restype = _c_p
+        lib.ref_tree2d_build.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_f]
+        lib.ref_tree2d_free.argtypes = [_c_p]
+        lib.ref_tree2d_num_nodes.restype = _c_i64
+        lib.ref_tree2d_num_nodes.argtypes = [_c_p]
+        lib.ref_tree2d_node_size.restype = _c_sz
+        lib.ref_tree2d_copy_leaf.argtypes = [_c_p, _c_p]
+        lib.ref_tree2d_copy_nodes.argtypes = [_c_p, _c_p]
+        lib.ref_tree2d_copy_contrib.argtypes = [_c_p, _c_p]
+        lib.ref_tree2d_eval.restype = _c_i
+        lib.ref_tree2d_eval.argtypes = [_c_p, _c_p, _c_i64, _c_f, _c_i, _c_p, _c_p, _c_i]
+        lib._typed = True
+    return lib
+
+
+class RefTree3D:
+    """The reference's CPU Tree3D (variant 0: <8,1>, 1: <1,1> = Octree1, 2: <1,3> = Octree3)."""
+
+    def __init__(self, points, masses, normals=None, min_corner=None, max_corner=None, variant=0,
+                 alpha=1.0, double=False, max_depth=100):
+        self.points = _f32(points)
+        self.masses = _f32(masses)
+        self.normals = _f32(normals) if normals is not None else np.zeros_like(self.points)
+        if min_corner is None:
+            min_corner = self.points.min(axis=0) - np.float32(1e-3)
+        if max_corner is None:
+            max_corner = self.points.max(axis=0) + np.float32(1e-3)
+        self.min_corner, self.max_corner = _f32(min_corner), _f32(max_corner)
+        self.variant = variant
+        self._lib = _refcpu(double)
+        self._h = self._lib.ref_tree3d_build(variant, _ptr(self.points), _ptr(self.normals), _ptr(self.masses),
+                                             self.points.shape[0], _ptr(self.min_corner), _ptr(self.max_corner),
+                                             float(alpha), int(max_depth))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ref_tree3d_free(self._h)
+            self._h = None
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self._lib.ref_tree3d_num_nodes(self._h))
+
+    def leaf_bytes(self) -> np.ndarray:
+        out = np.zeros(self.points.shape[0] * int(self._lib.ref_leaf3_size()), np.uint8)
+        self._lib.ref_tree3d_copy_leaf(self._h, _ptr(out))
+        return out
+
+    def node_bytes(self) -> np.ndarray:
+        out = np.zeros(self.num_nodes * int(self._lib.ref_tree3d_node_size(self.variant)), np.uint8)
+        self._lib.ref_tree3d_copy_nodes(self._h, _ptr(out))
+        return out
+
+    def contrib_bytes(self) -> np.ndarray:
+        out = np.zeros(self.num_nodes * int(self._lib.ref_leaf3_size()), np.uint8)
+        self._lib.ref_tree3d_copy_contrib(self._h, _ptr(out))
+        return out
+
+    def eval(self, queries, beta, kernel, eps=1e-3, cutoff=0.0, cot=None, threads=0):
+        q = _f32(queries)
+        vec = kernel in (REF_K_SOFT_FORCE, REF_K_SOFT_FORCE_VJP, REF_K_GRAVITY_GRAD)
+        out = np.zeros((q.shape[0], 3) if vec else q.shape[0], np.float64)
+        counts = np.zeros(q.shape[0], np.int32)
+        self._lib.ref_set_softening(float(eps), float(cutoff))
+        g = _f32(cot) if cot is not None else None
+        self._lib.ref_tree3d_eval(self._h, _ptr(q), q.shape[0], float(beta), int(kernel), _ptr(g), _ptr(out),
+                                  _ptr(counts), int(threads))
+        return out, counts
+
+    def mlpcv(self, queries, kernel, samples, seed, eps=1e-3, cutoff=0.0, threads=0):
+        q = _f32(queries)
+        vec = kernel in (REF_K_SOFT_FORCE, REF_K_GRAVITY_GRAD)
+        out = np.zeros((q.shape[0], 3) if vec else q.shape[0], np.float64)
+        counts = np.zeros(q.shape[0], np.int32)
+        self._lib.ref_set_softening(float(eps), float(cutoff))
+        self._lib.ref_tree3d_mlpcv(self._h, _ptr(q), q.shape[0], int(kernel), int(samples), int(seed) & 0xFFFFFFFF,
+                                   _ptr(out), _ptr(counts), int(threads))
+        return out, counts
+
+
+class RefTree2D:
+    """The reference's CPU Tree2D<1,3> (sbh.Quadtree3): the Node2 layout builder."""
+
+    def __init__(self, points, masses, normals=None, min_corner=None, max_corner=None, alpha=1.0):
+        self.points = _f32(points)
+        self.masses = _f32(masses)
+        self.normals = _f32(normals) if normals is not None else np.zeros_like(self.points)
+        if min_corner is None:
+            min_corner = self.points.min(axis=0) - np.float32(1e-3)
+        if max_corner is None:
+            max_corner = self.points.max(axis=0) + np.float32(1e-3)
+        self._lib = _refcpu(False)
+        self._h = self._lib.ref_tree2d_build(_ptr(self.points), _ptr(self.normals), _ptr(self.masses),
+                                             self.points.shape[0], _ptr(_f32(min_corner)), _ptr(_f32(max_corner)),
+                                             float(alpha))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.ref_tree2d_free(self._h)
+            self._h = None
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self._lib.ref_tree2d_num_nodes(self._h))
+
+    def leaf_bytes(self):
+        out = np.zeros(self.points.shape[0] * int(self._lib.ref_leaf2_size()), np.uint8)
+        self._lib.ref_tree2d_copy_leaf(self._h, _ptr(out))
+        return out
+
+    def node_bytes(self):
+        out = np.zeros(self.num_nodes * int(self._lib.ref_tree2d_node_size()), np.uint8)
+        self._lib.ref_tree2d_copy_nodes(self._h, _ptr(out))
+        return out
+
+    def contrib_bytes(self):
+        out = np.zeros(self.num_nodes * int(self._lib.ref_leaf2_size()), np.uint8)
+        self._lib.ref_tree2d_copy_contrib(self._h, _ptr(out))
+        return out
+
+    def eval(self, queries, beta, kernel, threads=0):
+        q = _f32(queries)
+        vec = kernel == REF_K_GRAVITY_GRAD
+        out = np.zeros((q.shape[0], 2) if vec else q.shape[0], np.float64)
+        counts = np.zeros(q.shape[0], np.int32)
+        self._lib.ref_tree2d_eval(self._h, _ptr(q), q.shape[0], float(beta), int(kernel), _ptr(out), _ptr(counts),
+                                  int(threads))
+        return out, counts
+
+
+# ---------------------------------------------------------------------------
+# reference GPU plugin (libsbh_ref_gpu.so); pointers are device addresses
+# ---------------------------------------------------------------------------
+def refgpu() -> ctypes.CDLL:
+    """The reference's src/sbh_ffi.cu handlers behind extern "C" wrappers."""
+    lib = _load("libsbh_ref_gpu.so")
+    if not getattr(lib, "_typed", False):
+        lib.ref_gpu_last_error.restype = ctypes.c_char_p
+        for nm in ("ref_gpu_leaf3_size", "ref_gpu_node3_size", "ref_gpu_octree8_node_size", "ref_gpu_level3_max_nodes"):
+            getattr(lib, nm).restype = _c_sz
+        lib.ref_bruteforce_gravity.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_i64, _c_p, _c_i, _c_f, _c_i]
+        lib.ref_direct_force_soft.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_i, _c_f, _c_i]
+        lib.ref_direct_force_soft_vjp.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f, _c_i,
+                                                  _c_f, _c_i]
+        lib.ref_build_octree_level3.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64,
+                                                _c_p, _c_i64]
+        lib.ref_build_octree8.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p,
+                                          _c_i64, _c_i]
+        lib.ref_barnes_hut_gravity.argtypes = [_c_p, _c_i, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f, _c_i,
+                                               _c_f, _c_i]
+        lib.ref_barnes_hut_force.argtypes = lib.ref_barnes_hut_gravity.argtypes
+        lib.ref_barnes_hut_force_soft.argtypes = [_c_p, _c_i, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f,
+                                                  _c_f, _c_f, _c_i, _c_f, _c_i]
+        lib.ref_stochastic_bh_gravity.argtypes = [_c_p, _c_i, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64,
+                                                  _c_p, _c_i, _c_i, _c_i, _c_f, _c_i]
+        lib.ref_stochastic_bh_force.argtypes = lib.ref_stochastic_bh_gravity.argtypes
+        lib.ref_stochastic_bh_force_soft.argtypes = [_c_p, _c_i, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p,
+                                                     _c_i64, _c_p, _c_i, _c_i, _c_f, _c_f, _c_i, _c_f, _c_i]
+        lib.ref_bh_force_octree8.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f, _c_i, _c_f, _c_i]
+        lib.ref_bh_force_octree8_soft.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f, _c_f,
+                                                  _c_f, _c_i, _c_f, _c_i, _c_f, _c_i]
+        lib.ref_bh_force_octree8_soft_vjp.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p, _c_f,
+                                                      _c_f, _c_f, _c_i, _c_f, _c_i, _c_f, _c_i]
+        lib.ref_stochastic_bh_force_octree8.argtypes = [_c_p, _c_i, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p,
+                                                        _c_i, _c_i, _c_f, _c_f, _c_f, _c_i, _c_f, _c_i, _c_f, _c_i]
+        lib.ref_stochastic_bh_force_octree8_vjp.argtypes = [_c_p, _c_i, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_i64, _c_p,
+                                                            _c_p, _c_i, _c_i, _c_f, _c_f, _c_f, _c_i, _c_f, _c_i, _c_f,
+                                                            _c_i]
+        for nm in ("ref_bruteforce_gravity", "ref_direct_force_soft", "ref_direct_force_soft_vjp",
+                   "ref_build_octree_level3", "ref_build_octree8", "ref_barnes_hut_gravity", "ref_barnes_hut_force",
+                   "ref_barnes_hut_force_soft", "ref_stochastic_bh_gravity", "ref_stochastic_bh_force",
+                   "ref_stochastic_bh_force_soft", "ref_bh_force_octree8", "ref_bh_force_octree8_soft",
+                   "ref_bh_force_octree8_soft_vjp", "ref_stochastic_bh_force_octree8",
+                   "ref_stochastic_bh_force_octree8_vjp"):
+            getattr(lib, nm).restype = _c_i
+        lib._typed = True
+    return lib
+
+
+def refgpu_check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError("reference handler failed: " + refgpu().ref_gpu_last_error().decode())
