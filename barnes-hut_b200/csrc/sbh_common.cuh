@@ -218,8 +218,8 @@ __device__ __forceinline__ void grav_grad_vjp_accum(float rx, float ry, float rz
   az += -mass * (id3 * gz - k * rz);
 }
 
-// Two-sum compensated accumulation of a partial into (s, c).
-__device__ __forceinline__ void two_sum_add(float& s, float& c, float v) {
+// Kahan-compensated accumulation of a partial sum v into (s, c).
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
   float y = v - c;
   float t = s + y;
   c = (t - s) - y;

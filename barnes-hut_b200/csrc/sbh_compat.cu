@@ -33,13 +33,6 @@
 
 namespace sbh {
 
-__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
-  float y = v - c;
-  float t = s + y;
-  c = (t - s) - y;
-  s = t;
-}
-
 // ---------------------------------------------------------------------------
 // Direct sums (src/sbh_ffi.cu:399-546), shared-memory tiled, one query per
 // thread, Kahan-compensated across tiles.

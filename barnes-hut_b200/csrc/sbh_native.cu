@@ -1,0 +1,1521 @@
+// Native adaptive Morton octree ("ntree"): build, group traversal for the
+// softened force with monopole + quadrupole far field, the full adjoint
+// (w.r.t. positions and masses), the winding number, and the batched forest
+// (many independent systems in one build and one launch).
+//
+// Tree definition (the CPU oracle restates it; integer fields are pinned
+// bit-exactly):
+//  1. per system: lo = per-axis min, span = max axis extent (1 if 0);
+//     q_a = floor((x_a - lo_a) * (2^21 / span)) in double, clamped to [0, 2^21);
+//  2. key = 63-bit Morton code (x in bit 3i, y in 3i+1, z in 3i+2); the sort
+//     is stable by (system, key, input index);
+//  3. the level-l cell of a key is its top 3l bits; a cell is a node when
+//     l == 0 or its parent cell holds more than leaf_size particles; a node
+//     is a leaf when it holds at most leaf_size particles or l == 21;
+//  4. nodes are numbered in DFS pre-order; skip[k] is the index after k's
+//     subtree, so a traversal is "k = accept ? skip[k] : k + 1".
+// Node numbering needs only per-position quantities and one scan: with
+// d(i) = common levels of key[i-1], key[i] and L(i) = the leaf level of
+// position i (1 + the largest common level of key[a], key[a+S] over the
+// windows a in [i-S, i]), position i starts internal nodes at levels
+// [d(i)+1, L(i)-1] and a leaf at L(i) when d(i) < L(i).
+//
+// No fast-math in this translation unit: quantisation and the acceptance
+// test use IEEE operations (explicit _rn intrinsics, no contraction) so the
+// oracle reproduces them bit for bit; the pair kernels use rsqrtf.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+
+#include "sbh_common.cuh"
+#include "sbh_native.cuh"
+#include "sbh_primitives.cuh"
+
+namespace sbh {
+namespace nt {
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t float_to_ordered(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ordered_to_float(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+// Segment (system) of element i given seg_off[0..nseg] (nseg >= 1).
+__device__ __forceinline__ int seg_of(const int64_t* seg_off, int nseg, int64_t i) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (seg_off[mid] <= i)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint64_t spread21(uint64_t v) {
+  v &= 0x1FFFFFull;
+  v = (v | (v << 32)) & 0x1F00000000FFFFull;
+  v = (v | (v << 16)) & 0x1F0000FF0000FFull;
+  v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+  v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t compact21(uint64_t v) {
+  v &= 0x1249249249249249ull;
+  v = (v ^ (v >> 2)) & 0x10C30C30C30C30C3ull;
+  v = (v ^ (v >> 4)) & 0x100F00F00F00F00Full;
+  v = (v ^ (v >> 8)) & 0x1F0000FF0000FFull;
+  v = (v ^ (v >> 16)) & 0x1F00000000FFFFull;
+  v = (v ^ (v >> 32)) & 0x1FFFFFull;
+  return static_cast<uint32_t>(v);
+}
+
+// Common tree levels (0..21) of two 63-bit keys.
+__device__ __forceinline__ int common_levels(uint64_t a, uint64_t b) {
+  uint64_t x = a ^ b;
+  if (x == 0) return 21;
+  return (__clzll(x) - 1) / 3;
+}
+
+// ---------------------------------------------------------------------------
+// 1. bounding boxes (per system)
+// ---------------------------------------------------------------------------
+__global__ void bbox_init_kernel(uint32_t* bb, int nseg) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  for (int d = 0; d < 3; d++) {
+    bb[6 * s + d] = 0xFFFFFFFFu;  // min (ordered)
+    bb[6 * s + 3 + d] = 0u;       // max (ordered)
+  }
+}
+
+__global__ void bbox_kernel(const float* __restrict__ pts, int64_t n, const int64_t* __restrict__ seg_off, int nseg,
+                            uint32_t* bb) {
+  int lane = threadIdx.x & 31;
+  int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < n; base += stride) {
+    int64_t i = base + threadIdx.x;
+    bool ok = i < n;
+    uint32_t mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0u, 0u, 0u};
+    int s = 0;
+    if (ok) {
+      s = nseg > 1 ? seg_of(seg_off, nseg, i) : 0;
+      for (int d = 0; d < 3; d++) {
+        uint32_t o = float_to_ordered(pts[3 * i + d]);
+        mn[d] = o;
+        mx[d] = o;
+      }
+    }
+    int s0 = __shfl_sync(0xffffffffu, s, 0);
+    bool uniform = __all_sync(0xffffffffu, !ok || s == s0);
+    if (uniform) {
+      for (int d = 0; d < 3; d++) {
+        for (int o = 16; o > 0; o >>= 1) {
+          mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+          mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+      }
+      bool any = __any_sync(0xffffffffu, ok);
+      if (lane == 0 && any) {
+        for (int d = 0; d < 3; d++) {
+          atomicMin(&bb[6 * s0 + d], mn[d]);
+          atomicMax(&bb[6 * s0 + 3 + d], mx[d]);
+        }
+      }
+    } else if (ok) {
+      for (int d = 0; d < 3; d++) {
+        atomicMin(&bb[6 * s + d], mn[d]);
+        atomicMax(&bb[6 * s + 3 + d], mx[d]);
+      }
+    }
+  }
+}
+
+// SegBox: lo (float3), span (float), scale (double) per system.
+__global__ void bbox_finalize_kernel(const uint32_t* bb, int nseg, const int64_t* seg_off, SegBox* boxes) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  SegBox b;
+  bool empty = seg_off[s + 1] <= seg_off[s];
+  float lo[3], hi[3];
+  for (int d = 0; d < 3; d++) {
+    lo[d] = empty ? 0.0f : ordered_to_float(bb[6 * s + d]);
+    hi[d] = empty ? 0.0f : ordered_to_float(bb[6 * s + 3 + d]);
+  }
+  float span = 0.0f;
+  for (int d = 0; d < 3; d++) span = fmaxf(span, __fsub_rn(hi[d], lo[d]));
+  if (!(span > 0.0f)) span = 1.0f;
+  for (int d = 0; d < 3; d++) b.lo[d] = lo[d];
+  b.span = span;
+  b.scale = __ddiv_rn(2097152.0, static_cast<double>(span));
+  boxes[s] = b;
+}
+
+// ---------------------------------------------------------------------------
+// 2. keys
+// ---------------------------------------------------------------------------
+__global__ void keys_kernel(const float* __restrict__ pts, int64_t n, const int64_t* __restrict__ seg_off, int nseg,
+                            const SegBox* __restrict__ boxes, uint64_t* __restrict__ keys,
+                            uint32_t* __restrict__ segkey) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int s = nseg > 1 ? seg_of(seg_off, nseg, i) : 0;
+    SegBox b = boxes[s];
+    uint64_t key = 0;
+    for (int d = 0; d < 3; d++) {
+      double t = __dmul_rn(__dsub_rn(static_cast<double>(pts[3 * i + d]), static_cast<double>(b.lo[d])), b.scale);
+      double f = floor(t);
+      uint64_t q = f < 0.0 ? 0ull : (f > 2097151.0 ? 2097151ull : static_cast<uint64_t>(f));
+      key |= spread21(q) << d;
+    }
+    keys[i] = key;
+    if (segkey) segkey[i] = static_cast<uint32_t>(s);
+  }
+}
+
+// gather sorted (segment id, key) order of the segment pass
+__global__ void gather_keys_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ perm, int64_t n,
+                                   uint64_t* __restrict__ out) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = keys[perm[i]];
+}
+
+// ---------------------------------------------------------------------------
+// 3. topology
+// ---------------------------------------------------------------------------
+// cl[a] = common levels of key[a], key[a+S] (same system), else -1
+// dd[i] = common levels of key[i-1], key[i] (same system), else -1
+__global__ void levels_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ sseg, int64_t n, int S,
+                              int8_t* __restrict__ cl, int8_t* __restrict__ dd) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint64_t k = keys[i];
+    uint32_t s = sseg ? sseg[i] : 0u;
+    int c = -1;
+    if (i + S < n && (!sseg || sseg[i + S] == s)) c = common_levels(k, keys[i + S]);
+    cl[i] = static_cast<int8_t>(c);
+    int d = -1;
+    if (i > 0 && (!sseg || sseg[i - 1] == s)) d = common_levels(keys[i - 1], k);
+    dd[i] = static_cast<int8_t>(d);
+  }
+}
+
+// leaf level L(i) and node-slot count of position i
+__global__ void slots_kernel(const int8_t* __restrict__ cl, const int8_t* __restrict__ dd, int64_t n, int S,
+                             int8_t* __restrict__ lv, uint32_t* __restrict__ cnt) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int mx = -1;
+    int64_t a0 = i - S < 0 ? 0 : i - S;
+    for (int64_t a = a0; a <= i; a++) mx = max(mx, static_cast<int>(cl[a]));
+    int L = mx + 1;
+    if (L > 21) L = 21;
+    int d = dd[i];
+    int lo = d + 1;
+    int nint = L - lo;
+    if (nint < 0) nint = 0;
+    int nleaf = d < L ? 1 : 0;
+    lv[i] = static_cast<int8_t>(L);
+    cnt[i] = static_cast<uint32_t>(nint + nleaf);
+  }
+}
+
+// end of the level-l cell that starts at i: first j > i outside it
+__device__ __forceinline__ int64_t cell_end(const uint64_t* keys, const uint32_t* sseg, int64_t i, int l,
+                                            int64_t seg_end) {
+  uint64_t pref = l == 0 ? 0ull : keys[i] >> (63 - 3 * l);
+  int64_t lo = i + 1, hi = seg_end;
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    uint64_t pm = l == 0 ? 0ull : keys[mid] >> (63 - 3 * l);
+    if (pm == pref)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void emit_nodes_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ sseg,
+                                  const int64_t* __restrict__ sorted_seg_off, int64_t n, const int8_t* __restrict__ dd,
+                                  const int8_t* __restrict__ lv, const uint32_t* __restrict__ base,
+                                  NodeRec* __restrict__ nodes, int64_t cap, uint32_t* status) {
+  uint32_t total = base[n];
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int d = dd[i];
+    int L = lv[i];
+    int lo = d + 1;
+    int top = d < L ? L : L - 1;
+    uint32_t slot = base[i];
+    int64_t seg_end = sseg ? sorted_seg_off[sseg[i] + 1] : n;
+    for (int l = lo; l <= top; l++, slot++) {
+      if (slot >= cap) {
+        raise_status(status, SBH_DEV_ITER_LIMIT);
+        return;
+      }
+      int64_t e = cell_end(keys, sseg, i, l, seg_end);
+      uint32_t skip = e < n ? base[e] : total;
+      bool leaf = (l == L);
+      nodes[slot].topo = make_int4(static_cast<int>(i), static_cast<int>(e), static_cast<int>(skip),
+                                   l | (leaf ? kLeafFlag : 0));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 4. sorted particles and FP64 moments
+// ---------------------------------------------------------------------------
+__global__ void gather_particles_kernel(const float* __restrict__ pts, const float* __restrict__ masses,
+                                        const float* __restrict__ nrm, const uint32_t* __restrict__ perm, int64_t n,
+                                        float4* __restrict__ sp, float4* __restrict__ sn) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t s = perm[i];
+    sp[i] = make_float4(pts[3 * s], pts[3 * s + 1], pts[3 * s + 2], masses[s]);
+    if (sn && nrm) sn[i] = make_float4(nrm[3 * s], nrm[3 * s + 1], nrm[3 * s + 2], 0.0f);
+  }
+}
+
+// moment vector of sorted particle i relative to its system's box centre
+struct MomentLoad {
+  const float4* sp;
+  const uint32_t* sseg;
+  const SegBox* boxes;
+  __device__ DVec<10> operator()(int64_t i) const {
+    float4 p = sp[i];
+    SegBox b = boxes[sseg ? sseg[i] : 0];
+    double half = 0.5 * static_cast<double>(b.span);
+    double y0 = static_cast<double>(p.x) - (static_cast<double>(b.lo[0]) + half);
+    double y1 = static_cast<double>(p.y) - (static_cast<double>(b.lo[1]) + half);
+    double y2 = static_cast<double>(p.z) - (static_cast<double>(b.lo[2]) + half);
+    double m = p.w;
+    DVec<10> r;
+    r.v[0] = m;
+    r.v[1] = m * y0;
+    r.v[2] = m * y1;
+    r.v[3] = m * y2;
+    r.v[4] = m * y0 * y0;
+    r.v[5] = m * y1 * y1;
+    r.v[6] = m * y2 * y2;
+    r.v[7] = m * y0 * y1;
+    r.v[8] = m * y0 * y2;
+    r.v[9] = m * y1 * y2;
+    return r;
+  }
+};
+
+struct NormalMomentLoad {
+  const float4* sp;
+  const float4* sn;
+  __device__ DVec<3> operator()(int64_t i) const {
+    float4 p = sp[i], q = sn[i];
+    double m = p.w;
+    DVec<3> r;
+    r.v[0] = m * q.x;
+    r.v[1] = m * q.y;
+    r.v[2] = m * q.z;
+    return r;
+  }
+};
+
+// Node records from topology + moments + cell geometry (NodeRec, 64 B).
+// The topology fields were written by emit_nodes_kernel into nodes[k].topo.
+__global__ void finalize_nodes_kernel(NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
+                                      const uint64_t* __restrict__ keys, const uint32_t* __restrict__ sseg,
+                                      const SegBox* __restrict__ boxes, const DVec<10>* __restrict__ P,
+                                      const DVec<3>* __restrict__ PN, float4* __restrict__ nnrm) {
+  uint32_t nn = *nn_ptr;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    int4 t = nodes[k].topo;
+    int level = t.w & 0xFF;
+    int64_t s0 = t.x, e0 = t.y;
+    SegBox b = boxes[sseg ? sseg[s0] : 0];
+    DVec<10> hi = P[e0], lo = P[s0];
+    double v[10];
+    for (int c = 0; c < 10; c++) v[c] = hi.v[c] - lo.v[c];
+    double M = v[0];
+    double half = 0.5 * static_cast<double>(b.span);
+    double c0[3] = {static_cast<double>(b.lo[0]) + half, static_cast<double>(b.lo[1]) + half,
+                    static_cast<double>(b.lo[2]) + half};
+    // cell geometry from the key prefix (exact in double, rounded once)
+    uint64_t pref = level == 0 ? 0ull : keys[s0] >> (63 - 3 * level);
+    float side = ldexpf(b.span, -level);
+    float ctr[3];
+    for (int d = 0; d < 3; d++) {
+      uint32_t cd = compact21(pref >> d);
+      ctr[d] = static_cast<float>(__dadd_rn(static_cast<double>(b.lo[d]),
+                                            __dmul_rn(static_cast<double>(cd) + 0.5, static_cast<double>(side))));
+    }
+    float X[3];
+    double S[6] = {0, 0, 0, 0, 0, 0};
+    if (M != 0.0) {
+      double Y[3] = {v[1] / M, v[2] / M, v[3] / M};
+      for (int d = 0; d < 3; d++) X[d] = static_cast<float>(Y[d] + c0[d]);
+      S[0] = v[4] - M * Y[0] * Y[0];
+      S[1] = v[5] - M * Y[1] * Y[1];
+      S[2] = v[6] - M * Y[2] * Y[2];
+      S[3] = v[7] - M * Y[0] * Y[1];
+      S[4] = v[8] - M * Y[0] * Y[2];
+      S[5] = v[9] - M * Y[1] * Y[2];
+    } else {
+      for (int d = 0; d < 3; d++) X[d] = ctr[d];
+    }
+    float dx = __fsub_rn(X[0], ctr[0]), dy = __fsub_rn(X[1], ctr[1]), dz = __fsub_rn(X[2], ctr[2]);
+    float delta = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+    float diag = __fmul_rn(side, 1.7320508f);
+    NodeRec r;
+    r.com = make_float4(X[0], X[1], X[2], static_cast<float>(M));
+    r.aux = make_float4(static_cast<float>(S[4]), static_cast<float>(S[5]), diag, delta);
+    r.quad = make_float4(static_cast<float>(S[0]), static_cast<float>(S[1]), static_cast<float>(S[2]),
+                         static_cast<float>(S[3]));
+    r.topo = t;
+    nodes[k] = r;
+    if (nnrm && PN) {
+      DVec<3> nh = PN[e0], nl = PN[s0];
+      nnrm[k] = M != 0.0 ? make_float4(static_cast<float>((nh.v[0] - nl.v[0]) / M),
+                                       static_cast<float>((nh.v[1] - nl.v[1]) / M),
+                                       static_cast<float>((nh.v[2] - nl.v[2]) / M), 1.0f)
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+}
+
+// Roots (first node of each system) and target groups (runs of <= 32 sorted
+// particles that never cross a system boundary).
+__global__ void roots_groups_kernel(const int64_t* __restrict__ sorted_seg_off, int nseg, const uint32_t* __restrict__ base,
+                                    const uint32_t* __restrict__ group_off, int2* __restrict__ roots,
+                                    int4* __restrict__ groups) {
+  int s = blockIdx.x;
+  if (s >= nseg) return;
+  int64_t a = sorted_seg_off[s], b = sorted_seg_off[s + 1];
+  uint32_t total = base[sorted_seg_off[nseg]];
+  uint32_t r0 = a < b ? base[a] : 0u;
+  uint32_t r1 = b < sorted_seg_off[nseg] ? base[b] : total;
+  if (threadIdx.x == 0) roots[s] = make_int2(static_cast<int>(r0), static_cast<int>(a < b ? r1 : r0));
+  uint32_t g0 = group_off[s];
+  int64_t ng = (b - a + 31) / 32;
+  for (int64_t g = threadIdx.x; g < ng; g += blockDim.x) {
+    int64_t st = a + 32 * g;
+    int64_t en = st + 32 < b ? st + 32 : b;
+    groups[g0 + g] = make_int4(static_cast<int>(st), static_cast<int>(en), s, 0);
+  }
+}
+
+__global__ void group_counts_kernel(const int64_t* __restrict__ sorted_seg_off, int nseg, uint32_t* __restrict__ gc) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  gc[s] = static_cast<uint32_t>((sorted_seg_off[s + 1] - sorted_seg_off[s] + 31) / 32);
+}
+
+__global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, int64_t n,
+                                  uint32_t* __restrict__ out) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = src[idx[i]];
+}
+
+__global__ void sseg_kernel(const int64_t* __restrict__ seg_off, int nseg, int64_t n, uint32_t* __restrict__ sseg) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    sseg[i] = static_cast<uint32_t>(seg_of(seg_off, nseg, i));
+}
+
+// meta[0] = number of nodes (base[n]); flags an overflow of the capacity.
+__global__ void node_count_kernel(const uint32_t* base, int64_t n, int64_t cap, uint32_t* meta) {
+  uint32_t total = base[n];
+  meta[0] = total <= cap ? total : static_cast<uint32_t>(cap);
+  meta[3] = total > cap ? 1u : 0u;
+}
+
+__global__ void group_total_kernel(const uint32_t* goff, int nseg, uint32_t* meta) { meta[1] = goff[nseg]; }
+
+__global__ void single_offsets_kernel(int64_t* seg_off, int64_t n) {
+  seg_off[0] = 0;
+  seg_off[1] = n;
+}
+
+// ---------------------------------------------------------------------------
+// 5. traversal
+// ---------------------------------------------------------------------------
+struct WalkTree {
+  const NodeRec* nodes;
+  const float4* sp;     // sorted sources (x, y, z, m)
+  const float4* sn;     // sorted source normals (winding number)
+  const float4* nnrm;   // node mean normals (winding number)
+  const int2* roots;    // per system: [root, end of the system's nodes)
+};
+
+struct WalkTargets {
+  const float4* tp;          // sorted target positions
+  const uint32_t* perm;      // sorted slot -> input index
+  const int4* groups;        // (start, end, system, 0), <= 32 targets each
+  const uint32_t* ngroups;   // device-side group count
+  int self;                  // targets are the sources (skip i == j pairs)
+};
+
+struct WalkParams {
+  float beta;
+  float eps2;    // softening^2 + 1e-12
+  float cutoff;  // <= 0: no attenuation
+};
+
+// Group bounding box: min/max over the active lanes (inactive lanes carry the
+// group's first target, which is inside the box).
+__device__ __forceinline__ void group_box(float4 q, float* gmin, float* gmax) {
+  float v[3] = {q.x, q.y, q.z};
+  for (int d = 0; d < 3; d++) {
+    float lo = v[d], hi = v[d];
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    gmin[d] = lo;
+    gmax[d] = hi;
+  }
+}
+
+// Acceptance test, IEEE operations in the oracle's order (no contraction).
+__device__ __forceinline__ bool accept_node(const float4& com, float diag, float delta, const float* gmin,
+                                            const float* gmax, float beta) {
+  float rc = __fadd_rn(__fmul_rn(diag, beta), delta);
+  float x[3] = {com.x, com.y, com.z};
+  float t[3];
+  for (int d = 0; d < 3; d++) {
+    float a = __fsub_rn(gmin[d], x[d]);
+    float b = __fsub_rn(x[d], gmax[d]);
+    float m = a > b ? a : b;
+    t[d] = m > 0.0f ? m : 0.0f;
+  }
+  float d2 = __fadd_rn(__fadd_rn(__fmul_rn(t[0], t[0]), __fmul_rn(t[1], t[1])), __fmul_rn(t[2], t[2]));
+  return d2 > __fmul_rn(rc, rc);
+}
+
+// erfc attenuation of the short-range force and its radial derivative term
+// (src/sbh_ffi.cu:142-160, 2062-2090); att = 1, cc = 0 without cutoff.
+__device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, float& att, float& cc) {
+  float dist = sqrtf(r2 + 1e-12f);
+  float u = dist / (2.0f * cutoff);
+  float e = expf(-(u * u));
+  att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+  cc = ir3 * dist * e / (2.0f * 1.772453850905516f * cutoff * cutoff * cutoff);
+}
+
+// Flop accounting used by the roofline (FP32 operations counted from the
+// formulas below, an FMA as 2): force walk near pair 20, far node 55
+// (monopole + quadrupole); adjoint walk (force + adjoint) near pair 55, far
+// node 200 including the 16-value warp reduction.
+
+template <bool QUAD, bool CUT>
+__global__ void __launch_bounds__(128)
+    force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
+                      unsigned long long* __restrict__ counters) {
+  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (gw >= static_cast<int>(*G.ngroups)) return;
+  int4 gr = G.groups[gw];
+  int i = gr.x + lane;
+  bool active = i < gr.y;
+  float4 q = G.tp[active ? i : gr.x];
+  float gmin[3], gmax[3];
+  group_box(q, gmin, gmax);
+  int2 rt = T.roots[gr.z];
+  float fx = 0.f, fy = 0.f, fz = 0.f;                        // far field
+  float nx = 0.f, ny = 0.f, nz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;  // near field, compensated
+  unsigned long long nfar = 0, nnear = 0;
+  int k = rt.x;
+  while (k < rt.y) {
+    const NodeRec* nd = T.nodes + k;
+    int4 tp = __ldg(&nd->topo);
+    float4 A = __ldg(&nd->com);
+    if (A.w == 0.0f) {
+      k = tp.z;
+      continue;
+    }
+    float4 X = __ldg(&nd->aux);
+    if (accept_node(A, X.z, X.w, gmin, gmax, P.beta)) {
+      float rx = q.x - A.x, ry = q.y - A.y, rz = q.z - A.z;
+      float r2 = rx * rx + ry * ry + rz * rz;
+      float ir = rsqrtf(r2 + P.eps2);
+      float ih = ir * ir;
+      float ir3 = ir * ih;
+      float c = -A.w * ir3;
+      if (CUT) {
+        float att, cc;
+        attenuation(r2, ir3, P.cutoff, att, cc);
+        c *= att;
+      }
+      if (QUAD) {
+        float4 Q = __ldg(&nd->quad);
+        // a_q = ir5 (3 S r + 1.5 tr(S) r) - 7.5 (r.S.r) ir7 r
+        float sx = Q.x * rx + Q.w * ry + X.x * rz;
+        float sy = Q.w * rx + Q.y * ry + X.y * rz;
+        float sz = X.x * rx + X.y * ry + Q.z * rz;
+        float rsr = rx * sx + ry * sy + rz * sz;
+        float ir5 = ir3 * ih;
+        float tr = Q.x + Q.y + Q.z;
+        float cr = c + ir5 * (1.5f * tr - 7.5f * rsr * ih);
+        float c3 = 3.0f * ir5;
+        fx += cr * rx + c3 * sx;
+        fy += cr * ry + c3 * sy;
+        fz += cr * rz + c3 * sz;
+      } else {
+        fx += c * rx;
+        fy += c * ry;
+        fz += c * rz;
+      }
+      nfar++;
+      k = tp.z;
+    } else if (tp.w & kLeafFlag) {
+      float ax = 0.f, ay = 0.f, az = 0.f;
+      for (int j = tp.x; j < tp.y; j++) {
+        float4 s = __ldg(&T.sp[j]);
+        float rx = q.x - s.x, ry = q.y - s.y, rz = q.z - s.z;
+        float r2 = rx * rx + ry * ry + rz * rz;
+        float ir = rsqrtf(r2 + P.eps2);
+        float ir3 = ir * ir * ir;
+        float c = -s.w * ir3;
+        if (CUT) {
+          float att, cc;
+          attenuation(r2, ir3, P.cutoff, att, cc);
+          c *= att;
+        }
+        ax += c * rx;
+        ay += c * ry;
+        az += c * rz;
+      }
+      kahan_add(nx, cx, ax);
+      kahan_add(ny, cy, ay);
+      kahan_add(nz, cz, az);
+      nnear += static_cast<unsigned long long>(tp.y - tp.x);
+      k = tp.z;
+    } else {
+      k++;
+    }
+  }
+  if (active) {
+    uint32_t o = G.perm[i];
+    out[3 * o] = fx + nx;
+    out[3 * o + 1] = fy + ny;
+    out[3 * o + 2] = fz + nz;
+  }
+  if (counters && lane == 0) {
+    unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
+    atomicAdd(&counters[0], nfar * na);
+    atomicAdd(&counters[1], nnear * na);
+  }
+}
+
+// Sum V = 4 values over the warp with 6 shuffles: afterwards lane 8*v holds
+// the warp total of value v (v = 0..3).
+__device__ __forceinline__ float reduce4(float v0, float v1, float v2, float v3) {
+  int lane = threadIdx.x & 31;
+  bool b4 = lane & 16;
+  float s0 = b4 ? v0 : v2, s1 = b4 ? v1 : v3;
+  float k0 = b4 ? v2 : v0, k1 = b4 ? v3 : v1;
+  k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+  k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+  bool b3 = lane & 8;
+  float s = b3 ? k0 : k1;
+  float v = b3 ? k1 : k0;
+  v += __shfl_xor_sync(0xffffffffu, s, 8);
+  v += __shfl_xor_sync(0xffffffffu, v, 4);
+  v += __shfl_xor_sync(0xffffffffu, v, 2);
+  v += __shfl_xor_sync(0xffffffffu, v, 1);
+  return v;  // lane with bits (b4, b3): value 2*b4 + b3
+}
+
+// Sum 16 values over the warp with 16 shuffles: afterwards lane 2*v holds
+// the total of value v (v = 0..15).
+__device__ __forceinline__ float reduce16(float* v) {
+  int lane = threadIdx.x & 31;
+  // step 16: keep 8
+  bool b = lane & 16;
+  float h[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    float send = b ? v[j] : v[8 + j];
+    float keep = b ? v[8 + j] : v[j];
+    h[j] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+  b = lane & 8;
+  float g[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    float send = b ? h[j] : h[4 + j];
+    float keep = b ? h[4 + j] : h[j];
+    g[j] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  b = lane & 4;
+  float f[2];
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    float send = b ? g[j] : g[2 + j];
+    float keep = b ? g[2 + j] : g[j];
+    f[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  b = lane & 2;
+  float send = b ? f[0] : f[1];
+  float e = (b ? f[1] : f[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
+  e += __shfl_xor_sync(0xffffffffu, e, 1);
+  return e;  // value index = 8*b4 + 4*b3 + 2*b2 + b1
+}
+
+__device__ __forceinline__ int reduce16_index(int lane) {
+  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+}
+
+__device__ __forceinline__ int reduce4_index(int lane) { return ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1); }
+
+// Fused force + adjoint walk. Per target lane: the query-side gradient
+// (written to gq in sorted order); per accepted node: A_X, A_M, G summed over
+// the warp and added to node_adj; per near source particle: (dx, dm) summed
+// over the warp and added to part_adj. Forces are written when out != null.
+template <bool QUAD, bool CUT>
+__global__ void __launch_bounds__(128)
+    adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
+                        float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
+                        float* __restrict__ part_adj, unsigned long long* __restrict__ counters) {
+  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (gw >= static_cast<int>(*G.ngroups)) return;
+  int4 gr = G.groups[gw];
+  int i = gr.x + lane;
+  bool active = i < gr.y;
+  float4 q = G.tp[active ? i : gr.x];
+  uint32_t o = active ? G.perm[i] : 0u;
+  float wx = active ? cot[3 * o] : 0.f, wy = active ? cot[3 * o + 1] : 0.f, wz = active ? cot[3 * o + 2] : 0.f;
+  float gmin[3], gmax[3];
+  group_box(q, gmin, gmax);
+  int2 rt = T.roots[gr.z];
+  float gx = 0.f, gy = 0.f, gz = 0.f;   // query-side gradient
+  float fx = 0.f, fy = 0.f, fz = 0.f;   // force
+  unsigned long long nfar = 0, nnear = 0;
+  int r4 = reduce4_index(lane), r16 = reduce16_index(lane);
+  int k = rt.x;
+  while (k < rt.y) {
+    const NodeRec* nd = T.nodes + k;
+    int4 tp = __ldg(&nd->topo);
+    float4 A = __ldg(&nd->com);
+    if (A.w == 0.0f) {
+      k = tp.z;
+      continue;
+    }
+    float4 X = __ldg(&nd->aux);
+    if (accept_node(A, X.z, X.w, gmin, gmax, P.beta)) {
+      float rx = q.x - A.x, ry = q.y - A.y, rz = q.z - A.z;
+      float r2 = rx * rx + ry * ry + rz * rz;
+      float ir = rsqrtf(r2 + P.eps2);
+      float ih = ir * ir;
+      float ir3 = ir * ih;
+      float ir5 = ir3 * ih;
+      float rw = rx * wx + ry * wy + rz * wz;
+      float att = 1.0f, cc = 0.0f;
+      if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
+      // per unit mass: phi = -att ir3 r ; J^T w = -att ir3 w + (3 att ir5 + cc) (r.w) r
+      float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
+      float jx = -lin * wx + rad * rx, jy = -lin * wy + rad * ry, jz = -lin * wz + rad * rz;
+      float v[16];
+      float M = A.w;
+      float qx_ = M * jx, qy_ = M * jy, qz_ = M * jz;
+      float am = -lin * rw;  // phi . w
+      if (out) {
+        float c = -M * lin;
+        fx += c * rx;
+        fy += c * ry;
+        fz += c * rz;
+      }
+#pragma unroll
+      for (int j = 0; j < 16; j++) v[j] = 0.f;
+      if (QUAD) {
+        float4 Q = __ldg(&nd->quad);
+        float Sxx = Q.x, Syy = Q.y, Szz = Q.z, Sxy = Q.w, Sxz = X.x, Syz = X.y;
+        float sx = Sxx * rx + Sxy * ry + Sxz * rz;
+        float sy = Sxy * rx + Syy * ry + Syz * rz;
+        float sz = Sxz * rx + Syz * ry + Szz * rz;
+        float swx = Sxx * wx + Sxy * wy + Sxz * wz;
+        float swy = Sxy * wx + Syy * wy + Syz * wz;
+        float swz = Sxz * wx + Syz * wy + Szz * wz;
+        float tr = Sxx + Syy + Szz;
+        float rsr = rx * sx + ry * sy + rz * sz;
+        float sxw = sx * wx + sy * wy + sz * wz;
+        float ir7 = ir5 * ih, ir9 = ir7 * ih;
+        // J_q^T w of the quadrupole term
+        float a1 = 5.0f * ir7 * rw;
+        float a2 = 7.5f * ir7 * rsr;
+        float a3 = 7.5f * (2.0f * ir7 * sxw - 7.0f * ir9 * rsr * rw);
+        float jqx = ir5 * (3.0f * swx + 1.5f * tr * wx) - a1 * (3.0f * sx + 1.5f * tr * rx) - a2 * wx - a3 * rx;
+        float jqy = ir5 * (3.0f * swy + 1.5f * tr * wy) - a1 * (3.0f * sy + 1.5f * tr * ry) - a2 * wy - a3 * ry;
+        float jqz = ir5 * (3.0f * swz + 1.5f * tr * wz) - a1 * (3.0f * sz + 1.5f * tr * rz) - a2 * wz - a3 * rz;
+        qx_ += jqx;
+        qy_ += jqy;
+        qz_ += jqz;
+        // G = sym d(w . a_q)/dS
+        float ga = 1.5f * ir5, gb = 1.5f * ir5 * rw, gc = 7.5f * ir7 * rw;
+        v[4] = 2.0f * ga * wx * rx + gb - gc * rx * rx;
+        v[5] = 2.0f * ga * wy * ry + gb - gc * ry * ry;
+        v[6] = 2.0f * ga * wz * rz + gb - gc * rz * rz;
+        v[7] = ga * (wx * ry + rx * wy) - gc * rx * ry;
+        v[8] = ga * (wx * rz + rx * wz) - gc * rx * rz;
+        v[9] = ga * (wy * rz + ry * wz) - gc * ry * rz;
+        if (out) {
+          float ir5b = ir5;
+          float cr = ir5b * (1.5f * tr - 7.5f * rsr * ih);
+          float c3 = 3.0f * ir5b;
+          fx += cr * rx + c3 * sx;
+          fy += cr * ry + c3 * sy;
+          fz += cr * rz + c3 * sz;
+        }
+      }
+      gx += qx_;
+      gy += qy_;
+      gz += qz_;
+      v[0] = -qx_;
+      v[1] = -qy_;
+      v[2] = -qz_;
+      v[3] = am;
+      if (!active) {
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = 0.f;
+      }
+      float tot = reduce16(v);
+      if ((lane & 1) == 0 && r16 < 10) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r16], tot);
+      nfar++;
+      k = tp.z;
+    } else if (tp.w & kLeafFlag) {
+      for (int j = tp.x; j < tp.y; j++) {
+        float4 s = __ldg(&T.sp[j]);
+        float rx = q.x - s.x, ry = q.y - s.y, rz = q.z - s.z;
+        float r2 = rx * rx + ry * ry + rz * rz;
+        float ir = rsqrtf(r2 + P.eps2);
+        float ih = ir * ir;
+        float ir3 = ir * ih;
+        float ir5 = ir3 * ih;
+        float rw = rx * wx + ry * wy + rz * wz;
+        float att = 1.0f, cc = 0.0f;
+        if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
+        float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
+        float jx = -lin * wx + rad * rx, jy = -lin * wy + rad * ry, jz = -lin * wz + rad * rz;
+        bool use = active && !(G.self && j == i);
+        float m = use ? s.w : 0.0f;
+        gx += m * jx;
+        gy += m * jy;
+        gz += m * jz;
+        if (out) {
+          float c = -m * lin;
+          fx += c * rx;
+          fy += c * ry;
+          fz += c * rz;
+        }
+        float am = use ? -lin * rw : 0.0f;
+        float tot = reduce4(-m * jx, -m * jy, -m * jz, am);
+        if ((lane & 7) == 0) atomicAdd(&part_adj[static_cast<int64_t>(j) * kPartAdj + r4], tot);
+      }
+      nnear += static_cast<unsigned long long>(tp.y - tp.x);
+      k = tp.z;
+    } else {
+      k++;
+    }
+  }
+  if (counters && lane == 0) {
+    unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
+    atomicAdd(&counters[0], nfar * na);
+    atomicAdd(&counters[1], nnear * na);
+  }
+  if (active) {
+    gq[3 * static_cast<int64_t>(i)] = gx;
+    gq[3 * static_cast<int64_t>(i) + 1] = gy;
+    gq[3 * static_cast<int64_t>(i) + 2] = gz;
+    if (out) {
+      out[3 * o] = fx;
+      out[3 * o + 1] = fy;
+      out[3 * o + 2] = fz;
+    }
+  }
+}
+
+// Node adjoints -> difference arrays over each node's particle range. Per
+// node (coordinates relative to the system's box centre c0, Xc = X - c0):
+//   V_X = A_X / M, V_Q = A_M - A_X . Xc / M, G, G Xc, Xc^T G Xc   (14 values)
+__global__ void node_push_kernel(const NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
+                                 const float* __restrict__ node_adj, const uint32_t* __restrict__ sseg,
+                                 const SegBox* __restrict__ boxes, DVec<14>* __restrict__ D) {
+  uint32_t nn = *nn_ptr;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const float* a = node_adj + static_cast<int64_t>(k) * kNodeAdj;
+    bool any = false;
+    for (int c = 0; c < 10; c++) any |= a[c] != 0.0f;
+    if (!any) continue;
+    NodeRec r = nodes[k];
+    double M = r.com.w;
+    if (M == 0.0) continue;
+    SegBox b = boxes[sseg ? sseg[r.topo.x] : 0];
+    double half = 0.5 * static_cast<double>(b.span);
+    double X[3] = {static_cast<double>(r.com.x) - (static_cast<double>(b.lo[0]) + half),
+                   static_cast<double>(r.com.y) - (static_cast<double>(b.lo[1]) + half),
+                   static_cast<double>(r.com.z) - (static_cast<double>(b.lo[2]) + half)};
+    double AX[3] = {a[0], a[1], a[2]};
+    double AM = a[3];
+    double G[6] = {a[4], a[5], a[6], a[7], a[8], a[9]};
+    double GX[3] = {G[0] * X[0] + G[3] * X[1] + G[4] * X[2], G[3] * X[0] + G[1] * X[1] + G[5] * X[2],
+                    G[4] * X[0] + G[5] * X[1] + G[2] * X[2]};
+    double val[14];
+    val[0] = AX[0] / M;
+    val[1] = AX[1] / M;
+    val[2] = AX[2] / M;
+    val[3] = AM - (AX[0] * X[0] + AX[1] * X[1] + AX[2] * X[2]) / M;
+    for (int c = 0; c < 6; c++) val[4 + c] = G[c];
+    for (int c = 0; c < 3; c++) val[10 + c] = GX[c];
+    val[13] = X[0] * GX[0] + X[1] * GX[1] + X[2] * GX[2];
+    for (int c = 0; c < 14; c++) {
+      atomicAdd(&D[r.topo.x].v[c], val[c]);
+      atomicAdd(&D[r.topo.y].v[c], -val[c]);
+    }
+  }
+}
+
+// Per sorted particle: query side + direct-source terms + node terms
+// (inclusive prefix of D = exclusive prefix at i + 1).
+__global__ void adjoint_combine_kernel(const float4* __restrict__ sp, const uint32_t* __restrict__ perm,
+                                       const uint32_t* __restrict__ sseg, const SegBox* __restrict__ boxes, int64_t n,
+                                       const float* __restrict__ gq, const float* __restrict__ part_adj,
+                                       const DVec<14>* __restrict__ C, float* __restrict__ dx,
+                                       float* __restrict__ dm) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    float4 p = sp[i];
+    SegBox b = boxes[sseg ? sseg[i] : 0];
+    double half = 0.5 * static_cast<double>(b.span);
+    double x[3] = {static_cast<double>(p.x) - (static_cast<double>(b.lo[0]) + half),
+                   static_cast<double>(p.y) - (static_cast<double>(b.lo[1]) + half),
+                   static_cast<double>(p.z) - (static_cast<double>(b.lo[2]) + half)};
+    const DVec<14>& c = C[i + 1];
+    const double* G = &c.v[4];
+    double Gx[3] = {G[0] * x[0] + G[3] * x[1] + G[4] * x[2], G[3] * x[0] + G[1] * x[1] + G[5] * x[2],
+                    G[4] * x[0] + G[5] * x[1] + G[2] * x[2]};
+    double m = p.w;
+    uint32_t o = perm[i];
+    for (int d = 0; d < 3; d++) {
+      double v = static_cast<double>(gq[3 * i + d]) + static_cast<double>(part_adj[kPartAdj * i + d]) +
+                 m * (c.v[d] + 2.0 * (Gx[d] - c.v[10 + d]));
+      dx[3 * o + d] = static_cast<float>(v);
+    }
+    double wq = c.v[3] + (c.v[0] * x[0] + c.v[1] * x[1] + c.v[2] * x[2]) +
+                (x[0] * Gx[0] + x[1] * Gx[1] + x[2] * Gx[2]) -
+                2.0 * (x[0] * c.v[10] + x[1] * c.v[11] + x[2] * c.v[12]) + c.v[13];
+    dm[o] = static_cast<float>(static_cast<double>(part_adj[kPartAdj * i + 3]) + wq);
+  }
+}
+
+// Winding number (include/kernel.h:73-80): w(q) = sum m n.(p - q) / (4 pi (|p-q|^3 + 1e-5));
+// far field: node mass and mass-weighted mean normal at the COM, as the
+// reference's trees aggregate them (include/tree3d.h:255-264, 310-327).
+__global__ void __launch_bounds__(128)
+    wn_walk_kernel(WalkTree T, WalkTargets G, float beta, float* __restrict__ out,
+                   unsigned long long* __restrict__ counters) {
+  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (gw >= static_cast<int>(*G.ngroups)) return;
+  int4 gr = G.groups[gw];
+  int i = gr.x + lane;
+  bool active = i < gr.y;
+  float4 q = G.tp[active ? i : gr.x];
+  float gmin[3], gmax[3];
+  group_box(q, gmin, gmax);
+  int2 rt = T.roots[gr.z];
+  const float k4pi = 0.07957747154594767f;  // 1 / (4 pi)
+  float far = 0.f, near = 0.f, comp = 0.f;
+  unsigned long long nfar = 0, nnear = 0;
+  int k = rt.x;
+  while (k < rt.y) {
+    const NodeRec* nd = T.nodes + k;
+    int4 tp = __ldg(&nd->topo);
+    float4 A = __ldg(&nd->com);
+    if (A.w == 0.0f) {
+      k = tp.z;
+      continue;
+    }
+    float4 X = __ldg(&nd->aux);
+    if (accept_node(A, X.z, X.w, gmin, gmax, beta)) {
+      float4 N = __ldg(&T.nnrm[k]);
+      float dx = A.x - q.x, dy = A.y - q.y, dz = A.z - q.z;
+      float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+      float nd_ = N.x * dx + N.y * dy + N.z * dz;
+      far += A.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
+      nfar++;
+      k = tp.z;
+    } else if (tp.w & kLeafFlag) {
+      float a = 0.f;
+      for (int j = tp.x; j < tp.y; j++) {
+        float4 s = __ldg(&T.sp[j]);
+        float4 nrm = __ldg(&T.sn[j]);
+        float dx = s.x - q.x, dy = s.y - q.y, dz = s.z - q.z;
+        float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+        float nd_ = nrm.x * dx + nrm.y * dy + nrm.z * dz;
+        a += s.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
+      }
+      kahan_add(near, comp, a);
+      nnear += static_cast<unsigned long long>(tp.y - tp.x);
+      k = tp.z;
+    } else {
+      k++;
+    }
+  }
+  if (active) out[G.perm[i]] = far + near;
+  if (counters && lane == 0) {
+    unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
+    atomicAdd(&counters[0], nfar * na);
+    atomicAdd(&counters[1], nnear * na);
+  }
+}
+
+// Query targets: keys in the box of system 0 (clamped), sorted, grouped.
+__global__ void query_keys_kernel(const float* __restrict__ q, int64_t nq, const SegBox* __restrict__ boxes,
+                                  uint64_t* __restrict__ keys) {
+  SegBox b = boxes[0];
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nq;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint64_t key = 0;
+    for (int d = 0; d < 3; d++) {
+      double t = __dmul_rn(__dsub_rn(static_cast<double>(q[3 * i + d]), static_cast<double>(b.lo[d])), b.scale);
+      double f = floor(t);
+      uint64_t qq = !(f >= 0.0) ? 0ull : (f > 2097151.0 ? 2097151ull : static_cast<uint64_t>(f));
+      key |= spread21(qq) << d;
+    }
+    keys[i] = key;
+  }
+}
+
+__global__ void query_gather_kernel(const float* __restrict__ q, const uint32_t* __restrict__ perm, int64_t nq,
+                                    float4* __restrict__ tp, int4* __restrict__ groups, uint32_t* __restrict__ ngroups) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nq;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t s = perm[i];
+    tp[i] = make_float4(q[3 * s], q[3 * s + 1], q[3 * s + 2], 0.0f);
+    if ((i & 31) == 0) {
+      int64_t e = i + 32 < nq ? i + 32 : nq;
+      groups[i >> 5] = make_int4(static_cast<int>(i), static_cast<int>(e), 0, 0);
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *ngroups = static_cast<uint32_t>((nq + 31) / 32);
+}
+
+}  // namespace nt
+}  // namespace sbh
+
+// ===========================================================================
+// host side
+// ===========================================================================
+namespace sbh {
+namespace nt {
+
+struct Layout {
+  // tree
+  SegBox* boxes;
+  uint32_t* bb;
+  uint64_t* k0;
+  uint64_t* k1;
+  uint32_t* v0;
+  uint32_t* v1;
+  uint32_t* segkey;
+  uint32_t* t0;
+  uint32_t* t1;
+  uint32_t* t2;
+  uint32_t* t3;
+  uint32_t* hist;
+  uint32_t* scan_tmp;
+  int8_t* cl;
+  int8_t* dd;
+  int8_t* lv;
+  uint32_t* base;  // n + 1 node-slot offsets
+  NodeRec* nodes;
+  DVec<10>* P;
+  DVec<10>* ptmp;
+  DVec<3>* PN;
+  DVec<3>* pntmp;
+  float4* nnrm;
+  float4* sp;
+  float4* sn;
+  uint32_t* perm;   // sorted slot -> input index (points into v0 or v1)
+  uint32_t* sseg;   // sorted slot -> system
+  int64_t* seg_off;
+  int2* roots;
+  uint32_t* gcount;
+  uint32_t* goff;
+  int4* groups;
+  uint32_t* meta;  // [0] node count, [1] group count, [2] which ping-pong buffer holds perm
+  unsigned long long* counters;
+  // adjoint scratch
+  float* node_adj;
+  float* part_adj;
+  float* gq;
+  DVec<14>* D;
+  DVec<14>* dtmp;
+  int64_t cap;
+};
+
+inline int64_t node_capacity(int64_t n, int nseg, int S) { return 21 * (n / (S + 1)) + n + nseg + 1; }
+
+template <typename C>
+void carve(C& c, int64_t n, int nseg, int S, bool normals, bool adjoint, Layout& L) {
+  int64_t nn = n > 0 ? n : 1;
+  int64_t cap = node_capacity(n, nseg, S);
+  L.cap = cap;
+  L.meta = c.template take<uint32_t>(8);
+  L.counters = c.template take<unsigned long long>(4);
+  L.boxes = c.template take<SegBox>(nseg);
+  L.bb = c.template take<uint32_t>(6 * nseg);
+  L.seg_off = c.template take<int64_t>(nseg + 1);
+  L.k0 = c.template take<uint64_t>(nn);
+  L.k1 = c.template take<uint64_t>(nn);
+  L.v0 = c.template take<uint32_t>(nn);
+  L.v1 = c.template take<uint32_t>(nn);
+  L.segkey = c.template take<uint32_t>(nn);
+  int64_t tn = nseg > 1 ? nn : 1;
+  L.t0 = c.template take<uint32_t>(tn);
+  L.t1 = c.template take<uint32_t>(tn);
+  L.t2 = c.template take<uint32_t>(tn);
+  L.t3 = c.template take<uint32_t>(tn);
+  int64_t hist_n = radix_hist_elems(nn);
+  L.hist = c.template take<uint32_t>(hist_n);
+  int64_t st = scan_tiles(hist_n), st2 = scan_tiles(nn + 1);
+  L.scan_tmp = c.template take<uint32_t>((st > st2 ? st : st2) + scan_tiles(nseg + 1));
+  L.cl = c.template take<int8_t>(nn);
+  L.dd = c.template take<int8_t>(nn);
+  L.lv = c.template take<int8_t>(nn);
+  L.base = c.template take<uint32_t>(nn + 1);
+  L.nodes = c.template take<NodeRec>(cap);
+  L.P = c.template take<DVec<10>>(nn + 1);
+  L.ptmp = c.template take<DVec<10>>(scan_tiles(nn));
+  L.sp = c.template take<float4>(nn);
+  L.sseg = c.template take<uint32_t>(nn);
+  L.roots = c.template take<int2>(nseg);
+  L.gcount = c.template take<uint32_t>(nseg + 1);
+  L.goff = c.template take<uint32_t>(nseg + 1);
+  L.groups = c.template take<int4>(nn / 32 + nseg + 1);
+  if (normals) {
+    L.PN = c.template take<DVec<3>>(nn + 1);
+    L.pntmp = c.template take<DVec<3>>(scan_tiles(nn));
+    L.nnrm = c.template take<float4>(cap);
+    L.sn = c.template take<float4>(nn);
+  } else {
+    L.PN = nullptr;
+    L.pntmp = nullptr;
+    L.nnrm = nullptr;
+    L.sn = nullptr;
+  }
+  if (adjoint) {
+    L.node_adj = c.template take<float>(cap * kNodeAdj);
+    L.part_adj = c.template take<float>(nn * kPartAdj);
+    L.gq = c.template take<float>(nn * 3);
+    L.D = c.template take<DVec<14>>(nn + 1);
+    L.dtmp = c.template take<DVec<14>>(scan_tiles(nn + 1));
+  } else {
+    L.node_adj = nullptr;
+    L.part_adj = nullptr;
+    L.gq = nullptr;
+    L.D = nullptr;
+    L.dtmp = nullptr;
+  }
+}
+
+// The tree handle stored in the first bytes after the status word: the
+// sizes the workspace was carved for, so later calls find the same layout.
+struct Header {
+  uint64_t magic;
+  int64_t n;
+  int32_t nseg;
+  int32_t leaf_size;
+  int32_t normals;
+  int32_t adjoint;
+};
+constexpr uint64_t kMagic = 0x5342483230304e54ull;  // "SBH200NT"
+
+inline unsigned gs(int64_t n, int t = 256) {
+  int64_t b = (n + t - 1) / t;
+  if (b > 148 * 32) b = 148 * 32;
+  return static_cast<unsigned>(b < 1 ? 1 : b);
+}
+
+struct SegCountLoad {
+  const uint32_t* gc;
+  __device__ uint32_t operator()(int64_t i) const { return gc[i]; }
+};
+
+}  // namespace nt
+}  // namespace sbh
+
+using namespace sbh;
+using namespace sbh::nt;
+
+namespace {
+
+// Host registry: which tree (sizes) a workspace holds, so evaluation calls
+// recover the workspace layout without reading device memory.
+std::mutex g_reg_mu;
+std::unordered_map<const void*, Header> g_registry;
+
+int register_tree(void* ws, const Header& h) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  g_registry[ws] = h;
+  return SBH_OK;
+}
+
+int native_layout(void* ws, size_t ws_bytes, const Header& h, Layout& L) {
+  Carver c(ws, ws_bytes);
+  carve(c, h.n, h.nseg, h.leaf_size, h.normals != 0, h.adjoint != 0, L);
+  if (!c.ok) return fail(SBH_ERR_WORKSPACE, "workspace too small for the native tree");
+  return SBH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int with_normals, int with_adjoint) {
+  if (n < 0 || num_systems < 1 || leaf_size < 1 || leaf_size > 32) return 0;
+  Sizer s;
+  Layout L;
+  carve(s, n, num_systems, leaf_size, with_normals != 0, with_adjoint != 0, L);
+  return s.off;
+}
+
+int sbh_native_build(cudaStream_t stream, const float* points, const float* masses, const float* normals, int64_t n,
+                     const int64_t* system_offsets, int num_systems, int leaf_size, int with_adjoint,
+                     void* workspace, size_t workspace_bytes) {
+  if (n < 0 || n >= (1ll << 31)) return invalid("number of points must be in [0, 2^31)");
+  if (num_systems < 1) return invalid("num_systems must be >= 1");
+  if (num_systems > 1 && !system_offsets) return invalid("system_offsets is required when num_systems > 1");
+  if (leaf_size < 1 || leaf_size > 32) return invalid("leaf_size must be in [1, 32]");
+  if (n > 0 && (!points || !masses)) return invalid("points and masses must be non-null");
+  if (!workspace) return fail(SBH_ERR_WORKSPACE, "workspace is null");
+  size_t need = sbh_native_workspace_bytes(n, num_systems, leaf_size, normals != nullptr, with_adjoint);
+  if (workspace_bytes < need)
+    return fail(SBH_ERR_WORKSPACE, "workspace too small: need " + std::to_string(need) + " bytes");
+  Header h{kMagic, n, num_systems, leaf_size, normals != nullptr, with_adjoint != 0};
+  Layout L;
+  if (int rc = native_layout(workspace, workspace_bytes, h, L)) return rc;
+  uint32_t* status = static_cast<uint32_t*>(workspace);
+  cudaError_t e = cudaMemsetAsync(status, 0, 64, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(L.meta, 0, 8 * sizeof(uint32_t), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, 4 * sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  // system offsets (device copy, or [0, n] for one system)
+  if (num_systems > 1) {
+    e = cudaMemcpyAsync(L.seg_off, system_offsets, (num_systems + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                        stream);
+  } else {
+    single_offsets_kernel<<<1, 1, 0, stream>>>(L.seg_off, n);
+  }
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  int nseg = num_systems;
+  bbox_init_kernel<<<(nseg + 255) / 256, 256, 0, stream>>>(L.bb, nseg);
+  if (n > 0) bbox_kernel<<<gs(n), 256, 0, stream>>>(points, n, L.seg_off, nseg, L.bb);
+  bbox_finalize_kernel<<<(nseg + 255) / 256, 256, 0, stream>>>(L.bb, nseg, L.seg_off, L.boxes);
+  const uint32_t* perm = L.v0;
+  if (n > 0) {
+    keys_kernel<<<gs(n), 256, 0, stream>>>(points, n, L.seg_off, nseg, L.boxes, L.k0, nseg > 1 ? L.segkey : nullptr);
+    int which = 0;
+    e = radix_sort<uint64_t>(stream, L.k0, L.v0, L.k1, L.v1, n, 63, false, L.hist, L.scan_tmp, &which);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    uint64_t* ksorted = which == 0 ? L.k0 : L.k1;
+    uint32_t* vsorted = which == 0 ? L.v0 : L.v1;
+    if (nseg > 1) {
+      // Stable pass on the system id over the key-sorted order: payload =
+      // position in that order, then gather keys and input indices.
+      gather_u32_kernel<<<gs(n), 256, 0, stream>>>(L.segkey, vsorted, n, L.t0);
+      int bits = 0;
+      while ((1 << bits) < nseg) bits++;
+      int w2 = 0;
+      e = radix_sort<uint32_t>(stream, L.t0, L.t2, L.t1, L.t3, n, bits, false, L.hist, L.scan_tmp, &w2);
+      if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+      const uint32_t* p2 = w2 == 0 ? L.t2 : L.t3;
+      uint64_t* kout = which == 0 ? L.k1 : L.k0;
+      uint32_t* vout = which == 0 ? L.v1 : L.v0;
+      gather_keys_kernel<<<gs(n), 256, 0, stream>>>(ksorted, p2, n, kout);
+      gather_u32_kernel<<<gs(n), 256, 0, stream>>>(vsorted, p2, n, vout);
+      ksorted = kout;
+      vsorted = vout;
+      sseg_kernel<<<gs(n), 256, 0, stream>>>(L.seg_off, nseg, n, L.sseg);
+    }
+    if (ksorted != L.k0) {
+      e = cudaMemcpyAsync(L.k0, ksorted, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(L.v0, vsorted, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
+      if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    }
+    perm = L.v0;
+    const uint32_t* sseg = nseg > 1 ? L.sseg : nullptr;
+    levels_kernel<<<gs(n), 256, 0, stream>>>(L.k0, sseg, n, leaf_size, L.cl, L.dd);
+    slots_kernel<<<gs(n), 256, 0, stream>>>(L.cl, L.dd, n, leaf_size, L.lv, L.base);
+    e = exclusive_scan<uint32_t>(stream, ArrayLoad<uint32_t>{L.base}, n, L.base, L.scan_tmp, true);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    emit_nodes_kernel<<<gs(n), 256, 0, stream>>>(L.k0, sseg, L.seg_off, n, L.dd, L.lv, L.base, L.nodes, L.cap, status);
+    node_count_kernel<<<1, 1, 0, stream>>>(L.base, n, L.cap, L.meta);
+    gather_particles_kernel<<<gs(n), 256, 0, stream>>>(points, masses, normals, perm, n, L.sp, L.sn);
+    e = exclusive_scan<DVec<10>>(stream, MomentLoad{L.sp, sseg, L.boxes}, n, L.P, L.ptmp, true);
+    if (e == cudaSuccess && normals)
+      e = exclusive_scan<DVec<3>>(stream, NormalMomentLoad{L.sp, L.sn}, n, L.PN, L.pntmp, true);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    finalize_nodes_kernel<<<gs(static_cast<int64_t>(L.cap)), 256, 0, stream>>>(L.nodes, L.meta, L.k0, sseg, L.boxes,
+                                                                                L.P, L.PN, L.nnrm);
+  } else {
+    e = cudaMemsetAsync(L.base, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  }
+  // roots and target groups
+  group_counts_kernel<<<(nseg + 255) / 256, 256, 0, stream>>>(L.seg_off, nseg, L.gcount);
+  e = exclusive_scan<uint32_t>(stream, ArrayLoad<uint32_t>{L.gcount}, nseg, L.goff, L.scan_tmp, true);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  roots_groups_kernel<<<nseg, 128, 0, stream>>>(L.seg_off, nseg, L.base, L.goff, L.roots, L.groups);
+  group_total_kernel<<<1, 1, 0, stream>>>(L.goff, nseg, L.meta);
+  if (int rc = check_launch("sbh_native_build")) return rc;
+  return register_tree(workspace, h);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// evaluation entry points
+// ---------------------------------------------------------------------------
+namespace {
+
+int lookup(const void* ws, size_t ws_bytes, Header& h, Layout& L) {
+  {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    auto it = g_registry.find(ws);
+    if (it == g_registry.end()) return invalid("workspace holds no native tree; call sbh_native_build first");
+    h = it->second;
+  }
+  return native_layout(const_cast<void*>(ws), ws_bytes, h, L);
+}
+
+__global__ void zero_node_adj_kernel(float* adj, const uint32_t* meta) {
+  int64_t total = static_cast<int64_t>(meta[0]) * kNodeAdj;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    adj[i] = 0.0f;
+}
+
+WalkTree tree_view(const Layout& L) { return WalkTree{L.nodes, L.sp, L.sn, L.nnrm, L.roots}; }
+
+WalkTargets self_targets(const Layout& L) { return WalkTargets{L.sp, L.v0, L.groups, L.meta + 1, 1}; }
+
+unsigned walk_blocks(int64_t n, int nseg) {
+  int64_t warps = n / 32 + nseg + 1;
+  return static_cast<unsigned>((warps + 3) / 4);
+}
+
+int check_params(const sbh_native_params* p) {
+  if (!p) return invalid("params must be non-null");
+  if (!(p->beta > 0.0f)) return invalid("beta must be > 0");
+  if (p->softening < 0.0f) return invalid("softening must be >= 0");
+  if (p->quadrupole && p->cutoff > 0.0f) return invalid("the quadrupole far field needs cutoff <= 0 (Plummer)");
+  return SBH_OK;
+}
+
+WalkParams walk_params(const sbh_native_params* p) {
+  float eps = fmaxf(p->softening, 0.0f);
+  return WalkParams{p->beta, eps * eps + 1e-12f, p->cutoff};
+}
+
+}  // namespace
+
+extern "C" {
+
+int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float* force_out, void* workspace,
+                     size_t workspace_bytes) {
+  if (int rc = check_params(params)) return rc;
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (h.n == 0) return SBH_OK;
+  if (!force_out) return invalid("force_out must be non-null");
+  cudaError_t e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  WalkParams wp = walk_params(params);
+  unsigned nb = walk_blocks(h.n, h.nseg);
+  bool cut = params->cutoff > 0.0f;
+  if (params->quadrupole)
+    force_walk_kernel<true, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, force_out, L.counters);
+  else if (cut)
+    force_walk_kernel<false, true><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, force_out, L.counters);
+  else
+    force_walk_kernel<false, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, force_out, L.counters);
+  return check_launch("sbh_native_force");
+}
+
+int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params, const float* cotangent,
+                            float* force_out, void* workspace, size_t workspace_bytes) {
+  if (int rc = check_params(params)) return rc;
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!h.adjoint) return invalid("the tree was built without adjoint scratch (with_adjoint = 0)");
+  if (h.n == 0) return SBH_OK;
+  if (!cotangent) return invalid("cotangent must be non-null");
+  int64_t n = h.n;
+  cudaError_t e = cudaMemsetAsync(L.part_adj, 0, n * kPartAdj * sizeof(float), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
+  WalkParams wp = walk_params(params);
+  unsigned nb = walk_blocks(n, h.nseg);
+  bool cut = params->cutoff > 0.0f;
+  if (params->quadrupole)
+    adjoint_walk_kernel<true, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, cotangent, force_out,
+                                                             L.gq, L.node_adj, L.part_adj, L.counters);
+  else if (cut)
+    adjoint_walk_kernel<false, true><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, cotangent, force_out,
+                                                             L.gq, L.node_adj, L.part_adj, L.counters);
+  else
+    adjoint_walk_kernel<false, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, cotangent,
+                                                              force_out, L.gq, L.node_adj, L.part_adj, L.counters);
+  return check_launch("sbh_native_adjoint_walk");
+}
+
+int sbh_native_adjoint_finalize(cudaStream_t stream, float* grad_points, float* grad_masses, void* workspace,
+                                size_t workspace_bytes) {
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!h.adjoint) return invalid("the tree was built without adjoint scratch (with_adjoint = 0)");
+  if (h.n == 0) return SBH_OK;
+  if (!grad_points || !grad_masses) return invalid("gradient outputs must be non-null");
+  int64_t n = h.n;
+  cudaError_t e = cudaMemsetAsync(L.D, 0, (n + 1) * sizeof(DVec<14>), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  const uint32_t* sseg = h.nseg > 1 ? L.sseg : nullptr;
+  node_push_kernel<<<gs(L.cap), 256, 0, stream>>>(L.nodes, L.meta, L.node_adj, sseg, L.boxes, L.D);
+  e = exclusive_scan<DVec<14>>(stream, ArrayLoad<DVec<14>>{L.D}, n + 1, L.D, L.dtmp, false);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  adjoint_combine_kernel<<<gs(n), 256, 0, stream>>>(L.sp, L.v0, sseg, L.boxes, n, L.gq, L.part_adj, L.D, grad_points,
+                                                    grad_masses);
+  return check_launch("sbh_native_adjoint_finalize");
+}
+
+int sbh_native_force_vjp(cudaStream_t stream, const sbh_native_params* params, const float* cotangent,
+                         float* force_out, float* grad_points, float* grad_masses, void* workspace,
+                         size_t workspace_bytes) {
+  if (!grad_points || !grad_masses) return invalid("gradient outputs must be non-null");
+  if (int rc = sbh_native_adjoint_walk(stream, params, cotangent, force_out, workspace, workspace_bytes)) return rc;
+  return sbh_native_adjoint_finalize(stream, grad_points, grad_masses, workspace, workspace_bytes);
+}
+
+size_t sbh_native_query_workspace_bytes(int64_t nq) {
+  if (nq < 0) return 0;
+  Sizer s;
+  int64_t nn = nq > 0 ? nq : 1;
+  s.take<uint32_t>(8);
+  s.take<uint64_t>(nn);
+  s.take<uint64_t>(nn);
+  s.take<uint32_t>(nn);
+  s.take<uint32_t>(nn);
+  s.take<uint32_t>(radix_hist_elems(nn));
+  s.take<uint32_t>(scan_tiles(radix_hist_elems(nn)));
+  s.take<float4>(nn);
+  s.take<int4>(nn / 32 + 1);
+  return s.off;
+}
+
+int sbh_native_winding_number(cudaStream_t stream, float beta, const float* queries, int64_t nq, float* out,
+                              void* workspace, size_t workspace_bytes, void* query_workspace,
+                              size_t query_workspace_bytes) {
+  if (!(beta > 0.0f)) return invalid("beta must be > 0");
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!h.normals) return invalid("the tree was built without normals");
+  if (h.nseg != 1) return invalid("query evaluation needs a single-system tree");
+  if (nq < 0 || nq >= (1ll << 31)) return invalid("number of queries must be in [0, 2^31)");
+  if (nq == 0) return SBH_OK;
+  if (!queries || !out) return invalid("queries and out must be non-null");
+  size_t need = sbh_native_query_workspace_bytes(nq);
+  if (!query_workspace || query_workspace_bytes < need)
+    return fail(SBH_ERR_WORKSPACE, "query workspace too small: need " + std::to_string(need) + " bytes");
+  if (h.n == 0) {
+    cudaError_t e = cudaMemsetAsync(out, 0, nq * sizeof(float), stream);
+    return e == cudaSuccess ? SBH_OK : fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  }
+  Carver c(query_workspace, query_workspace_bytes);
+  uint32_t* qmeta = c.take<uint32_t>(8);
+  uint64_t* k0 = c.take<uint64_t>(nq);
+  uint64_t* k1 = c.take<uint64_t>(nq);
+  uint32_t* v0 = c.take<uint32_t>(nq);
+  uint32_t* v1 = c.take<uint32_t>(nq);
+  uint32_t* hist = c.take<uint32_t>(radix_hist_elems(nq));
+  uint32_t* stmp = c.take<uint32_t>(scan_tiles(radix_hist_elems(nq)));
+  float4* tp = c.take<float4>(nq);
+  int4* groups = c.take<int4>(nq / 32 + 1);
+  query_keys_kernel<<<gs(nq), 256, 0, stream>>>(queries, nq, L.boxes, k0);
+  int which = 0;
+  cudaError_t e = radix_sort<uint64_t>(stream, k0, v0, k1, v1, nq, 63, false, hist, stmp, &which);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  const uint32_t* qperm = which == 0 ? v0 : v1;
+  query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
+  e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  WalkTargets G{tp, qperm, groups, qmeta, 0};
+  unsigned nb = static_cast<unsigned>((nq / 32 + 1 + 3) / 4);
+  wn_walk_kernel<<<nb, 128, 0, stream>>>(tree_view(L), G, beta, out, L.counters);
+  return check_launch("sbh_native_winding_number");
+}
+
+// Synchronises the stream and reports [node count, group count, far
+// interactions, near interactions] of the last build / evaluation.
+int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspace_bytes, uint64_t* out4) {
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  uint32_t meta[8];
+  unsigned long long cnt[2];
+  cudaError_t e = cudaMemcpyAsync(meta, L.meta, sizeof(meta), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, L.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  out4[0] = meta[0];
+  out4[1] = meta[1];
+  out4[2] = cnt[0];
+  out4[3] = cnt[1];
+  if (meta[3]) return fail(SBH_ERR_LIMIT, "node capacity exceeded");
+  return SBH_OK;
+}
+
+// Copies the tree to caller buffers (device pointers; any may be null):
+// sorted keys (n), permutation (n, sorted slot -> input index), nodes
+// (num_nodes x 64 bytes), and the node count to *num_nodes (synchronises).
+int sbh_native_export(cudaStream_t stream, const void* workspace, size_t workspace_bytes, uint64_t* keys_out,
+                      uint32_t* perm_out, void* nodes_out, size_t nodes_capacity, uint64_t* num_nodes) {
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  uint32_t nn = 0;
+  cudaError_t e = cudaMemcpyAsync(&nn, L.meta, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  if (num_nodes) *num_nodes = nn;
+  if (keys_out && h.n > 0) e = cudaMemcpyAsync(keys_out, L.k0, h.n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream);
+  if (e == cudaSuccess && perm_out && h.n > 0)
+    e = cudaMemcpyAsync(perm_out, L.v0, h.n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream);
+  if (e == cudaSuccess && nodes_out) {
+    if (nodes_capacity < nn) return invalid("nodes_out too small");
+    e = cudaMemcpyAsync(nodes_out, L.nodes, static_cast<size_t>(nn) * sizeof(NodeRec), cudaMemcpyDeviceToDevice,
+                        stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  return SBH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,31 @@
+// Device-side records of the native adaptive octree (see sbh_native.cu).
+#pragma once
+
+#include <cstdint>
+
+namespace sbh {
+namespace nt {
+
+// Bounding cube of one system.
+struct SegBox {
+  float lo[3];
+  float span;
+  double scale;  // 2^21 / span
+};
+
+// One node, 64 bytes, read by the traversal with four 16-byte loads.
+struct NodeRec {
+  float4 com;   // COM x, y, z and total mass M
+  float4 aux;   // S_xz, S_yz, diag = side * sqrt(3), delta = |COM - cell centre|
+  float4 quad;  // S_xx, S_yy, S_zz, S_xy (second moment about the COM)
+  int4 topo;    // particle range [start, end), skip index, level | 0x100 if leaf
+};
+static_assert(sizeof(NodeRec) == 64, "NodeRec must be 64 bytes");
+
+constexpr int kLeafFlag = 0x100;
+constexpr int kGroup = 32;      // targets per warp
+constexpr int kNodeAdj = 12;    // per-node adjoint floats: A_X(3) A_M(1) G(6) pad(2)
+constexpr int kPartAdj = 4;     // per-particle adjoint floats: dx(3) dm(1)
+
+}  // namespace nt
+}  // namespace sbh

@@ -61,3 +61,40 @@ uint64_t sbh_octree8_total_nodes(int max_depth) {
 size_t sbh_traversal_workspace_bytes(void) { return sbh::kStatusBytes; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// FP32 peak probe: independent FMA chains, 8 per thread, no memory traffic
+// inside the loop. Used to report the traversal kernels' FP32-pipe roofline
+// against a number measured on the same GPU.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void __launch_bounds__(256) fp32_probe_kernel(float* out, int iters, float a, float b) {
+  float x0 = threadIdx.x * 1e-7f, x1 = x0 + 1e-3f, x2 = x0 + 2e-3f, x3 = x0 + 3e-3f;
+  float x4 = x0 + 4e-3f, x5 = x0 + 5e-3f, x6 = x0 + 6e-3f, x7 = x0 + 7e-3f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      x0 = fmaf(x0, a, b);
+      x1 = fmaf(x1, a, b);
+      x2 = fmaf(x2, a, b);
+      x3 = fmaf(x3, a, b);
+      x4 = fmaf(x4, a, b);
+      x5 = fmaf(x5, a, b);
+      x6 = fmaf(x6, a, b);
+      x7 = fmaf(x7, a, b);
+    }
+  }
+  float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 12345.678f) out[blockIdx.x] = s;  // keeps the chains alive
+}
+}  // namespace
+
+extern "C" {
+// Launches blocks x 256 threads of 8 independent FMA chains x 16 x iters:
+// flops = blocks * 256 * 8 * 16 * iters * 2.
+int sbh_probe_fp32(cudaStream_t stream, float* out, int blocks, int iters) {
+  if (blocks <= 0 || iters <= 0 || !out) return sbh::invalid("blocks, iters > 0 and out non-null required");
+  fp32_probe_kernel<<<blocks, 256, 0, stream>>>(out, iters, 0.999999f, 1e-7f);
+  return sbh::check_launch("probe_fp32");
+}
+}

@@ -103,7 +103,32 @@ _SIGS = {
                                          _c_f, _c_f, _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_stochastic_bh_force_octree8_vjp": ([_c_p, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p, _c_i,
                                              _c_i, _c_f, _c_f, _c_f, _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_probe_fp32": ([_c_p, _c_p, _c_i, _c_i], _c_i),
+    "sbh_build_octree_level3_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_build_octree_level3": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p,
+                                 _c_sz], _c_i),
+    "sbh_barnes_hut_tree": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_f, _c_i,
+                             _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_stochastic_bh_tree": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_i, _c_i,
+                                _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_native_workspace_bytes": ([_c_i64, _c_i, _c_i, _c_i, _c_i], _c_sz),
+    "sbh_native_build": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_i, _c_i, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_native_force": ([_c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
+    "sbh_native_force_vjp": ([_c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
+    "sbh_native_adjoint_walk": ([_c_p, _c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
+    "sbh_native_adjoint_finalize": ([_c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
+    "sbh_native_query_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_native_winding_number": ([_c_p, _c_f, _c_p, _c_i64, _c_p, _c_p, _c_sz, _c_p, _c_sz], _c_i),
+    "sbh_native_stats": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
+    "sbh_native_export": ([_c_p, _c_p, _c_sz, _c_p, _c_p, _c_p, _c_sz, _c_p], _c_i),
 }
+
+
+class NativeParams(ctypes.Structure):
+    """sbh_native_params of include/sbh_b200.h."""
+
+    _fields_ = [("beta", ctypes.c_float), ("softening", ctypes.c_float), ("cutoff", ctypes.c_float),
+                ("quadrupole", ctypes.c_int)]
 
 _lib_handle = None
 _lib_lock = threading.Lock()
@@ -604,3 +629,319 @@ for _name in ("register_bruteforce_gravity", "register_softened_direct_force", "
               "register_stochastic_barnes_hut_force_octree8_vjp",
               "register_softened_stochastic_barnes_hut_force_octree8_vjp"):
     globals()[_name] = _register
+
+
+# ---------------------------------------------------------------------------
+# native adaptive octree (new entry points; no reference counterpart)
+# ---------------------------------------------------------------------------
+class NativeTree:
+    """A native tree (or forest of independent systems) living in a device
+    workspace. build() once, then force(), force_vjp() and
+    winding_number() evaluate it; the workspace is reused across builds of
+    the same size."""
+
+    NODE_BYTES = 64
+
+    def __init__(self, device=None):
+        self.device = device or _device()
+        self.ws = None
+        self.qws = None
+        self.n = 0
+        self.num_systems = 1
+        self.leaf_size = 16
+        self.normals = False
+        self.adjoint = False
+
+    def build(self, points, masses, normals=None, system_offsets=None, *, leaf_size: int = 16,
+              with_adjoint: bool = True):
+        dev = self.device
+        points, masses = _f32(points, dev), _f32(masses, dev)
+        if points.ndim != 2 or points.shape[1] != 3:
+            raise ValueError("points must have shape (N, 3)")
+        if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
+            raise ValueError("masses must have shape (N,)")
+        nrm = None
+        if normals is not None:
+            nrm = _f32(normals, dev)
+            if nrm.shape != points.shape:
+                raise ValueError("normals shape mismatch")
+        if not 1 <= leaf_size <= 32:
+            raise ValueError("leaf_size must be in [1, 32]")
+        offs = None
+        nsys = 1
+        if system_offsets is not None:
+            offs = torch.as_tensor(np.asarray(system_offsets, dtype=np.int64), device=dev) \
+                if not isinstance(system_offsets, torch.Tensor) else system_offsets.to(dev, torch.int64)
+            nsys = int(offs.numel()) - 1
+            if nsys < 1:
+                raise ValueError("system_offsets needs at least two entries")
+        n = points.shape[0]
+        need = int(lib().sbh_native_workspace_bytes(n, nsys, int(leaf_size), int(nrm is not None), int(with_adjoint)))
+        if self.ws is None or self.ws.numel() < need:
+            self.ws = torch.empty(need, dtype=torch.uint8, device=dev)
+        self._keep = (points, masses, nrm, offs)
+        _check(lib().sbh_native_build(_stream_ptr(dev), _p(points), _p(masses), _p(nrm), n, _p(offs), nsys,
+                                      int(leaf_size), int(with_adjoint), _p(self.ws), self.ws.numel()),
+               "native_build")
+        self.n, self.num_systems, self.leaf_size = n, nsys, int(leaf_size)
+        self.normals, self.adjoint = nrm is not None, bool(with_adjoint)
+        return self
+
+    @staticmethod
+    def params(beta=2.0, softening=1e-3, cutoff=0.0, quadrupole=True) -> NativeParams:
+        return NativeParams(float(beta), float(softening), float(cutoff), int(bool(quadrupole)))
+
+    def force(self, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0, quadrupole: bool = True,
+              out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        prm = self.params(beta, softening, cutoff, quadrupole)
+        out = out if out is not None else torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
+        _check(lib().sbh_native_force(_stream_ptr(self.device), ctypes.byref(prm), _p(out), _p(self.ws),
+                                      self.ws.numel()), "native_force")
+        return out
+
+    def force_vjp(self, cotangent, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,
+                  quadrupole: bool = True, want_force: bool = True):
+        """(force or None, d/d points, d/d masses) of sum(cotangent * force)."""
+        prm = self.params(beta, softening, cutoff, quadrupole)
+        cot = _f32(cotangent, self.device)
+        if cot.shape != (self.n, 3):
+            raise ValueError("cotangent must have shape (N, 3)")
+        f = torch.empty((self.n, 3), dtype=torch.float32, device=self.device) if want_force else None
+        gx = torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
+        gm = torch.empty(self.n, dtype=torch.float32, device=self.device)
+        _check(lib().sbh_native_force_vjp(_stream_ptr(self.device), ctypes.byref(prm), _p(cot), _p(f), _p(gx),
+                                          _p(gm), _p(self.ws), self.ws.numel()), "native_force_vjp")
+        return f, gx, gm
+
+    def adjoint_walk(self, cotangent, params: NativeParams, force_out=None):
+        """Phase 1 of force_vjp (the traversal)."""
+        _check(lib().sbh_native_adjoint_walk(_stream_ptr(self.device), ctypes.byref(params), _p(cotangent),
+                                             _p(force_out), _p(self.ws), self.ws.numel()), "native_adjoint_walk")
+
+    def adjoint_finalize(self, grad_points, grad_masses):
+        """Phase 2 of force_vjp (node adjoints to particles, input order)."""
+        _check(lib().sbh_native_adjoint_finalize(_stream_ptr(self.device), _p(grad_points), _p(grad_masses),
+                                                 _p(self.ws), self.ws.numel()), "native_adjoint_finalize")
+
+    def winding_number(self, queries, *, beta: float = 2.0) -> torch.Tensor:
+        q = _f32(queries, self.device)
+        if q.ndim != 2 or q.shape[1] != 3:
+            raise ValueError("queries must be (M, 3)")
+        need = int(lib().sbh_native_query_workspace_bytes(q.shape[0]))
+        if self.qws is None or self.qws.numel() < need:
+            self.qws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
+        out = torch.empty(q.shape[0], dtype=torch.float32, device=self.device)
+        _check(lib().sbh_native_winding_number(_stream_ptr(self.device), float(beta), _p(q), q.shape[0], _p(out),
+                                               _p(self.ws), self.ws.numel(), _p(self.qws), self.qws.numel()),
+               "native_winding_number")
+        return out
+
+    def stats(self) -> dict:
+        out = (ctypes.c_uint64 * 4)()
+        rc = lib().sbh_native_stats(_stream_ptr(self.device), _p(self.ws), self.ws.numel(), out)
+        _check(rc, "native_stats")
+        return dict(nodes=int(out[0]), groups=int(out[1]), far=int(out[2]), near=int(out[3]))
+
+    def export(self):
+        """(sorted keys u64, permutation, node records (nn x 64 bytes)) as CPU numpy arrays."""
+        nn = ctypes.c_uint64(0)
+        _check(lib().sbh_native_export(_stream_ptr(self.device), _p(self.ws), self.ws.numel(), None, None, None, 0,
+                                       ctypes.byref(nn)), "native_export")
+        keys = torch.empty(self.n, dtype=torch.int64, device=self.device)
+        perm = torch.empty(self.n, dtype=torch.int32, device=self.device)
+        nodes = torch.empty(int(nn.value) * self.NODE_BYTES, dtype=torch.uint8, device=self.device)
+        _check(lib().sbh_native_export(_stream_ptr(self.device), _p(self.ws), self.ws.numel(), _p(keys), _p(perm),
+                                       _p(nodes), int(nn.value), ctypes.byref(nn)), "native_export")
+        return (keys.cpu().numpy().view(np.uint64), perm.cpu().numpy().view(np.uint32),
+                nodes.cpu().numpy().reshape(-1, self.NODE_BYTES))
+
+
+def native_force(points, masses, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,
+                 leaf_size: int = 16, quadrupole: bool = True) -> torch.Tensor:
+    """Softened self-gravity on the native tree (build + force)."""
+    t = NativeTree().build(points, masses, leaf_size=leaf_size, with_adjoint=False)
+    return t.force(beta=beta, softening=softening, cutoff=cutoff, quadrupole=quadrupole)
+
+
+class _NativeGravity(torch.autograd.Function):
+    """Self-gravity with the full adjoint. forward builds the tree and sums;
+    backward rebuilds it from the saved inputs (recompute, like the
+    reference's custom_vjp) and runs the adjoint walk: gradients w.r.t. both
+    positions and masses."""
+
+    @staticmethod
+    def forward(ctx, points, masses, cfg):
+        beta, soft, cut, leaf, quad = cfg
+        ctx.save_for_backward(points, masses)
+        ctx.cfg = cfg
+        t = NativeTree().build(points.detach(), masses.detach(), leaf_size=leaf, with_adjoint=False)
+        return t.force(beta=beta, softening=soft, cutoff=cut, quadrupole=quad)
+
+    @staticmethod
+    def backward(ctx, cot):
+        points, masses = ctx.saved_tensors
+        beta, soft, cut, leaf, quad = ctx.cfg
+        t = NativeTree().build(points.detach(), masses.detach(), leaf_size=leaf, with_adjoint=True)
+        _, gx, gm = t.force_vjp(cot.contiguous(), beta=beta, softening=soft, cutoff=cut, quadrupole=quad,
+                                want_force=False)
+        return gx, gm, None
+
+
+def native_force_recompute_vjp(points, masses, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,
+                               leaf_size: int = 16, quadrupole: bool = True) -> torch.Tensor:
+    """Differentiable native self-gravity (gradients w.r.t. points and masses)."""
+    if beta <= 0:
+        raise ValueError("beta must be > 0")
+    if softening < 0:
+        raise ValueError("softening must be >= 0")
+    dev = _device()
+    points = points if isinstance(points, torch.Tensor) else _f32(points, dev)
+    masses = masses if isinstance(masses, torch.Tensor) else _f32(masses, dev)
+    return _NativeGravity.apply(points, masses, (float(beta), float(softening), float(cutoff), int(leaf_size),
+                                                 bool(quadrupole)))
+
+
+# ---------------------------------------------------------------------------
+# level-3 tree and Node2 / Node3 targets (python/jax_sbh_ffi.py:744-862,
+# 963-1334)
+# ---------------------------------------------------------------------------
+TREE_POTENTIAL, TREE_FORCE, TREE_SOFT_FORCE, TREE_WINDING = 0, 1, 2, 3
+
+
+def build_octree_buffers_with_contrib(points, normals, masses, min_corner=None, max_corner=None, *,
+                                      alpha: float = 1.0, level: int = 3, backend: str = "ffi"):
+    """Root + up to 512 leaf children on the 8^3 grid of [min, max], in the
+    Tree3DNode<1,3> layout (src/sbh_ffi.cu:736-1037). backend="cpu" (the
+    reference's sbh.Octree3 builder) is not part of this library."""
+    del alpha
+    if level != 3:
+        raise ValueError("level must be 3 (FFI expects Tree3DNode<1, 3>)")
+    if backend != "ffi":
+        raise ValueError("backend must be 'ffi' (the CPU builder is the reference's sbh module)")
+    dev = _device()
+    points, normals, masses = _f32(points, dev), _f32(normals, dev), _f32(masses, dev)
+    if points.ndim != 2 or points.shape[1] != 3:
+        raise ValueError("points must have shape (N, 3)")
+    if normals.shape != points.shape:
+        raise ValueError("normals shape mismatch")
+    if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
+        raise ValueError("masses must have shape (N,)")
+    if points.shape[0] == 0 and (min_corner is None or max_corner is None):
+        raise ValueError("empty point set needs explicit min_corner/max_corner")
+    mn, mx = _default_corners(points, min_corner, max_corner, dev)
+    n = points.shape[0]
+    nmax = octree_level3_max_nodes()
+    leaf = torch.empty(n * leaf3_size(), dtype=torch.uint8, device=dev)
+    node = torch.empty(nmax * node3_size(), dtype=torch.uint8, device=dev)
+    contrib = torch.empty(nmax * leaf3_size(), dtype=torch.uint8, device=dev)
+    ws = workspace(int(lib().sbh_build_octree_level3_workspace_bytes(n)), dev)
+    _check(lib().sbh_build_octree_level3(_stream_ptr(dev), _p(points), _p(normals), _p(masses), n, _p(mn), _p(mx),
+                                         _p(leaf), leaf.numel(), _p(node), node.numel(), _p(contrib), contrib.numel(),
+                                         _p(ws), ws.numel()), "build_octree_buffers")
+    return leaf, node, contrib
+
+
+def build_octree_buffers(points, normals, masses, min_corner=None, max_corner=None, *, alpha: float = 1.0,
+                         level: int = 3, backend: str = "ffi"):
+    leaf, node, _ = build_octree_buffers_with_contrib(points, normals, masses, min_corner, max_corner, alpha=alpha,
+                                                      level=level, backend=backend)
+    return leaf, node
+
+
+def _tree_call(kernel, leaf_bytes, node_bytes, queries, beta, softening_scale, cutoff_scale, periodic, box_length,
+               threads, check_status=False):
+    dev = _device()
+    leaf, node, queries = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
+    if queries.ndim != 2 or queries.shape[1] not in (2, 3):
+        raise ValueError("queries must be (M, 2) or (M, 3)")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    dim = queries.shape[1]
+    vec = kernel in (TREE_FORCE, TREE_SOFT_FORCE)
+    out = torch.empty((queries.shape[0], dim) if vec else queries.shape[0], dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_barnes_hut_tree(_stream_ptr(dev), dim, kernel, _p(leaf), leaf.numel(), _p(node), node.numel(),
+                                     _p(queries), queries.shape[0], _p(out), float(beta), float(softening_scale),
+                                     float(cutoff_scale), int(bool(periodic)), float(box_length), int(threads), _p(ws),
+                                     ws.numel()), "barnes_hut_tree")
+    _status_after(ws, "barnes_hut_tree", check_status)
+    return out
+
+
+def barnes_hut_gravity(leaf_bytes, node_bytes, queries, *, beta: float = 2.0, periodic: bool = False,
+                       box_length: float = 1.0, threads: int = 64):
+    return _tree_call(TREE_POTENTIAL, leaf_bytes, node_bytes, queries, beta, 0.0, 1.0, periodic, box_length, threads)
+
+
+def barnes_hut_force(leaf_bytes, node_bytes, queries, *, beta: float = 2.0, periodic: bool = False,
+                     box_length: float = 1.0, threads: int = 256):
+    return _tree_call(TREE_FORCE, leaf_bytes, node_bytes, queries, beta, 0.0, 1.0, periodic, box_length, threads)
+
+
+def softened_barnes_hut_force(leaf_bytes, node_bytes, queries, *, beta: float = 2.0, softening_scale: float = 1e-2,
+                              cutoff_scale: float = 1.0, periodic: bool = False, box_length: float = 1.0,
+                              threads: int = 256):
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    return _tree_call(TREE_SOFT_FORCE, leaf_bytes, node_bytes, queries, beta, softening_scale, cutoff_scale, periodic,
+                      box_length, threads)
+
+
+def barnes_hut_winding_number(leaf_bytes, node_bytes, queries, *, beta: float = 2.0, threads: int = 256):
+    """Winding number on a Node2/Node3 tree (new target; the reference has it
+    only in its pybind module, src/sbh_gpu.cu:100-120)."""
+    return _tree_call(TREE_WINDING, leaf_bytes, node_bytes, queries, beta, 0.0, 1.0, False, 1.0, threads)
+
+
+def _stochastic_tree_call(kernel, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain, seed,
+                          softening_scale, cutoff_scale, periodic, box_length, threads):
+    dev = _device()
+    leaf, node, contrib = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _u8(contrib_bytes, dev)
+    queries = _f32(queries, dev)
+    if queries.ndim != 2 or queries.shape[1] not in (2, 3):
+        raise ValueError("queries must be (M, 2) or (M, 3)")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    if samples_per_subdomain < 1:
+        raise ValueError("samples_per_subdomain must be >= 1")
+    dim = queries.shape[1]
+    vec = kernel in (TREE_FORCE, TREE_SOFT_FORCE)
+    out = torch.empty((queries.shape[0], dim) if vec else queries.shape[0], dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_stochastic_bh_tree(_stream_ptr(dev), dim, kernel, _p(leaf), leaf.numel(), _p(node), node.numel(),
+                                        _p(contrib), contrib.numel(), _p(queries), queries.shape[0], _p(out),
+                                        int(samples_per_subdomain), int(seed), float(softening_scale),
+                                        float(cutoff_scale), int(bool(periodic)), float(box_length), int(threads),
+                                        _p(ws), ws.numel()), "stochastic_bh_tree")
+    return out
+
+
+def stochastic_barnes_hut_gravity(leaf_bytes, node_bytes, contrib_bytes, queries, *, samples_per_subdomain: int = 1,
+                                  seed: int = 0, periodic: bool = False, box_length: float = 1.0, threads: int = 256):
+    return _stochastic_tree_call(TREE_POTENTIAL, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain,
+                                 seed, 0.0, 1.0, periodic, box_length, threads)
+
+
+def stochastic_barnes_hut_force(leaf_bytes, node_bytes, contrib_bytes, queries, *, samples_per_subdomain: int = 1,
+                                seed: int = 0, periodic: bool = False, box_length: float = 1.0, threads: int = 256):
+    return _stochastic_tree_call(TREE_FORCE, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain,
+                                 seed, 0.0, 1.0, periodic, box_length, threads)
+
+
+def softened_stochastic_barnes_hut_force(leaf_bytes, node_bytes, contrib_bytes, queries, *,
+                                         samples_per_subdomain: int = 1, seed: int = 0, softening_scale: float = 1e-2,
+                                         cutoff_scale: float = 1.0, periodic: bool = False, box_length: float = 1.0,
+                                         threads: int = 256):
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    return _stochastic_tree_call(TREE_SOFT_FORCE, leaf_bytes, node_bytes, contrib_bytes, queries,
+                                 samples_per_subdomain, seed, softening_scale, cutoff_scale, periodic, box_length,
+                                 threads)
+
+
+def stochastic_barnes_hut_winding_number(leaf_bytes, node_bytes, contrib_bytes, queries, *,
+                                         samples_per_subdomain: int = 1, seed: int = 0, threads: int = 256):
+    return _stochastic_tree_call(TREE_WINDING, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain,
+                                 seed, 0.0, 1.0, False, 1.0, threads)

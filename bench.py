@@ -1,0 +1,412 @@
+"""Benchmark: force+VJP evaluations per second of softened self-gravity at
+N = 1,048,576 (Plummer sphere, a = 1, truncated at 10a, equal masses,
+epsilon = 1e-3, theta = 0.5 i.e. beta = 2, float32), one evaluation = build
+the native octree + the softened force of every particle + the full adjoint
+(d/d positions and masses of sum w . a for a random cotangent w).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One process per GPU (torchrun for N > 1); every rank evaluates its own
+independent system (replicas, weak scaling; the path needs no collective).
+Timing: CUDA events on the launching stream, L2 flushed (256 MB write)
+between steps outside the timed events, the max over ranks. Rank 0 prints one
+JSON line.
+
+--impl reference times the reference's own CPU path (its Tree3D build and
+evaluateBarnesHut_stackless, compiled from its headers into oracle/_ref)
+with all host threads on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "barnes-hut_b200"))
+
+import sbh_workloads as W  # noqa: E402
+
+N_DEFAULT = 1 << 20
+BETA = 2.0
+EPS = 1e-3
+LEAF = 16
+METRIC = "force+VJP evals/sec at N=1M, rel-L2<=1e-4 vs FP64 direct; batched vs plain"
+WORKLOAD = "plummer_n1048576_eps1e-3_theta0.5_force_plus_full_vjp"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--cpu-sample", type=int, default=32768, help="queries timed by the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=5)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU code (oracle/_ref), bounded sample
+# ---------------------------------------------------------------------------
+def cpu_reference_eval_time(points, masses, sample: int, threads: int):
+    """Seconds for one force+VJP evaluation of the full system by the
+    reference's CPU path, extrapolated from a timed sample of queries."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sbh_oracle as O
+
+    n = points.shape[0]
+    rng = np.random.default_rng(123)
+    idx = np.sort(rng.choice(n, min(sample, n), replace=False))
+    q = points[idx]
+    cot = rng.normal(size=q.shape).astype(np.float32)
+    t0 = time.perf_counter()
+    tree = O.RefTree3D(points, masses, variant=0)  # Tree3D<8,1>: leaf size 8
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tree.eval(q, BETA, O.REF_K_SOFT_FORCE, eps=EPS, threads=threads)
+    t_force = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tree.eval(q, BETA, O.REF_K_SOFT_FORCE_VJP, eps=EPS, cot=cot, threads=threads)
+    t_vjp = time.perf_counter() - t0
+    scale = n / q.shape[0]
+    return t_build + (t_force + t_vjp) * scale, dict(build_s=t_build, force_sample_s=t_force, vjp_sample_s=t_vjp,
+                                                     sample_queries=int(q.shape[0]))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    p, m = W.plummer(args.n, seed=1000)
+    times = []
+    info = {}
+    for s in range(args.warmup + args.steps):
+        t, info = cpu_reference_eval_time(p, m, args.cpu_sample, threads)
+        if s >= args.warmup:
+            times.append(t)
+    t = statistics.mean(times)
+    value = 1.0 / t
+    sample = (f"Tree3D<8,1> build of all {args.n} points + force and query-side VJP of "
+              f"{info['sample_queries']} sampled particles, extrapolated x{args.n / info['sample_queries']:.0f}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer sphere)",
+        "config": {"workload": WORKLOAD, "n": args.n, "beta": BETA, "softening": EPS, "leaf_size": 8,
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "detail": info,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def fp64_direct_subset(points_d, masses_d, idx, eps):
+    """Float64 direct sum at a subset of targets (plain PyTorch, chunked)."""
+    import torch
+
+    p = points_d.double()
+    m = masses_d.double()
+    q = p[idx]
+    out = torch.zeros_like(q)
+    for a in range(0, q.shape[0], 64):
+        d = q[a:a + 64, None, :] - p[None, :, :]
+        r2 = (d * d).sum(-1)
+        c = -m[None, :] * (r2 + eps * eps + 1e-12) ** -1.5
+        out[a:a + 64] = (c[..., None] * d).sum(1)
+    return out
+
+
+def measure_fp32_peak(B, torch, dev):
+    buf = torch.zeros(1024, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    blocks, iters = 148 * 16, 2048
+    for _ in range(2):
+        B.lib().sbh_probe_fp32(stream, buf.data_ptr(), blocks, 64)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    B._check(B.lib().sbh_probe_fp32(stream, buf.data_ptr(), blocks, iters), "probe_fp32")
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    flops = blocks * 256 * 8 * 16 * iters * 2
+    return flops / (ms * 1e-3) / 1e12
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import sbh_b200 as B
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    p, m = W.plummer(n, seed=1000 + rank)
+    w = np.random.default_rng(77 + rank).normal(size=p.shape).astype(np.float32)
+    P = torch.tensor(p, device=dev)
+    M = torch.tensor(m, device=dev)
+    Wt = torch.tensor(w, device=dev)
+    F = torch.empty((n, 3), device=dev)
+    GX = torch.empty((n, 3), device=dev)
+    GM = torch.empty(n, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    prm = B.NativeTree.params(BETA, EPS, 0.0, True)
+    tree = B.NativeTree(dev)
+    tree.build(P, M, leaf_size=LEAF, with_adjoint=True)  # sizes the workspace
+
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+
+    def step(times=None):
+        s0, s1, s2 = ev(), ev(), ev()
+        s0.record()
+        tree.build(P, M, leaf_size=LEAF, with_adjoint=True)
+        s1.record()
+        tree.adjoint_walk(Wt, prm, F)
+        s2.record()
+        tree.adjoint_finalize(GX, GM)
+        return s0, s1, s2
+
+    # accuracy of the timed configuration (outside the timed region)
+    step()
+    torch.cuda.synchronize()
+    idx = torch.tensor(np.random.default_rng(5).choice(n, 1024, replace=False), device=dev)
+    ref = fp64_direct_subset(P, M, idx, EPS)
+    rel = float(torch.linalg.norm(F[idx].double() - ref) / torch.linalg.norm(ref))
+    st = tree.stats()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms, walk_ms = 0.0, 0.0
+    marks = []
+    e_end = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b, c = step()
+        d = ev()
+        d.record()
+        marks.append((a, b, c, d))
+    torch.cuda.synchronize()
+    for a, b, c, d in marks:
+        total_ms += a.elapsed_time(d)
+        walk_ms += b.elapsed_time(c)
+    clocks = sampler.stop()
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * 1000.0 / ms_per_step
+
+    # plain path: separate C-ABI calls with the tree rebuilt for the VJP,
+    # like the reference's custom_vjp recompute flow
+    def plain():
+        t1 = B.NativeTree(dev)
+        t1.build(P, M, leaf_size=LEAF, with_adjoint=False)
+        t1.force(beta=BETA, softening=EPS, out=F)
+        t2 = B.NativeTree(dev)
+        t2.build(P, M, leaf_size=LEAF, with_adjoint=True)
+        t2.force_vjp(Wt, beta=BETA, softening=EPS, want_force=False)
+        torch.cuda.synchronize()
+
+    plain()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        plain()
+    plain_ms = (time.perf_counter() - t0) / 2 * 1e3
+
+    # e2e: host buffers in, host buffers out, through the public API
+    Ph = torch.tensor(p).pin_memory()
+    Mh = torch.tensor(m).pin_memory()
+    Wh = torch.tensor(w).pin_memory()
+    Fh = torch.empty((n, 3)).pin_memory()
+    GXh = torch.empty((n, 3)).pin_memory()
+    GMh = torch.empty(n).pin_memory()
+
+    def e2e_step():
+        Pd = Ph.to(dev, non_blocking=True)
+        Md = Mh.to(dev, non_blocking=True)
+        Wd = Wh.to(dev, non_blocking=True)
+        tree.build(Pd, Md, leaf_size=LEAF, with_adjoint=True)
+        tree.adjoint_walk(Wd, prm, F)
+        tree.adjoint_finalize(GX, GM)
+        Fh.copy_(F, non_blocking=True)
+        GXh.copy_(GX, non_blocking=True)
+        GMh.copy_(GM, non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = ev(), ev()
+        a.record()
+        e2e_step()
+        b.record()
+        torch.cuda.synchronize()
+        e_ms += a.elapsed_time(b)
+    e_ms /= args.steps
+    if world > 1:
+        t = torch.tensor([e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+
+    # roofline of the dominant kernel (the adjoint walk)
+    walk_s = walk_ms / args.steps * 1e-3
+    flops_walk = adjoint_walk_flops(st)
+    fp32_peak = measure_fp32_peak(B, torch, dev)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "adjoint_walk_traffic.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        traffic = tj.get("dram_bytes_per_interaction", 0) * (st["far"] + st["near"]) or None
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            t_eval, info = cpu_reference_eval_time(p, m, args.cpu_sample, threads)
+            cpu = {"value": 1.0 / t_eval, "unit": "evals/s", "cores": threads, "kind": "reference",
+                   "sample": (f"reference Tree3D<8,1> build of all {n} points + force and query-side VJP of "
+                              f"{info['sample_queries']} sampled particles (beta 2), extrapolated to all")}
+        launches = args.steps * (BUILD_LAUNCHES + WALK_LAUNCHES + FINALIZE_LAUNCHES)
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer sphere, a=1, r<10a)",
+            "config": {"workload": WORKLOAD, "n": n, "beta": BETA, "theta": 1.0 / BETA, "softening": EPS,
+                       "leaf_size": LEAF, "far_field": "monopole+quadrupole", "vjp": "positions and masses",
+                       "l2": "flushed between steps (256 MB write, outside the timed events)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "accuracy": {"rel_l2_vs_fp64_direct": rel, "subset": 1024},
+            "plain_vs_batched": {"plain_ms_per_eval": plain_ms, "batched_ms_per_eval": ms_per_step,
+                                 "ratio": plain_ms / ms_per_step},
+            "roofline": {"kernel": "adjoint_walk_kernel<quad>", "bound": "fp32", "achieved": flops_walk / walk_s / 1e12,
+                         "peak": fp32_peak, "unit": "TFLOP/s", "frac": flops_walk / walk_s / 1e12 / fp32_peak,
+                         "peak_source": "measured in this run: sbh_probe_fp32 FMA chains",
+                         "traffic": traffic, "walk_ms": walk_s * 1e3,
+                         "interactions": {"far": st["far"], "near": st["near"]}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * 1000.0 / e_ms, "unit": "evals/s",
+                    "h2d_bytes_per_step": int(n * 28), "d2h_bytes_per_step": int(n * 28)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "tree": {"nodes": st["nodes"], "groups": st["groups"]},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+# Kernels per step of the timed path (counted from the host code):
+# build: bbox 3 + keys 1 + 8 radix passes x (count 1 + scan 3 + scatter 1) +
+#        levels 1 + slots 1 + scan 3 + emit 1 + node count 1 + gather 1 +
+#        moment scan 3 + finalize 1 + offsets 1 + group counts 1 + scan 3 +
+#        roots 1 + group total 1 = 64
+# walk: zero adjoint 1 + walk 1 = 2; finalize: push 1 + scan 3 + combine 1 = 5
+BUILD_LAUNCHES = 64
+WALK_LAUNCHES = 2
+FINALIZE_LAUNCHES = 5
+
+# FP32 flops per interaction of the adjoint walk (force + adjoint, counted
+# from adjoint_walk_kernel): far node (monopole + quadrupole) and near pair.
+ADJ_FLOPS_FAR = 200
+ADJ_FLOPS_NEAR = 55
+
+
+def adjoint_walk_flops(st) -> float:
+    return ADJ_FLOPS_FAR * st["far"] + ADJ_FLOPS_NEAR * st["near"]
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

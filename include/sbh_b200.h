@@ -164,6 +164,11 @@ int sbh_stochastic_bh_force_octree8_vjp(cudaStream_t stream, int softened, const
                                         float box_length, int threads, void* workspace,
                                         size_t workspace_bytes);
 
+/* Measurement helper (no reference counterpart): launches blocks x 256
+ * threads of independent FMA chains; flops = blocks*256*8*16*iters*2. Times
+ * the FP32 pipe peak that the traversal rooflines are reported against. */
+int sbh_probe_fp32(cudaStream_t stream, float* out, int blocks, int iters);
+
 /* Bytes of device workspace every octree8 / Node2 / Node3 traversal needs
  * (the device status word). */
 size_t sbh_traversal_workspace_bytes(void);
@@ -205,6 +210,83 @@ int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void*
                            float softening_scale, float cutoff_scale, int periodic,
                            float box_length, int threads, void* workspace,
                            size_t workspace_bytes);
+
+/* ---------------------------------------------------------------------- */
+/* Native adaptive octree (no reference counterpart: a new B200 path)     */
+/* ---------------------------------------------------------------------- */
+/* Opening rule in the reference's convention (distance / cell diagonal >=
+ * beta, beta = 1/theta, src/sbh_ffi.cu:1878-1893), made conservative for a
+ * group of 32 targets: accept a node when the distance from the group's
+ * bounding box to the node's centre of mass exceeds beta * diagonal + |COM -
+ * cell centre|. The far field is the node monopole plus (quadrupole = 1) its
+ * second moment about the COM; near-field leaves are summed pairwise. */
+typedef struct sbh_native_params {
+  float beta;      /* 1 / theta, > 0 */
+  float softening; /* Plummer softening epsilon, >= 0 */
+  float cutoff;    /* erfc attenuation scale of the short-range split; <= 0 disables */
+  int quadrupole;  /* 1: monopole + quadrupole far field (needs cutoff <= 0), 0: monopole */
+} sbh_native_params;
+
+/* Workspace for a tree of n points in num_systems independent systems. */
+size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int with_normals,
+                                  int with_adjoint);
+
+/* Builds the tree(s) inside `workspace`. points (n x 3), masses (n), normals
+ * (n x 3, optional: winding number). system_offsets: device int64 array of
+ * num_systems + 1 offsets into the concatenated inputs (NULL for one system).
+ * leaf_size in [1, 32]. with_adjoint reserves the scratch of
+ * sbh_native_force_vjp. Later calls on the same workspace evaluate this tree. */
+int sbh_native_build(cudaStream_t stream, const float* points, const float* masses,
+                     const float* normals, int64_t n, const int64_t* system_offsets,
+                     int num_systems, int leaf_size, int with_adjoint, void* workspace,
+                     size_t workspace_bytes);
+
+/* Softened self-gravity of every point of every system: force_out (n x 3,
+ * input order). */
+int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float* force_out,
+                     void* workspace, size_t workspace_bytes);
+
+/* One traversal computing the force (optional force_out) and the full
+ * adjoint of L = sum_i w_i . a_i: grad_points (n x 3) and grad_masses (n),
+ * exact for the evaluated approximation (query side, direct sources, and the
+ * chain rule through every accepted node's mass, centroid and second moment;
+ * opening decisions are recomputed, not stored). */
+int sbh_native_force_vjp(cudaStream_t stream, const sbh_native_params* params,
+                         const float* cotangent, float* force_out, float* grad_points,
+                         float* grad_masses, void* workspace, size_t workspace_bytes);
+
+/* The two phases of sbh_native_force_vjp, for callers that time or overlap
+ * them: the traversal (query-side gradient, per-node and per-particle source
+ * adjoints, optional force) and the finalize pass (node adjoints pushed down
+ * to particles, combined with the traversal's terms, written in input order). */
+int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params,
+                            const float* cotangent, float* force_out, void* workspace,
+                            size_t workspace_bytes);
+int sbh_native_adjoint_finalize(cudaStream_t stream, float* grad_points, float* grad_masses,
+                                void* workspace, size_t workspace_bytes);
+
+/* Query workspace of sbh_native_winding_number. */
+size_t sbh_native_query_workspace_bytes(int64_t nq);
+
+/* Generalized winding number (include/kernel.h:73-80) of the oriented points
+ * of a single-system tree built with normals, at nq query points. Far field:
+ * node mass and mass-weighted mean normal at the COM (as the reference's
+ * trees aggregate them, include/tree3d.h:255-264). out: nq floats. */
+int sbh_native_winding_number(cudaStream_t stream, float beta, const float* queries, int64_t nq,
+                              float* out, void* workspace, size_t workspace_bytes,
+                              void* query_workspace, size_t query_workspace_bytes);
+
+/* Synchronises; out4 = {nodes, target groups, far interactions, near
+ * interactions} of the last build / evaluation on this workspace. */
+int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
+                     uint64_t* out4);
+
+/* Synchronises; copies sorted keys (n x u64), the permutation (n x u32,
+ * sorted slot -> input index) and the 64-byte node records to device buffers
+ * (each may be NULL) and the node count to *num_nodes. */
+int sbh_native_export(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
+                      uint64_t* keys_out, uint32_t* perm_out, void* nodes_out,
+                      size_t nodes_capacity, uint64_t* num_nodes);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -83,7 +83,7 @@ def octree8_fixture(out_dir):
             res[key + "_cot"] = cot
             nq = q.shape[0]
 
-            def run(fn, *args):
+            def run(fn, args):
                 out = torch.zeros((nq, 3), dtype=torch.float32, device=DEV)
                 O.refgpu_check(fn(S(), *args(out)))
                 torch.cuda.synchronize()

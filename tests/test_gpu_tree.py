@@ -1,0 +1,170 @@
+"""GPU parity of the level-3 builder and the Node2 / Node3 targets
+(src/sbh_ffi.cu:192-397, 1422-1680, 2444-3131) against the reference's own
+kernels on the same buffers. The deeper Node3 / Node2 trees come from the
+reference's CPU builders (Tree3D<1,3>, Tree2D<1,3> compiled into oracle/_ref),
+as the reference's own Python does (python/jax_sbh_ffi.py:658-742)."""
+import numpy as np
+import pytest
+import torch
+
+import sbh_b200 as B
+import sbh_oracle as O
+import sbh_workloads as W
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+HAVE_REF = O.available("libsbh_ref_gpu.so")
+needs_ref = pytest.mark.skipif(not HAVE_REF, reason="reference GPU build missing (make -C oracle ref)")
+
+
+def _t(a, dev, dtype=torch.float32):
+    return torch.as_tensor(np.ascontiguousarray(a), device=dev, dtype=dtype)
+
+
+def _S():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _u8(a, dev):
+    return torch.as_tensor(np.ascontiguousarray(a), device=dev, dtype=torch.uint8)
+
+
+def node3_fields(nb):
+    a = np.asarray(nb.cpu() if isinstance(nb, torch.Tensor) else nb).reshape(-1, 4272)
+    u64 = a[:, :32].copy().view(np.uint64)
+    f = a[:, 32:92].copy().view(np.float32)
+    mask = a[:, 96:160].copy().view(np.uint64)
+    child = a[:, 160:4256].copy().view(np.uint64)
+    ints = a[:, 4256:4268].copy().view(np.int32)
+    return dict(u64=u64, f=f, mask=mask, child=child, ints=ints, leaf=a[:, 4268])
+
+
+def ref_level3(dev, p, nrm, m, mn, mx):
+    L = O.refgpu()
+    n = p.shape[0]
+    leaf = torch.zeros(n * 32, dtype=torch.uint8, device=dev)
+    node = torch.zeros(513 * 4272, dtype=torch.uint8, device=dev)
+    contrib = torch.zeros(513 * 32, dtype=torch.uint8, device=dev)
+    P, N, M, MN, MX = _t(p, dev), _t(nrm, dev), _t(m, dev), _t(mn, dev), _t(mx, dev)
+    O.refgpu_check(L.ref_build_octree_level3(_S(), P.data_ptr(), N.data_ptr(), M.data_ptr(), n, MN.data_ptr(),
+                                             MX.data_ptr(), leaf.data_ptr(), leaf.numel(), node.data_ptr(),
+                                             node.numel(), contrib.data_ptr(), contrib.numel()))
+    torch.cuda.synchronize()
+    return leaf, node, contrib
+
+
+@needs_ref
+def test_level3_build_matches_reference(cuda):
+    p, m = W.plummer(6000, seed=3)
+    nrm = np.random.default_rng(1).normal(size=p.shape).astype(np.float32)
+    mn = p.min(0) - np.float32(1e-3)
+    mx = p.max(0) + np.float32(1e-3)
+    leaf, node, contrib = B.build_octree_buffers_with_contrib(p, nrm, m, mn, mx)
+    rleaf, rnode, rcontrib = ref_level3(cuda, p, nrm, m, mn, mx)
+    a, b = node3_fields(node), node3_fields(rnode)
+    np.testing.assert_array_equal(a["u64"], b["u64"])
+    np.testing.assert_array_equal(a["mask"], b["mask"])
+    np.testing.assert_array_equal(a["child"], b["child"])
+    np.testing.assert_array_equal(a["ints"], b["ints"])
+    np.testing.assert_array_equal(a["leaf"], b["leaf"])
+    np.testing.assert_array_equal(a["f"][:, :7], b["f"][:, :7])  # bounds and diameter
+    np.testing.assert_allclose(a["f"][:, 7:], b["f"][:, 7:], rtol=2e-5, atol=1e-6)  # contrib sums
+    la = leaf.cpu().numpy().reshape(-1, 32).copy().view(np.float32)
+    lb = rleaf.cpu().numpy().reshape(-1, 32).copy().view(np.float32)
+    for s, e in b["u64"][1:, :2]:
+        if e > s:
+            assert sorted(map(tuple, la[s:e])) == sorted(map(tuple, lb[s:e]))
+
+
+def _ref_tree_call(fn_name, dev, dim, leaf, node, q, *args, vec):
+    L = O.refgpu()
+    nq = q.shape[0]
+    out = torch.zeros((nq, dim) if vec else nq, device=dev)
+    Q = _t(q, dev)
+    O.refgpu_check(getattr(L, fn_name)(_S(), dim, leaf.data_ptr(), leaf.numel(), node.data_ptr(), node.numel(),
+                                       Q.data_ptr(), nq, out.data_ptr(), *args))
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@needs_ref
+@pytest.mark.parametrize("threads", [64, 256, 96])
+def test_node3_level3_traversals_match_reference(cuda, threads):
+    p, m = W.plummer(3000, seed=5)
+    p = p * np.float32(0.3)
+    leaf, node, contrib = B.build_octree_buffers_with_contrib(p, np.zeros_like(p), m)
+    rng = np.random.default_rng(2)
+    q = np.concatenate([p[:400], rng.uniform(-8, 8, (200, 3)).astype(np.float32)])
+    for beta in (2.0, 0.3):
+        want = _ref_tree_call("ref_barnes_hut_gravity", cuda, 3, leaf, node, q, beta, 0, 1.0, threads, vec=False)
+        got = B.barnes_hut_gravity(leaf, node, q, beta=beta, threads=threads).cpu().numpy()
+        assert rel_l2(got, want) < 1e-6
+        want = _ref_tree_call("ref_barnes_hut_force", cuda, 3, leaf, node, q, beta, 0, 1.0, threads, vec=True)
+        got = B.barnes_hut_force(leaf, node, q, beta=beta, threads=threads).cpu().numpy()
+        assert rel_l2(got, want) < 1e-6
+        want = _ref_tree_call("ref_barnes_hut_force_soft", cuda, 3, leaf, node, q, beta, 5e-2, 1.5, 0, 1.0, threads,
+                              vec=True)
+        got = B.softened_barnes_hut_force(leaf, node, q, beta=beta, softening_scale=5e-2, cutoff_scale=1.5,
+                                          threads=threads).cpu().numpy()
+        assert rel_l2(got, want) < 1e-6
+
+
+@needs_ref
+def test_node3_and_node2_cpu_built_trees_match_reference(cuda):
+    p, m = W.uniform_cube(1500, seed=7)
+    t3 = O.RefTree3D(p, m, variant=2)
+    leaf3, node3 = _u8(t3.leaf_bytes(), cuda), _u8(t3.node_bytes(), cuda)
+    q = p[:300]
+    want = _ref_tree_call("ref_barnes_hut_force", cuda, 3, leaf3, node3, q, 2.0, 0, 1.0, 64, vec=True)
+    got = B.barnes_hut_force(leaf3, node3, q, beta=2.0, threads=64).cpu().numpy()
+    assert rel_l2(got, want) < 1e-6
+    p2 = p[:, :2].copy()
+    t2 = O.RefTree2D(p2, m)
+    leaf2, node2 = _u8(t2.leaf_bytes(), cuda), _u8(t2.node_bytes(), cuda)
+    q2 = p2[:300]
+    want = _ref_tree_call("ref_barnes_hut_gravity", cuda, 2, leaf2, node2, q2, 2.0, 0, 1.0, 64, vec=False)
+    got = B.barnes_hut_gravity(leaf2, node2, q2, beta=2.0, threads=64).cpu().numpy()
+    assert rel_l2(got, want) < 1e-6
+    want = _ref_tree_call("ref_barnes_hut_force_soft", cuda, 2, leaf2, node2, q2, 2.0, 5e-2, 1.5, 0, 1.0, 64, vec=True)
+    got = B.softened_barnes_hut_force(leaf2, node2, q2, beta=2.0, softening_scale=5e-2, cutoff_scale=1.5,
+                                      threads=64).cpu().numpy()
+    assert rel_l2(got, want) < 1e-6
+
+
+@needs_ref
+@pytest.mark.parametrize("dim", [2, 3])
+def test_tree_mlpcv_fixed_seed_matches_reference(cuda, dim):
+    p, m = W.uniform_cube(1200, seed=9)
+    if dim == 3:
+        t = O.RefTree3D(p, m, variant=2)
+    else:
+        p = p[:, :2].copy()
+        t = O.RefTree2D(p, m)
+    leaf, node, contrib = _u8(t.leaf_bytes(), cuda), _u8(t.node_bytes(), cuda), _u8(t.contrib_bytes(), cuda)
+    q = p[:256]
+    L = O.refgpu()
+    Q = _t(q, cuda)
+    for kernel, fn, vec in ((B.TREE_POTENTIAL, "ref_stochastic_bh_gravity", False),
+                            (B.TREE_FORCE, "ref_stochastic_bh_force", True)):
+        out = torch.zeros((256, dim) if vec else 256, device=cuda)
+        O.refgpu_check(getattr(L, fn)(_S(), dim, leaf.data_ptr(), leaf.numel(), node.data_ptr(), node.numel(),
+                                      contrib.data_ptr(), contrib.numel(), Q.data_ptr(), 256, out.data_ptr(), 2, 5, 0,
+                                      1.0, 64))
+        torch.cuda.synchronize()
+        got = B._stochastic_tree_call(kernel, leaf, node, contrib, q, 2, 5, 0.0, 1.0, False, 1.0, 64).cpu().numpy()
+        want = out.cpu().numpy()
+        row = np.abs(got - want).reshape(256, -1).max(1) / np.maximum(np.abs(want).reshape(256, -1).max(1), 1e-30)
+        assert (row < 1e-4).mean() > 0.99
+
+
+def test_node3_winding_number_and_direct_limit(cuda):
+    pts, nrm, w = W.ellipsoid_surface(3000, seed=4)
+    t = O.RefTree3D(pts, w, normals=nrm, variant=2)
+    leaf, node = _u8(t.leaf_bytes(), cuda), _u8(t.node_bytes(), cuda)
+    q = W.uniform_box_queries(512, seed=8)
+    got = B.barnes_hut_winding_number(leaf, node, q, beta=1e30).cpu().numpy()
+    want = O.direct_winding_number(pts, nrm, w, q)
+    assert rel_l2(got, want) < 1e-5
+    bh = B.barnes_hut_winding_number(leaf, node, q, beta=2.0).cpu().numpy()
+    assert np.abs(bh - want).max() < 5e-2

@@ -1,0 +1,100 @@
+"""CPU tests of the native-tree restatement in the oracle: topology
+invariants, the infinite-beta direct limit, and the adjoint (query side,
+direct sources, and the chain rule through node mass, centroid and second
+moment) against central finite differences of the same frozen-plan forward
+in float64."""
+import numpy as np
+import pytest
+
+import sbh_oracle as O
+import sbh_workloads as W
+from conftest import rel_l2
+
+
+def _topology_invariants(T):
+    a = T.arrays()
+    start, end, skip, level = a["start"], a["end"], a["skip"], a["level"]
+    nn = T.num_nodes
+    n = T.points.shape[0]
+    assert start[0] == 0 and end[0] == n and skip[0] == nn
+    leaf = (np.arange(nn) + 1 >= nn) | (skip == np.arange(nn) + 1)
+    # pre-order: a child starts where its parent starts or later, inside it
+    for k in range(1, nn):
+        assert skip[k] > k
+    assert ((end - start)[leaf & (level < 21)] <= T.leaf_size).all()
+    assert ((end - start)[~leaf] > T.leaf_size).all()
+    # leaves partition the particles in order
+    ls, le = start[leaf], end[leaf]
+    assert ls[0] == 0 and le[-1] == n and (ls[1:] == le[:-1]).all()
+    keys = a["keys"]
+    assert (np.diff(keys.astype(np.float64)) >= 0).all()
+    assert sorted(a["perm"].tolist()) == list(range(n))
+
+
+@pytest.mark.parametrize("dist", ["uniform", "plummer", "dupes", "tiny"])
+def test_native_topology_invariants(dist):
+    if dist == "uniform":
+        p, m = W.uniform_cube(3000, seed=1)
+    elif dist == "plummer":
+        p, m = W.plummer(5000, seed=2)
+    elif dist == "dupes":
+        p, m = W.uniform_cube(400, seed=3)
+        p = np.concatenate([p, np.repeat(p[:5], 40, axis=0)])
+        m = np.full(p.shape[0], 1.0 / p.shape[0], np.float32)
+    else:
+        p, m = W.uniform_cube(7, seed=4)
+    T = O.NativeTree(p, m, leaf_size=16)
+    _topology_invariants(T)
+
+
+def test_native_infinite_beta_is_direct():
+    p, m = W.plummer(2000, seed=5)
+    T = O.NativeTree(p, m, leaf_size=16)
+    T.plan(1e30, 32)
+    f, _ = T.force(1e-3)
+    want = O.direct_force_soft(p, m, p, 1e-3)
+    assert rel_l2(f, want) < 1e-12
+
+
+@pytest.mark.parametrize("quad", [False, True])
+def test_native_adjoint_matches_finite_differences(quad):
+    rng = np.random.default_rng(6)
+    p, m = W.plummer(600, seed=6)
+    m = (m * rng.uniform(0.5, 1.5, m.shape)).astype(np.float32)
+    w = rng.normal(size=p.shape).astype(np.float32)
+    eps = 1e-2
+    T = O.NativeTree(p, m, leaf_size=8)
+    T.plan(2.0, 32)
+    dx, dm = T.adjoint(w, eps, quad=quad)
+    p64 = p.astype(np.float64)
+    h = 1e-4
+    idx = rng.choice(p.shape[0], 24, replace=False)
+    for k in idx:
+        for d in range(3):
+            pp = p64.copy()
+            pp[k, d] += h
+            lp = T.force(eps, points=pp.astype(np.float32), masses=m, w=w, quad=quad)[1]
+            pp[k, d] -= 2 * h
+            lm = T.force(eps, points=pp.astype(np.float32), masses=m, w=w, quad=quad)[1]
+            fd = (lp - lm) / (2 * h)
+            assert abs(fd - dx[k, d]) <= 2e-3 * (abs(fd) + 1.0), (k, d, fd, dx[k, d])
+        mm = m.astype(np.float64).copy()
+        dh = 1e-3 * m[k]
+        mm[k] += dh
+        lp = T.force(eps, points=p, masses=mm.astype(np.float32), w=w, quad=quad)[1]
+        mm[k] -= 2 * dh
+        lm = T.force(eps, points=p, masses=mm.astype(np.float32), w=w, quad=quad)[1]
+        fd = (lp - lm) / (2 * dh)
+        assert abs(fd - dm[k]) <= 2e-3 * (abs(fd) + 1.0), (k, fd, dm[k])
+
+
+def test_native_adjoint_approximates_exact_gradient():
+    rng = np.random.default_rng(8)
+    p, m = W.plummer(3000, seed=8)
+    w = rng.normal(size=p.shape).astype(np.float32)
+    T = O.NativeTree(p, m, leaf_size=16)
+    T.plan(2.0, 32)
+    dx, dm = T.adjoint(w, 1e-3, quad=True)
+    ex, em = O.direct_full_adjoint(p, m, w, 1e-3)
+    assert rel_l2(dx, ex) < 1e-3
+    assert rel_l2(dm, em) < 1e-3
