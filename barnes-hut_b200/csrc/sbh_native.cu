@@ -396,7 +396,7 @@ __global__ void finalize_nodes_kernel(NodeRec* __restrict__ nodes, const uint32_
 // Roots (first node of each system) and target groups (runs of <= 32 sorted
 // particles that never cross a system boundary).
 __global__ void roots_groups_kernel(const int64_t* __restrict__ sorted_seg_off, int nseg, const uint32_t* __restrict__ base,
-                                    const uint32_t* __restrict__ group_off, int2* __restrict__ roots,
+                                    const uint32_t* __restrict__ group_off, int64_t cap, int2* __restrict__ roots,
                                     int4* __restrict__ groups) {
   int s = blockIdx.x;
   if (s >= nseg) return;
@@ -404,6 +404,10 @@ __global__ void roots_groups_kernel(const int64_t* __restrict__ sorted_seg_off, 
   uint32_t total = base[sorted_seg_off[nseg]];
   uint32_t r0 = a < b ? base[a] : 0u;
   uint32_t r1 = b < sorted_seg_off[nseg] ? base[b] : total;
+  // never walk past the node array, even if the capacity check tripped
+  uint32_t ucap = static_cast<uint32_t>(cap);
+  r0 = r0 < ucap ? r0 : ucap;
+  r1 = r1 < ucap ? r1 : ucap;
   if (threadIdx.x == 0) roots[s] = make_int2(static_cast<int>(r0), static_cast<int>(a < b ? r1 : r0));
   uint32_t g0 = group_off[s];
   int64_t ng = (b - a + 31) / 32;
@@ -1278,7 +1282,7 @@ int sbh_native_build(cudaStream_t stream, const float* points, const float* mass
   group_counts_kernel<<<(nseg + 255) / 256, 256, 0, stream>>>(L.seg_off, nseg, L.gcount);
   e = exclusive_scan<uint32_t>(stream, ArrayLoad<uint32_t>{L.gcount}, nseg, L.goff, L.scan_tmp, true);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  roots_groups_kernel<<<nseg, 128, 0, stream>>>(L.seg_off, nseg, L.base, L.goff, L.roots, L.groups);
+  roots_groups_kernel<<<nseg, 128, 0, stream>>>(L.seg_off, nseg, L.base, L.goff, L.cap, L.roots, L.groups);
   group_total_kernel<<<1, 1, 0, stream>>>(L.goff, nseg, L.meta);
   if (int rc = check_launch("sbh_native_build")) return rc;
   return register_tree(workspace, h);

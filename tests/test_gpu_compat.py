@@ -248,7 +248,7 @@ def test_octree8_traversals_match_reference_kernels_on_same_buffers(cuda):
     Q, C = _t(q, cuda), _t(cot, cuda)
     nq = q.shape[0]
 
-    def ref(fn, *args):
+    def ref(fn, args):
         out = torch.zeros((nq, 3), device=cuda)
         O.refgpu_check(fn(_S(), *args(out)))
         torch.cuda.synchronize()
