@@ -684,7 +684,7 @@ static void o8_carve(C& c, int64_t n, int depth, O8Params** prm, uint32_t** k0, 
   int64_t st2 = scan_tiles(hist_n);
   *scan_tmp = c.template take<uint32_t>(st > st2 ? st : st2);
   *P = c.template take<DVec<7>>(nn + 1);
-  *ptmp = c.template take<DVec<7>>(scan_tiles(nn));
+  *ptmp = c.template take<DVec<7>>(scan_tiles<DVec<7>>(nn));
 }
 
 }  // namespace sbh

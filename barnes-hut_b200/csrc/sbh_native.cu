@@ -1102,7 +1102,7 @@ void carve(C& c, int64_t n, int nseg, int S, bool normals, bool adjoint, Layout&
   L.base = c.template take<uint32_t>(nn + 1);
   L.nodes = c.template take<NodeRec>(cap);
   L.P = c.template take<DVec<10>>(nn + 1);
-  L.ptmp = c.template take<DVec<10>>(scan_tiles(nn));
+  L.ptmp = c.template take<DVec<10>>(scan_tiles<DVec<10>>(nn));
   L.sp = c.template take<float4>(nn);
   L.sseg = c.template take<uint32_t>(nn);
   L.roots = c.template take<int2>(nseg);
@@ -1111,7 +1111,7 @@ void carve(C& c, int64_t n, int nseg, int S, bool normals, bool adjoint, Layout&
   L.groups = c.template take<int4>(nn / 32 + nseg + 1);
   if (normals) {
     L.PN = c.template take<DVec<3>>(nn + 1);
-    L.pntmp = c.template take<DVec<3>>(scan_tiles(nn));
+    L.pntmp = c.template take<DVec<3>>(scan_tiles<DVec<3>>(nn));
     L.nnrm = c.template take<float4>(cap);
     L.sn = c.template take<float4>(nn);
   } else {
@@ -1125,7 +1125,7 @@ void carve(C& c, int64_t n, int nseg, int S, bool normals, bool adjoint, Layout&
     L.part_adj = c.template take<float>(nn * kPartAdj);
     L.gq = c.template take<float>(nn * 3);
     L.D = c.template take<DVec<14>>(nn + 1);
-    L.dtmp = c.template take<DVec<14>>(scan_tiles(nn + 1));
+    L.dtmp = c.template take<DVec<14>>(scan_tiles<DVec<14>>(nn + 1));
   } else {
     L.node_adj = nullptr;
     L.part_adj = nullptr;

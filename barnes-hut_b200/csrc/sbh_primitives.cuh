@@ -13,8 +13,14 @@
 namespace sbh {
 
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 8;
-constexpr int kScanTile = kScanThreads * kScanItems;  // 2048
+
+// Items per thread: 8 for 4-8 byte elements, fewer for the FP64 moment
+// vectors so a tile stays in registers without spilling.
+template <typename T>
+struct ScanCfg {
+  static constexpr int kItems = sizeof(T) <= 8 ? 8 : (sizeof(T) <= 32 ? 4 : 2);
+  static constexpr int kTile = kScanThreads * kItems;
+};
 
 // K doubles summed component-wise.
 template <int K>
@@ -102,10 +108,11 @@ __device__ T block_exclusive(T x, T* total) {
 // Phase 1: per-tile totals.
 template <typename T, typename Load>
 __global__ void __launch_bounds__(kScanThreads) scan_tile_totals(Load load, int64_t n, T* tile_tot) {
-  int64_t tile0 = static_cast<int64_t>(blockIdx.x) * kScanTile;
+  constexpr int kItems = ScanCfg<T>::kItems;
+  int64_t tile0 = static_cast<int64_t>(blockIdx.x) * ScanCfg<T>::kTile;
   T acc = zero_t<T>();
-  for (int k = 0; k < kScanItems; k++) {
-    int64_t i = tile0 + static_cast<int64_t>(threadIdx.x) * kScanItems + k;
+  for (int k = 0; k < kItems; k++) {
+    int64_t i = tile0 + static_cast<int64_t>(threadIdx.x) * kItems + k;
     if (i < n) acc = acc + load(i);
   }
   T tot;
@@ -138,18 +145,19 @@ template <typename T, typename Load>
 __global__ void __launch_bounds__(kScanThreads) scan_tile_apply(Load load, int64_t n,
                                                                const T* tile_off, T* out,
                                                                int write_total, T* total_out) {
-  int64_t tile0 = static_cast<int64_t>(blockIdx.x) * kScanTile;
-  T items[kScanItems];
+  constexpr int kItems = ScanCfg<T>::kItems;
+  int64_t tile0 = static_cast<int64_t>(blockIdx.x) * ScanCfg<T>::kTile;
+  T items[kItems];
   T acc = zero_t<T>();
-  for (int k = 0; k < kScanItems; k++) {
-    int64_t i = tile0 + static_cast<int64_t>(threadIdx.x) * kScanItems + k;
+  for (int k = 0; k < kItems; k++) {
+    int64_t i = tile0 + static_cast<int64_t>(threadIdx.x) * kItems + k;
     items[k] = i < n ? load(i) : zero_t<T>();
     acc = acc + items[k];
   }
   T tot;
   T run = tile_off[blockIdx.x] + block_exclusive(acc, &tot);
-  for (int k = 0; k < kScanItems; k++) {
-    int64_t i = tile0 + static_cast<int64_t>(threadIdx.x) * kScanItems + k;
+  for (int k = 0; k < kItems; k++) {
+    int64_t i = tile0 + static_cast<int64_t>(threadIdx.x) * kItems + k;
     if (i < n) out[i] = run;
     run = run + items[k];
   }
@@ -160,14 +168,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_tile_apply(Load load, int64
   }
 }
 
-inline int64_t scan_tiles(int64_t n) { return n <= 0 ? 1 : (n + kScanTile - 1) / kScanTile; }
+// Number of tiles (= temporaries of type T) of a scan over n elements of T.
+template <typename T = uint32_t>
+inline int64_t scan_tiles(int64_t n) {
+  return n <= 0 ? 1 : (n + ScanCfg<T>::kTile - 1) / ScanCfg<T>::kTile;
+}
 
 // Exclusive scan of load(0..n-1) into out[0..n-1] (and out[n] = total when
-// write_total). tmp: scan_tiles(n) elements of T.
+// write_total). tmp: scan_tiles<T>(n) elements of T.
 template <typename T, typename Load>
 cudaError_t exclusive_scan(cudaStream_t s, Load load, int64_t n, T* out, T* tmp,
                            bool write_total) {
-  int64_t nt = scan_tiles(n);
+  int64_t nt = scan_tiles<T>(n);
   scan_tile_totals<T, Load><<<static_cast<unsigned>(nt), kScanThreads, 0, s>>>(load, n, tmp);
   scan_tile_offsets<T><<<1, kScanThreads, 0, s>>>(tmp, nt);
   scan_tile_apply<T, Load><<<static_cast<unsigned>(nt), kScanThreads, 0, s>>>(

@@ -512,7 +512,7 @@ void l3_carve(C& c, int64_t n, uint32_t** k0, uint32_t** v0, uint32_t** k1, uint
   *hist = c.template take<uint32_t>(hn);
   *stmp = c.template take<uint32_t>(scan_tiles(hn) + scan_tiles(kLevel3Bins + 1));
   *P = c.template take<DVec<7>>(nn + 1);
-  *ptmp = c.template take<DVec<7>>(scan_tiles(nn));
+  *ptmp = c.template take<DVec<7>>(scan_tiles<DVec<7>>(nn));
 }
 
 unsigned gsz(int64_t n) {

@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--cpu-sample", type=int, default=32768, help="queries timed by the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the forest and winding-number measurements")
     return ap.parse_args()
 
 
@@ -184,6 +185,107 @@ def fp64_direct_subset(points_d, masses_d, idx, eps):
         c = -m[None, :] * (r2 + eps * eps + 1e-12) ** -1.5
         out[a:a + 64] = (c[..., None] * d).sum(1)
     return out
+
+
+def forest_measurement(B, torch, dev, rank, world, flush):
+    """Config 4: 256 Plummer systems, N log-uniform in [1e3, 2e5]. Batched =
+    one forest build + one fused force/adjoint walk for all systems; plain =
+    build, force, rebuild, VJP per system (the recompute flow). Systems are
+    sharded across ranks with no collective."""
+    import sbh_dist
+
+    systems, sizes = W.forest(256, 1000, 200000, seed=0)
+    a, b = sbh_dist.shard_systems(sizes, world, rank)
+    mine = systems[a:b]
+    pts = torch.tensor(np.concatenate([s[0] for s in mine]), device=dev)
+    ms = torch.tensor(np.concatenate([s[1] for s in mine]), device=dev)
+    offs = torch.tensor(sbh_dist.system_offsets([s[0].shape[0] for s in mine]), device=dev)
+    w = torch.randn(pts.shape, device=dev, generator=torch.Generator(device=dev).manual_seed(5))
+    n = pts.shape[0]
+    F, GX, GM = torch.empty_like(pts), torch.empty_like(pts), torch.empty(n, device=dev)
+    prm = B.NativeTree.params(BETA, EPS, 0.0, True)
+    tree = B.NativeTree(dev)
+
+    def batched():
+        tree.build(pts, ms, system_offsets=offs, leaf_size=LEAF, with_adjoint=True)
+        tree.adjoint_walk(w, prm, F)
+        tree.adjoint_finalize(GX, GM)
+
+    trees = [B.NativeTree(dev) for _ in range(2)]
+    views = [(pts[o0:o1], ms[o0:o1], w[o0:o1]) for o0, o1 in zip(offs[:-1].tolist(), offs[1:].tolist())]
+
+    def plain():
+        for p_, m_, w_ in views:
+            trees[0].build(p_, m_, leaf_size=LEAF, with_adjoint=False)
+            trees[0].force(beta=BETA, softening=EPS)
+            trees[1].build(p_, m_, leaf_size=LEAF, with_adjoint=True)
+            trees[1].force_vjp(w_, beta=BETA, softening=EPS, want_force=False)
+
+    # CUDA graph of the batched step (build + walk + finalize, no host sync inside)
+    batched()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s):
+        batched()
+        torch.cuda.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            batched()
+    torch.cuda.current_stream(dev).wait_stream(s)
+    torch.cuda.synchronize()
+
+    def timed(fn, reps):
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / reps
+
+    plain()
+    t_plain = timed(plain, 2)
+    t_batched = timed(batched, 3)
+    t_graph = timed(g.replay, 3)
+    del g
+    return dict(systems=int(b - a), particles=int(n), plain_ms=t_plain, batched_ms=t_batched, graph_ms=t_graph,
+                batched_over_plain=t_plain / t_graph,
+                particle_evals_per_s_graph=n / (t_graph * 1e-3), particle_evals_per_s_plain=n / (t_plain * 1e-3))
+
+
+def winding_measurement(B, torch, dev, flush):
+    """Config 2b: winding number of 262,144 oriented points on the ellipsoid
+    (1, 0.7, 0.5) at 1,048,576 queries uniform in [-1.5, 1.5]^3."""
+    pts, nrm, wgt = W.ellipsoid_surface(262144, seed=2)
+    q = W.uniform_box_queries(1048576, seed=3)
+    inside = torch.tensor(W.ellipsoid_inside(q), device=dev)
+    P, N, M, Q = (torch.tensor(a, device=dev) for a in (pts, nrm, wgt, q))
+    tree = B.NativeTree(dev)
+
+    def step():
+        tree.build(P, M, normals=N, leaf_size=LEAF, with_adjoint=False)
+        return tree.winding_number(Q, beta=BETA)
+
+    out = step()
+    torch.cuda.synchronize()
+    tot = 0.0
+    for _ in range(3):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = step()
+        e1.record()
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    ms = tot / 3
+    err_in = float((out[inside] - 1.0).abs().mean())
+    err_out = float(out[~inside].abs().mean())
+    return dict(sources=262144, queries=1048576, ms=ms, queries_per_s=1048576 / (ms * 1e-3),
+                mean_abs_err_inside=err_in, mean_abs_err_outside=err_out)
 
 
 def measure_fp32_peak(B, torch, dev):
@@ -342,6 +444,12 @@ def run_ours(args):
         tj = json.load(open(tpath))
         traffic = tj.get("dram_bytes_per_interaction", 0) * (st["far"] + st["near"]) or None
 
+    extras = {}
+    if not args.no_extras:
+        extras["forest"] = forest_measurement(B, torch, dev, rank, world, flush)
+        if world == 1:
+            extras["winding_number"] = winding_measurement(B, torch, dev, flush)
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -373,6 +481,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "tree": {"nodes": st["nodes"], "groups": st["groups"]},
+            "extras": extras,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -106,10 +106,12 @@ def test_native_forest_equals_separate_systems(cuda):
         a, b = offs[i], offs[i + 1]
         ti = B.NativeTree().build(p + np.float32(50.0 * i), m, leaf_size=16)
         fi = ti.force(beta=2.0, softening=1e-3).cpu().numpy()
-        np.testing.assert_array_equal(f[a:b], fi)
+        # same tree and groups; node moments differ in the last bits because
+        # the forest's FP64 prefix sums also carry the earlier systems
+        assert rel_l2(f[a:b], fi) < 1e-6
         _, gxi, gmi = ti.force_vjp(w[a:b], beta=2.0, softening=1e-3, want_force=False)
-        np.testing.assert_allclose(gx[a:b].cpu().numpy(), gxi.cpu().numpy(), rtol=1e-5, atol=1e-5)
-        np.testing.assert_allclose(gm[a:b].cpu().numpy(), gmi.cpu().numpy(), rtol=1e-5, atol=1e-5)
+        assert rel_l2(gx[a:b].cpu().numpy(), gxi.cpu().numpy()) < 1e-5
+        assert rel_l2(gm[a:b].cpu().numpy(), gmi.cpu().numpy()) < 1e-5
 
 
 def test_native_winding_number(cuda):
@@ -134,8 +136,9 @@ def test_native_autograd_matches_force_vjp(cuda):
     (f * w).sum().backward()
     t = B.NativeTree().build(p, m, leaf_size=16)
     _, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3)
-    np.testing.assert_allclose(pt.grad.cpu().numpy(), gx.cpu().numpy(), rtol=1e-5, atol=1e-6)
-    np.testing.assert_allclose(mt.grad.cpu().numpy(), gm.cpu().numpy(), rtol=1e-5, atol=1e-6)
+    # the adjoint's FP32 atomics are summed in a run-dependent order
+    assert rel_l2(pt.grad.cpu().numpy(), gx.cpu().numpy()) < 1e-6
+    assert rel_l2(mt.grad.cpu().numpy(), gm.cpu().numpy()) < 1e-6
 
 
 def test_native_empty_and_invalid(cuda):

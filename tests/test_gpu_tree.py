@@ -69,7 +69,10 @@ def test_level3_build_matches_reference(cuda):
     np.testing.assert_array_equal(a["ints"], b["ints"])
     np.testing.assert_array_equal(a["leaf"], b["leaf"])
     np.testing.assert_array_equal(a["f"][:, :7], b["f"][:, :7])  # bounds and diameter
-    np.testing.assert_allclose(a["f"][:, 7:], b["f"][:, 7:], rtol=2e-5, atol=1e-6)  # contrib sums
+    # contrib: the reference sums with FP32 atomics (its root mass here is
+    # 0.99995 instead of 1); ours sums in FP64
+    np.testing.assert_allclose(a["f"][:, 7:], b["f"][:, 7:], rtol=2e-4, atol=2e-6)
+    assert abs(float(a["f"][0, 13]) - float(m.astype(np.float64).sum())) < 1e-6
     la = leaf.cpu().numpy().reshape(-1, 32).copy().view(np.float32)
     lb = rleaf.cpu().numpy().reshape(-1, 32).copy().view(np.float32)
     for s, e in b["u64"][1:, :2]:
