@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -393,11 +394,9 @@ __global__ void finalize_nodes_kernel(NodeRec* __restrict__ nodes, const uint32_
   }
 }
 
-// Roots (first node of each system) and target groups (runs of <= 32 sorted
-// particles that never cross a system boundary).
-__global__ void roots_groups_kernel(const int64_t* __restrict__ sorted_seg_off, int nseg, const uint32_t* __restrict__ base,
-                                    const uint32_t* __restrict__ group_off, int64_t cap, int2* __restrict__ roots,
-                                    int4* __restrict__ groups) {
+// Roots: [first node, end of the nodes) of each system.
+__global__ void roots_kernel(const int64_t* __restrict__ sorted_seg_off, int nseg, const uint32_t* __restrict__ base,
+                             int64_t cap, int2* __restrict__ roots) {
   int s = blockIdx.x;
   if (s >= nseg) return;
   int64_t a = sorted_seg_off[s], b = sorted_seg_off[s + 1];
@@ -409,19 +408,66 @@ __global__ void roots_groups_kernel(const int64_t* __restrict__ sorted_seg_off, 
   r0 = r0 < ucap ? r0 : ucap;
   r1 = r1 < ucap ? r1 : ucap;
   if (threadIdx.x == 0) roots[s] = make_int2(static_cast<int>(r0), static_cast<int>(a < b ? r1 : r0));
-  uint32_t g0 = group_off[s];
-  int64_t ng = (b - a + 31) / 32;
-  for (int64_t g = threadIdx.x; g < ng; g += blockDim.x) {
-    int64_t st = a + 32 * g;
-    int64_t en = st + 32 < b ? st + 32 : b;
-    groups[g0 + g] = make_int4(static_cast<int>(st), static_cast<int>(en), s, 0);
-  }
 }
 
-__global__ void group_counts_kernel(const int64_t* __restrict__ sorted_seg_off, int nseg, uint32_t* __restrict__ gc) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nseg) return;
-  gc[s] = static_cast<uint32_t>((sorted_seg_off[s + 1] - sorted_seg_off[s] + 31) / 32);
+// Target groups packed from the tree. For every node holding more than
+// kGroup particles (or a system root), its children are taken in order and
+// consecutive children holding at most kGroup particles are packed into
+// groups of at most kGroup particles; a child with more particles is packed
+// the same way one level down, and a leaf with more than kGroup particles
+// (coincident points at level 21) is cut into runs. Each group lies inside
+// the cell of a node with more than kGroup particles, so its bounding box is
+// compact (runs of consecutive Morton positions can straddle distant cells).
+// Slots come from an atomic counter: the group order varies between runs,
+// each group's result does not.
+__device__ __forceinline__ void emit_group(int4* groups, uint32_t* count, int64_t cap, int s, int e, int sys,
+                                           uint32_t* status) {
+  uint32_t slot = atomicAdd(count, 1u);
+  if (slot < cap)
+    groups[slot] = make_int4(s, e, sys, 0);
+  else
+    raise_status(status, SBH_DEV_ITER_LIMIT);
+}
+
+__global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
+                                   const uint32_t* __restrict__ sseg, int4* __restrict__ groups, int64_t cap,
+                                   uint32_t* __restrict__ count, uint32_t* status) {
+  uint32_t nn = *nn_ptr;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    int4 t = nodes[k].topo;
+    int cnt = t.y - t.x;
+    bool leaf = (t.w & kLeafFlag) != 0;
+    bool root = (t.w & 0xFF) == 0;
+    int sys = sseg ? static_cast<int>(sseg[t.x]) : 0;
+    if (leaf) {
+      if (root || cnt > kGroup)
+        for (int s = t.x; s < t.y; s += kGroup) emit_group(groups, count, cap, s, min(s + kGroup, t.y), sys, status);
+      continue;
+    }
+    if (cnt <= kGroup) {
+      if (root) emit_group(groups, count, cap, t.x, t.y, sys, status);
+      continue;
+    }
+    int run_s = -1, run_e = -1;
+    for (uint32_t c = k + 1; c < static_cast<uint32_t>(t.z) && c < nn;) {
+      int4 tc = nodes[c].topo;
+      int cc = tc.y - tc.x;
+      if (cc > kGroup) {
+        if (run_s >= 0) emit_group(groups, count, cap, run_s, run_e, sys, status);
+        run_s = -1;
+      } else {
+        if (run_s >= 0 && tc.y - run_s > kGroup) {
+          emit_group(groups, count, cap, run_s, run_e, sys, status);
+          run_s = -1;
+        }
+        if (run_s < 0) run_s = tc.x;
+        run_e = tc.y;
+      }
+      if (static_cast<uint32_t>(tc.z) <= c) break;  // malformed skip: never loop
+      c = static_cast<uint32_t>(tc.z);
+    }
+    if (run_s >= 0) emit_group(groups, count, cap, run_s, run_e, sys, status);
+  }
 }
 
 __global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, int64_t n,
@@ -444,7 +490,6 @@ __global__ void node_count_kernel(const uint32_t* base, int64_t n, int64_t cap, 
   meta[3] = total > cap ? 1u : 0u;
 }
 
-__global__ void group_total_kernel(const uint32_t* goff, int nseg, uint32_t* meta) { meta[1] = goff[nseg]; }
 
 __global__ void single_offsets_kernel(int64_t* seg_off, int64_t n) {
   seg_off[0] = 0;
@@ -468,7 +513,20 @@ struct WalkTargets {
   const int4* groups;        // (start, end, system, 0), <= 32 targets each
   const uint32_t* ngroups;   // device-side group count
   int self;                  // targets are the sources (skip i == j pairs)
+  uint32_t* counter;         // work counter, zero at launch
+  uint32_t capacity;         // entries of groups (bounds the device-side count)
 };
+
+// Persistent walks: the grid holds as many warps as the SMs keep resident,
+// and each warp takes its next group from an atomic counter until none is
+// left, so a warp that drew cheap groups keeps working while another is
+// still on an expensive one (group costs in one tree differ by 10x and
+// more between the core and the halo of a clustered distribution).
+__device__ __forceinline__ uint32_t next_group(const WalkTargets& G) {
+  uint32_t s = 0;
+  if ((threadIdx.x & 31) == 0) s = atomicAdd(G.counter, 1u);
+  return __shfl_sync(0xffffffffu, s, 0);
+}
 
 struct WalkParams {
   float beta;
@@ -526,9 +584,11 @@ template <bool QUAD, bool CUT>
 __global__ void __launch_bounds__(128)
     force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
                       unsigned long long* __restrict__ counters) {
-  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (gw >= static_cast<int>(*G.ngroups)) return;
+  const uint32_t ng = min(*G.ngroups, G.capacity);
+  for (;;) {
+  uint32_t gw = next_group(G);
+  if (gw >= ng) break;
   int4 gr = G.groups[gw];
   int i = gr.x + lane;
   bool active = i < gr.y;
@@ -620,6 +680,7 @@ __global__ void __launch_bounds__(128)
     atomicAdd(&counters[0], nfar * na);
     atomicAdd(&counters[1], nnear * na);
   }
+  }
 }
 
 // Sum V = 4 values over the warp with 6 shuffles: afterwards lane 8*v holds
@@ -692,9 +753,11 @@ __global__ void __launch_bounds__(128)
     adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
                         float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
                         float* __restrict__ part_adj, unsigned long long* __restrict__ counters) {
-  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (gw >= static_cast<int>(*G.ngroups)) return;
+  const uint32_t ng = min(*G.ngroups, G.capacity);
+  for (;;) {
+  uint32_t gw = next_group(G);
+  if (gw >= ng) break;
   int4 gr = G.groups[gw];
   int i = gr.x + lane;
   bool active = i < gr.y;
@@ -848,6 +911,7 @@ __global__ void __launch_bounds__(128)
       out[3 * o + 2] = fz;
     }
   }
+  }
 }
 
 // Node adjoints -> difference arrays over each node's particle range. Per
@@ -929,9 +993,11 @@ __global__ void adjoint_combine_kernel(const float4* __restrict__ sp, const uint
 __global__ void __launch_bounds__(128)
     wn_walk_kernel(WalkTree T, WalkTargets G, float beta, float* __restrict__ out,
                    unsigned long long* __restrict__ counters) {
-  int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
-  if (gw >= static_cast<int>(*G.ngroups)) return;
+  const uint32_t ng = min(*G.ngroups, G.capacity);
+  for (;;) {
+  uint32_t gw = next_group(G);
+  if (gw >= ng) break;
   int4 gr = G.groups[gw];
   int i = gr.x + lane;
   bool active = i < gr.y;
@@ -982,6 +1048,7 @@ __global__ void __launch_bounds__(128)
     unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
     atomicAdd(&counters[0], nfar * na);
     atomicAdd(&counters[1], nnear * na);
+  }
   }
 }
 
@@ -1056,9 +1123,8 @@ struct Layout {
   uint32_t* sseg;   // sorted slot -> system
   int64_t* seg_off;
   int2* roots;
-  uint32_t* gcount;
-  uint32_t* goff;
   int4* groups;
+  uint32_t* work;  // persistent-walk work counters
   uint32_t* meta;  // [0] node count, [1] group count, [2] which ping-pong buffer holds perm
   unsigned long long* counters;
   // adjoint scratch
@@ -1106,9 +1172,8 @@ void carve(C& c, int64_t n, int nseg, int S, bool normals, bool adjoint, Layout&
   L.sp = c.template take<float4>(nn);
   L.sseg = c.template take<uint32_t>(nn);
   L.roots = c.template take<int2>(nseg);
-  L.gcount = c.template take<uint32_t>(nseg + 1);
-  L.goff = c.template take<uint32_t>(nseg + 1);
-  L.groups = c.template take<int4>(nn / 32 + nseg + 1);
+  L.groups = c.template take<int4>(nn + nseg + 1);
+  L.work = c.template take<uint32_t>(4);
   if (normals) {
     L.PN = c.template take<DVec<3>>(nn + 1);
     L.pntmp = c.template take<DVec<3>>(scan_tiles<DVec<3>>(nn));
@@ -1278,12 +1343,11 @@ int sbh_native_build(cudaStream_t stream, const float* points, const float* mass
     e = cudaMemsetAsync(L.base, 0, sizeof(uint32_t), stream);
     if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   }
-  // roots and target groups
-  group_counts_kernel<<<(nseg + 255) / 256, 256, 0, stream>>>(L.seg_off, nseg, L.gcount);
-  e = exclusive_scan<uint32_t>(stream, ArrayLoad<uint32_t>{L.gcount}, nseg, L.goff, L.scan_tmp, true);
-  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  roots_groups_kernel<<<nseg, 128, 0, stream>>>(L.seg_off, nseg, L.base, L.goff, L.cap, L.roots, L.groups);
-  group_total_kernel<<<1, 1, 0, stream>>>(L.goff, nseg, L.meta);
+  // system roots and target groups (meta[1] counts the groups)
+  roots_kernel<<<nseg, 32, 0, stream>>>(L.seg_off, nseg, L.base, L.cap, L.roots);
+  if (n > 0)
+    group_nodes_kernel<<<gs(static_cast<int64_t>(L.cap)), 256, 0, stream>>>(
+        L.nodes, L.meta, nseg > 1 ? L.sseg : nullptr, L.groups, n + nseg + 1, L.meta + 1, status);
   if (int rc = check_launch("sbh_native_build")) return rc;
   return register_tree(workspace, h);
 }
@@ -1314,11 +1378,52 @@ __global__ void zero_node_adj_kernel(float* adj, const uint32_t* meta) {
 
 WalkTree tree_view(const Layout& L) { return WalkTree{L.nodes, L.sp, L.sn, L.nnrm, L.roots}; }
 
-WalkTargets self_targets(const Layout& L) { return WalkTargets{L.sp, L.v0, L.groups, L.meta + 1, 1}; }
+WalkTargets self_targets(const Layout& L, int64_t n, int nseg) {
+  return WalkTargets{L.sp, L.v0, L.groups, L.meta + 1, 1, L.work, static_cast<uint32_t>(n + nseg + 1)};
+}
 
-unsigned walk_blocks(int64_t n, int nseg) {
-  int64_t warps = n / 32 + nseg + 1;
-  return static_cast<unsigned>((warps + 3) / 4);
+// Blocks of a persistent walk: resident blocks per SM x SMs, and no more
+// than one warp per possible group. Occupancy is queried per kernel and
+// device once (a host-side query; nothing is enqueued).
+template <typename K>
+unsigned walk_blocks(K kernel, int64_t max_groups) {
+  struct Key {
+    const void* k;
+    int dev;
+    bool operator<(const Key& o) const { return k < o.k || (k == o.k && dev < o.dev); }
+  };
+  static std::mutex mu;
+  static std::map<Key, unsigned> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  Key key{reinterpret_cast<const void*>(kernel), dev};
+  unsigned resident = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) resident = it->second;
+  }
+  if (resident == 0) {
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, 0) != cudaSuccess || per_sm <= 0)
+      per_sm = 4;
+    resident = static_cast<unsigned>(sms * per_sm);
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = resident;
+  }
+  int64_t need = (max_groups + 3) / 4;
+  if (need < 1) need = 1;
+  return need < resident ? static_cast<unsigned>(need) : resident;
+}
+
+// Zeroes the work counter and launches a persistent walk over the groups.
+template <typename K, typename... A>
+cudaError_t launch_walk(cudaStream_t stream, uint32_t* counter, int64_t max_groups, K kernel, A... args) {
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  kernel<<<walk_blocks(kernel, max_groups), 128, 0, stream>>>(args...);
+  return cudaGetLastError();
 }
 
 int check_params(const sbh_native_params* p) {
@@ -1349,14 +1454,12 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   cudaError_t e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   WalkParams wp = walk_params(params);
-  unsigned nb = walk_blocks(h.n, h.nseg);
+  int64_t mg = h.n + h.nseg;
   bool cut = params->cutoff > 0.0f;
-  if (params->quadrupole)
-    force_walk_kernel<true, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, force_out, L.counters);
-  else if (cut)
-    force_walk_kernel<false, true><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, force_out, L.counters);
-  else
-    force_walk_kernel<false, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, force_out, L.counters);
+  auto k = params->quadrupole ? force_walk_kernel<true, false>
+                              : (cut ? force_walk_kernel<false, true> : force_walk_kernel<false, false>);
+  e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h.n, h.nseg), wp, force_out, L.counters);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_force");
 }
 
@@ -1375,17 +1478,12 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
   WalkParams wp = walk_params(params);
-  unsigned nb = walk_blocks(n, h.nseg);
   bool cut = params->cutoff > 0.0f;
-  if (params->quadrupole)
-    adjoint_walk_kernel<true, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, cotangent, force_out,
-                                                             L.gq, L.node_adj, L.part_adj, L.counters);
-  else if (cut)
-    adjoint_walk_kernel<false, true><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, cotangent, force_out,
-                                                             L.gq, L.node_adj, L.part_adj, L.counters);
-  else
-    adjoint_walk_kernel<false, false><<<nb, 128, 0, stream>>>(tree_view(L), self_targets(L), wp, cotangent,
-                                                              force_out, L.gq, L.node_adj, L.part_adj, L.counters);
+  auto k = params->quadrupole ? adjoint_walk_kernel<true, false>
+                              : (cut ? adjoint_walk_kernel<false, true> : adjoint_walk_kernel<false, false>);
+  e = launch_walk(stream, L.work, n + h.nseg, k, tree_view(L), self_targets(L, h.n, h.nseg), wp, cotangent, force_out, L.gq,
+                  L.node_adj, L.part_adj, L.counters);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_adjoint_walk");
 }
 
@@ -1470,9 +1568,9 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
   e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  WalkTargets G{tp, qperm, groups, qmeta, 0};
-  unsigned nb = static_cast<unsigned>((nq / 32 + 1 + 3) / 4);
-  wn_walk_kernel<<<nb, 128, 0, stream>>>(tree_view(L), G, beta, out, L.counters);
+  WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / 32 + 1)};
+  e = launch_walk(stream, qmeta + 2, nq / 32 + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_winding_number");
 }
 

@@ -493,10 +493,9 @@ def run_ours(args):
 # Kernels per step of the timed path (counted from the host code):
 # build: bbox 3 + keys 1 + 8 radix passes x (count 1 + scan 3 + scatter 1) +
 #        levels 1 + slots 1 + scan 3 + emit 1 + node count 1 + gather 1 +
-#        moment scan 3 + finalize 1 + offsets 1 + group counts 1 + scan 3 +
-#        roots 1 + group total 1 = 64
+#        moment scan 3 + finalize 1 + offsets 1 + roots 1 + groups 1 = 59
 # walk: zero adjoint 1 + walk 1 = 2; finalize: push 1 + scan 3 + combine 1 = 5
-BUILD_LAUNCHES = 64
+BUILD_LAUNCHES = 59
 WALK_LAUNCHES = 2
 FINALIZE_LAUNCHES = 5
 

@@ -756,6 +756,8 @@ typedef struct {
   int32_t* far_idx;
   int64_t* near_off;
   int32_t* near_idx; /* near-field leaf node ids */
+  int64_t* gstart;
+  int64_t* gend;
 } NativeTree;
 
 static void cell_geometry(const NativeTree* t, int64_t nd, uint64_t key) {
@@ -809,6 +811,8 @@ void orc_native_free(void* h) {
   free(t->far_idx);
   free(t->near_off);
   free(t->near_idx);
+  free(t->gstart);
+  free(t->gend);
   free(t);
 }
 
@@ -969,6 +973,76 @@ static int native_accept(const NativeTree* t, int64_t k, const float* X, const f
  * Mass-zero nodes are skipped. Returns the total interaction count
  * (sum over groups of active targets x (accepted nodes + near particles)).
  */
+/*
+ * Target groups packed from the tree: for every node holding more than G
+ * particles (or the root), its children are taken in order and consecutive
+ * children holding at most G particles are packed into groups of at most G
+ * particles; a child with more than G particles is split the same way one
+ * level down, and a leaf with more than G particles (coincident points) is
+ * cut into runs of G. Each group lies inside the cell of a node with more
+ * than G particles, so its bounding box stays compact.
+ * Writes group starts/ends (sorted positions) and returns the count.
+ */
+static int64_t native_node_groups(const NativeTree* t, int G, int64_t* gs, int64_t* ge) {
+  int64_t ng = 0;
+  if (t->nn == 0) return 0;
+  for (int64_t k = 0; k < t->nn; k++) {
+    int32_t cnt = t->end[k] - t->start[k];
+    int is_leaf = (k + 1 >= t->nn) || (t->skip[k] == k + 1);
+    int is_root = t->level[k] == 0;
+    if (is_leaf) {
+      if (is_root || cnt > G) {
+        /* root leaf or oversized leaf: runs of G (a root leaf holds <= leaf_size) */
+        for (int32_t s = t->start[k]; s < t->end[k]; s += G) {
+          gs[ng] = s;
+          ge[ng] = s + G < t->end[k] ? s + G : t->end[k];
+          ng++;
+        }
+      }
+      continue;
+    }
+    if (cnt <= G) {
+      if (is_root) {
+        gs[ng] = t->start[k];
+        ge[ng] = t->end[k];
+        ng++;
+      }
+      continue;
+    }
+    /* children of k: k+1, skip[k+1], ... until skip[k] */
+    int64_t run_s = -1, run_e = -1;
+    for (int64_t c = k + 1; c < t->skip[k]; c = t->skip[c]) {
+      int32_t cc = t->end[c] - t->start[c];
+      if (cc > G) {
+        if (run_s >= 0) {
+          gs[ng] = run_s;
+          ge[ng] = run_e;
+          ng++;
+          run_s = -1;
+        }
+        continue;
+      }
+      if (run_s >= 0 && (t->end[c] - run_s) > G) {
+        gs[ng] = run_s;
+        ge[ng] = run_e;
+        ng++;
+        run_s = -1;
+      }
+      if (run_s < 0) run_s = t->start[c];
+      run_e = t->end[c];
+    }
+    if (run_s >= 0) {
+      gs[ng] = run_s;
+      ge[ng] = run_e;
+      ng++;
+    }
+  }
+  return ng;
+}
+
+int g_orc_group_mode = 1; /* 1: node-packed groups (the CUDA walk's definition), 0: runs of G sorted particles */
+void orc_native_set_group_mode(int mode) { g_orc_group_mode = mode; }
+
 int64_t orc_native_plan(void* h, const float* pts, const float* masses, double beta,
                         int group_size) {
   NativeTree* t = (NativeTree*)h;
@@ -978,7 +1052,20 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
   free(t->near_off);
   free(t->near_idx);
   t->group_size = group_size;
-  int64_t ng = (n + group_size - 1) / group_size;
+  free(t->gstart);
+  free(t->gend);
+  t->gstart = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
+  t->gend = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
+  int64_t ng;
+  if (g_orc_group_mode == 1) {
+    ng = native_node_groups(t, group_size, t->gstart, t->gend);
+  } else {
+    ng = (n + group_size - 1) / group_size;
+    for (int64_t g = 0; g < ng; g++) {
+      t->gstart[g] = g * group_size;
+      t->gend[g] = g * group_size + group_size < n ? g * group_size + group_size : n;
+    }
+  }
   t->ngroups = ng;
   double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
   native_moments(t, pts, masses, mom);
@@ -992,7 +1079,7 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
   for (int64_t g = 0; g < ng; g++) {
     t->far_off[g] = nf;
     t->near_off[g] = nr;
-    int64_t s0 = g * group_size, s1 = s0 + group_size < n ? s0 + group_size : n;
+    int64_t s0 = t->gstart[g], s1 = t->gend[g];
     float gmin[3] = {INFINITY, INFINITY, INFINITY}, gmax[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int64_t i = s0; i < s1; i++)
       for (int d = 0; d < 3; d++) {
@@ -1054,7 +1141,7 @@ void orc_native_eval(void* h, const float* pts, const float* masses, double eps,
   double L = 0.0;
 #pragma omp parallel for schedule(dynamic, 8) reduction(+ : L)
   for (int64_t g = 0; g < t->ngroups; g++) {
-    int64_t s0 = g * t->group_size, s1 = s0 + t->group_size < n ? s0 + t->group_size : n;
+    int64_t s0 = t->gstart[g], s1 = t->gend[g];
     for (int64_t i = s0; i < s1; i++) {
       int64_t qi = t->perm[i];
       double q[3] = {pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]};
@@ -1111,7 +1198,7 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
   memset(dx, 0, sizeof(double) * 3 * n);
   memset(dm, 0, sizeof(double) * n);
   for (int64_t g = 0; g < t->ngroups; g++) {
-    int64_t s0 = g * t->group_size, s1 = s0 + t->group_size < n ? s0 + t->group_size : n;
+    int64_t s0 = t->gstart[g], s1 = t->gend[g];
     for (int64_t i = s0; i < s1; i++) {
       int64_t qi = t->perm[i];
       double q[3] = {pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]};
@@ -1179,4 +1266,18 @@ void orc_native_plan_stats(void* h, int64_t* ngroups, int64_t* nfar, int64_t* nn
   *ngroups = t->ngroups;
   *nfar = t->far_off ? t->far_off[t->ngroups] : 0;
   *nnear = t->near_off ? t->near_off[t->ngroups] : 0;
+}
+
+/* Per-group list lengths of the recorded plan: far nodes and near particles. */
+void orc_native_group_costs(void* h, int64_t* far, int64_t* near_particles) {
+  NativeTree* t = (NativeTree*)h;
+  for (int64_t g = 0; g < t->ngroups; g++) {
+    far[g] = t->far_off[g + 1] - t->far_off[g];
+    int64_t np_ = 0;
+    for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
+      int32_t k = t->near_idx[e];
+      np_ += t->end[k] - t->start[k];
+    }
+    near_particles[g] = np_;
+  }
 }

@@ -62,6 +62,8 @@ def test_native_force_matches_oracle_same_plan(cuda):
         inter = T.plan(2.0, 32)
         want, _ = T.force(1e-3, quad=quad)
         assert rel_l2(f, want) < 1e-5, quad
+        # same node-packed target groups
+        assert st["groups"] == T.plan_stats()[0]
         # same opening decisions up to ulp-level ties
         assert abs((st["far"] + st["near"]) - inter) <= 1e-4 * inter
 
