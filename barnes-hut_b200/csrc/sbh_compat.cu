@@ -26,6 +26,7 @@
 #include <curand_kernel.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "sbh_common.cuh"
@@ -934,6 +935,74 @@ int sbh_stochastic_bh_force_octree8_vjp(cudaStream_t stream, int softened, const
   return o8_launch_stochastic(true, softened, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, cotangent,
                               out, samples_per_subdomain, seed, beta, softening_scale, cutoff_scale, prune_enabled,
                               prune_r_cut_mult, periodic, box_length, threads, workspace, workspace_bytes);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// octree8 build with library-owned scratch (no allocation by the caller or
+// by the library at call time)
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory when they need a tree: an XLA
+// custom call running under JAX's default preallocation (the framework holds
+// most of the GPU, so a cudaMalloc from inside the handler can fail), code
+// that runs with a fixed, pre-reserved memory budget, or a caller that must
+// not trigger the implicit device synchronisation a cudaMalloc may cause.
+// For them this variant of sbh_build_octree8 takes its temporaries from one
+// fixed array that is part of the library image. Every GPU that loads the
+// library holds these bytes until the process exits. The build clears what
+// must start at zero (status word, cell counters) on every call, so what an
+// earlier call left in the array does not matter. Calls that may overlap on
+// the GPU (two streams, or two host threads) share the array and race: the
+// caller serialises them.
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;  // 16 MiB
+__device__ __align__(256) unsigned char g_o8_static_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mu;
+void* g_static_addr[128] = {};  // device address of the array, per device ordinal
+
+// Device address of the scratch on the current device. On the host the
+// array's name only stands for the device symbol; the address a kernel can
+// use comes from cudaGetSymbolAddress with that device current.
+int static_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  if (dev < 0 || dev >= 128) return fail(SBH_ERR_CUDA, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_o8_static_scratch);
+    if (e != cudaSuccess || !p) return fail(SBH_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_static_addr[dev] = p;
+  }
+  *out = g_static_addr[dev];
+  return SBH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t sbh_build_octree8_static_scratch_bytes(void) { return kStaticScratchBytes; }
+
+int sbh_build_octree8_static(cudaStream_t stream, const float* points, const float* normals, const float* masses,
+                             int64_t n, const float* min_corner, const float* max_corner, int max_depth,
+                             void* leaf_out, size_t leaf_bytes, void* node_out, size_t node_bytes, void* contrib_out,
+                             size_t contrib_bytes) {
+  if (max_depth < 1 || max_depth > 10) return invalid("max_depth must be in [1, 10]");
+  if (n < 0) return invalid("number of points must be >= 0");
+  size_t need = sbh_build_octree8_workspace_bytes(n, max_depth);
+  if (need > kStaticScratchBytes)
+    return invalid("n = " + std::to_string(n) + " at max_depth = " + std::to_string(max_depth) + " needs " +
+                   std::to_string(need) + " bytes of scratch; the built-in scratch holds " +
+                   std::to_string(kStaticScratchBytes) + " (use sbh_build_octree8 with a workspace)");
+  void* ws = nullptr;
+  if (int rc = static_scratch(&ws)) return rc;
+  return sbh_build_octree8(stream, points, normals, masses, n, min_corner, max_corner, max_depth, leaf_out, leaf_bytes,
+                           node_out, node_bytes, contrib_out, contrib_bytes, ws, kStaticScratchBytes);
 }
 
 }  // extern "C"

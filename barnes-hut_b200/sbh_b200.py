@@ -91,6 +91,9 @@ _SIGS = {
     "sbh_direct_force_soft_vjp": ([_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f, _c_i, _c_f, _c_i],
                                   _c_i),
     "sbh_build_octree8_workspace_bytes": ([_c_i64, _c_i], _c_sz),
+    "sbh_build_octree8_static_scratch_bytes": ([], _c_sz),
+    "sbh_build_octree8_static": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p,
+                                  _c_sz], _c_i),
     "sbh_build_octree8": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz,
                            _c_p, _c_sz], _c_i),
     "sbh_barnes_hut_force_octree8": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_f, _c_i, _c_f, _c_i,

@@ -113,6 +113,29 @@ int sbh_build_octree8(cudaStream_t stream, const float* points, const float* nor
                       size_t leaf_bytes, void* node_out, size_t node_bytes, void* contrib_out,
                       size_t contrib_bytes, void* workspace, size_t workspace_bytes);
 
+/* No counterpart in the reference. Same result as sbh_build_octree8, for
+ * callers that cannot allocate device memory at call time (an XLA custom
+ * call under JAX's preallocating allocator, a fixed memory budget, code that
+ * must avoid the implicit synchronisation of cudaMalloc): the temporaries
+ * live in a 16 MiB array that is part of the library and stays resident on
+ * every GPU that loads it. Nothing is allocated. Sizes whose
+ * sbh_build_octree8_workspace_bytes(n, max_depth) exceeds
+ * sbh_build_octree8_static_scratch_bytes() are rejected with
+ * SBH_ERR_INVALID_ARGUMENT (for example n = 200,000 fits at max_depth 6,
+ * n = 100,000 at max_depth 7). The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and caches it. Each call
+ * clears what must start at zero (status word, cell counters) itself. All
+ * calls share the one array, so calls that may overlap on the GPU
+ * (different streams, or several host threads) race and must be serialised
+ * by the caller. An invalid bounds span is recorded in the array's status
+ * word, which this entry point does not expose. */
+size_t sbh_build_octree8_static_scratch_bytes(void);
+int sbh_build_octree8_static(cudaStream_t stream, const float* points, const float* normals,
+                             const float* masses, int64_t n, const float* min_corner,
+                             const float* max_corner, int max_depth, void* leaf_out,
+                             size_t leaf_bytes, void* node_out, size_t node_bytes,
+                             void* contrib_out, size_t contrib_bytes);
+
 /* Replaces BarnesHutForceOctree8 (src/sbh_ffi.cu:3133-3181). */
 int sbh_barnes_hut_force_octree8(cudaStream_t stream, const void* leaf, size_t leaf_bytes,
                                  const void* nodes, size_t node_bytes, const float* queries,
