@@ -374,14 +374,13 @@ __global__ void finalize_nodes_kernel(NodeRec* __restrict__ nodes, const uint32_
     } else {
       for (int d = 0; d < 3; d++) X[d] = ctr[d];
     }
-    float dx = __fsub_rn(X[0], ctr[0]), dy = __fsub_rn(X[1], ctr[1]), dz = __fsub_rn(X[2], ctr[2]);
-    float delta = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
     float diag = __fmul_rn(side, 1.7320508f);
     NodeRec r;
     r.com = make_float4(X[0], X[1], X[2], static_cast<float>(M));
-    r.aux = make_float4(static_cast<float>(S[4]), static_cast<float>(S[5]), diag, delta);
+    r.cell = make_float4(ctr[0], ctr[1], ctr[2], diag);
     r.quad = make_float4(static_cast<float>(S[0]), static_cast<float>(S[1]), static_cast<float>(S[2]),
                          static_cast<float>(S[3]));
+    r.quad2 = make_float4(static_cast<float>(S[4]), static_cast<float>(S[5]), 0.0f, 0.0f);
     r.topo = t;
     nodes[k] = r;
     if (nnrm && PN) {
@@ -534,26 +533,58 @@ struct WalkParams {
   float cutoff;  // <= 0: no attenuation
 };
 
-// Group bounding box: min/max over the active lanes (inactive lanes carry the
-// group's first target, which is inside the box).
-__device__ __forceinline__ void group_box(float4 q, float* gmin, float* gmax) {
-  float v[3] = {q.x, q.y, q.z};
-  for (int d = 0; d < 3; d++) {
-    float lo = v[d], hi = v[d];
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
-    gmin[d] = lo;
-    gmax[d] = hi;
+// Targets of one group as a lane holds them: slots lane and lane + 32.
+// Inactive slots carry the group's first target (inside the group box) and
+// a zero cotangent or mass, so they add nothing to the sums over the warp.
+struct LaneTargets {
+  float x[kTPL], y[kTPL], z[kTPL];
+  int idx[kTPL];
+  bool act[kTPL];
+};
+
+__device__ __forceinline__ void load_targets(const WalkTargets& G, const int4& gr, int lane, LaneTargets& Q) {
+#pragma unroll
+  for (int t = 0; t < kTPL; t++) {
+    int i = gr.x + lane + 32 * t;
+    Q.act[t] = i < gr.y;
+    Q.idx[t] = i;
+    float4 q = G.tp[Q.act[t] ? i : gr.x];
+    Q.x[t] = q.x;
+    Q.y[t] = q.y;
+    Q.z[t] = q.z;
   }
 }
 
-// Acceptance test, IEEE operations in the oracle's order (no contraction).
-__device__ __forceinline__ bool accept_node(const float4& com, float diag, float delta, const float* gmin,
-                                            const float* gmax, float beta) {
-  float rc = __fadd_rn(__fmul_rn(diag, beta), delta);
-  float x[3] = {com.x, com.y, com.z};
+// Group bounding box: min/max over every slot of the warp.
+__device__ __forceinline__ void group_box(const LaneTargets& Q, float* gmin, float* gmax) {
+  float lo[3] = {Q.x[0], Q.y[0], Q.z[0]}, hi[3] = {Q.x[0], Q.y[0], Q.z[0]};
+#pragma unroll
+  for (int t = 1; t < kTPL; t++) {
+    lo[0] = fminf(lo[0], Q.x[t]);
+    lo[1] = fminf(lo[1], Q.y[t]);
+    lo[2] = fminf(lo[2], Q.z[t]);
+    hi[0] = fmaxf(hi[0], Q.x[t]);
+    hi[1] = fmaxf(hi[1], Q.y[t]);
+    hi[2] = fmaxf(hi[2], Q.z[t]);
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+    gmin[d] = lo[d];
+    gmax[d] = hi[d];
+  }
+}
+
+// Acceptance test: the reference's rule |q - cell centre| / diag >= beta
+// (include/tree3d.h:134-153, src/sbh_ffi.cu:1878-1893) made to hold for every
+// target of the group: dist(group box, cell centre) > beta * diag. IEEE
+// operations in the oracle's order (no contraction).
+__device__ __forceinline__ bool accept_node(const float4& cell, const float* gmin, const float* gmax, float beta) {
+  float rc = __fmul_rn(cell.w, beta);
+  float x[3] = {cell.x, cell.y, cell.z};
   float t[3];
   for (int d = 0; d < 3; d++) {
     float a = __fsub_rn(gmin[d], x[d]);
@@ -576,115 +607,133 @@ __device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, f
 }
 
 // Flop accounting used by the roofline (FP32 operations counted from the
-// formulas below, an FMA as 2): force walk near pair 20, far node 55
-// (monopole + quadrupole); adjoint walk (force + adjoint) near pair 55, far
-// node 200 including the 16-value warp reduction.
+// formulas below, an FMA as 2, per target): force walk near pair 20, far
+// node 55 (monopole + quadrupole); adjoint walk (force + adjoint) near pair
+// 55, far node 200 including the share of the warp reductions.
 
 template <bool QUAD, bool CUT>
 __global__ void __launch_bounds__(128)
     force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
                       unsigned long long* __restrict__ counters) {
-  int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
   const uint32_t ng = min(*G.ngroups, G.capacity);
   for (;;) {
-  uint32_t gw = next_group(G);
-  if (gw >= ng) break;
-  int4 gr = G.groups[gw];
-  int i = gr.x + lane;
-  bool active = i < gr.y;
-  float4 q = G.tp[active ? i : gr.x];
-  float gmin[3], gmax[3];
-  group_box(q, gmin, gmax);
-  int2 rt = T.roots[gr.z];
-  float fx = 0.f, fy = 0.f, fz = 0.f;                        // far field
-  float nx = 0.f, ny = 0.f, nz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;  // near field, compensated
-  unsigned long long nfar = 0, nnear = 0;
-  int k = rt.x;
-  while (k < rt.y) {
-    const NodeRec* nd = T.nodes + k;
-    int4 tp = __ldg(&nd->topo);
-    float4 A = __ldg(&nd->com);
-    if (A.w == 0.0f) {
-      k = tp.z;
-      continue;
-    }
-    float4 X = __ldg(&nd->aux);
-    if (accept_node(A, X.z, X.w, gmin, gmax, P.beta)) {
-      float rx = q.x - A.x, ry = q.y - A.y, rz = q.z - A.z;
-      float r2 = rx * rx + ry * ry + rz * rz;
-      float ir = rsqrtf(r2 + P.eps2);
-      float ih = ir * ir;
-      float ir3 = ir * ih;
-      float c = -A.w * ir3;
-      if (CUT) {
-        float att, cc;
-        attenuation(r2, ir3, P.cutoff, att, cc);
-        c *= att;
+    uint32_t gw = next_group(G);
+    if (gw >= ng) break;
+    int4 gr = G.groups[gw];
+    LaneTargets Q;
+    load_targets(G, gr, lane, Q);
+    float gmin[3], gmax[3];
+    group_box(Q, gmin, gmax);
+    int2 rt = T.roots[gr.z];
+    float fx[kTPL], fy[kTPL], fz[kTPL];                                     // far field
+    float nx[kTPL], ny[kTPL], nz[kTPL], cx[kTPL], cy[kTPL], cz[kTPL];       // near field, compensated
+#pragma unroll
+    for (int t = 0; t < kTPL; t++) fx[t] = fy[t] = fz[t] = nx[t] = ny[t] = nz[t] = cx[t] = cy[t] = cz[t] = 0.f;
+    unsigned long long nfar = 0, nnear = 0;
+    int k = rt.x;
+    while (k < rt.y) {
+      const NodeRec* nd = T.nodes + k;
+      int4 tp = __ldg(&nd->topo);
+      float4 A = __ldg(&nd->com);
+      if (A.w == 0.0f) {
+        k = tp.z;
+        continue;
       }
-      if (QUAD) {
-        float4 Q = __ldg(&nd->quad);
-        // a_q = ir5 (3 S r + 1.5 tr(S) r) - 7.5 (r.S.r) ir7 r
-        float sx = Q.x * rx + Q.w * ry + X.x * rz;
-        float sy = Q.w * rx + Q.y * ry + X.y * rz;
-        float sz = X.x * rx + X.y * ry + Q.z * rz;
-        float rsr = rx * sx + ry * sy + rz * sz;
-        float ir5 = ir3 * ih;
-        float tr = Q.x + Q.y + Q.z;
-        float cr = c + ir5 * (1.5f * tr - 7.5f * rsr * ih);
-        float c3 = 3.0f * ir5;
-        fx += cr * rx + c3 * sx;
-        fy += cr * ry + c3 * sy;
-        fz += cr * rz + c3 * sz;
-      } else {
-        fx += c * rx;
-        fy += c * ry;
-        fz += c * rz;
-      }
-      nfar++;
-      k = tp.z;
-    } else if (tp.w & kLeafFlag) {
-      float ax = 0.f, ay = 0.f, az = 0.f;
-      for (int j = tp.x; j < tp.y; j++) {
-        float4 s = __ldg(&T.sp[j]);
-        float rx = q.x - s.x, ry = q.y - s.y, rz = q.z - s.z;
-        float r2 = rx * rx + ry * ry + rz * rz;
-        float ir = rsqrtf(r2 + P.eps2);
-        float ir3 = ir * ir * ir;
-        float c = -s.w * ir3;
-        if (CUT) {
-          float att, cc;
-          attenuation(r2, ir3, P.cutoff, att, cc);
-          c *= att;
+      if (accept_node(__ldg(&nd->cell), gmin, gmax, P.beta)) {
+        float4 Qd = make_float4(0.f, 0.f, 0.f, 0.f), X = Qd;
+        if (QUAD) {
+          Qd = __ldg(&nd->quad);
+          X = __ldg(&nd->quad2);
         }
-        ax += c * rx;
-        ay += c * ry;
-        az += c * rz;
+#pragma unroll
+        for (int t = 0; t < kTPL; t++) {
+          float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+          float r2 = rx * rx + ry * ry + rz * rz;
+          float ir = rsqrtf(r2 + P.eps2);
+          float ih = ir * ir;
+          float ir3 = ir * ih;
+          float c = -A.w * ir3;
+          if (CUT) {
+            float att, cc;
+            attenuation(r2, ir3, P.cutoff, att, cc);
+            c *= att;
+          }
+          if (QUAD) {
+            // a_q = ir5 (3 S r + 1.5 tr(S) r) - 7.5 (r.S.r) ir7 r
+            float sx = Qd.x * rx + Qd.w * ry + X.x * rz;
+            float sy = Qd.w * rx + Qd.y * ry + X.y * rz;
+            float sz = X.x * rx + X.y * ry + Qd.z * rz;
+            float rsr = rx * sx + ry * sy + rz * sz;
+            float ir5 = ir3 * ih;
+            float tr = Qd.x + Qd.y + Qd.z;
+            float cr = c + ir5 * (1.5f * tr - 7.5f * rsr * ih);
+            float c3 = 3.0f * ir5;
+            fx[t] += cr * rx + c3 * sx;
+            fy[t] += cr * ry + c3 * sy;
+            fz[t] += cr * rz + c3 * sz;
+          } else {
+            fx[t] += c * rx;
+            fy[t] += c * ry;
+            fz[t] += c * rz;
+          }
+        }
+        nfar++;
+        k = tp.z;
+      } else if (tp.w & kLeafFlag) {
+        float ax[kTPL], ay[kTPL], az[kTPL];
+#pragma unroll
+        for (int t = 0; t < kTPL; t++) ax[t] = ay[t] = az[t] = 0.f;
+        for (int j = tp.x; j < tp.y; j++) {
+          float4 s = __ldg(&T.sp[j]);
+#pragma unroll
+          for (int t = 0; t < kTPL; t++) {
+            float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
+            float r2 = rx * rx + ry * ry + rz * rz;
+            float ir = rsqrtf(r2 + P.eps2);
+            float ir3 = ir * ir * ir;
+            float c = -s.w * ir3;
+            if (CUT) {
+              float att, cc;
+              attenuation(r2, ir3, P.cutoff, att, cc);
+              c *= att;
+            }
+            ax[t] += c * rx;
+            ay[t] += c * ry;
+            az[t] += c * rz;
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < kTPL; t++) {
+          kahan_add(nx[t], cx[t], ax[t]);
+          kahan_add(ny[t], cy[t], ay[t]);
+          kahan_add(nz[t], cz[t], az[t]);
+        }
+        nnear += static_cast<unsigned long long>(tp.y - tp.x);
+        k = tp.z;
+      } else {
+        k++;
       }
-      kahan_add(nx, cx, ax);
-      kahan_add(ny, cy, ay);
-      kahan_add(nz, cz, az);
-      nnear += static_cast<unsigned long long>(tp.y - tp.x);
-      k = tp.z;
-    } else {
-      k++;
     }
-  }
-  if (active) {
-    uint32_t o = G.perm[i];
-    out[3 * o] = fx + nx;
-    out[3 * o + 1] = fy + ny;
-    out[3 * o + 2] = fz + nz;
-  }
-  if (counters && lane == 0) {
-    unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
-    atomicAdd(&counters[0], nfar * na);
-    atomicAdd(&counters[1], nnear * na);
-  }
+#pragma unroll
+    for (int t = 0; t < kTPL; t++) {
+      if (Q.act[t]) {
+        uint32_t o = G.perm[Q.idx[t]];
+        out[3 * o] = fx[t] + nx[t];
+        out[3 * o + 1] = fy[t] + ny[t];
+        out[3 * o + 2] = fz[t] + nz[t];
+      }
+    }
+    if (counters && lane == 0) {
+      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
+      atomicAdd(&counters[0], nfar * na);
+      atomicAdd(&counters[1], nnear * na);
+    }
   }
 }
 
-// Sum V = 4 values over the warp with 6 shuffles: afterwards lane 8*v holds
-// the warp total of value v (v = 0..3).
+// Sum 4 values over the warp with 6 shuffles: afterwards lane 8*v holds the
+// warp total of value v (v = 0..3).
 __device__ __forceinline__ float reduce4(float v0, float v1, float v2, float v3) {
   int lane = threadIdx.x & 31;
   bool b4 = lane & 16;
@@ -702,215 +751,243 @@ __device__ __forceinline__ float reduce4(float v0, float v1, float v2, float v3)
   return v;  // lane with bits (b4, b3): value 2*b4 + b3
 }
 
-// Sum 16 values over the warp with 16 shuffles: afterwards lane 2*v holds
-// the total of value v (v = 0..15).
-__device__ __forceinline__ float reduce16(float* v) {
+__device__ __forceinline__ int reduce4_index(int lane) { return ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1); }
+
+// Sum 10 values over the warp with 12 shuffles (a transposed butterfly: at
+// each step a lane keeps one half of its values and receives its partner's
+// share of that half). Afterwards lane l holds the warp total of value
+// reduce10_index(l); lanes where that is -1 hold padding.
+__device__ __forceinline__ float reduce10(const float* v) {
   int lane = threadIdx.x & 31;
-  // step 16: keep 8
   bool b = lane & 16;
-  float h[8];
+  float h[6];
 #pragma unroll
-  for (int j = 0; j < 8; j++) {
-    float send = b ? v[j] : v[8 + j];
-    float keep = b ? v[8 + j] : v[j];
+  for (int j = 0; j < 5; j++) {
+    float send = b ? v[j] : v[j + 5];
+    float keep = b ? v[j + 5] : v[j];
     h[j] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
   }
+  h[5] = 0.f;
   b = lane & 8;
   float g[4];
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    float send = b ? h[j] : h[4 + j];
-    float keep = b ? h[4 + j] : h[j];
+  for (int j = 0; j < 3; j++) {
+    float send = b ? h[j] : h[j + 3];
+    float keep = b ? h[j + 3] : h[j];
     g[j] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
   }
+  g[3] = 0.f;
   b = lane & 4;
-  float f[2];
+  float e[2];
 #pragma unroll
   for (int j = 0; j < 2; j++) {
-    float send = b ? g[j] : g[2 + j];
-    float keep = b ? g[2 + j] : g[j];
-    f[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    float send = b ? g[j] : g[j + 2];
+    float keep = b ? g[j + 2] : g[j];
+    e[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
   }
   b = lane & 2;
-  float send = b ? f[0] : f[1];
-  float e = (b ? f[1] : f[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
-  e += __shfl_xor_sync(0xffffffffu, e, 1);
-  return e;  // value index = 8*b4 + 4*b3 + 2*b2 + b1
+  float send = b ? e[0] : e[1];
+  float d = (b ? e[1] : e[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
+  d += __shfl_xor_sync(0xffffffffu, d, 1);
+  return d;
 }
 
-__device__ __forceinline__ int reduce16_index(int lane) {
-  return ((lane >> 4) & 1) * 8 + ((lane >> 3) & 1) * 4 + ((lane >> 2) & 1) * 2 + ((lane >> 1) & 1);
+// Value index held by lane l after reduce10: value (c + 3 b3) + 5 b4 with
+// c = b1 + 2 b2, for even lanes with c < 3 and c + 3 b3 < 5; otherwise -1.
+__device__ __forceinline__ int reduce10_index(int lane) {
+  if (lane & 1) return -1;
+  int c = ((lane >> 1) & 1) + 2 * ((lane >> 2) & 1);
+  if (c >= 3) return -1;
+  int hj = c + 3 * ((lane >> 3) & 1);
+  if (hj >= 5) return -1;
+  return hj + 5 * ((lane >> 4) & 1);
 }
 
-__device__ __forceinline__ int reduce4_index(int lane) { return ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1); }
-
-// Fused force + adjoint walk. Per target lane: the query-side gradient
+// Fused force + adjoint walk. Per target slot: the query-side gradient
 // (written to gq in sorted order); per accepted node: A_X, A_M, G summed over
-// the warp and added to node_adj; per near source particle: (dx, dm) summed
-// over the warp and added to part_adj. Forces are written when out != null.
+// the group and added to node_adj; per near source particle: (dx, dm) summed
+// over the group and added to part_adj. Forces are written when out != null.
+// Every node-side term is linear in the cotangent, so inactive slots (zero
+// cotangent) add nothing.
 template <bool QUAD, bool CUT>
 __global__ void __launch_bounds__(128)
     adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
                         float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
                         float* __restrict__ part_adj, unsigned long long* __restrict__ counters) {
-  int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
   const uint32_t ng = min(*G.ngroups, G.capacity);
+  const int r4 = reduce4_index(lane), r10 = reduce10_index(lane);
   for (;;) {
-  uint32_t gw = next_group(G);
-  if (gw >= ng) break;
-  int4 gr = G.groups[gw];
-  int i = gr.x + lane;
-  bool active = i < gr.y;
-  float4 q = G.tp[active ? i : gr.x];
-  uint32_t o = active ? G.perm[i] : 0u;
-  float wx = active ? cot[3 * o] : 0.f, wy = active ? cot[3 * o + 1] : 0.f, wz = active ? cot[3 * o + 2] : 0.f;
-  float gmin[3], gmax[3];
-  group_box(q, gmin, gmax);
-  int2 rt = T.roots[gr.z];
-  float gx = 0.f, gy = 0.f, gz = 0.f;   // query-side gradient
-  float fx = 0.f, fy = 0.f, fz = 0.f;   // force
-  unsigned long long nfar = 0, nnear = 0;
-  int r4 = reduce4_index(lane), r16 = reduce16_index(lane);
-  int k = rt.x;
-  while (k < rt.y) {
-    const NodeRec* nd = T.nodes + k;
-    int4 tp = __ldg(&nd->topo);
-    float4 A = __ldg(&nd->com);
-    if (A.w == 0.0f) {
-      k = tp.z;
-      continue;
-    }
-    float4 X = __ldg(&nd->aux);
-    if (accept_node(A, X.z, X.w, gmin, gmax, P.beta)) {
-      float rx = q.x - A.x, ry = q.y - A.y, rz = q.z - A.z;
-      float r2 = rx * rx + ry * ry + rz * rz;
-      float ir = rsqrtf(r2 + P.eps2);
-      float ih = ir * ir;
-      float ir3 = ir * ih;
-      float ir5 = ir3 * ih;
-      float rw = rx * wx + ry * wy + rz * wz;
-      float att = 1.0f, cc = 0.0f;
-      if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
-      // per unit mass: phi = -att ir3 r ; J^T w = -att ir3 w + (3 att ir5 + cc) (r.w) r
-      float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
-      float jx = -lin * wx + rad * rx, jy = -lin * wy + rad * ry, jz = -lin * wz + rad * rz;
-      float v[16];
-      float M = A.w;
-      float qx_ = M * jx, qy_ = M * jy, qz_ = M * jz;
-      float am = -lin * rw;  // phi . w
-      if (out) {
-        float c = -M * lin;
-        fx += c * rx;
-        fy += c * ry;
-        fz += c * rz;
-      }
+    uint32_t gw = next_group(G);
+    if (gw >= ng) break;
+    int4 gr = G.groups[gw];
+    LaneTargets Q;
+    load_targets(G, gr, lane, Q);
+    float wx[kTPL], wy[kTPL], wz[kTPL];
+    uint32_t o[kTPL];
 #pragma unroll
-      for (int j = 0; j < 16; j++) v[j] = 0.f;
-      if (QUAD) {
-        float4 Q = __ldg(&nd->quad);
-        float Sxx = Q.x, Syy = Q.y, Szz = Q.z, Sxy = Q.w, Sxz = X.x, Syz = X.y;
-        float sx = Sxx * rx + Sxy * ry + Sxz * rz;
-        float sy = Sxy * rx + Syy * ry + Syz * rz;
-        float sz = Sxz * rx + Syz * ry + Szz * rz;
-        float swx = Sxx * wx + Sxy * wy + Sxz * wz;
-        float swy = Sxy * wx + Syy * wy + Syz * wz;
-        float swz = Sxz * wx + Syz * wy + Szz * wz;
-        float tr = Sxx + Syy + Szz;
-        float rsr = rx * sx + ry * sy + rz * sz;
-        float sxw = sx * wx + sy * wy + sz * wz;
-        float ir7 = ir5 * ih, ir9 = ir7 * ih;
-        // J_q^T w of the quadrupole term
-        float a1 = 5.0f * ir7 * rw;
-        float a2 = 7.5f * ir7 * rsr;
-        float a3 = 7.5f * (2.0f * ir7 * sxw - 7.0f * ir9 * rsr * rw);
-        float jqx = ir5 * (3.0f * swx + 1.5f * tr * wx) - a1 * (3.0f * sx + 1.5f * tr * rx) - a2 * wx - a3 * rx;
-        float jqy = ir5 * (3.0f * swy + 1.5f * tr * wy) - a1 * (3.0f * sy + 1.5f * tr * ry) - a2 * wy - a3 * ry;
-        float jqz = ir5 * (3.0f * swz + 1.5f * tr * wz) - a1 * (3.0f * sz + 1.5f * tr * rz) - a2 * wz - a3 * rz;
-        qx_ += jqx;
-        qy_ += jqy;
-        qz_ += jqz;
-        // G = sym d(w . a_q)/dS
-        float ga = 1.5f * ir5, gb = 1.5f * ir5 * rw, gc = 7.5f * ir7 * rw;
-        v[4] = 2.0f * ga * wx * rx + gb - gc * rx * rx;
-        v[5] = 2.0f * ga * wy * ry + gb - gc * ry * ry;
-        v[6] = 2.0f * ga * wz * rz + gb - gc * rz * rz;
-        v[7] = ga * (wx * ry + rx * wy) - gc * rx * ry;
-        v[8] = ga * (wx * rz + rx * wz) - gc * rx * rz;
-        v[9] = ga * (wy * rz + ry * wz) - gc * ry * rz;
+    for (int t = 0; t < kTPL; t++) {
+      o[t] = Q.act[t] ? G.perm[Q.idx[t]] : 0u;
+      wx[t] = Q.act[t] ? cot[3 * o[t]] : 0.f;
+      wy[t] = Q.act[t] ? cot[3 * o[t] + 1] : 0.f;
+      wz[t] = Q.act[t] ? cot[3 * o[t] + 2] : 0.f;
+    }
+    float gmin[3], gmax[3];
+    group_box(Q, gmin, gmax);
+    int2 rt = T.roots[gr.z];
+    float gx[kTPL], gy[kTPL], gz[kTPL];  // query-side gradient
+    float fx[kTPL], fy[kTPL], fz[kTPL];  // force
+#pragma unroll
+    for (int t = 0; t < kTPL; t++) gx[t] = gy[t] = gz[t] = fx[t] = fy[t] = fz[t] = 0.f;
+    unsigned long long nfar = 0, nnear = 0;
+    int k = rt.x;
+    while (k < rt.y) {
+      const NodeRec* nd = T.nodes + k;
+      int4 tp = __ldg(&nd->topo);
+      float4 A = __ldg(&nd->com);
+      if (A.w == 0.0f) {
+        k = tp.z;
+        continue;
+      }
+      if (accept_node(__ldg(&nd->cell), gmin, gmax, P.beta)) {
+        float4 Qd = make_float4(0.f, 0.f, 0.f, 0.f), X = Qd;
+        if (QUAD) {
+          Qd = __ldg(&nd->quad);
+          X = __ldg(&nd->quad2);
+        }
+        const float M = A.w;
+        float v[10];
+#pragma unroll
+        for (int j = 0; j < 10; j++) v[j] = 0.f;
+#pragma unroll
+        for (int t = 0; t < kTPL; t++) {
+          float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+          float r2 = rx * rx + ry * ry + rz * rz;
+          float ir = rsqrtf(r2 + P.eps2);
+          float ih = ir * ir;
+          float ir3 = ir * ih;
+          float ir5 = ir3 * ih;
+          float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
+          float att = 1.0f, cc = 0.0f;
+          if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
+          // per unit mass: phi = -att ir3 r ; J^T w = -att ir3 w + (3 att ir5 + cc) (r.w) r
+          float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
+          float jx = -lin * wx[t] + rad * rx, jy = -lin * wy[t] + rad * ry, jz = -lin * wz[t] + rad * rz;
+          float qx_ = M * jx, qy_ = M * jy, qz_ = M * jz;
+          v[3] -= lin * rw;  // phi . w
+          if (out) {
+            float c = -M * lin;
+            fx[t] += c * rx;
+            fy[t] += c * ry;
+            fz[t] += c * rz;
+          }
+          if (QUAD) {
+            float Sxx = Qd.x, Syy = Qd.y, Szz = Qd.z, Sxy = Qd.w, Sxz = X.x, Syz = X.y;
+            float sx = Sxx * rx + Sxy * ry + Sxz * rz;
+            float sy = Sxy * rx + Syy * ry + Syz * rz;
+            float sz = Sxz * rx + Syz * ry + Szz * rz;
+            float swx = Sxx * wx[t] + Sxy * wy[t] + Sxz * wz[t];
+            float swy = Sxy * wx[t] + Syy * wy[t] + Syz * wz[t];
+            float swz = Sxz * wx[t] + Syz * wy[t] + Szz * wz[t];
+            float tr = Sxx + Syy + Szz;
+            float rsr = rx * sx + ry * sy + rz * sz;
+            float sxw = sx * wx[t] + sy * wy[t] + sz * wz[t];
+            float ir7 = ir5 * ih, ir9 = ir7 * ih;
+            // J_q^T w of the quadrupole term
+            float a1 = 5.0f * ir7 * rw;
+            float a2 = 7.5f * ir7 * rsr;
+            float a3 = 7.5f * (2.0f * ir7 * sxw - 7.0f * ir9 * rsr * rw);
+            qx_ += ir5 * (3.0f * swx + 1.5f * tr * wx[t]) - a1 * (3.0f * sx + 1.5f * tr * rx) - a2 * wx[t] - a3 * rx;
+            qy_ += ir5 * (3.0f * swy + 1.5f * tr * wy[t]) - a1 * (3.0f * sy + 1.5f * tr * ry) - a2 * wy[t] - a3 * ry;
+            qz_ += ir5 * (3.0f * swz + 1.5f * tr * wz[t]) - a1 * (3.0f * sz + 1.5f * tr * rz) - a2 * wz[t] - a3 * rz;
+            // G = sym d(w . a_q)/dS
+            float ga = 1.5f * ir5, gb = 1.5f * ir5 * rw, gc = 7.5f * ir7 * rw;
+            v[4] += 2.0f * ga * wx[t] * rx + gb - gc * rx * rx;
+            v[5] += 2.0f * ga * wy[t] * ry + gb - gc * ry * ry;
+            v[6] += 2.0f * ga * wz[t] * rz + gb - gc * rz * rz;
+            v[7] += ga * (wx[t] * ry + rx * wy[t]) - gc * rx * ry;
+            v[8] += ga * (wx[t] * rz + rx * wz[t]) - gc * rx * rz;
+            v[9] += ga * (wy[t] * rz + ry * wz[t]) - gc * ry * rz;
+            if (out) {
+              float cr = ir5 * (1.5f * tr - 7.5f * rsr * ih);
+              float c3 = 3.0f * ir5;
+              fx[t] += cr * rx + c3 * sx;
+              fy[t] += cr * ry + c3 * sy;
+              fz[t] += cr * rz + c3 * sz;
+            }
+          }
+          gx[t] += qx_;
+          gy[t] += qy_;
+          gz[t] += qz_;
+          v[0] -= qx_;
+          v[1] -= qy_;
+          v[2] -= qz_;
+        }
+        float tot = reduce10(v);
+        if (r10 >= 0) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r10], tot);
+        nfar++;
+        k = tp.z;
+      } else if (tp.w & kLeafFlag) {
+        for (int j = tp.x; j < tp.y; j++) {
+          float4 s = __ldg(&T.sp[j]);
+          float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+          for (int t = 0; t < kTPL; t++) {
+            float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
+            float r2 = rx * rx + ry * ry + rz * rz;
+            float ir = rsqrtf(r2 + P.eps2);
+            float ih = ir * ir;
+            float ir3 = ir * ih;
+            float ir5 = ir3 * ih;
+            float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
+            float att = 1.0f, cc = 0.0f;
+            if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
+            float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
+            float jx = -lin * wx[t] + rad * rx, jy = -lin * wy[t] + rad * ry, jz = -lin * wz[t] + rad * rz;
+            bool use = Q.act[t] && !(G.self && j == Q.idx[t]);
+            float m = use ? s.w : 0.0f;
+            gx[t] += m * jx;
+            gy[t] += m * jy;
+            gz[t] += m * jz;
+            if (out) {
+              float c = -m * lin;
+              fx[t] += c * rx;
+              fy[t] += c * ry;
+              fz[t] += c * rz;
+            }
+            a0 -= m * jx;
+            a1 -= m * jy;
+            a2 -= m * jz;
+            a3 += use ? -lin * rw : 0.0f;
+          }
+          float tot = reduce4(a0, a1, a2, a3);
+          if ((lane & 7) == 0) atomicAdd(&part_adj[static_cast<int64_t>(j) * kPartAdj + r4], tot);
+        }
+        nnear += static_cast<unsigned long long>(tp.y - tp.x);
+        k = tp.z;
+      } else {
+        k++;
+      }
+    }
+    if (counters && lane == 0) {
+      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
+      atomicAdd(&counters[0], nfar * na);
+      atomicAdd(&counters[1], nnear * na);
+    }
+#pragma unroll
+    for (int t = 0; t < kTPL; t++) {
+      if (Q.act[t]) {
+        int64_t i = Q.idx[t];
+        gq[3 * i] = gx[t];
+        gq[3 * i + 1] = gy[t];
+        gq[3 * i + 2] = gz[t];
         if (out) {
-          float ir5b = ir5;
-          float cr = ir5b * (1.5f * tr - 7.5f * rsr * ih);
-          float c3 = 3.0f * ir5b;
-          fx += cr * rx + c3 * sx;
-          fy += cr * ry + c3 * sy;
-          fz += cr * rz + c3 * sz;
+          out[3 * o[t]] = fx[t];
+          out[3 * o[t] + 1] = fy[t];
+          out[3 * o[t] + 2] = fz[t];
         }
       }
-      gx += qx_;
-      gy += qy_;
-      gz += qz_;
-      v[0] = -qx_;
-      v[1] = -qy_;
-      v[2] = -qz_;
-      v[3] = am;
-      if (!active) {
-#pragma unroll
-        for (int j = 0; j < 16; j++) v[j] = 0.f;
-      }
-      float tot = reduce16(v);
-      if ((lane & 1) == 0 && r16 < 10) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r16], tot);
-      nfar++;
-      k = tp.z;
-    } else if (tp.w & kLeafFlag) {
-      for (int j = tp.x; j < tp.y; j++) {
-        float4 s = __ldg(&T.sp[j]);
-        float rx = q.x - s.x, ry = q.y - s.y, rz = q.z - s.z;
-        float r2 = rx * rx + ry * ry + rz * rz;
-        float ir = rsqrtf(r2 + P.eps2);
-        float ih = ir * ir;
-        float ir3 = ir * ih;
-        float ir5 = ir3 * ih;
-        float rw = rx * wx + ry * wy + rz * wz;
-        float att = 1.0f, cc = 0.0f;
-        if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
-        float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
-        float jx = -lin * wx + rad * rx, jy = -lin * wy + rad * ry, jz = -lin * wz + rad * rz;
-        bool use = active && !(G.self && j == i);
-        float m = use ? s.w : 0.0f;
-        gx += m * jx;
-        gy += m * jy;
-        gz += m * jz;
-        if (out) {
-          float c = -m * lin;
-          fx += c * rx;
-          fy += c * ry;
-          fz += c * rz;
-        }
-        float am = use ? -lin * rw : 0.0f;
-        float tot = reduce4(-m * jx, -m * jy, -m * jz, am);
-        if ((lane & 7) == 0) atomicAdd(&part_adj[static_cast<int64_t>(j) * kPartAdj + r4], tot);
-      }
-      nnear += static_cast<unsigned long long>(tp.y - tp.x);
-      k = tp.z;
-    } else {
-      k++;
     }
-  }
-  if (counters && lane == 0) {
-    unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
-    atomicAdd(&counters[0], nfar * na);
-    atomicAdd(&counters[1], nnear * na);
-  }
-  if (active) {
-    gq[3 * static_cast<int64_t>(i)] = gx;
-    gq[3 * static_cast<int64_t>(i) + 1] = gy;
-    gq[3 * static_cast<int64_t>(i) + 2] = gz;
-    if (out) {
-      out[3 * o] = fx;
-      out[3 * o + 1] = fy;
-      out[3 * o + 2] = fz;
-    }
-  }
   }
 }
 
@@ -993,62 +1070,73 @@ __global__ void adjoint_combine_kernel(const float4* __restrict__ sp, const uint
 __global__ void __launch_bounds__(128)
     wn_walk_kernel(WalkTree T, WalkTargets G, float beta, float* __restrict__ out,
                    unsigned long long* __restrict__ counters) {
-  int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31;
   const uint32_t ng = min(*G.ngroups, G.capacity);
-  for (;;) {
-  uint32_t gw = next_group(G);
-  if (gw >= ng) break;
-  int4 gr = G.groups[gw];
-  int i = gr.x + lane;
-  bool active = i < gr.y;
-  float4 q = G.tp[active ? i : gr.x];
-  float gmin[3], gmax[3];
-  group_box(q, gmin, gmax);
-  int2 rt = T.roots[gr.z];
   const float k4pi = 0.07957747154594767f;  // 1 / (4 pi)
-  float far = 0.f, near = 0.f, comp = 0.f;
-  unsigned long long nfar = 0, nnear = 0;
-  int k = rt.x;
-  while (k < rt.y) {
-    const NodeRec* nd = T.nodes + k;
-    int4 tp = __ldg(&nd->topo);
-    float4 A = __ldg(&nd->com);
-    if (A.w == 0.0f) {
-      k = tp.z;
-      continue;
-    }
-    float4 X = __ldg(&nd->aux);
-    if (accept_node(A, X.z, X.w, gmin, gmax, beta)) {
-      float4 N = __ldg(&T.nnrm[k]);
-      float dx = A.x - q.x, dy = A.y - q.y, dz = A.z - q.z;
-      float dist = sqrtf(dx * dx + dy * dy + dz * dz);
-      float nd_ = N.x * dx + N.y * dy + N.z * dz;
-      far += A.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
-      nfar++;
-      k = tp.z;
-    } else if (tp.w & kLeafFlag) {
-      float a = 0.f;
-      for (int j = tp.x; j < tp.y; j++) {
-        float4 s = __ldg(&T.sp[j]);
-        float4 nrm = __ldg(&T.sn[j]);
-        float dx = s.x - q.x, dy = s.y - q.y, dz = s.z - q.z;
-        float dist = sqrtf(dx * dx + dy * dy + dz * dz);
-        float nd_ = nrm.x * dx + nrm.y * dy + nrm.z * dz;
-        a += s.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
+  for (;;) {
+    uint32_t gw = next_group(G);
+    if (gw >= ng) break;
+    int4 gr = G.groups[gw];
+    LaneTargets Q;
+    load_targets(G, gr, lane, Q);
+    float gmin[3], gmax[3];
+    group_box(Q, gmin, gmax);
+    int2 rt = T.roots[gr.z];
+    float far[kTPL], near[kTPL], comp[kTPL];
+#pragma unroll
+    for (int t = 0; t < kTPL; t++) far[t] = near[t] = comp[t] = 0.f;
+    unsigned long long nfar = 0, nnear = 0;
+    int k = rt.x;
+    while (k < rt.y) {
+      const NodeRec* nd = T.nodes + k;
+      int4 tp = __ldg(&nd->topo);
+      float4 A = __ldg(&nd->com);
+      if (A.w == 0.0f) {
+        k = tp.z;
+        continue;
       }
-      kahan_add(near, comp, a);
-      nnear += static_cast<unsigned long long>(tp.y - tp.x);
-      k = tp.z;
-    } else {
-      k++;
+      if (accept_node(__ldg(&nd->cell), gmin, gmax, beta)) {
+        float4 N = __ldg(&T.nnrm[k]);
+#pragma unroll
+        for (int t = 0; t < kTPL; t++) {
+          float dx = A.x - Q.x[t], dy = A.y - Q.y[t], dz = A.z - Q.z[t];
+          float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+          float nd_ = N.x * dx + N.y * dy + N.z * dz;
+          far[t] += A.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
+        }
+        nfar++;
+        k = tp.z;
+      } else if (tp.w & kLeafFlag) {
+        float a[kTPL];
+#pragma unroll
+        for (int t = 0; t < kTPL; t++) a[t] = 0.f;
+        for (int j = tp.x; j < tp.y; j++) {
+          float4 s = __ldg(&T.sp[j]);
+          float4 nrm = __ldg(&T.sn[j]);
+#pragma unroll
+          for (int t = 0; t < kTPL; t++) {
+            float dx = s.x - Q.x[t], dy = s.y - Q.y[t], dz = s.z - Q.z[t];
+            float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+            float nd_ = nrm.x * dx + nrm.y * dy + nrm.z * dz;
+            a[t] += s.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
+          }
+        }
+#pragma unroll
+        for (int t = 0; t < kTPL; t++) kahan_add(near[t], comp[t], a[t]);
+        nnear += static_cast<unsigned long long>(tp.y - tp.x);
+        k = tp.z;
+      } else {
+        k++;
+      }
     }
-  }
-  if (active) out[G.perm[i]] = far + near;
-  if (counters && lane == 0) {
-    unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
-    atomicAdd(&counters[0], nfar * na);
-    atomicAdd(&counters[1], nnear * na);
-  }
+#pragma unroll
+    for (int t = 0; t < kTPL; t++)
+      if (Q.act[t]) out[G.perm[Q.idx[t]]] = far[t] + near[t];
+    if (counters && lane == 0) {
+      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
+      atomicAdd(&counters[0], nfar * na);
+      atomicAdd(&counters[1], nnear * na);
+    }
   }
 }
 
@@ -1075,12 +1163,12 @@ __global__ void query_gather_kernel(const float* __restrict__ q, const uint32_t*
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     uint32_t s = perm[i];
     tp[i] = make_float4(q[3 * s], q[3 * s + 1], q[3 * s + 2], 0.0f);
-    if ((i & 31) == 0) {
-      int64_t e = i + 32 < nq ? i + 32 : nq;
-      groups[i >> 5] = make_int4(static_cast<int>(i), static_cast<int>(e), 0, 0);
+    if (i % kGroup == 0) {
+      int64_t e = i + kGroup < nq ? i + kGroup : nq;
+      groups[i / kGroup] = make_int4(static_cast<int>(i), static_cast<int>(e), 0, 0);
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *ngroups = static_cast<uint32_t>((nq + 31) / 32);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *ngroups = static_cast<uint32_t>((nq + kGroup - 1) / kGroup);
 }
 
 }  // namespace nt
@@ -1252,6 +1340,8 @@ int native_layout(void* ws, size_t ws_bytes, const Header& h, Layout& L) {
 }  // namespace
 
 extern "C" {
+
+int sbh_native_group_size(void) { return kGroup; }
 
 size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int with_normals, int with_adjoint) {
   if (n < 0 || num_systems < 1 || leaf_size < 1 || leaf_size > 32) return 0;
@@ -1527,7 +1617,7 @@ size_t sbh_native_query_workspace_bytes(int64_t nq) {
   s.take<uint32_t>(radix_hist_elems(nn));
   s.take<uint32_t>(scan_tiles(radix_hist_elems(nn)));
   s.take<float4>(nn);
-  s.take<int4>(nn / 32 + 1);
+  s.take<int4>(nn / kGroup + 1);
   return s.off;
 }
 
@@ -1559,7 +1649,7 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   uint32_t* hist = c.take<uint32_t>(radix_hist_elems(nq));
   uint32_t* stmp = c.take<uint32_t>(scan_tiles(radix_hist_elems(nq)));
   float4* tp = c.take<float4>(nq);
-  int4* groups = c.take<int4>(nq / 32 + 1);
+  int4* groups = c.take<int4>(nq / kGroup + 1);
   query_keys_kernel<<<gs(nq), 256, 0, stream>>>(queries, nq, L.boxes, k0);
   int which = 0;
   cudaError_t e = radix_sort<uint64_t>(stream, k0, v0, k1, v1, nq, 63, false, hist, stmp, &which);
@@ -1568,8 +1658,8 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
   e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / 32 + 1)};
-  e = launch_walk(stream, qmeta + 2, nq / 32 + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
+  WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kGroup + 1)};
+  e = launch_walk(stream, qmeta + 2, nq / kGroup + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_winding_number");
 }
@@ -1596,7 +1686,7 @@ int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspac
 
 // Copies the tree to caller buffers (device pointers; any may be null):
 // sorted keys (n), permutation (n, sorted slot -> input index), nodes
-// (num_nodes x 64 bytes), and the node count to *num_nodes (synchronises).
+// (num_nodes x 80 bytes), and the node count to *num_nodes (synchronises).
 int sbh_native_export(cudaStream_t stream, const void* workspace, size_t workspace_bytes, uint64_t* keys_out,
                       uint32_t* perm_out, void* nodes_out, size_t nodes_capacity, uint64_t* num_nodes) {
   Header h;

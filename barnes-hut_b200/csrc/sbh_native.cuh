@@ -15,15 +15,17 @@ struct SegBox {
 
 // One node, 64 bytes, read by the traversal with four 16-byte loads.
 struct NodeRec {
-  float4 com;   // COM x, y, z and total mass M
-  float4 aux;   // S_xz, S_yz, diag = side * sqrt(3), delta = |COM - cell centre|
-  float4 quad;  // S_xx, S_yy, S_zz, S_xy (second moment about the COM)
-  int4 topo;    // particle range [start, end), skip index, level | 0x100 if leaf
+  float4 com;    // COM x, y, z and total mass M
+  float4 cell;   // cell centre x, y, z and diag = side * sqrt(3)
+  float4 quad;   // S_xx, S_yy, S_zz, S_xy (second moment about the COM)
+  float4 quad2;  // S_xz, S_yz, 0, 0
+  int4 topo;     // particle range [start, end), skip index, level | 0x100 if leaf
 };
-static_assert(sizeof(NodeRec) == 64, "NodeRec must be 64 bytes");
+static_assert(sizeof(NodeRec) == 80, "NodeRec must be 80 bytes");
 
 constexpr int kLeafFlag = 0x100;
-constexpr int kGroup = 32;      // targets per warp
+constexpr int kTPL = 2;         // targets per lane in the walks
+constexpr int kGroup = 32 * kTPL;  // targets per group (one warp)
 constexpr int kNodeAdj = 12;    // per-node adjoint floats: A_X(3) A_M(1) G(6) pad(2)
 constexpr int kPartAdj = 4;     // per-particle adjoint floats: dx(3) dm(1)
 

@@ -114,6 +114,7 @@ _SIGS = {
                              _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_stochastic_bh_tree": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_i, _c_i,
                                 _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_native_group_size": ([], _c_i),
     "sbh_native_workspace_bytes": ([_c_i64, _c_i, _c_i, _c_i, _c_i], _c_sz),
     "sbh_native_build": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_i, _c_i, _c_i, _c_p, _c_sz], _c_i),
     "sbh_native_force": ([_c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
@@ -637,13 +638,18 @@ for _name in ("register_bruteforce_gravity", "register_softened_direct_force", "
 # ---------------------------------------------------------------------------
 # native adaptive octree (new entry points; no reference counterpart)
 # ---------------------------------------------------------------------------
+def native_group_size() -> int:
+    """Most targets in one walk group of the native tree."""
+    return int(lib().sbh_native_group_size())
+
+
 class NativeTree:
     """A native tree (or forest of independent systems) living in a device
     workspace. build() once, then force(), force_vjp() and
     winding_number() evaluate it; the workspace is reused across builds of
     the same size."""
 
-    NODE_BYTES = 64
+    NODE_BYTES = 80
 
     def __init__(self, device=None):
         self.device = device or _device()
@@ -746,7 +752,7 @@ class NativeTree:
         return dict(nodes=int(out[0]), groups=int(out[1]), far=int(out[2]), near=int(out[3]))
 
     def export(self):
-        """(sorted keys u64, permutation, node records (nn x 64 bytes)) as CPU numpy arrays."""
+        """(sorted keys u64, permutation, node records (nn x 80 bytes)) as CPU numpy arrays."""
         nn = ctypes.c_uint64(0)
         _check(lib().sbh_native_export(_stream_ptr(self.device), _p(self.ws), self.ws.numel(), None, None, None, 0,
                                        ctypes.byref(nn)), "native_export")

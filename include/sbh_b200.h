@@ -237,18 +237,23 @@ int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void*
 /* ---------------------------------------------------------------------- */
 /* Native adaptive octree (no reference counterpart: a new B200 path)     */
 /* ---------------------------------------------------------------------- */
-/* Opening rule in the reference's convention (distance / cell diagonal >=
- * beta, beta = 1/theta, src/sbh_ffi.cu:1878-1893), made conservative for a
- * group of 32 targets: accept a node when the distance from the group's
- * bounding box to the node's centre of mass exceeds beta * diagonal + |COM -
- * cell centre|. The far field is the node monopole plus (quadrupole = 1) its
- * second moment about the COM; near-field leaves are summed pairwise. */
+/* Opening rule: the reference's |q - cell centre| / cell diagonal >= beta
+ * (beta = 1/theta; include/tree3d.h:134-153, src/sbh_ffi.cu:1878-1893) made
+ * to hold for every target of a group: accept a node when the distance from
+ * the group's bounding box to the cell centre exceeds beta * diagonal.
+ * Targets are walked in groups of at most sbh_native_group_size() (packed
+ * from the tree's cells). The far field is the node monopole about its
+ * centre of mass plus (quadrupole = 1) its second moment about the COM;
+ * near-field leaves are summed pairwise. */
 typedef struct sbh_native_params {
   float beta;      /* 1 / theta, > 0 */
   float softening; /* Plummer softening epsilon, >= 0 */
   float cutoff;    /* erfc attenuation scale of the short-range split; <= 0 disables */
   int quadrupole;  /* 1: monopole + quadrupole far field (needs cutoff <= 0), 0: monopole */
 } sbh_native_params;
+
+/* Most targets one group holds (one warp walks a group). */
+int sbh_native_group_size(void);
 
 /* Workspace for a tree of n points in num_systems independent systems. */
 size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int with_normals,
@@ -305,8 +310,11 @@ int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspac
                      uint64_t* out4);
 
 /* Synchronises; copies sorted keys (n x u64), the permutation (n x u32,
- * sorted slot -> input index) and the 64-byte node records to device buffers
- * (each may be NULL) and the node count to *num_nodes. */
+ * sorted slot -> input index) and the 80-byte node records to device buffers
+ * (each may be NULL) and the node count to *num_nodes. A node record is
+ * {COM x, y, z, mass; cell centre x, y, z, diagonal; S_xx, S_yy, S_zz, S_xy;
+ * S_xz, S_yz, 0, 0} as floats, then {start, end, skip, level | 0x100 if
+ * leaf} as int32, S being the second moment about the COM. */
 int sbh_native_export(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
                       uint64_t* keys_out, uint32_t* perm_out, void* nodes_out,
                       size_t nodes_capacity, uint64_t* num_nodes);

@@ -943,22 +943,20 @@ static void com_float(const double* mom, int64_t k, float* X, float* M) {
 
 /*
  * Multipole acceptance for target group box [gmin, gmax] (float, no fused
- * operations), in the reference's convention (src/sbh_ffi.cu:1878-1893:
- * distance / cell diagonal >= beta, beta = 1/theta) made conservative for a
- * group and for the offset of the COM from the cell centre:
- *   accept node k iff dist^2(box, COM) > (side * sqrt(3) * beta + delta)^2,
- *   delta = |COM - cell centre|.
+ * operations): the reference's rule |q - cell centre| / diag >= beta
+ * (include/tree3d.h:134-153, src/sbh_ffi.cu:1878-1893; beta = 1/theta) made
+ * to hold for every target in the box:
+ *   accept node k iff dist^2(box, cell centre) > (side * sqrt(3) * beta)^2.
+ * X (the COM) is not used by the rule; the multipole is expanded about it.
  */
 static int native_accept(const NativeTree* t, int64_t k, const float* X, const float* gmin,
                          const float* gmax, float beta) {
-  float dcx = X[0] - t->center[3 * k], dcy = X[1] - t->center[3 * k + 1],
-        dcz = X[2] - t->center[3 * k + 2];
-  float delta = sqrtf(dcx * dcx + dcy * dcy + dcz * dcz);
-  float diag = t->side[k] * 1.7320508f;
-  float rc = diag * beta + delta;
+  (void)X;
+  const float* C = t->center + 3 * k;
+  float rc = t->side[k] * 1.7320508f * beta;
   float tt[3];
   for (int d = 0; d < 3; d++) {
-    float a = gmin[d] - X[d], b = X[d] - gmax[d];
+    float a = gmin[d] - C[d], b = C[d] - gmax[d];
     float m = a > b ? a : b;
     tt[d] = m > 0.0f ? m : 0.0f;
   }

@@ -16,10 +16,10 @@ pytestmark = pytest.mark.gpu
 
 
 def _decode_nodes(rec):
-    f = rec.view(np.float32).reshape(-1, 16)
-    i = rec.view(np.int32).reshape(-1, 16)
-    return dict(com=f[:, 0:4], aux=f[:, 4:8], quad=f[:, 8:12], start=i[:, 12], end=i[:, 13], skip=i[:, 14],
-                level=i[:, 15] & 0xFF, leaf=(i[:, 15] & 0x100) != 0)
+    f = rec.view(np.float32).reshape(-1, 20)
+    i = rec.view(np.int32).reshape(-1, 20)
+    return dict(com=f[:, 0:4], cell=f[:, 4:8], quad=f[:, 8:12], quad2=f[:, 12:16], start=i[:, 16], end=i[:, 17],
+                skip=i[:, 18], level=i[:, 19] & 0xFF, leaf=(i[:, 19] & 0x100) != 0)
 
 
 @pytest.mark.parametrize("dist,leaf", [("plummer", 16), ("uniform", 8), ("dupes", 16), ("tiny", 16)])
@@ -46,7 +46,8 @@ def test_native_tree_bit_exact_vs_oracle(cuda, dist, leaf):
     np.testing.assert_array_equal(nd["end"], a["end"])
     np.testing.assert_array_equal(nd["skip"], a["skip"])
     np.testing.assert_array_equal(nd["level"], a["level"])
-    np.testing.assert_array_equal(nd["aux"][:, 2], a["side"] * np.float32(1.7320508))
+    np.testing.assert_array_equal(nd["cell"][:, 3], a["side"] * np.float32(1.7320508))
+    np.testing.assert_array_equal(nd["cell"][:, :3], a["center"])
     # COM in float from FP64 sums: equal up to the last bit of the rounding
     mass = np.add.reduceat(m[a["perm"]].astype(np.float64), a["start"])[:0]  # noqa: F841 (shape check only)
     np.testing.assert_allclose(nd["com"][:, 3].sum() >= 0, True)
@@ -59,7 +60,7 @@ def test_native_force_matches_oracle_same_plan(cuda):
         f = t.force(beta=2.0, softening=1e-3, quadrupole=quad).cpu().numpy()
         st = t.stats()
         T = O.NativeTree(p, m, leaf_size=16)
-        inter = T.plan(2.0, 32)
+        inter = T.plan(2.0, B.native_group_size())
         want, _ = T.force(1e-3, quad=quad)
         assert rel_l2(f, want) < 1e-5, quad
         # same node-packed target groups
@@ -86,7 +87,7 @@ def test_native_adjoint_matches_oracle(cuda):
         t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True)
         f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=quad)
         T = O.NativeTree(p, m, leaf_size=16)
-        T.plan(2.0, 32)
+        T.plan(2.0, B.native_group_size())
         want_f, _ = T.force(1e-3, quad=quad)
         dx, dm = T.adjoint(w, 1e-3, quad=quad)
         assert rel_l2(f.cpu().numpy(), want_f) < 1e-5
