@@ -409,23 +409,30 @@ __global__ void roots_kernel(const int64_t* __restrict__ sorted_seg_off, int nse
   if (threadIdx.x == 0) roots[s] = make_int2(static_cast<int>(r0), static_cast<int>(a < b ? r1 : r0));
 }
 
-// Target groups packed from the tree. For every node holding more than
-// kGroup particles (or a system root), its children are taken in order and
-// consecutive children holding at most kGroup particles are packed into
-// groups of at most kGroup particles; a child with more particles is packed
-// the same way one level down, and a leaf with more than kGroup particles
-// (coincident points at level 21) is cut into runs. Each group lies inside
-// the cell of a node with more than kGroup particles, so its bounding box is
-// compact (runs of consecutive Morton positions can straddle distant cells).
+// Target groups cut from the tree. For every node holding more than kGroup
+// particles its children are taken in order; each maximal run of consecutive
+// children that hold at most kGroup particles each is one range of sorted
+// particles, cut into chunks of kGroup (the last one shorter). Children with
+// more particles are handled the same way one level down; a leaf with more
+// than kGroup particles (coincident points at level 21) and a system root
+// holding at most kGroup are cut into chunks directly. Every group lies
+// inside the cell of a node with more than kGroup particles, so its bounding
+// box is compact (runs of consecutive Morton positions can straddle distant
+// cells), and the chunks fill the lanes better than one group per child run.
 // Slots come from an atomic counter: the group order varies between runs,
 // each group's result does not.
-__device__ __forceinline__ void emit_group(int4* groups, uint32_t* count, int64_t cap, int s, int e, int sys,
-                                           uint32_t* status) {
-  uint32_t slot = atomicAdd(count, 1u);
-  if (slot < cap)
-    groups[slot] = make_int4(s, e, sys, 0);
-  else
-    raise_status(status, SBH_DEV_ITER_LIMIT);
+__device__ __forceinline__ void emit_chunks(int4* groups, uint32_t* count, int64_t cap, int s0, int s1, int sys,
+                                            uint32_t* status) {
+  int ng = (s1 - s0 + kGroup - 1) / kGroup;
+  if (ng <= 0) return;
+  uint32_t slot = atomicAdd(count, static_cast<uint32_t>(ng));
+  for (int g = 0; g < ng; g++) {
+    int s = s0 + g * kGroup;
+    if (slot + g < cap)
+      groups[slot + g] = make_int4(s, min(s + kGroup, s1), sys, 0);
+    else
+      raise_status(status, SBH_DEV_ITER_LIMIT);
+  }
 }
 
 __global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
@@ -438,34 +445,24 @@ __global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint
     bool leaf = (t.w & kLeafFlag) != 0;
     bool root = (t.w & 0xFF) == 0;
     int sys = sseg ? static_cast<int>(sseg[t.x]) : 0;
-    if (leaf) {
-      if (root || cnt > kGroup)
-        for (int s = t.x; s < t.y; s += kGroup) emit_group(groups, count, cap, s, min(s + kGroup, t.y), sys, status);
-      continue;
-    }
-    if (cnt <= kGroup) {
-      if (root) emit_group(groups, count, cap, t.x, t.y, sys, status);
+    if (leaf || cnt <= kGroup) {
+      if (root || (leaf && cnt > kGroup)) emit_chunks(groups, count, cap, t.x, t.y, sys, status);
       continue;
     }
     int run_s = -1, run_e = -1;
     for (uint32_t c = k + 1; c < static_cast<uint32_t>(t.z) && c < nn;) {
       int4 tc = nodes[c].topo;
-      int cc = tc.y - tc.x;
-      if (cc > kGroup) {
-        if (run_s >= 0) emit_group(groups, count, cap, run_s, run_e, sys, status);
+      if (tc.y - tc.x > kGroup) {
+        if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, status);
         run_s = -1;
       } else {
-        if (run_s >= 0 && tc.y - run_s > kGroup) {
-          emit_group(groups, count, cap, run_s, run_e, sys, status);
-          run_s = -1;
-        }
         if (run_s < 0) run_s = tc.x;
         run_e = tc.y;
       }
       if (static_cast<uint32_t>(tc.z) <= c) break;  // malformed skip: never loop
       c = static_cast<uint32_t>(tc.z);
     }
-    if (run_s >= 0) emit_group(groups, count, cap, run_s, run_e, sys, status);
+    if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, status);
   }
 }
 
@@ -623,6 +620,7 @@ __global__ void __launch_bounds__(128)
     int4 gr = G.groups[gw];
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
+    const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
     float gmin[3], gmax[3];
     group_box(Q, gmin, gmax);
     int2 rt = T.roots[gr.z];
@@ -648,6 +646,7 @@ __global__ void __launch_bounds__(128)
         }
 #pragma unroll
         for (int t = 0; t < kTPL; t++) {
+          if (t > 0 && !two) break;
           float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
           float r2 = rx * rx + ry * ry + rz * rz;
           float ir = rsqrtf(r2 + P.eps2);
@@ -688,6 +687,7 @@ __global__ void __launch_bounds__(128)
           float4 s = __ldg(&T.sp[j]);
 #pragma unroll
           for (int t = 0; t < kTPL; t++) {
+            if (t > 0 && !two) break;
             float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
             float r2 = rx * rx + ry * ry + rz * rz;
             float ir = rsqrtf(r2 + P.eps2);
@@ -823,6 +823,7 @@ __global__ void __launch_bounds__(128)
     int4 gr = G.groups[gw];
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
+    const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
     float wx[kTPL], wy[kTPL], wz[kTPL];
     uint32_t o[kTPL];
 #pragma unroll
@@ -861,6 +862,7 @@ __global__ void __launch_bounds__(128)
         for (int j = 0; j < 10; j++) v[j] = 0.f;
 #pragma unroll
         for (int t = 0; t < kTPL; t++) {
+          if (t > 0 && !two) break;
           float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
           float r2 = rx * rx + ry * ry + rz * rz;
           float ir = rsqrtf(r2 + P.eps2);
@@ -933,6 +935,7 @@ __global__ void __launch_bounds__(128)
           float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
 #pragma unroll
           for (int t = 0; t < kTPL; t++) {
+            if (t > 0 && !two) break;
             float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
             float r2 = rx * rx + ry * ry + rz * rz;
             float ir = rsqrtf(r2 + P.eps2);
@@ -1079,6 +1082,7 @@ __global__ void __launch_bounds__(128)
     int4 gr = G.groups[gw];
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
+    const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
     float gmin[3], gmax[3];
     group_box(Q, gmin, gmax);
     int2 rt = T.roots[gr.z];
@@ -1099,6 +1103,7 @@ __global__ void __launch_bounds__(128)
         float4 N = __ldg(&T.nnrm[k]);
 #pragma unroll
         for (int t = 0; t < kTPL; t++) {
+          if (t > 0 && !two) break;
           float dx = A.x - Q.x[t], dy = A.y - Q.y[t], dz = A.z - Q.z[t];
           float dist = sqrtf(dx * dx + dy * dy + dz * dz);
           float nd_ = N.x * dx + N.y * dy + N.z * dz;
@@ -1115,6 +1120,7 @@ __global__ void __launch_bounds__(128)
           float4 nrm = __ldg(&T.sn[j]);
 #pragma unroll
           for (int t = 0; t < kTPL; t++) {
+            if (t > 0 && !two) break;
             float dx = s.x - Q.x[t], dy = s.y - Q.y[t], dz = s.z - Q.z[t];
             float dist = sqrtf(dx * dx + dy * dy + dz * dz);
             float nd_ = nrm.x * dx + nrm.y * dy + nrm.z * dz;

@@ -972,73 +972,53 @@ static int native_accept(const NativeTree* t, int64_t k, const float* X, const f
  * (sum over groups of active targets x (accepted nodes + near particles)).
  */
 /*
- * Target groups packed from the tree: for every node holding more than G
- * particles (or the root), its children are taken in order and consecutive
- * children holding at most G particles are packed into groups of at most G
- * particles; a child with more than G particles is split the same way one
- * level down, and a leaf with more than G particles (coincident points) is
- * cut into runs of G. Each group lies inside the cell of a node with more
- * than G particles, so its bounding box stays compact.
+ * Target groups cut from the tree. For every node holding more than G
+ * particles its children are taken in order; each maximal run of
+ * consecutive children that hold at most G particles each is one range of
+ * sorted particles, cut into chunks of G (the last one shorter). Children
+ * with more than G particles are handled the same way one level down; a leaf
+ * with more than G particles (coincident points) and a root holding at most G
+ * are cut into chunks of G directly. Every group lies inside the cell of a
+ * node with more than G particles, so its bounding box stays compact, and
+ * the chunks fill the walk's lanes better than one group per child run.
  * Writes group starts/ends (sorted positions) and returns the count.
  */
+static int64_t emit_chunks(int64_t s0, int64_t s1, int G, int64_t* gs, int64_t* ge, int64_t ng) {
+  for (int64_t s = s0; s < s1; s += G) {
+    gs[ng] = s;
+    ge[ng] = s + G < s1 ? s + G : s1;
+    ng++;
+  }
+  return ng;
+}
+
 static int64_t native_node_groups(const NativeTree* t, int G, int64_t* gs, int64_t* ge) {
   int64_t ng = 0;
-  if (t->nn == 0) return 0;
   for (int64_t k = 0; k < t->nn; k++) {
     int32_t cnt = t->end[k] - t->start[k];
     int is_leaf = (k + 1 >= t->nn) || (t->skip[k] == k + 1);
     int is_root = t->level[k] == 0;
-    if (is_leaf) {
-      if (is_root || cnt > G) {
-        /* root leaf or oversized leaf: runs of G (a root leaf holds <= leaf_size) */
-        for (int32_t s = t->start[k]; s < t->end[k]; s += G) {
-          gs[ng] = s;
-          ge[ng] = s + G < t->end[k] ? s + G : t->end[k];
-          ng++;
-        }
-      }
-      continue;
-    }
-    if (cnt <= G) {
-      if (is_root) {
-        gs[ng] = t->start[k];
-        ge[ng] = t->end[k];
-        ng++;
-      }
+    if (is_leaf || cnt <= G) {
+      if (is_root || (is_leaf && cnt > G)) ng = emit_chunks(t->start[k], t->end[k], G, gs, ge, ng);
       continue;
     }
     /* children of k: k+1, skip[k+1], ... until skip[k] */
     int64_t run_s = -1, run_e = -1;
     for (int64_t c = k + 1; c < t->skip[k]; c = t->skip[c]) {
-      int32_t cc = t->end[c] - t->start[c];
-      if (cc > G) {
-        if (run_s >= 0) {
-          gs[ng] = run_s;
-          ge[ng] = run_e;
-          ng++;
-          run_s = -1;
-        }
-        continue;
-      }
-      if (run_s >= 0 && (t->end[c] - run_s) > G) {
-        gs[ng] = run_s;
-        ge[ng] = run_e;
-        ng++;
+      if (t->end[c] - t->start[c] > G) {
+        if (run_s >= 0) ng = emit_chunks(run_s, run_e, G, gs, ge, ng);
         run_s = -1;
+        continue;
       }
       if (run_s < 0) run_s = t->start[c];
       run_e = t->end[c];
     }
-    if (run_s >= 0) {
-      gs[ng] = run_s;
-      ge[ng] = run_e;
-      ng++;
-    }
+    if (run_s >= 0) ng = emit_chunks(run_s, run_e, G, gs, ge, ng);
   }
   return ng;
 }
 
-int g_orc_group_mode = 1; /* 1: node-packed groups (the CUDA walk's definition), 0: runs of G sorted particles */
+int g_orc_group_mode = 1; /* 1: groups cut from the tree (the CUDA walk's definition), 0: runs of G sorted particles */
 void orc_native_set_group_mode(int mode) { g_orc_group_mode = mode; }
 
 int64_t orc_native_plan(void* h, const float* pts, const float* masses, double beta,
