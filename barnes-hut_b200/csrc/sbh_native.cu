@@ -609,7 +609,7 @@ __device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, f
 // 55, far node 200 including the share of the warp reductions.
 
 template <bool QUAD, bool CUT>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
                       unsigned long long* __restrict__ counters) {
   const int lane = threadIdx.x & 31;
@@ -809,8 +809,17 @@ __device__ __forceinline__ int reduce10_index(int lane) {
 // over the group and added to part_adj. Forces are written when out != null.
 // Every node-side term is linear in the cotangent, so inactive slots (zero
 // cotangent) add nothing.
+//
+// Per (target, node) pair with r = q - X, h = |r|^2 + eps^2, ir = h^-1/2,
+// lin = att ir^3, rad = (3 att ir^5 + cc)(r.w), and S the node's second
+// moment, the query-side gradient is
+//   M (rad r - lin w) + 3 ir^5 S w - 15 ir^7 (r.w) S r
+//     + (1.5 tr(S) ir^5 - 7.5 ir^7 rSr) w - (7.5 tr(S) ir^7 (r.w) + a3) r,
+// a3 = 15 ir^7 (r.Sw) - 52.5 ir^9 (rSr)(r.w), and the node-side terms are
+// A_X = -(that gradient), A_M = -lin (r.w) and
+// G = 1.5 ir^5 (w r^T + r w^T) + 1.5 ir^5 (r.w) I - 7.5 ir^7 (r.w) r r^T.
 template <bool QUAD, bool CUT>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
                         float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
                         float* __restrict__ part_adj, unsigned long long* __restrict__ counters) {
@@ -857,7 +866,9 @@ __global__ void __launch_bounds__(128)
           X = __ldg(&nd->quad2);
         }
         const float M = A.w;
-        float v[10];
+        const float Sxx = Qd.x, Syy = Qd.y, Szz = Qd.z, Sxy = Qd.w, Sxz = X.x, Syz = X.y;
+        const float tr15 = 1.5f * (Sxx + Syy + Szz);
+        float v[10], vb = 0.f;  // vb: the (r.w) I part of G, added to its diagonal once
 #pragma unroll
         for (int j = 0; j < 10; j++) v[j] = 0.f;
 #pragma unroll
@@ -872,50 +883,55 @@ __global__ void __launch_bounds__(128)
           float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
           float att = 1.0f, cc = 0.0f;
           if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
-          // per unit mass: phi = -att ir3 r ; J^T w = -att ir3 w + (3 att ir5 + cc) (r.w) r
-          float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
-          float jx = -lin * wx[t] + rad * rx, jy = -lin * wy[t] + rad * ry, jz = -lin * wz[t] + rad * rz;
-          float qx_ = M * jx, qy_ = M * jy, qz_ = M * jz;
-          v[3] -= lin * rw;  // phi . w
-          if (out) {
-            float c = -M * lin;
-            fx[t] += c * rx;
-            fy[t] += c * ry;
-            fz[t] += c * rz;
-          }
+          float lin = att * ir3;
+          float mlin = M * lin, mrad = M * (rw * (3.0f * att * ir5 + cc));
+          v[3] -= lin * rw;  // A_M
+          float qx_, qy_, qz_;
           if (QUAD) {
-            float Sxx = Qd.x, Syy = Qd.y, Szz = Qd.z, Sxy = Qd.w, Sxz = X.x, Syz = X.y;
             float sx = Sxx * rx + Sxy * ry + Sxz * rz;
             float sy = Sxy * rx + Syy * ry + Syz * rz;
             float sz = Sxz * rx + Syz * ry + Szz * rz;
             float swx = Sxx * wx[t] + Sxy * wy[t] + Sxz * wz[t];
             float swy = Sxy * wx[t] + Syy * wy[t] + Syz * wz[t];
             float swz = Sxz * wx[t] + Syz * wy[t] + Szz * wz[t];
-            float tr = Sxx + Syy + Szz;
             float rsr = rx * sx + ry * sy + rz * sz;
-            float sxw = sx * wx[t] + sy * wy[t] + sz * wz[t];
+            float rsw = rx * swx + ry * swy + rz * swz;
             float ir7 = ir5 * ih, ir9 = ir7 * ih;
-            // J_q^T w of the quadrupole term
+            float c1 = 3.0f * ir5;
             float a1 = 5.0f * ir7 * rw;
-            float a2 = 7.5f * ir7 * rsr;
-            float a3 = 7.5f * (2.0f * ir7 * sxw - 7.0f * ir9 * rsr * rw);
-            qx_ += ir5 * (3.0f * swx + 1.5f * tr * wx[t]) - a1 * (3.0f * sx + 1.5f * tr * rx) - a2 * wx[t] - a3 * rx;
-            qy_ += ir5 * (3.0f * swy + 1.5f * tr * wy[t]) - a1 * (3.0f * sy + 1.5f * tr * ry) - a2 * wy[t] - a3 * ry;
-            qz_ += ir5 * (3.0f * swz + 1.5f * tr * wz[t]) - a1 * (3.0f * sz + 1.5f * tr * rz) - a2 * wz[t] - a3 * rz;
-            // G = sym d(w . a_q)/dS
-            float ga = 1.5f * ir5, gb = 1.5f * ir5 * rw, gc = 7.5f * ir7 * rw;
-            v[4] += 2.0f * ga * wx[t] * rx + gb - gc * rx * rx;
-            v[5] += 2.0f * ga * wy[t] * ry + gb - gc * ry * ry;
-            v[6] += 2.0f * ga * wz[t] * rz + gb - gc * rz * rz;
-            v[7] += ga * (wx[t] * ry + rx * wy[t]) - gc * rx * ry;
-            v[8] += ga * (wx[t] * rz + rx * wz[t]) - gc * rx * rz;
-            v[9] += ga * (wy[t] * rz + ry * wz[t]) - gc * ry * rz;
+            float a3 = 15.0f * ir7 * rsw - 52.5f * ir9 * rsr * rw;
+            float cw = tr15 * ir5 - 7.5f * ir7 * rsr - mlin;
+            float cr = mrad - tr15 * a1 - a3;
+            float c2 = 3.0f * a1;
+            qx_ = c1 * swx - c2 * sx + cw * wx[t] + cr * rx;
+            qy_ = c1 * swy - c2 * sy + cw * wy[t] + cr * ry;
+            qz_ = c1 * swz - c2 * sz + cw * wz[t] + cr * rz;
+            // G, off-diagonals doubled (halved once below)
+            float al = 1.5f * ir5, ga = 7.5f * ir7 * rw;
+            vb += al * rw;
+            float ux = 2.0f * al * wx[t] - ga * rx;
+            float uy = 2.0f * al * wy[t] - ga * ry;
+            float uz = 2.0f * al * wz[t] - ga * rz;
+            v[4] += ux * rx;
+            v[5] += uy * ry;
+            v[6] += uz * rz;
+            v[7] += ux * ry + uy * rx;
+            v[8] += ux * rz + uz * rx;
+            v[9] += uy * rz + uz * ry;
             if (out) {
-              float cr = ir5 * (1.5f * tr - 7.5f * rsr * ih);
-              float c3 = 3.0f * ir5;
-              fx[t] += cr * rx + c3 * sx;
-              fy[t] += cr * ry + c3 * sy;
-              fz[t] += cr * rz + c3 * sz;
+              float cf = ir5 * (tr15 - 7.5f * rsr * ih) - mlin;
+              fx[t] += cf * rx + c1 * sx;
+              fy[t] += cf * ry + c1 * sy;
+              fz[t] += cf * rz + c1 * sz;
+            }
+          } else {
+            qx_ = mrad * rx - mlin * wx[t];
+            qy_ = mrad * ry - mlin * wy[t];
+            qz_ = mrad * rz - mlin * wz[t];
+            if (out) {
+              fx[t] -= mlin * rx;
+              fy[t] -= mlin * ry;
+              fz[t] -= mlin * rz;
             }
           }
           gx[t] += qx_;
@@ -925,11 +941,24 @@ __global__ void __launch_bounds__(128)
           v[1] -= qy_;
           v[2] -= qz_;
         }
-        float tot = reduce10(v);
-        if (r10 >= 0) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r10], tot);
+        if (QUAD) {
+          v[4] += vb;
+          v[5] += vb;
+          v[6] += vb;
+          v[7] *= 0.5f;
+          v[8] *= 0.5f;
+          v[9] *= 0.5f;
+          float tot = reduce10(v);
+          if (r10 >= 0) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r10], tot);
+        } else {
+          float tot = reduce4(v[0], v[1], v[2], v[3]);
+          if ((lane & 7) == 0) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r4], tot);
+        }
         nfar++;
         k = tp.z;
       } else if (tp.w & kLeafFlag) {
+        // the self pair (r = 0) only occurs when the leaf overlaps the group
+        const bool selfchk = G.self && tp.x < gr.y && gr.x < tp.y;
         for (int j = tp.x; j < tp.y; j++) {
           float4 s = __ldg(&T.sp[j]);
           float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
@@ -945,23 +974,24 @@ __global__ void __launch_bounds__(128)
             float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
             float att = 1.0f, cc = 0.0f;
             if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
-            float lin = att * ir3, rad = rw * (3.0f * att * ir5 + cc);
-            float jx = -lin * wx[t] + rad * rx, jy = -lin * wy[t] + rad * ry, jz = -lin * wz[t] + rad * rz;
-            bool use = Q.act[t] && !(G.self && j == Q.idx[t]);
-            float m = use ? s.w : 0.0f;
-            gx[t] += m * jx;
-            gy[t] += m * jy;
-            gz[t] += m * jz;
+            float lin = att * ir3;
+            float m = (selfchk && j == Q.idx[t]) ? 0.0f : s.w;
+            float mlin = m * lin, mrad = m * (rw * (3.0f * att * ir5 + cc));
+            float qx_ = mrad * rx - mlin * wx[t];
+            float qy_ = mrad * ry - mlin * wy[t];
+            float qz_ = mrad * rz - mlin * wz[t];
+            gx[t] += qx_;
+            gy[t] += qy_;
+            gz[t] += qz_;
             if (out) {
-              float c = -m * lin;
-              fx[t] += c * rx;
-              fy[t] += c * ry;
-              fz[t] += c * rz;
+              fx[t] -= mlin * rx;
+              fy[t] -= mlin * ry;
+              fz[t] -= mlin * rz;
             }
-            a0 -= m * jx;
-            a1 -= m * jy;
-            a2 -= m * jz;
-            a3 += use ? -lin * rw : 0.0f;
+            a0 -= qx_;
+            a1 -= qy_;
+            a2 -= qz_;
+            a3 -= lin * rw;  // zero for the self pair (r = 0) and inactive slots (w = 0)
           }
           float tot = reduce4(a0, a1, a2, a3);
           if ((lane & 7) == 0) atomicAdd(&part_adj[static_cast<int64_t>(j) * kPartAdj + r4], tot);
@@ -1070,7 +1100,7 @@ __global__ void adjoint_combine_kernel(const float4* __restrict__ sp, const uint
 // Winding number (include/kernel.h:73-80): w(q) = sum m n.(p - q) / (4 pi (|p-q|^3 + 1e-5));
 // far field: node mass and mass-weighted mean normal at the COM, as the
 // reference's trees aggregate them (include/tree3d.h:255-264, 310-327).
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 4)
     wn_walk_kernel(WalkTree T, WalkTargets G, float beta, float* __restrict__ out,
                    unsigned long long* __restrict__ counters) {
   const int lane = threadIdx.x & 31;
@@ -1146,7 +1176,9 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-// Query targets: keys in the box of system 0 (clamped), sorted, grouped.
+// Query targets: keys in the box of system 0 (clamped), sorted, grouped in
+// runs of kQueryGroup (one slot per lane: for queries spread evenly through
+// the box, wider groups only add interactions).
 __global__ void query_keys_kernel(const float* __restrict__ q, int64_t nq, const SegBox* __restrict__ boxes,
                                   uint64_t* __restrict__ keys) {
   SegBox b = boxes[0];
@@ -1169,12 +1201,12 @@ __global__ void query_gather_kernel(const float* __restrict__ q, const uint32_t*
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     uint32_t s = perm[i];
     tp[i] = make_float4(q[3 * s], q[3 * s + 1], q[3 * s + 2], 0.0f);
-    if (i % kGroup == 0) {
-      int64_t e = i + kGroup < nq ? i + kGroup : nq;
-      groups[i / kGroup] = make_int4(static_cast<int>(i), static_cast<int>(e), 0, 0);
+    if (i % kQueryGroup == 0) {
+      int64_t e = i + kQueryGroup < nq ? i + kQueryGroup : nq;
+      groups[i / kQueryGroup] = make_int4(static_cast<int>(i), static_cast<int>(e), 0, 0);
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *ngroups = static_cast<uint32_t>((nq + kGroup - 1) / kGroup);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *ngroups = static_cast<uint32_t>((nq + kQueryGroup - 1) / kQueryGroup);
 }
 
 }  // namespace nt
@@ -1623,7 +1655,7 @@ size_t sbh_native_query_workspace_bytes(int64_t nq) {
   s.take<uint32_t>(radix_hist_elems(nn));
   s.take<uint32_t>(scan_tiles(radix_hist_elems(nn)));
   s.take<float4>(nn);
-  s.take<int4>(nn / kGroup + 1);
+  s.take<int4>(nn / kQueryGroup + 1);
   return s.off;
 }
 
@@ -1655,7 +1687,7 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   uint32_t* hist = c.take<uint32_t>(radix_hist_elems(nq));
   uint32_t* stmp = c.take<uint32_t>(scan_tiles(radix_hist_elems(nq)));
   float4* tp = c.take<float4>(nq);
-  int4* groups = c.take<int4>(nq / kGroup + 1);
+  int4* groups = c.take<int4>(nq / kQueryGroup + 1);
   query_keys_kernel<<<gs(nq), 256, 0, stream>>>(queries, nq, L.boxes, k0);
   int which = 0;
   cudaError_t e = radix_sort<uint64_t>(stream, k0, v0, k1, v1, nq, 63, false, hist, stmp, &which);
@@ -1664,8 +1696,8 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
   e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kGroup + 1)};
-  e = launch_walk(stream, qmeta + 2, nq / kGroup + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
+  WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1)};
+  e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_winding_number");
 }

@@ -26,6 +26,7 @@ static_assert(sizeof(NodeRec) == 80, "NodeRec must be 80 bytes");
 constexpr int kLeafFlag = 0x100;
 constexpr int kTPL = 2;         // targets per lane in the walks
 constexpr int kGroup = 32 * kTPL;  // targets per group (one warp)
+constexpr int kQueryGroup = 32;    // targets per group of external queries
 constexpr int kNodeAdj = 12;    // per-node adjoint floats: A_X(3) A_M(1) G(6) pad(2)
 constexpr int kPartAdj = 4;     // per-particle adjoint floats: dx(3) dm(1)
 

@@ -1,13 +1,20 @@
 """Benchmark: force+VJP evaluations per second of softened self-gravity at
-N = 1,048,576 (Plummer sphere, a = 1, truncated at 10a, equal masses,
-epsilon = 1e-3, theta = 0.5 i.e. beta = 2, float32), one evaluation = build
-the native octree + the softened force of every particle + the full adjoint
+N = 1,048,576 per system (Plummer spheres, a = 1, truncated at 10a, equal
+masses, epsilon = 1e-3, theta = 0.5 i.e. beta = 2, float32). One evaluation
+= the softened force of every particle of one system + the full adjoint
 (d/d positions and masses of sum w . a for a random cotangent w).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--systems S] [--impl reference]
+
+Batched step (the timed region): S systems (default 8) in one forest, one
+build + one fused force/adjoint walk + one finalize for all of them; value =
+S evaluations / step time. The same step captured in a CUDA graph, the plain
+path (build, force, rebuild, force+VJP as separate calls on one system) and
+the reference algorithm on this GPU (dense octree8 through the
+reference-compatible entry points) are reported beside it.
 
 One process per GPU (torchrun for N > 1); every rank evaluates its own
-independent system (replicas, weak scaling; the path needs no collective).
+independent systems (replicas, weak scaling; the path needs no collective).
 Timing: CUDA events on the launching stream, L2 flushed (256 MB write)
 between steps outside the timed events, the max over ranks. Rank 0 prints one
 JSON line.
@@ -40,7 +47,10 @@ BETA = 2.0
 EPS = 1e-3
 LEAF = 16
 METRIC = "force+VJP evals/sec at N=1M, rel-L2<=1e-4 vs FP64 direct; batched vs plain"
-WORKLOAD = "plummer_n1048576_eps1e-3_theta0.5_force_plus_full_vjp"
+
+
+def workload(n: int, systems: int) -> str:
+    return f"plummer_n{n}_eps1e-3_theta0.5_force_plus_full_vjp_{systems}_systems_per_step"
 
 
 def parse():
@@ -49,10 +59,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=N_DEFAULT)
+    ap.add_argument("--n", type=int, default=N_DEFAULT, help="particles per system")
+    ap.add_argument("--systems", type=int, default=8, help="systems batched in one step")
     ap.add_argument("--cpu-sample", type=int, default=32768, help="queries timed by the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extras", action="store_true", help="skip the forest and winding-number measurements")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the octree8, forest and winding-number measurements")
     return ap.parse_args()
 
 
@@ -157,7 +169,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer sphere)",
-        "config": {"workload": WORKLOAD, "n": args.n, "beta": BETA, "softening": EPS, "leaf_size": 8,
+        "config": {"workload": workload(args.n, args.systems), "n": args.n, "beta": BETA, "softening": EPS, "leaf_size": 8,
                    "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "reference",
                          "sample": sample},
@@ -304,6 +316,39 @@ def measure_fp32_peak(B, torch, dev):
     return flops / (ms * 1e-3) / 1e12
 
 
+def octree8_plain_measurement(B, torch, P0, M0, W0, idx, ref, flush):
+    """The reference's own algorithm on this GPU: the dense octree8 build
+    (depth 7, corners = data min/max -+ 1e-3) + softened force + (rebuild) +
+    query-side VJP, as separate calls through the reference-compatible
+    entry points, the custom_vjp recompute flow of the reference's
+    softened_barnes_hut_force_octree8. "No cutoff" in the reference's
+    convention is cutoff = 1e6 x the box size; pruning is off."""
+    span = float((P0.max(0).values - P0.min(0).values).max())
+    cut = 1e6 * span
+    kw = dict(beta=BETA, softening_scale=EPS, cutoff_scale=cut, prune_enabled=False)
+    Z = torch.zeros_like(P0)
+
+    def call():
+        leaf, node = B.build_octree8_buffers(P0, Z, M0, max_depth=7)
+        f = B.softened_barnes_hut_force_octree8(leaf, node, P0, **kw)
+        leaf, node = B.build_octree8_buffers(P0, Z, M0, max_depth=7)
+        B.softened_barnes_hut_force_octree8_vjp(leaf, node, P0, W0, **kw)
+        return f
+
+    f = call()
+    torch.cuda.synchronize()
+    rel = float(torch.linalg.norm(f[idx].double() - ref) / torch.linalg.norm(ref))
+    flush.zero_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    call()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return dict(ms_per_eval=ms, evals_per_s=1000.0 / ms, rel_l2_vs_fp64_direct=rel, max_depth=7,
+                note="query-side VJP only (the reference's VJP has no source or mass terms)")
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -317,37 +362,46 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    n = args.n
-    p, m = W.plummer(n, seed=1000 + rank)
+    n, K = args.n, args.systems
+    systems = [W.plummer(n, seed=1000 + rank * K + s) for s in range(K)]
+    p = np.concatenate([s_[0] for s_ in systems])
+    m = np.concatenate([s_[1] for s_ in systems])
+    offs = np.arange(K + 1, dtype=np.int64) * n
     w = np.random.default_rng(77 + rank).normal(size=p.shape).astype(np.float32)
     P = torch.tensor(p, device=dev)
     M = torch.tensor(m, device=dev)
     Wt = torch.tensor(w, device=dev)
-    F = torch.empty((n, 3), device=dev)
-    GX = torch.empty((n, 3), device=dev)
-    GM = torch.empty(n, device=dev)
+    OFFS = torch.tensor(offs, device=dev) if K > 1 else None
+    F = torch.empty_like(P)
+    GX = torch.empty_like(P)
+    GM = torch.empty_like(M)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     prm = B.NativeTree.params(BETA, EPS, 0.0, True)
     tree = B.NativeTree(dev)
-    tree.build(P, M, leaf_size=LEAF, with_adjoint=True)  # sizes the workspace
+    tree.build(P, M, system_offsets=OFFS, leaf_size=LEAF, with_adjoint=True)  # sizes the workspace
 
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
 
-    def step(times=None):
+    def run_step():
+        tree.build(P, M, system_offsets=OFFS, leaf_size=LEAF, with_adjoint=True)
+        tree.adjoint_walk(Wt, prm, F)
+        tree.adjoint_finalize(GX, GM)
+
+    def step():
         s0, s1, s2 = ev(), ev(), ev()
         s0.record()
-        tree.build(P, M, leaf_size=LEAF, with_adjoint=True)
+        tree.build(P, M, system_offsets=OFFS, leaf_size=LEAF, with_adjoint=True)
         s1.record()
         tree.adjoint_walk(Wt, prm, F)
         s2.record()
         tree.adjoint_finalize(GX, GM)
         return s0, s1, s2
 
-    # accuracy of the timed configuration (outside the timed region)
+    # accuracy of the timed configuration (outside the timed region): system 0
     step()
     torch.cuda.synchronize()
     idx = torch.tensor(np.random.default_rng(5).choice(n, 1024, replace=False), device=dev)
-    ref = fp64_direct_subset(P, M, idx, EPS)
+    ref = fp64_direct_subset(P[:n], M[:n], idx, EPS)
     rel = float(torch.linalg.norm(F[idx].double() - ref) / torch.linalg.norm(ref))
     st = tree.stats()
 
@@ -361,7 +415,6 @@ def run_ours(args):
     torch.cuda.synchronize()
     total_ms, walk_ms = 0.0, 0.0
     marks = []
-    e_end = []
     for _ in range(args.steps):
         flush.zero_()
         a, b, c = step()
@@ -378,57 +431,83 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
-    value = world * 1000.0 / ms_per_step
+    value = world * K * 1000.0 / ms_per_step
 
-    # plain path: separate C-ABI calls with the tree rebuilt for the VJP,
-    # like the reference's custom_vjp recompute flow
-    def plain():
-        t1 = B.NativeTree(dev)
-        t1.build(P, M, leaf_size=LEAF, with_adjoint=False)
-        t1.force(beta=BETA, softening=EPS, out=F)
-        t2 = B.NativeTree(dev)
-        t2.build(P, M, leaf_size=LEAF, with_adjoint=True)
-        t2.force_vjp(Wt, beta=BETA, softening=EPS, want_force=False)
+    # the same step captured in one CUDA graph and replayed
+    g = torch.cuda.CUDAGraph()
+    gs_ = torch.cuda.Stream(dev)
+    gs_.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(gs_):
+        run_step()
         torch.cuda.synchronize()
-
-    plain()
-    t0 = time.perf_counter()
+        with torch.cuda.graph(g, stream=gs_):
+            run_step()
+    torch.cuda.current_stream(dev).wait_stream(gs_)
+    torch.cuda.synchronize()
+    graph_ms = 0.0
     for _ in range(2):
-        plain()
-    plain_ms = (time.perf_counter() - t0) / 2 * 1e3
+        flush.zero_()
+        a, b = ev(), ev()
+        a.record()
+        g.replay()
+        b.record()
+        torch.cuda.synchronize()
+        graph_ms += a.elapsed_time(b)
+    graph_ms /= 2
+    del g
+
+    # plain path on system 0: separate C-ABI calls, the tree rebuilt for the
+    # VJP (the reference's custom_vjp recompute flow)
+    P0, M0, W0 = P[:n], M[:n], Wt[:n]
+    F0 = torch.empty_like(P0)
+    t1, t2 = B.NativeTree(dev), B.NativeTree(dev)
+
+    def plain():
+        t1.build(P0, M0, leaf_size=LEAF, with_adjoint=False)
+        t1.force(beta=BETA, softening=EPS, out=F0)
+        t2.build(P0, M0, leaf_size=LEAF, with_adjoint=True)
+        t2.force_vjp(W0, beta=BETA, softening=EPS, want_force=False)
+
+    def plain_force():
+        t1.build(P0, M0, leaf_size=LEAF, with_adjoint=False)
+        t1.force(beta=BETA, softening=EPS, out=F0)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            a, b = ev(), ev()
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        return tot / reps
+
+    plain_ms = timed(plain, 2)
+    force_ms = timed(plain_force, 2)
+    plain_force_rel = float(torch.linalg.norm(F0[idx].double() - ref) / torch.linalg.norm(ref))
 
     # e2e: host buffers in, host buffers out, through the public API
-    Ph = torch.tensor(p).pin_memory()
-    Mh = torch.tensor(m).pin_memory()
-    Wh = torch.tensor(w).pin_memory()
-    Fh = torch.empty((n, 3)).pin_memory()
-    GXh = torch.empty((n, 3)).pin_memory()
-    GMh = torch.empty(n).pin_memory()
+    Ph, Mh, Wh = (torch.tensor(a_).pin_memory() for a_ in (p, m, w))
+    Fh = torch.empty(P.shape).pin_memory()
+    GXh = torch.empty(P.shape).pin_memory()
+    GMh = torch.empty(M.shape).pin_memory()
 
     def e2e_step():
         Pd = Ph.to(dev, non_blocking=True)
         Md = Mh.to(dev, non_blocking=True)
         Wd = Wh.to(dev, non_blocking=True)
-        tree.build(Pd, Md, leaf_size=LEAF, with_adjoint=True)
+        tree.build(Pd, Md, system_offsets=OFFS, leaf_size=LEAF, with_adjoint=True)
         tree.adjoint_walk(Wd, prm, F)
         tree.adjoint_finalize(GX, GM)
         Fh.copy_(F, non_blocking=True)
         GXh.copy_(GX, non_blocking=True)
         GMh.copy_(GM, non_blocking=True)
 
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
-    e_ms = 0.0
-    for _ in range(args.steps):
-        flush.zero_()
-        a, b = ev(), ev()
-        a.record()
-        e2e_step()
-        b.record()
-        torch.cuda.synchronize()
-        e_ms += a.elapsed_time(b)
-    e_ms /= args.steps
+    e_ms = timed(e2e_step, args.steps)
     if world > 1:
         t = torch.tensor([e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -446,6 +525,8 @@ def run_ours(args):
 
     extras = {}
     if not args.no_extras:
+        if world == 1:
+            extras["octree8_plain"] = octree8_plain_measurement(B, torch, P0, M0, W0, idx, ref, flush)
         extras["forest"] = forest_measurement(B, torch, dev, rank, world, flush)
         if world == 1:
             extras["winding_number"] = winding_measurement(B, torch, dev, flush)
@@ -454,30 +535,37 @@ def run_ours(args):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
-            t_eval, info = cpu_reference_eval_time(p, m, args.cpu_sample, threads)
+            t_eval, info = cpu_reference_eval_time(systems[0][0], systems[0][1], args.cpu_sample, threads)
             cpu = {"value": 1.0 / t_eval, "unit": "evals/s", "cores": threads, "kind": "reference",
                    "sample": (f"reference Tree3D<8,1> build of all {n} points + force and query-side VJP of "
                               f"{info['sample_queries']} sampled particles (beta 2), extrapolated to all")}
-        launches = args.steps * (BUILD_LAUNCHES + WALK_LAUNCHES + FINALIZE_LAUNCHES)
+        launches = args.steps * (build_launches(K) + WALK_LAUNCHES + FINALIZE_LAUNCHES)
+        plain_eps = 1000.0 / plain_ms
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer sphere, a=1, r<10a)",
-            "config": {"workload": WORKLOAD, "n": n, "beta": BETA, "theta": 1.0 / BETA, "softening": EPS,
-                       "leaf_size": LEAF, "far_field": "monopole+quadrupole", "vjp": "positions and masses",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer spheres, a=1, r<10a)",
+            "config": {"workload": workload(n, K), "n": n, "systems_per_gpu": K, "beta": BETA, "theta": 1.0 / BETA,
+                       "softening": EPS, "leaf_size": LEAF, "far_field": "monopole+quadrupole",
+                       "vjp": "positions and masses",
+                       "batched": f"{K} systems in one forest: one build, one walk, one finalize per step",
                        "l2": "flushed between steps (256 MB write, outside the timed events)",
                        "parallelism": "replicas" if world > 1 else "single"},
-            "accuracy": {"rel_l2_vs_fp64_direct": rel, "subset": 1024},
-            "plain_vs_batched": {"plain_ms_per_eval": plain_ms, "batched_ms_per_eval": ms_per_step,
-                                 "ratio": plain_ms / ms_per_step},
+            "accuracy": {"rel_l2_vs_fp64_direct": rel, "subset": 1024, "system": 0},
+            "batched_vs_plain": {"batched_evals_per_s": value / world, "plain_evals_per_s": plain_eps,
+                                 "ratio": value / world / plain_eps, "plain_ms_per_eval": plain_ms,
+                                 "graph_ms_per_step": graph_ms, "eager_ms_per_step": ms_per_step,
+                                 "plain": "build, force, rebuild, force+VJP as separate calls on one system"},
+            "plain_force": {"ms_per_eval": force_ms, "rel_l2_vs_fp64_direct": plain_force_rel,
+                            "what": "build + force of one N=1M system (classic BH, theta 0.5)"},
             "roofline": {"kernel": "adjoint_walk_kernel<quad>", "bound": "fp32", "achieved": flops_walk / walk_s / 1e12,
                          "peak": fp32_peak, "unit": "TFLOP/s", "frac": flops_walk / walk_s / 1e12 / fp32_peak,
                          "peak_source": "measured in this run: sbh_probe_fp32 FMA chains",
                          "traffic": traffic, "walk_ms": walk_s * 1e3,
                          "interactions": {"far": st["far"], "near": st["near"]}},
             "cpu_baseline": cpu,
-            "e2e": {"value": world * 1000.0 / e_ms, "unit": "evals/s",
-                    "h2d_bytes_per_step": int(n * 28), "d2h_bytes_per_step": int(n * 28)},
+            "e2e": {"value": world * K * 1000.0 / e_ms, "unit": "evals/s",
+                    "h2d_bytes_per_step": int(K * n * 28), "d2h_bytes_per_step": int(K * n * 28)},
             "gpu_launches": launches,
             "clocks": clocks,
             "tree": {"nodes": st["nodes"], "groups": st["groups"]},
@@ -491,11 +579,20 @@ def run_ours(args):
 
 
 # Kernels per step of the timed path (counted from the host code):
-# build: bbox 3 + keys 1 + 8 radix passes x (count 1 + scan 3 + scatter 1) +
-#        levels 1 + slots 1 + scan 3 + emit 1 + node count 1 + gather 1 +
-#        moment scan 3 + finalize 1 + offsets 1 + roots 1 + groups 1 = 59
+# build of one system: offsets 1 + bbox 3 + keys 1 + 8 radix passes x
+#   (count 1 + scan 3 + scatter 1) + levels 1 + slots 1 + scan 3 + emit 1 +
+#   node count 1 + gather 1 + moment scan 3 + finalize 1 + roots 1 +
+#   groups 1 = 59; a forest of K > 1 systems copies its offsets instead of
+#   the offsets kernel and adds a stable pass on the system id (gather 1 +
+#   ceil(log2 K / 8) radix passes x 5 + gathers 2 + system ids 1)
 # walk: zero adjoint 1 + walk 1 = 2; finalize: push 1 + scan 3 + combine 1 = 5
-BUILD_LAUNCHES = 59
+def build_launches(k: int) -> int:
+    if k <= 1:
+        return 59
+    bits = max(1, (k - 1).bit_length())
+    return 59 - 1 + 1 + 5 * ((bits + 7) // 8) + 3
+
+
 WALK_LAUNCHES = 2
 FINALIZE_LAUNCHES = 5
 
