@@ -815,6 +815,10 @@ static int o8_launch_bh(int kernel, cudaStream_t stream, const void* leaf, size_
       o8_bh_kernel<O8_SOFT><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per, out,
                                                    status, bd);
       break;
+    case O8_GRAV_GRAD_VJP:
+      o8_bh_kernel<O8_GRAV_GRAD_VJP><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out, status,
+                                                            bd);
+      break;
     default:
       o8_bh_kernel<O8_SOFT_VJP><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per,
                                                        out, status, bd);
@@ -835,6 +839,15 @@ int sbh_barnes_hut_force_octree8(cudaStream_t stream, const void* leaf, size_t l
                                  int periodic, float box_length, int threads, void* workspace,
                                  size_t workspace_bytes) {
   return o8_launch_bh(O8_GRAV_GRAD, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, nullptr, out, beta,
+                      Soft{0.f, 0.f}, 0, 0.f, Periodic{periodic, box_length}, threads, workspace, workspace_bytes);
+}
+
+int sbh_barnes_hut_force_octree8_vjp(cudaStream_t stream, const void* leaf, size_t leaf_bytes, const void* nodes,
+                                     size_t node_bytes, const float* queries, int64_t nq, const float* cotangent,
+                                     float* out, float beta, int periodic, float box_length, int threads,
+                                     void* workspace, size_t workspace_bytes) {
+  if (nq > 0 && !cotangent) return invalid("cotangent must be non-null");
+  return o8_launch_bh(O8_GRAV_GRAD_VJP, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, cotangent, out, beta,
                       Soft{0.f, 0.f}, 0, 0.f, Periodic{periodic, box_length}, threads, workspace, workspace_bytes);
 }
 

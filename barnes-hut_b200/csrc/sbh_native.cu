@@ -609,7 +609,7 @@ __device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, f
 // 55, far node 200 including the share of the warp reductions.
 
 template <bool QUAD, bool CUT>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, 5)
     force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
                       unsigned long long* __restrict__ counters) {
   const int lane = threadIdx.x & 31;
@@ -629,16 +629,31 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int t = 0; t < kTPL; t++) fx[t] = fy[t] = fz[t] = nx[t] = ny[t] = nz[t] = cx[t] = cy[t] = cz[t] = 0.f;
     unsigned long long nfar = 0, nnear = 0;
+    // Pre-order walk. The next node is known once this node's opening test
+    // is done, so its opening data is loaded before this node's terms are
+    // evaluated and the load latency hides behind that arithmetic.
     int k = rt.x;
+    int4 tp = make_int4(0, 0, rt.y, 0);
+    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), C = A;
+    if (k < rt.y) {
+      tp = __ldg(&T.nodes[k].topo);
+      A = __ldg(&T.nodes[k].com);
+      C = __ldg(&T.nodes[k].cell);
+    }
     while (k < rt.y) {
       const NodeRec* nd = T.nodes + k;
-      int4 tp = __ldg(&nd->topo);
-      float4 A = __ldg(&nd->com);
-      if (A.w == 0.0f) {
-        k = tp.z;
-        continue;
+      const bool live = A.w != 0.0f;  // mass-zero nodes are skipped
+      const bool acc = live && accept_node(C, gmin, gmax, P.beta);
+      const bool leaf = (tp.w & kLeafFlag) != 0;
+      const int next = (!live || acc || leaf) ? tp.z : k + 1;
+      int4 tpn = tp;
+      float4 An = A, Cn = C;
+      if (next < rt.y) {
+        tpn = __ldg(&T.nodes[next].topo);
+        An = __ldg(&T.nodes[next].com);
+        Cn = __ldg(&T.nodes[next].cell);
       }
-      if (accept_node(__ldg(&nd->cell), gmin, gmax, P.beta)) {
+      if (acc) {
         float4 Qd = make_float4(0.f, 0.f, 0.f, 0.f), X = Qd;
         if (QUAD) {
           Qd = __ldg(&nd->quad);
@@ -678,8 +693,7 @@ __global__ void __launch_bounds__(128, 4)
           }
         }
         nfar++;
-        k = tp.z;
-      } else if (tp.w & kLeafFlag) {
+      } else if (live && leaf) {
         float ax[kTPL], ay[kTPL], az[kTPL];
 #pragma unroll
         for (int t = 0; t < kTPL; t++) ax[t] = ay[t] = az[t] = 0.f;
@@ -710,10 +724,11 @@ __global__ void __launch_bounds__(128, 4)
           kahan_add(nz[t], cz[t], az[t]);
         }
         nnear += static_cast<unsigned long long>(tp.y - tp.x);
-        k = tp.z;
-      } else {
-        k++;
       }
+      k = next;
+      tp = tpn;
+      A = An;
+      C = Cn;
     }
 #pragma unroll
     for (int t = 0; t < kTPL; t++) {
@@ -1120,16 +1135,31 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
     for (int t = 0; t < kTPL; t++) far[t] = near[t] = comp[t] = 0.f;
     unsigned long long nfar = 0, nnear = 0;
+    // Pre-order walk. The next node is known once this node's opening test
+    // is done, so its opening data is loaded before this node's terms are
+    // evaluated and the load latency hides behind that arithmetic.
     int k = rt.x;
+    int4 tp = make_int4(0, 0, rt.y, 0);
+    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), C = A;
+    if (k < rt.y) {
+      tp = __ldg(&T.nodes[k].topo);
+      A = __ldg(&T.nodes[k].com);
+      C = __ldg(&T.nodes[k].cell);
+    }
     while (k < rt.y) {
       const NodeRec* nd = T.nodes + k;
-      int4 tp = __ldg(&nd->topo);
-      float4 A = __ldg(&nd->com);
-      if (A.w == 0.0f) {
-        k = tp.z;
-        continue;
+      const bool live = A.w != 0.0f;  // mass-zero nodes are skipped
+      const bool acc = live && accept_node(C, gmin, gmax, beta);
+      const bool leaf = (tp.w & kLeafFlag) != 0;
+      const int next = (!live || acc || leaf) ? tp.z : k + 1;
+      int4 tpn = tp;
+      float4 An = A, Cn = C;
+      if (next < rt.y) {
+        tpn = __ldg(&T.nodes[next].topo);
+        An = __ldg(&T.nodes[next].com);
+        Cn = __ldg(&T.nodes[next].cell);
       }
-      if (accept_node(__ldg(&nd->cell), gmin, gmax, beta)) {
+      if (acc) {
         float4 N = __ldg(&T.nnrm[k]);
 #pragma unroll
         for (int t = 0; t < kTPL; t++) {
@@ -1140,8 +1170,7 @@ __global__ void __launch_bounds__(128, 4)
           far[t] += A.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
         }
         nfar++;
-        k = tp.z;
-      } else if (tp.w & kLeafFlag) {
+      } else if (live && leaf) {
         float a[kTPL];
 #pragma unroll
         for (int t = 0; t < kTPL; t++) a[t] = 0.f;
@@ -1160,10 +1189,11 @@ __global__ void __launch_bounds__(128, 4)
 #pragma unroll
         for (int t = 0; t < kTPL; t++) kahan_add(near[t], comp[t], a[t]);
         nnear += static_cast<unsigned long long>(tp.y - tp.x);
-        k = tp.z;
-      } else {
-        k++;
       }
+      k = next;
+      tp = tpn;
+      A = An;
+      C = Cn;
     }
 #pragma unroll
     for (int t = 0; t < kTPL; t++)

@@ -278,14 +278,26 @@ __device__ int64_t contained_in_child(const NodeT<N>* nodes, int64_t idx, const 
 }
 
 // ---------------------------------------------------------------------------
-// kernels of include/kernel.h on a leaf record: scalar (K < 2 result in v[0])
-// or vector (v[0..N-1])
+// kernels of include/kernel.h on a leaf record: scalar (potential, winding
+// number: v[0]) or vector (v[0..N-1]). The two VJP kinds are the query-side
+// vector-Jacobian products of the force kernels with the cotangent g
+// (gravityGradVjp and gravityGradSoftCutoffVjp, src/sbh_ffi.cu:2044-2090,
+// written for N = 2 and 3).
 // ---------------------------------------------------------------------------
-enum TreeKernel { TK_POTENTIAL = 0, TK_GRAVITY_GRAD = 1, TK_SOFT = 2, TK_WINDING = 3 };
+enum TreeKernel {
+  TK_POTENTIAL = 0,
+  TK_GRAVITY_GRAD = 1,
+  TK_SOFT = 2,
+  TK_WINDING = 3,
+  TK_GRAVITY_GRAD_VJP = 4,
+  TK_SOFT_VJP = 5
+};
+
+constexpr bool is_vjp(int K) { return K == TK_GRAVITY_GRAD_VJP || K == TK_SOFT_VJP; }
 
 template <int N, int K>
-__device__ __forceinline__ void tree_kernel(const LeafT<N>& d, const Vec<N>& q, const Soft& s, const Periodic& per,
-                                            float* acc) {
+__device__ __forceinline__ void tree_kernel(const LeafT<N>& d, const Vec<N>& q, const Vec<N>& g, const Soft& s,
+                                            const Periodic& per, float* acc) {
   float r[N];
   if (K == TK_POTENTIAL || K == TK_WINDING) {
     for (int k = 0; k < N; k++) r[k] = min_image_floor(d.pos[k] - q.v[k], per);
@@ -308,9 +320,36 @@ __device__ __forceinline__ void tree_kernel(const LeafT<N>& d, const Vec<N>& q, 
   } else if (K == TK_GRAVITY_GRAD) {
     float c = grav_grad_coeff(r2, d.mass);
     for (int k = 0; k < N; k++) acc[k] += c * r[k];
-  } else {
+  } else if (K == TK_SOFT) {
     float c = soft_coeff(r2, d.mass, s);
     for (int k = 0; k < N; k++) acc[k] += c * r[k];
+  } else if (K == TK_GRAVITY_GRAD_VJP) {
+    // f = -m r / (|r| + 0.1)^3:  J^T g = -m (g / den^3 - 3 (r.g) / (|r| den^4) r)
+    float dist = sqrtf(r2 + 1e-12f);
+    float den = dist + 1e-1f;
+    float id3 = 1.0f / (den * den * den);
+    float id4 = id3 / den;
+    float rg = 0.f;
+    for (int k = 0; k < N; k++) rg += r[k] * g.v[k];
+    float kr = 3.0f * rg * (1.0f / (dist + 1e-12f)) * id4;
+    for (int k = 0; k < N; k++) acc[k] += -d.mass * (id3 * g.v[k] - kr * r[k]);
+  } else {
+    // f = -m att(r) (r^2 + eps^2)^-3/2 r:  J^T g = -m (att ir^3 g - (r.g)(3 att ir^5 + cc) r)
+    float ir = rsqrtf(r2 + s.eps * s.eps + 1e-12f);
+    float ir3 = ir * ir * ir;
+    float ir5 = ir3 * ir * ir;
+    float att = 1.0f, cc = 0.0f;
+    if (s.cutoff > 0.0f) {
+      float dist = sqrtf(r2 + 1e-12f);
+      float u = dist / (2.0f * s.cutoff);
+      float e = expf(-(u * u));
+      att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+      cc = ir3 * dist * e / (2.0f * 1.772453850905516f * s.cutoff * s.cutoff * s.cutoff);
+    }
+    float rg = 0.f;
+    for (int k = 0; k < N; k++) rg += r[k] * g.v[k];
+    float rad = rg * (3.0f * att * ir5 + cc);
+    for (int k = 0; k < N; k++) acc[k] += -d.mass * (att * ir3 * g.v[k] - rad * r[k]);
   }
 }
 
@@ -330,8 +369,8 @@ constexpr int kOut(int N, int K) { return (K == TK_POTENTIAL || K == TK_WINDING)
 // evaluateBarnesHutGPUVote (include/barnes_hut_gpu.h:19-72).
 template <int N, int K>
 __global__ void vote_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* __restrict__ nodes,
-                            const float* __restrict__ queries, int64_t nq, float beta, Soft s, Periodic per,
-                            float* __restrict__ out, Bounds bd, uint32_t* status) {
+                            const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq, float beta,
+                            Soft s, Periodic per, float* __restrict__ out, Bounds bd, uint32_t* status) {
   int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   bool active = qi < nq;
   // The lanes that exist in this warp (a block size that is not a multiple
@@ -341,9 +380,10 @@ __global__ void vote_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* _
   unsigned lanes = __activemask();
   unsigned warp_active = __ballot_sync(lanes, active);
   if (warp_active == 0) return;
-  Vec<N> q;
+  Vec<N> q, g;
   int64_t qq = active ? qi : 0;
   for (int k = 0; k < N; k++) q.v[k] = queries[N * qq + k];
+  for (int k = 0; k < N; k++) g.v[k] = is_vjp(K) ? cot[N * qq + k] : 0.0f;
   constexpr int NO = kOut(N, K);
   float acc[NO];
   for (int k = 0; k < NO; k++) acc[k] = 0.f;
@@ -363,9 +403,9 @@ __global__ void vote_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* _
         if (nd.is_leaf) {
           uint64_t e = nd.end <= bd.num_leaves ? nd.end : bd.num_leaves;
           if (nd.end > bd.num_leaves) raise_status(status, SBH_DEV_BAD_BOUNDS);
-          for (uint64_t i = nd.start; i < e; i++) tree_kernel<N, K>(leaf[i], q, s, per, acc);
+          for (uint64_t i = nd.start; i < e; i++) tree_kernel<N, K>(leaf[i], q, g, s, per, acc);
         } else {
-          tree_kernel<N, K>(nd.contrib, q, s, per, acc);
+          tree_kernel<N, K>(nd.contrib, q, g, s, per, acc);
         }
       } else {
         int fb = first_bit<N>(nd);
@@ -397,14 +437,20 @@ __global__ void vote_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* _
 
 // multiLevelPrefixControlVariateSampleGPUQuery (include/tree_sampler_gpu.h:25-140).
 template <int N, int K>
+// With a VJP kind the sampled paths and their weights are those of the
+// forward estimate for the same seed and only the kernel evaluations are
+// differentiated, as the reference's stochastic VJP does
+// (src/sbh_ffi.cu:2293-2442); the result is an unbiased estimate of the
+// exact sum's query-side VJP.
 __global__ void mlpcv_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* __restrict__ nodes,
-                             const LeafT<N>* __restrict__ contrib, const float* __restrict__ queries, int64_t nq,
-                             int samples, int seed, Soft s, Periodic per, float* __restrict__ out, Bounds bd,
-                             uint64_t num_contrib, uint32_t* status) {
+                             const LeafT<N>* __restrict__ contrib, const float* __restrict__ queries,
+                             const float* __restrict__ cot, int64_t nq, int samples, int seed, Soft s, Periodic per,
+                             float* __restrict__ out, Bounds bd, uint64_t num_contrib, uint32_t* status) {
   int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (qi >= nq) return;
-  Vec<N> q;
+  Vec<N> q, g;
   for (int k = 0; k < N; k++) q.v[k] = queries[N * qi + k];
+  for (int k = 0; k < N; k++) g.v[k] = is_vjp(K) ? cot[N * qi + k] : 0.0f;
   constexpr int NO = kOut(N, K);
   curandState st, st2;
   int sq = seed + static_cast<int>(qi);
@@ -418,9 +464,9 @@ __global__ void mlpcv_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* 
     if (si < 0) continue;
     const NodeT<N>& sub = nodes[si];
     if (sub.is_leaf) {
-      for (uint64_t i = sub.start; i < sub.end && i < bd.num_leaves; i++) tree_kernel<N, K>(leaf[i], q, s, per, bh);
+      for (uint64_t i = sub.start; i < sub.end && i < bd.num_leaves; i++) tree_kernel<N, K>(leaf[i], q, g, s, per, bh);
     } else {
-      tree_kernel<N, K>(sub.contrib, q, s, per, bh);
+      tree_kernel<N, K>(sub.contrib, q, g, s, per, bh);
     }
     uint64_t num_el = sub.end - sub.start;
     float sub_total[NO];
@@ -463,7 +509,7 @@ __global__ void mlpcv_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* 
         const NodeT<N>& pv = nodes[prev];
         float prev_res[NO], cur_res[NO];
         for (int k = 0; k < NO; k++) prev_res[k] = cur_res[k] = 0.f;
-        tree_kernel<N, K>(pv.contrib, q, s, per, prev_res);
+        tree_kernel<N, K>(pv.contrib, q, g, s, per, prev_res);
         int fb = first_bit<N>(pv);
         int64_t first = fb < TreeCfg<N>::kBranch ? static_cast<int64_t>(pv.child_idx[fb]) : 0;
         for (int off = 0; off < pv.num_children; off++) {
@@ -475,9 +521,9 @@ __global__ void mlpcv_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* 
           const NodeT<N>& ch = nodes[ci];
           if (ch.is_leaf) {
             for (uint64_t i = ch.start; i < ch.end && i < bd.num_leaves; i++)
-              tree_kernel<N, K>(leaf[i], q, s, per, cur_res);
+              tree_kernel<N, K>(leaf[i], q, g, s, per, cur_res);
           } else if (static_cast<uint64_t>(ci) < num_contrib) {
-            tree_kernel<N, K>(contrib[ci], q, s, per, cur_res);
+            tree_kernel<N, K>(contrib[ci], q, g, s, per, cur_res);
           }
         }
         float wgt = sample_prob_inv / (event_prob * static_cast<float>(pv.end - pv.start));
@@ -521,35 +567,55 @@ unsigned gsz(int64_t n) {
   return static_cast<unsigned>(b < 1 ? 1 : b);
 }
 
+template <int N, int K>
+void vote_launch(unsigned g, int threads, cudaStream_t stream, const LeafT<N>* L, const NodeT<N>* T,
+                 const float* queries, const float* cot, int64_t nq, float beta, Soft s, Periodic per, float* out,
+                 Bounds bd, uint32_t* status) {
+  vote_kernel<N, K><<<g, threads, 0, stream>>>(L, T, queries, cot, nq, beta, s, per, out, bd, status);
+}
+
 template <int N>
 int launch_tree(int kernel, cudaStream_t stream, const void* leaf, size_t leaf_bytes, const void* nodes,
-                size_t node_bytes, const float* queries, int64_t nq, float* out, float beta, Soft s, Periodic per,
-                int threads, uint32_t* status) {
+                size_t node_bytes, const float* queries, const float* cot, int64_t nq, float* out, float beta, Soft s,
+                Periodic per, int threads, uint32_t* status) {
   Bounds bd{node_bytes / sizeof(NodeT<N>), leaf_bytes / sizeof(LeafT<N>)};
   unsigned g = static_cast<unsigned>((nq + threads - 1) / threads);
   auto L = static_cast<const LeafT<N>*>(leaf);
   auto T = static_cast<const NodeT<N>*>(nodes);
   switch (kernel) {
     case TK_POTENTIAL:
-      vote_kernel<N, TK_POTENTIAL><<<g, threads, 0, stream>>>(L, T, queries, nq, beta, s, per, out, bd, status);
+      vote_launch<N, TK_POTENTIAL>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
       break;
     case TK_GRAVITY_GRAD:
-      vote_kernel<N, TK_GRAVITY_GRAD><<<g, threads, 0, stream>>>(L, T, queries, nq, beta, s, per, out, bd, status);
+      vote_launch<N, TK_GRAVITY_GRAD>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
       break;
     case TK_SOFT:
-      vote_kernel<N, TK_SOFT><<<g, threads, 0, stream>>>(L, T, queries, nq, beta, s, per, out, bd, status);
+      vote_launch<N, TK_SOFT>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
+      break;
+    case TK_GRAVITY_GRAD_VJP:
+      vote_launch<N, TK_GRAVITY_GRAD_VJP>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
+      break;
+    case TK_SOFT_VJP:
+      vote_launch<N, TK_SOFT_VJP>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
       break;
     default:
-      vote_kernel<N, TK_WINDING><<<g, threads, 0, stream>>>(L, T, queries, nq, beta, s, per, out, bd, status);
+      vote_launch<N, TK_WINDING>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
       break;
   }
   return check_launch("barnes_hut_tree");
 }
 
+template <int N, int K>
+void mlpcv_launch(unsigned g, int threads, cudaStream_t stream, const LeafT<N>* L, const NodeT<N>* T,
+                  const LeafT<N>* C, const float* queries, const float* cot, int64_t nq, int samples, int seed, Soft s,
+                  Periodic per, float* out, Bounds bd, uint64_t nc, uint32_t* status) {
+  mlpcv_kernel<N, K><<<g, threads, 0, stream>>>(L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc, status);
+}
+
 template <int N>
 int launch_mlpcv(int kernel, cudaStream_t stream, const void* leaf, size_t leaf_bytes, const void* nodes,
-                 size_t node_bytes, const void* contrib, size_t contrib_bytes, const float* queries, int64_t nq,
-                 float* out, int samples, int seed, Soft s, Periodic per, int threads, uint32_t* status) {
+                 size_t node_bytes, const void* contrib, size_t contrib_bytes, const float* queries, const float* cot,
+                 int64_t nq, float* out, int samples, int seed, Soft s, Periodic per, int threads, uint32_t* status) {
   Bounds bd{node_bytes / sizeof(NodeT<N>), leaf_bytes / sizeof(LeafT<N>)};
   uint64_t nc = contrib_bytes / sizeof(LeafT<N>);
   unsigned g = static_cast<unsigned>((nq + threads - 1) / threads);
@@ -558,20 +624,28 @@ int launch_mlpcv(int kernel, cudaStream_t stream, const void* leaf, size_t leaf_
   auto C = static_cast<const LeafT<N>*>(contrib);
   switch (kernel) {
     case TK_POTENTIAL:
-      mlpcv_kernel<N, TK_POTENTIAL><<<g, threads, 0, stream>>>(L, T, C, queries, nq, samples, seed, s, per, out, bd, nc,
-                                                               status);
+      mlpcv_launch<N, TK_POTENTIAL>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
+                                    status);
       break;
     case TK_GRAVITY_GRAD:
-      mlpcv_kernel<N, TK_GRAVITY_GRAD><<<g, threads, 0, stream>>>(L, T, C, queries, nq, samples, seed, s, per, out, bd,
-                                                                  nc, status);
+      mlpcv_launch<N, TK_GRAVITY_GRAD>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd,
+                                       nc, status);
       break;
     case TK_SOFT:
-      mlpcv_kernel<N, TK_SOFT><<<g, threads, 0, stream>>>(L, T, C, queries, nq, samples, seed, s, per, out, bd, nc,
-                                                          status);
+      mlpcv_launch<N, TK_SOFT>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
+                               status);
+      break;
+    case TK_GRAVITY_GRAD_VJP:
+      mlpcv_launch<N, TK_GRAVITY_GRAD_VJP>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out,
+                                           bd, nc, status);
+      break;
+    case TK_SOFT_VJP:
+      mlpcv_launch<N, TK_SOFT_VJP>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
+                                   status);
       break;
     default:
-      mlpcv_kernel<N, TK_WINDING><<<g, threads, 0, stream>>>(L, T, C, queries, nq, samples, seed, s, per, out, bd, nc,
-                                                             status);
+      mlpcv_launch<N, TK_WINDING>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
+                                  status);
       break;
   }
   return check_launch("stochastic_bh_tree");
@@ -631,17 +705,21 @@ int sbh_build_octree_level3(cudaStream_t stream, const float* points, const floa
   return check_launch("build_octree_level3");
 }
 
-int sbh_barnes_hut_tree(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes,
-                        const void* nodes, size_t node_bytes, const float* queries, int64_t nq, float* out, float beta,
-                        float softening_scale, float cutoff_scale, int periodic, float box_length, int threads,
-                        void* workspace, size_t workspace_bytes) {
+}  // extern "C"
+
+namespace {
+
+int tree_entry(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes, const void* nodes,
+               size_t node_bytes, const float* queries, const float* cot, int64_t nq, float* out, float beta,
+               float softening_scale, float cutoff_scale, int periodic, float box_length, int threads, void* workspace,
+               size_t workspace_bytes) {
   if (dim != 2 && dim != 3) return invalid("dim must be 2 or 3");
-  if (kernel < 0 || kernel > 3) return invalid("kernel must be 0 (potential), 1 (force), 2 (softened force) or 3 (winding number)");
   size_t ls = dim == 3 ? sizeof(Leaf3) : sizeof(Leaf2), ns = dim == 3 ? sizeof(Node3) : sizeof(Node2);
   if (leaf_bytes % ls != 0) return invalid("leaf_bytes size mismatch");
   if (node_bytes % ns != 0 || node_bytes == 0) return invalid("node_bytes size mismatch");
   if (threads <= 0 || threads > 1024) return invalid("threads must be in [1, 1024]");
   if (nq < 0) return invalid("num_queries must be >= 0");
+  if (is_vjp(kernel) && nq > 0 && !cot) return invalid("cotangent must be non-null");
   if (!workspace || workspace_bytes < kStatusBytes) return fail(SBH_ERR_WORKSPACE, "workspace too small");
   uint32_t* status = static_cast<uint32_t*>(workspace);
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
@@ -650,19 +728,18 @@ int sbh_barnes_hut_tree(cudaStream_t stream, int dim, int kernel, const void* le
   Soft s{fmaxf(softening_scale, 0.0f), cutoff_scale};
   Periodic per{periodic, box_length};
   if (dim == 3)
-    return launch_tree<3>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, out, beta, s, per, threads,
-                          status);
-  return launch_tree<2>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, queries, nq, out, beta, s, per, threads,
-                        status);
+    return launch_tree<3>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, queries, cot, nq, out, beta, s, per,
+                          threads, status);
+  return launch_tree<2>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, queries, cot, nq, out, beta, s, per,
+                        threads, status);
 }
 
-int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes,
-                           const void* nodes, size_t node_bytes, const void* contrib, size_t contrib_bytes,
-                           const float* queries, int64_t nq, float* out, int samples_per_subdomain, int seed,
-                           float softening_scale, float cutoff_scale, int periodic, float box_length, int threads,
-                           void* workspace, size_t workspace_bytes) {
+int stochastic_entry(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes, const void* nodes,
+                     size_t node_bytes, const void* contrib, size_t contrib_bytes, const float* queries,
+                     const float* cot, int64_t nq, float* out, int samples_per_subdomain, int seed,
+                     float softening_scale, float cutoff_scale, int periodic, float box_length, int threads,
+                     void* workspace, size_t workspace_bytes) {
   if (dim != 2 && dim != 3) return invalid("dim must be 2 or 3");
-  if (kernel < 0 || kernel > 3) return invalid("kernel must be in [0, 3]");
   size_t ls = dim == 3 ? sizeof(Leaf3) : sizeof(Leaf2), ns = dim == 3 ? sizeof(Node3) : sizeof(Node2);
   if (leaf_bytes % ls != 0) return invalid("leaf_bytes size mismatch");
   if (node_bytes % ns != 0 || node_bytes == 0) return invalid("node_bytes size mismatch");
@@ -670,6 +747,7 @@ int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void*
   if (threads <= 0 || threads > 1024) return invalid("threads must be in [1, 1024]");
   if (samples_per_subdomain <= 0) return invalid("samples_per_subdomain must be >= 1");
   if (nq < 0) return invalid("num_queries must be >= 0");
+  if (is_vjp(kernel) && nq > 0 && !cot) return invalid("cotangent must be non-null");
   if (!workspace || workspace_bytes < kStatusBytes) return fail(SBH_ERR_WORKSPACE, "workspace too small");
   uint32_t* status = static_cast<uint32_t*>(workspace);
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
@@ -678,10 +756,54 @@ int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void*
   Soft s{fmaxf(softening_scale, 0.0f), cutoff_scale};
   Periodic per{periodic, box_length};
   if (dim == 3)
-    return launch_mlpcv<3>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries, nq,
-                           out, samples_per_subdomain, seed, s, per, threads, status);
-  return launch_mlpcv<2>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries, nq, out,
-                         samples_per_subdomain, seed, s, per, threads, status);
+    return launch_mlpcv<3>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries, cot,
+                           nq, out, samples_per_subdomain, seed, s, per, threads, status);
+  return launch_mlpcv<2>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries, cot, nq,
+                         out, samples_per_subdomain, seed, s, per, threads, status);
+}
+
+}  // namespace
+
+extern "C" {
+
+int sbh_barnes_hut_tree(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes,
+                        const void* nodes, size_t node_bytes, const float* queries, int64_t nq, float* out, float beta,
+                        float softening_scale, float cutoff_scale, int periodic, float box_length, int threads,
+                        void* workspace, size_t workspace_bytes) {
+  if (kernel < 0 || kernel > 3)
+    return invalid("kernel must be 0 (potential), 1 (force), 2 (softened force) or 3 (winding number)");
+  return tree_entry(stream, dim, kernel, leaf, leaf_bytes, nodes, node_bytes, queries, nullptr, nq, out, beta,
+                    softening_scale, cutoff_scale, periodic, box_length, threads, workspace, workspace_bytes);
+}
+
+int sbh_barnes_hut_tree_vjp(cudaStream_t stream, int dim, int softened, const void* leaf, size_t leaf_bytes,
+                            const void* nodes, size_t node_bytes, const float* queries, int64_t nq,
+                            const float* cotangent, float* out, float beta, float softening_scale, float cutoff_scale,
+                            int periodic, float box_length, int threads, void* workspace, size_t workspace_bytes) {
+  return tree_entry(stream, dim, softened ? TK_SOFT_VJP : TK_GRAVITY_GRAD_VJP, leaf, leaf_bytes, nodes, node_bytes,
+                    queries, cotangent, nq, out, beta, softening_scale, cutoff_scale, periodic, box_length, threads,
+                    workspace, workspace_bytes);
+}
+
+int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes,
+                           const void* nodes, size_t node_bytes, const void* contrib, size_t contrib_bytes,
+                           const float* queries, int64_t nq, float* out, int samples_per_subdomain, int seed,
+                           float softening_scale, float cutoff_scale, int periodic, float box_length, int threads,
+                           void* workspace, size_t workspace_bytes) {
+  if (kernel < 0 || kernel > 3) return invalid("kernel must be in [0, 3]");
+  return stochastic_entry(stream, dim, kernel, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries,
+                          nullptr, nq, out, samples_per_subdomain, seed, softening_scale, cutoff_scale, periodic,
+                          box_length, threads, workspace, workspace_bytes);
+}
+
+int sbh_stochastic_bh_tree_vjp(cudaStream_t stream, int dim, int softened, const void* leaf, size_t leaf_bytes,
+                               const void* nodes, size_t node_bytes, const void* contrib, size_t contrib_bytes,
+                               const float* queries, int64_t nq, const float* cotangent, float* out,
+                               int samples_per_subdomain, int seed, float softening_scale, float cutoff_scale,
+                               int periodic, float box_length, int threads, void* workspace, size_t workspace_bytes) {
+  return stochastic_entry(stream, dim, softened ? TK_SOFT_VJP : TK_GRAVITY_GRAD_VJP, leaf, leaf_bytes, nodes,
+                          node_bytes, contrib, contrib_bytes, queries, cotangent, nq, out, samples_per_subdomain, seed,
+                          softening_scale, cutoff_scale, periodic, box_length, threads, workspace, workspace_bytes);
 }
 
 }  // extern "C"

@@ -98,6 +98,8 @@ _SIGS = {
                            _c_p, _c_sz], _c_i),
     "sbh_barnes_hut_force_octree8": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_f, _c_i, _c_f, _c_i,
                                       _c_p, _c_sz], _c_i),
+    "sbh_barnes_hut_force_octree8_vjp": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_i, _c_f,
+                                          _c_i, _c_p, _c_sz], _c_i),
     "sbh_barnes_hut_force_octree8_soft": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_f,
                                            _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_barnes_hut_force_octree8_soft_vjp": ([_c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f,
@@ -112,8 +114,12 @@ _SIGS = {
                                  _c_sz], _c_i),
     "sbh_barnes_hut_tree": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_f, _c_i,
                              _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_barnes_hut_tree_vjp": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f,
+                                 _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_stochastic_bh_tree": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_i, _c_i,
                                 _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_stochastic_bh_tree_vjp": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p,
+                                    _c_i, _c_i, _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_native_group_size": ([], _c_i),
     "sbh_native_workspace_bytes": ([_c_i64, _c_i, _c_i, _c_i, _c_i], _c_sz),
     "sbh_native_build": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_i, _c_i, _c_i, _c_p, _c_sz], _c_i),
@@ -447,6 +453,28 @@ def barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: float = 2
     return out
 
 
+def barnes_hut_force_octree8_vjp(leaf_bytes, node_bytes, queries, cotangent, *, beta: float = 2.0,
+                                 periodic: bool = False, box_length: float = 1.0, threads: int = 256,
+                                 check_status: bool = False):
+    """Analytic query-side VJP of barnes_hut_force_octree8 (the reference's
+    function of this name takes central finite differences of the forward,
+    python/jax_sbh_ffi.py:1372-1395)."""
+    dev = _device()
+    leaf, node, queries = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
+    cot = _f32(cotangent, dev)
+    _check_traversal(queries, periodic, box_length, threads)
+    if cot.shape != queries.shape:
+        raise ValueError("cotangent must have same shape as queries")
+    out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_barnes_hut_force_octree8_vjp(_stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(),
+                                                  _p(queries), queries.shape[0], _p(cot), _p(out), float(beta),
+                                                  int(bool(periodic)), float(box_length), int(threads), _p(ws),
+                                                  ws.numel()), "barnes_hut_force_octree8_vjp")
+    _status_after(ws, "barnes_hut_force_octree8_vjp", check_status)
+    return out
+
+
 def softened_barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: float = 2.0,
                                       softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
                                       prune_enabled: bool = True, prune_r_cut_mult: float = 4.0,
@@ -615,6 +643,72 @@ def softened_barnes_hut_force_octree8_recompute_vjp(points, masses, *, beta: flo
     cfg = (float(beta), float(softening_scale), float(cutoff_scale), int(max_depth), bool(prune_enabled),
            float(prune_r_cut_mult), bool(periodic), float(box_length), int(threads))
     return _SoftenedOctree8Recompute.apply(points, masses, cfg)
+
+
+class _StochasticOctree8Recompute(torch.autograd.Function):
+    """custom_vjp of python/jax_sbh_ffi.py:1900-2046 (softened variant
+    :2049-2248): forward builds the tree and evaluates the stochastic
+    estimate at the points themselves; backward rebuilds the tree from the
+    saved inputs and applies the query-side VJP with the same seed;
+    grad_masses = 0."""
+
+    @staticmethod
+    def forward(ctx, points, masses, softened, cfg):
+        ctx.save_for_backward(points, masses)
+        ctx.softened, ctx.cfg = softened, cfg
+        return _stochastic_octree8_self(False, softened, points, masses, None, cfg)
+
+    @staticmethod
+    def backward(ctx, cot):
+        points, masses = ctx.saved_tensors
+        gp = _stochastic_octree8_self(True, ctx.softened, points, masses, cot.contiguous(), ctx.cfg)
+        return gp, torch.zeros_like(masses), None, None
+
+
+def _stochastic_octree8_self(vjp, softened, points, masses, cot, cfg):
+    beta, sps, seed, s, c, depth, prune, mult, per, box, thr = cfg
+    leaf, node = build_octree8_buffers(points, torch.zeros_like(points), masses, max_depth=depth)
+    return _stochastic_octree8(vjp, softened, leaf, node, points, cot, beta, sps, seed, s, c, prune, mult, per, box,
+                               thr, False)
+
+
+def stochastic_barnes_hut_force_octree8_recompute_vjp(points, masses, *, beta: float = 1.0,
+                                                      samples_per_subdomain: int = 1, seed: int = 0,
+                                                      max_depth: int = 7, periodic: bool = False,
+                                                      box_length: float = 1.0, threads: int = 256) -> torch.Tensor:
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    dev = _device()
+    points = points if isinstance(points, torch.Tensor) else _f32(points, dev)
+    masses = masses if isinstance(masses, torch.Tensor) else _f32(masses, dev)
+    cfg = (float(beta), int(samples_per_subdomain), int(seed), 0.0, 1.0, int(max_depth), False, 4.0, bool(periodic),
+           float(box_length), int(threads))
+    return _StochasticOctree8Recompute.apply(points, masses, False, cfg)
+
+
+def softened_stochastic_barnes_hut_force_octree8_recompute_vjp(points, masses, *, beta: float = 1.0,
+                                                               samples_per_subdomain: int = 1, seed: int = 0,
+                                                               softening_scale: float = 1e-2,
+                                                               cutoff_scale: float = 1.0, max_depth: int = 7,
+                                                               prune_enabled: bool = True,
+                                                               prune_r_cut_mult: float = 4.0, periodic: bool = False,
+                                                               box_length: float = 1.0,
+                                                               threads: int = 256) -> torch.Tensor:
+    if prune_enabled and prune_r_cut_mult <= 0:
+        raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    dev = _device()
+    points = points if isinstance(points, torch.Tensor) else _f32(points, dev)
+    masses = masses if isinstance(masses, torch.Tensor) else _f32(masses, dev)
+    cfg = (float(beta), int(samples_per_subdomain), int(seed), float(softening_scale), float(cutoff_scale),
+           int(max_depth), bool(prune_enabled), float(prune_r_cut_mult), bool(periodic), float(box_length),
+           int(threads))
+    return _StochasticOctree8Recompute.apply(points, masses, True, cfg)
 
 
 # register_* exist in the reference to hand handler capsules to XLA; with
@@ -897,6 +991,47 @@ def softened_barnes_hut_force(leaf_bytes, node_bytes, queries, *, beta: float = 
                       box_length, threads)
 
 
+def _tree_vjp_call(softened, leaf_bytes, node_bytes, queries, cotangent, beta, softening_scale, cutoff_scale, periodic,
+                   box_length, threads):
+    dev = _device()
+    leaf, node, queries = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
+    cot = _f32(cotangent, dev)
+    if queries.ndim != 2 or queries.shape[1] not in (2, 3):
+        raise ValueError("queries must be (M, 2) or (M, 3)")
+    if cot.shape != queries.shape:
+        raise ValueError("cotangent must have same shape as queries")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    out = torch.empty(queries.shape, dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_barnes_hut_tree_vjp(_stream_ptr(dev), queries.shape[1], int(softened), _p(leaf), leaf.numel(),
+                                         _p(node), node.numel(), _p(queries), queries.shape[0], _p(cot), _p(out),
+                                         float(beta), float(softening_scale), float(cutoff_scale), int(bool(periodic)),
+                                         float(box_length), int(threads), _p(ws), ws.numel()), "barnes_hut_tree_vjp")
+    return out
+
+
+def barnes_hut_force_vjp(leaf_bytes, node_bytes, queries, cotangent, *, beta: float = 2.0, periodic: bool = False,
+                         box_length: float = 1.0, threads: int = 256):
+    """Analytic query-side VJP of barnes_hut_force with the forward's opening
+    decisions (the reference's function of this name takes central finite
+    differences, python/jax_sbh_ffi.py:1037-1060)."""
+    return _tree_vjp_call(False, leaf_bytes, node_bytes, queries, cotangent, beta, 0.0, 1.0, periodic, box_length,
+                          threads)
+
+
+def softened_barnes_hut_force_vjp(leaf_bytes, node_bytes, queries, cotangent, *, beta: float = 2.0,
+                                  softening_scale: float = 1e-2, cutoff_scale: float = 1.0, periodic: bool = False,
+                                  box_length: float = 1.0, threads: int = 256):
+    """Analytic query-side VJP of softened_barnes_hut_force (finite
+    differences in the reference, python/jax_sbh_ffi.py:1108-1135)."""
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    return _tree_vjp_call(True, leaf_bytes, node_bytes, queries, cotangent, beta, softening_scale, cutoff_scale,
+                          periodic, box_length, threads)
+
+
 def barnes_hut_winding_number(leaf_bytes, node_bytes, queries, *, beta: float = 2.0, threads: int = 256):
     """Winding number on a Node2/Node3 tree (new target; the reference has it
     only in its pybind module, src/sbh_gpu.cu:100-120)."""
@@ -948,6 +1083,55 @@ def softened_stochastic_barnes_hut_force(leaf_bytes, node_bytes, contrib_bytes, 
     return _stochastic_tree_call(TREE_SOFT_FORCE, leaf_bytes, node_bytes, contrib_bytes, queries,
                                  samples_per_subdomain, seed, softening_scale, cutoff_scale, periodic, box_length,
                                  threads)
+
+
+def _stochastic_tree_vjp_call(softened, leaf_bytes, node_bytes, contrib_bytes, queries, cotangent,
+                              samples_per_subdomain, seed, softening_scale, cutoff_scale, periodic, box_length,
+                              threads):
+    dev = _device()
+    leaf, node, contrib = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _u8(contrib_bytes, dev)
+    queries, cot = _f32(queries, dev), _f32(cotangent, dev)
+    if queries.ndim != 2 or queries.shape[1] not in (2, 3):
+        raise ValueError("queries must be (M, 2) or (M, 3)")
+    if cot.shape != queries.shape:
+        raise ValueError("cotangent must have same shape as queries")
+    if periodic and box_length <= 0:
+        raise ValueError("box_length must be > 0 when periodic=True")
+    if threads < 1:
+        raise ValueError("threads must be >= 1")
+    if samples_per_subdomain < 1:
+        raise ValueError("samples_per_subdomain must be >= 1")
+    out = torch.empty(queries.shape, dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    _check(lib().sbh_stochastic_bh_tree_vjp(_stream_ptr(dev), queries.shape[1], int(softened), _p(leaf), leaf.numel(),
+                                            _p(node), node.numel(), _p(contrib), contrib.numel(), _p(queries),
+                                            queries.shape[0], _p(cot), _p(out), int(samples_per_subdomain), int(seed),
+                                            float(softening_scale), float(cutoff_scale), int(bool(periodic)),
+                                            float(box_length), int(threads), _p(ws), ws.numel()),
+           "stochastic_bh_tree_vjp")
+    return out
+
+
+def stochastic_barnes_hut_force_vjp(leaf_bytes, node_bytes, contrib_bytes, queries, cotangent, *,
+                                    samples_per_subdomain: int = 1, seed: int = 0, periodic: bool = False,
+                                    box_length: float = 1.0, threads: int = 256):
+    """Query-side VJP of stochastic_barnes_hut_force with the forward's
+    sampled paths and weights for the same seed (finite differences in the
+    reference, python/jax_sbh_ffi.py:1222-1250)."""
+    return _stochastic_tree_vjp_call(False, leaf_bytes, node_bytes, contrib_bytes, queries, cotangent,
+                                     samples_per_subdomain, seed, 0.0, 1.0, periodic, box_length, threads)
+
+
+def softened_stochastic_barnes_hut_force_vjp(leaf_bytes, node_bytes, contrib_bytes, queries, cotangent, *,
+                                             samples_per_subdomain: int = 1, seed: int = 0,
+                                             softening_scale: float = 1e-2, cutoff_scale: float = 1.0,
+                                             periodic: bool = False, box_length: float = 1.0, threads: int = 256):
+    """Query-side VJP of softened_stochastic_barnes_hut_force (finite
+    differences in the reference, python/jax_sbh_ffi.py:1302-1334)."""
+    _check_soft(softening_scale, cutoff_scale, periodic, box_length, threads)
+    return _stochastic_tree_vjp_call(True, leaf_bytes, node_bytes, contrib_bytes, queries, cotangent,
+                                     samples_per_subdomain, seed, softening_scale, cutoff_scale, periodic, box_length,
+                                     threads)
 
 
 def stochastic_barnes_hut_winding_number(leaf_bytes, node_bytes, contrib_bytes, queries, *,

@@ -143,6 +143,16 @@ int sbh_barnes_hut_force_octree8(cudaStream_t stream, const void* leaf, size_t l
                                  float box_length, int threads, void* workspace,
                                  size_t workspace_bytes);
 
+/* Query-side VJP of sbh_barnes_hut_force_octree8 (gravityGradVjp,
+ * src/sbh_ffi.cu:2044-2060, in the same traversal). No handler counterpart:
+ * the reference's barnes_hut_force_octree8_vjp (python/jax_sbh_ffi.py:1372)
+ * takes central finite differences of the forward. */
+int sbh_barnes_hut_force_octree8_vjp(cudaStream_t stream, const void* leaf, size_t leaf_bytes,
+                                     const void* nodes, size_t node_bytes, const float* queries,
+                                     int64_t nq, const float* cotangent, float* out, float beta,
+                                     int periodic, float box_length, int threads, void* workspace,
+                                     size_t workspace_bytes);
+
 /* Replaces SoftenedBarnesHutForceOctree8 (src/sbh_ffi.cu:3183-3248). */
 int sbh_barnes_hut_force_octree8_soft(cudaStream_t stream, const void* leaf, size_t leaf_bytes,
                                       const void* nodes, size_t node_bytes,
@@ -233,6 +243,33 @@ int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void*
                            float softening_scale, float cutoff_scale, int periodic,
                            float box_length, int threads, void* workspace,
                            size_t workspace_bytes);
+
+/* Query-side VJPs on Node2/Node3 trees: out[nq*dim] = J(q)^T cotangent of the
+ * force (softened = 0: gravityGrad, 1: softened force), with the opening
+ * decisions of the forward traversal. No handler counterpart: the
+ * reference's barnes_hut_force_vjp and softened_barnes_hut_force_vjp
+ * (python/jax_sbh_ffi.py:1037-1135) take central finite differences of the
+ * forward; these evaluate the derivative kernels gravityGradVjp /
+ * gravityGradSoftCutoffVjp (src/sbh_ffi.cu:2044-2090) in the same walk. */
+int sbh_barnes_hut_tree_vjp(cudaStream_t stream, int dim, int softened, const void* leaf,
+                            size_t leaf_bytes, const void* nodes, size_t node_bytes,
+                            const float* queries, int64_t nq, const float* cotangent, float* out,
+                            float beta, float softening_scale, float cutoff_scale, int periodic,
+                            float box_length, int threads, void* workspace,
+                            size_t workspace_bytes);
+
+/* MLPCV query-side VJP with the forward's sampled paths and weights for the
+ * same seed (the convention of the reference's stochastic octree8 VJP,
+ * src/sbh_ffi.cu:2293-2442); replaces the finite differences of
+ * stochastic_barnes_hut_force_vjp and softened_stochastic_barnes_hut_force_vjp
+ * (python/jax_sbh_ffi.py:1222-1334). */
+int sbh_stochastic_bh_tree_vjp(cudaStream_t stream, int dim, int softened, const void* leaf,
+                               size_t leaf_bytes, const void* nodes, size_t node_bytes,
+                               const void* contrib, size_t contrib_bytes, const float* queries,
+                               int64_t nq, const float* cotangent, float* out,
+                               int samples_per_subdomain, int seed, float softening_scale,
+                               float cutoff_scale, int periodic, float box_length, int threads,
+                               void* workspace, size_t workspace_bytes);
 
 /* ---------------------------------------------------------------------- */
 /* Native adaptive octree (no reference counterpart: a new B200 path)     */
