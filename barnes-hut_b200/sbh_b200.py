@@ -120,6 +120,9 @@ _SIGS = {
                                 _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_stochastic_bh_tree_vjp": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p,
                                     _c_i, _c_i, _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_build_quadtree_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_build_quadtree": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz,
+                            _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_group_size": ([], _c_i),
     "sbh_native_workspace_bytes": ([_c_i64, _c_i, _c_i, _c_i, _c_i], _c_sz),
     "sbh_native_build": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_i, _c_i, _c_i, _c_p, _c_sz], _c_i),
@@ -948,6 +951,56 @@ def build_octree_buffers(points, normals, masses, min_corner=None, max_corner=No
                          level: int = 3, backend: str = "ffi"):
     leaf, node, _ = build_octree_buffers_with_contrib(points, normals, masses, min_corner, max_corner, alpha=alpha,
                                                       level=level, backend=backend)
+    return leaf, node
+
+
+NODE2_BYTES = 616
+LEAF2_BYTES = 24
+
+
+def build_quadtree_buffers_with_contrib(points, normals, masses, min_corner=None, max_corner=None, *,
+                                       alpha: float = 1.0, level: int = 3):
+    """The adaptive quadtree Tree2DNode<1,3> (leaf size 1, 8 x 8 split per
+    node) as (leaf_bytes, node_bytes, contrib_bytes) uint8 device tensors,
+    built on the GPU with the bytes of the reference's CPU builder
+    sbh.Quadtree3 (python/jax_sbh_ffi.py:692-742, include/tree2d.h)."""
+    if level != 3:
+        raise ValueError("level must be 3 (FFI expects Tree2DNode<1, 3>)")
+    dev = _device()
+    points, masses = _f32(points, dev), _f32(masses, dev)
+    if points.ndim != 2 or points.shape[1] != 2:
+        raise ValueError("points must have shape (N, 2)")
+    normals = _f32(normals, dev) if normals is not None else torch.zeros_like(points)
+    if normals.shape != points.shape:
+        raise ValueError("normals shape mismatch")
+    if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
+        raise ValueError("masses must have shape (N,)")
+    n = points.shape[0]
+    if n == 0:
+        raise ValueError("the quadtree needs at least one point")
+    mn, mx = _default_corners(points, min_corner, max_corner, dev)
+    leaf = torch.empty(n * LEAF2_BYTES, dtype=torch.uint8, device=dev)
+    ws = workspace(int(lib().sbh_build_quadtree_workspace_bytes(n)), dev)
+    cap = n + n // 2 + 64
+    while True:
+        node = torch.empty(cap * NODE2_BYTES, dtype=torch.uint8, device=dev)
+        contrib = torch.empty(cap * LEAF2_BYTES, dtype=torch.uint8, device=dev)
+        nn = ctypes.c_uint64(0)
+        rc = lib().sbh_build_quadtree(_stream_ptr(dev), _p(points), _p(normals), _p(masses), n, _p(mn), _p(mx),
+                                      float(alpha), _p(leaf), leaf.numel(), _p(node), node.numel(), _p(contrib),
+                                      contrib.numel(), ctypes.byref(nn), _p(ws), ws.numel())
+        if rc == SBH_ERR_LIMIT and nn.value > cap:
+            cap = int(nn.value)
+            continue
+        _check(rc, "build_quadtree_buffers")
+        k = int(nn.value)
+        return leaf, node[:k * NODE2_BYTES], contrib[:k * LEAF2_BYTES]
+
+
+def build_quadtree_buffers(points, normals, masses, min_corner=None, max_corner=None, *, alpha: float = 1.0,
+                           level: int = 3):
+    leaf, node, _ = build_quadtree_buffers_with_contrib(points, normals, masses, min_corner, max_corner, alpha=alpha,
+                                                        level=level)
     return leaf, node
 
 

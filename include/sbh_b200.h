@@ -244,6 +244,25 @@ int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void*
                            float box_length, int threads, void* workspace,
                            size_t workspace_bytes);
 
+/* GPU build of the adaptive quadtree Tree2DNode<1,3> (Node2, 616 bytes) that
+ * the reference builds on the CPU (sbh.Quadtree3, include/tree2d.h:237-330,
+ * include/py_tree.h:29-45, max_depth 100; used by build_quadtree_buffers,
+ * python/jax_sbh_ffi.py:658-724): leaf size 1, an 8 x 8 split per node,
+ * nodes in breadth-first order, the same bytes as the reference's builder
+ * for distinct points. points / normals (NULL: zeros) are n x 2, masses n,
+ * min_corner / max_corner 2 floats on the device. leaf_out is n * 24 bytes;
+ * node_out and contrib_out hold up to node_capacity_bytes / 616 nodes and
+ * contrib records. Synchronises the stream (once per tree level). On
+ * success *num_nodes is the node count; when node_out is too small the call
+ * returns SBH_ERR_LIMIT with a larger capacity to retry with in *num_nodes. */
+size_t sbh_build_quadtree_workspace_bytes(int64_t n);
+int sbh_build_quadtree(cudaStream_t stream, const float* points, const float* normals,
+                       const float* masses, int64_t n, const float* min_corner,
+                       const float* max_corner, float alpha, void* leaf_out, size_t leaf_bytes,
+                       void* node_out, size_t node_capacity_bytes, void* contrib_out,
+                       size_t contrib_capacity_bytes, uint64_t* num_nodes, void* workspace,
+                       size_t workspace_bytes);
+
 /* Query-side VJPs on Node2/Node3 trees: out[nq*dim] = J(q)^T cotangent of the
  * force (softened = 0: gravityGrad, 1: softened force), with the opening
  * decisions of the forward traversal. No handler counterpart: the

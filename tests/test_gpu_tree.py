@@ -171,3 +171,59 @@ def test_node3_winding_number_and_direct_limit(cuda):
     assert rel_l2(got, want) < 1e-5
     bh = B.barnes_hut_winding_number(leaf, node, q, beta=2.0).cpu().numpy()
     assert np.abs(bh - want).max() < 5e-2
+
+
+@pytest.mark.parametrize("dist", ["uniform", "plummer", "clustered", "one", "dupes"])
+def test_quadtree_build_matches_reference_cpu_builder(cuda, dist):
+    """The GPU quadtree builder gives the bytes of the reference's CPU builder
+    Tree2D<1,3> (sbh.Quadtree3) for leaves, nodes and contrib records."""
+    rng = np.random.default_rng(61)
+    if dist == "uniform":
+        p, m = W.uniform_cube(4000, seed=51)
+    elif dist == "plummer":
+        p, m = W.plummer(20000, seed=52)
+    elif dist == "clustered":
+        p, m = W.plummer(3000, seed=53)
+        p = p * np.float32(1e-3)  # deep chains of single-child nodes
+    elif dist == "one":
+        p, m = W.uniform_cube(1, seed=54)
+    else:
+        p, m = W.uniform_cube(500, seed=55)
+        p = np.concatenate([p, np.repeat(p[:2], 3, axis=0)])  # identical records: depth-100 leaves
+        m = np.full(p.shape[0], 1.0 / p.shape[0], np.float32)
+    p = np.ascontiguousarray(p[:, :2])
+    nrm = rng.normal(size=p.shape).astype(np.float32)
+    if dist == "dupes":
+        nrm[500:] = nrm[np.array([0, 0, 0, 1, 1, 1])]
+    mn = (p.min(0) - np.float32(1e-3)).astype(np.float32)
+    mx = (p.max(0) + np.float32(1e-3)).astype(np.float32)
+    t = O.RefTree2D(p, m, normals=nrm, min_corner=mn, max_corner=mx, alpha=0.75)
+    leaf, node, contrib = B.build_quadtree_buffers_with_contrib(p, nrm, m, mn, mx, alpha=0.75)
+    assert node.numel() == t.num_nodes * B.NODE2_BYTES
+    np.testing.assert_array_equal(leaf.cpu().numpy(), t.leaf_bytes())
+    # every byte but the struct padding (76-79 after the contrib record and
+    # 613-615 after is_leaf), which the reference's node copies leave
+    # unspecified and which we write as zeros
+    keep = np.ones(B.NODE2_BYTES, bool)
+    keep[76:80] = False
+    keep[613:616] = False
+    a = node.cpu().numpy().reshape(-1, B.NODE2_BYTES)[:, keep]
+    b = t.node_bytes().reshape(-1, B.NODE2_BYTES)[:, keep]
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(contrib.cpu().numpy(), t.contrib_bytes())
+
+
+def test_quadtree_buffers_drive_the_2d_targets(cuda):
+    p, m = W.plummer(6000, seed=57)
+    p = np.ascontiguousarray(p[:, :2])
+    leaf, node, contrib = B.build_quadtree_buffers_with_contrib(p, np.zeros_like(p), m)
+    q = p[:256]
+    got = B.barnes_hut_force(leaf, node, q, beta=1e30, threads=64).cpu().numpy()
+    r = q[:, None, :].astype(np.float64) - p[None, :, :].astype(np.float64)
+    d = np.sqrt((r * r).sum(-1))
+    want = (-m[None, :, None] * r / (d[..., None] + 0.1) ** 3).sum(1)
+    assert rel_l2(got, want) < 1e-5
+    bh = B.barnes_hut_force(leaf, node, q, beta=2.0, threads=64).cpu().numpy()
+    assert rel_l2(bh, want) < 2e-2
+    s = B.stochastic_barnes_hut_force(leaf, node, contrib, q, samples_per_subdomain=2, seed=1, threads=64)
+    assert torch.isfinite(s).all()
