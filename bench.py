@@ -517,11 +517,7 @@ def run_ours(args):
     walk_s = walk_ms / args.steps * 1e-3
     flops_walk = adjoint_walk_flops(st)
     fp32_peak = measure_fp32_peak(B, torch, dev)
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "adjoint_walk_traffic.json")
-    if os.path.exists(tpath):
-        tj = json.load(open(tpath))
-        traffic = tj.get("dram_bytes_per_interaction", 0) * (st["far"] + st["near"]) or None
+    traffic = WALK_DRAM_BYTES_PER_PARTICLE * n * K
 
     extras = {}
     if not args.no_extras:
@@ -594,6 +590,13 @@ def build_launches(k: int) -> int:
 
 
 WALK_LAUNCHES = 2
+
+# DRAM bytes (read + write) of one adjoint walk per particle, from one ncu
+# capture (dram__bytes_read.sum + dram__bytes_write.sum) of the walk over 4
+# Plummer systems of 262,144 particles: 163.89 MB + 55.94 MB for 1,048,576
+# particles. The walk's DRAM traffic is its L2 misses on the tree, the
+# particles and the adjoint arrays, which grow with the particle count.
+WALK_DRAM_BYTES_PER_PARTICLE = 209.6
 FINALIZE_LAUNCHES = 5
 
 # FP32 flops per interaction of the adjoint walk (force + adjoint, counted
