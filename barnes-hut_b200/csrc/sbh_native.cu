@@ -524,6 +524,20 @@ __device__ __forceinline__ uint32_t next_group(const WalkTargets& G) {
   return __shfl_sync(0xffffffffu, s, 0);
 }
 
+// Resident blocks of 128 threads per SM the walks are compiled for (this
+// caps their registers at 65536 / (128 x blocks)). Measured on a B200 with
+// 2 x 2^20 Plummer particles: the adjoint walk takes 145 ms at 4 blocks (96
+// registers), 138 ms at 6 (80 registers, no spills), 136 ms at 7 (72
+// registers, 24 bytes of spills); the force walk 63 ms at 5, 60 ms at 6.
+#ifndef SBH_ADJOINT_WALK_MIN_BLOCKS
+#define SBH_ADJOINT_WALK_MIN_BLOCKS 6
+#endif
+#ifndef SBH_FORCE_WALK_MIN_BLOCKS
+#define SBH_FORCE_WALK_MIN_BLOCKS 6
+#endif
+constexpr int kAdjointWalkMinBlocks = SBH_ADJOINT_WALK_MIN_BLOCKS;
+constexpr int kForceWalkMinBlocks = SBH_FORCE_WALK_MIN_BLOCKS;
+
 struct WalkParams {
   float beta;
   float eps2;    // softening^2 + 1e-12
@@ -609,7 +623,7 @@ __device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, f
 // 55, far node 200 including the share of the warp reductions.
 
 template <bool QUAD, bool CUT>
-__global__ void __launch_bounds__(128, 5)
+__global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
                       unsigned long long* __restrict__ counters) {
   const int lane = threadIdx.x & 31;
@@ -834,7 +848,7 @@ __device__ __forceinline__ int reduce10_index(int lane) {
 // A_X = -(that gradient), A_M = -lin (r.w) and
 // G = 1.5 ir^5 (w r^T + r w^T) + 1.5 ir^5 (r.w) I - 7.5 ir^7 (r.w) r r^T.
 template <bool QUAD, bool CUT>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
                         float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
                         float* __restrict__ part_adj, unsigned long long* __restrict__ counters) {
