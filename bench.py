@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=32768, help="queries timed by the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the octree8, forest and winding-number measurements")
+                    help="skip the octree8, forest, winding-number, stochastic and trajectory measurements")
     return ap.parse_args()
 
 
@@ -267,6 +267,81 @@ def forest_measurement(B, torch, dev, rank, world, flush):
     return dict(systems=int(b - a), particles=int(n), plain_ms=t_plain, batched_ms=t_batched, graph_ms=t_graph,
                 batched_over_plain=t_plain / t_graph,
                 particle_evals_per_s_graph=n / (t_graph * 1e-3), particle_evals_per_s_plain=n / (t_plain * 1e-3))
+
+
+def stochastic_measurement(B, torch, P0, M0, idx, ref, flush):
+    """Config 2a, stochastic variant: the reference's stochastic octree8
+    estimator (MLPCV, src/sbh_ffi.cu:2146-2291) on the 2^20-particle Plummer
+    system, depth-7 tree, at a sample of 65,536 queries (the first 1,024 of
+    them the accuracy subset). The reference has no "nodes per query" knob;
+    one and 32 particle paths per depth-3 subdomain (samples_per_subdomain)
+    are measured. Classic octree8 BH on the same queries beside it."""
+    rng = np.random.default_rng(17)
+    others = rng.choice(P0.shape[0], 65536 - idx.numel(), replace=False)
+    qidx = torch.cat([idx, torch.tensor(others, device=P0.device)])
+    Q = P0[qidx].contiguous()
+    Z = torch.zeros_like(P0)
+    span = float((P0.max(0).values - P0.min(0).values).max())
+    leaf, node = B.build_octree8_buffers(P0, Z, M0, max_depth=7)
+    kw = dict(beta=BETA, softening_scale=EPS, cutoff_scale=1e6 * span, prune_enabled=False)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1)
+
+    k = idx.numel()
+    rel = lambda f: float(torch.linalg.norm(f[:k].double() - ref) / torch.linalg.norm(ref))  # noqa: E731
+    out = dict(queries=int(Q.shape[0]), max_depth=7)
+    for sps in (1, 32):
+        st, st_ms = timed(lambda: B.softened_stochastic_barnes_hut_force_octree8(  # noqa: B023
+            leaf, node, Q, samples_per_subdomain=sps, seed=3, **kw))
+        out[f"stochastic_s{sps}"] = dict(ms=st_ms, queries_per_s=Q.shape[0] / (st_ms * 1e-3),
+                                         rel_l2_vs_fp64_direct=rel(st))
+    cl, cl_ms = timed(lambda: B.softened_barnes_hut_force_octree8(leaf, node, Q, **kw))
+    out["classic"] = dict(ms=cl_ms, queries_per_s=Q.shape[0] / (cl_ms * 1e-3), rel_l2_vs_fp64_direct=rel(cl))
+    return out
+
+
+def trajectory_measurement(torch, dev, flush):
+    """Config 5: 128^3 perturbed lattice (2,097,152 particles, P(k) ~ k^-2,
+    rms 0.2 cell), eps 2e-3, theta 0.6, 50 kick-drift-kick steps of dt 1e-3;
+    gradient of the mean squared final-position error to a seeded target
+    with respect to the initial displacements, checkpointing every 10 steps
+    (sbh_trajectory: native force and full adjoint per step)."""
+    import sbh_trajectory as T
+
+    p, m, disp = W.perturbed_lattice(128, seed=5, rms_cells=0.2)
+    target = p + np.random.default_rng(6).normal(scale=1e-3, size=p.shape).astype(np.float32)
+    x0 = torch.tensor(p, device=dev)
+    v0 = torch.zeros_like(x0)
+    mt = torch.tensor(m, device=dev)
+    tgt = torch.tensor(target, device=dev)
+    grav = T.Gravity(beta=1.0 / 0.6, softening=2e-3, leaf_size=LEAF)
+    steps, dt, ck = 50, 1e-3, 10
+    T.kdk(x0, v0, mt, 1, dt, grav)  # warm-up (workspaces)
+    torch.cuda.synchronize()
+    flush.zero_()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    xT, vT, ckpts = T.forward_with_checkpoints(x0, v0, mt, steps, dt, grav, checkpoint_every=ck)
+    e1.record()
+    n = x0.shape[0]
+    lx = 2.0 * (xT - tgt) / (n * 3)
+    gx0, gv0, gm = T.adjoint(ckpts, lx, torch.zeros_like(lx), mt, steps, dt, grav, checkpoint_every=ck)
+    e2.record()
+    torch.cuda.synchronize()
+    fwd, bwd = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    return dict(particles=int(n), steps=steps, checkpoint_every=ck, forward_ms=fwd, backward_ms=bwd,
+                total_s=(fwd + bwd) * 1e-3, force_evals=steps + 1, recomputed_forces=steps,
+                force_vjp_evals=steps + 1, grad_norm=float(torch.linalg.norm(gx0)),
+                loss=float(((xT - tgt) ** 2).mean()))
 
 
 def winding_measurement(B, torch, dev, flush):
@@ -526,6 +601,8 @@ def run_ours(args):
         extras["forest"] = forest_measurement(B, torch, dev, rank, world, flush)
         if world == 1:
             extras["winding_number"] = winding_measurement(B, torch, dev, flush)
+            extras["stochastic_octree8"] = stochastic_measurement(B, torch, P0, M0, idx, ref, flush)
+            extras["trajectory"] = trajectory_measurement(torch, dev, flush)
 
     if rank == 0:
         cpu = None
