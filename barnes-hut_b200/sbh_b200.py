@@ -121,6 +121,9 @@ _SIGS = {
     "sbh_stochastic_bh_tree_vjp": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p,
                                     _c_i, _c_i, _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_build_quadtree_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_build_adaptive_octree_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_build_adaptive_octree": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_p, _c_sz, _c_p, _c_sz, _c_p,
+                                   _c_sz, _c_p, _c_p, _c_sz], _c_i),
     "sbh_build_quadtree": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz,
                             _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_group_size": ([], _c_i),
@@ -916,14 +919,18 @@ TREE_POTENTIAL, TREE_FORCE, TREE_SOFT_FORCE, TREE_WINDING = 0, 1, 2, 3
 
 def build_octree_buffers_with_contrib(points, normals, masses, min_corner=None, max_corner=None, *,
                                       alpha: float = 1.0, level: int = 3, backend: str = "ffi"):
-    """Root + up to 512 leaf children on the 8^3 grid of [min, max], in the
-    Tree3DNode<1,3> layout (src/sbh_ffi.cu:736-1037). backend="cpu" (the
-    reference's sbh.Octree3 builder) is not part of this library."""
+    """Tree3DNode<1,3> buffers (python/jax_sbh_ffi.py:805-878).
+    backend="ffi": root + up to 512 leaf children on the 8^3 grid of
+    [min, max] (src/sbh_ffi.cu:736-1037). backend="cpu": the full adaptive
+    tree of the reference's CPU builder sbh.Octree3 (leaf size 1, alpha 1,
+    as the reference passes it), built here on the GPU with the same bytes."""
     del alpha
     if level != 3:
         raise ValueError("level must be 3 (FFI expects Tree3DNode<1, 3>)")
+    if backend == "cpu":
+        return _adaptive_tree(3, points, normals, masses, min_corner, max_corner, 1.0)
     if backend != "ffi":
-        raise ValueError("backend must be 'ffi' (the CPU builder is the reference's sbh module)")
+        raise ValueError("backend must be 'ffi' or 'cpu'")
     dev = _device()
     points, normals, masses = _f32(points, dev), _f32(normals, dev), _f32(masses, dev)
     if points.ndim != 2 or points.shape[1] != 3:
@@ -958,6 +965,43 @@ NODE2_BYTES = 616
 LEAF2_BYTES = 24
 
 
+def _adaptive_tree(dim, points, normals, masses, min_corner, max_corner, alpha):
+    """Leaf / node / contrib buffers of the reference's adaptive trees
+    (Tree2D<1,3> for dim 2, Tree3D<1,3> for dim 3), built on the GPU."""
+    dev = _device()
+    points, masses = _f32(points, dev), _f32(masses, dev)
+    if points.ndim != 2 or points.shape[1] != dim:
+        raise ValueError(f"points must have shape (N, {dim})")
+    normals = _f32(normals, dev) if normals is not None else torch.zeros_like(points)
+    if normals.shape != points.shape:
+        raise ValueError("normals shape mismatch")
+    if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
+        raise ValueError("masses must have shape (N,)")
+    n = points.shape[0]
+    if n == 0:
+        raise ValueError("the tree needs at least one point")
+    mn, mx = _default_corners(points, min_corner, max_corner, dev)
+    node_b, leaf_b = (NODE2_BYTES, LEAF2_BYTES) if dim == 2 else (node3_size(), leaf3_size())
+    build = lib().sbh_build_quadtree if dim == 2 else lib().sbh_build_adaptive_octree
+    wsb = lib().sbh_build_quadtree_workspace_bytes if dim == 2 else lib().sbh_build_adaptive_octree_workspace_bytes
+    leaf = torch.empty(n * leaf_b, dtype=torch.uint8, device=dev)
+    ws = workspace(int(wsb(n)), dev)
+    cap = n + n // 2 + 64
+    while True:
+        node = torch.empty(cap * node_b, dtype=torch.uint8, device=dev)
+        contrib = torch.empty(cap * leaf_b, dtype=torch.uint8, device=dev)
+        nn = ctypes.c_uint64(0)
+        rc = build(_stream_ptr(dev), _p(points), _p(normals), _p(masses), n, _p(mn), _p(mx), float(alpha), _p(leaf),
+                   leaf.numel(), _p(node), node.numel(), _p(contrib), contrib.numel(), ctypes.byref(nn), _p(ws),
+                   ws.numel())
+        if rc == SBH_ERR_LIMIT and nn.value > cap:
+            cap = int(nn.value)
+            continue
+        _check(rc, "build_quadtree_buffers" if dim == 2 else "build_octree_buffers")
+        k = int(nn.value)
+        return leaf, node[:k * node_b], contrib[:k * leaf_b]
+
+
 def build_quadtree_buffers_with_contrib(points, normals, masses, min_corner=None, max_corner=None, *,
                                        alpha: float = 1.0, level: int = 3):
     """The adaptive quadtree Tree2DNode<1,3> (leaf size 1, 8 x 8 split per
@@ -966,35 +1010,7 @@ def build_quadtree_buffers_with_contrib(points, normals, masses, min_corner=None
     sbh.Quadtree3 (python/jax_sbh_ffi.py:692-742, include/tree2d.h)."""
     if level != 3:
         raise ValueError("level must be 3 (FFI expects Tree2DNode<1, 3>)")
-    dev = _device()
-    points, masses = _f32(points, dev), _f32(masses, dev)
-    if points.ndim != 2 or points.shape[1] != 2:
-        raise ValueError("points must have shape (N, 2)")
-    normals = _f32(normals, dev) if normals is not None else torch.zeros_like(points)
-    if normals.shape != points.shape:
-        raise ValueError("normals shape mismatch")
-    if masses.ndim != 1 or masses.shape[0] != points.shape[0]:
-        raise ValueError("masses must have shape (N,)")
-    n = points.shape[0]
-    if n == 0:
-        raise ValueError("the quadtree needs at least one point")
-    mn, mx = _default_corners(points, min_corner, max_corner, dev)
-    leaf = torch.empty(n * LEAF2_BYTES, dtype=torch.uint8, device=dev)
-    ws = workspace(int(lib().sbh_build_quadtree_workspace_bytes(n)), dev)
-    cap = n + n // 2 + 64
-    while True:
-        node = torch.empty(cap * NODE2_BYTES, dtype=torch.uint8, device=dev)
-        contrib = torch.empty(cap * LEAF2_BYTES, dtype=torch.uint8, device=dev)
-        nn = ctypes.c_uint64(0)
-        rc = lib().sbh_build_quadtree(_stream_ptr(dev), _p(points), _p(normals), _p(masses), n, _p(mn), _p(mx),
-                                      float(alpha), _p(leaf), leaf.numel(), _p(node), node.numel(), _p(contrib),
-                                      contrib.numel(), ctypes.byref(nn), _p(ws), ws.numel())
-        if rc == SBH_ERR_LIMIT and nn.value > cap:
-            cap = int(nn.value)
-            continue
-        _check(rc, "build_quadtree_buffers")
-        k = int(nn.value)
-        return leaf, node[:k * NODE2_BYTES], contrib[:k * LEAF2_BYTES]
+    return _adaptive_tree(2, points, normals, masses, min_corner, max_corner, alpha)
 
 
 def build_quadtree_buffers(points, normals, masses, min_corner=None, max_corner=None, *, alpha: float = 1.0,

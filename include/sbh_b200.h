@@ -263,6 +263,19 @@ int sbh_build_quadtree(cudaStream_t stream, const float* points, const float* no
                        size_t contrib_capacity_bytes, uint64_t* num_nodes, void* workspace,
                        size_t workspace_bytes);
 
+/* The same for the adaptive octree Tree3DNode<1,3> (Node3, 4272 bytes; 8^3
+ * split per node) that the reference builds on the CPU (sbh.Octree3,
+ * include/tree3d.h:238-327, include/py_tree.h:58-75) for
+ * build_octree_buffers(backend="cpu") (python/jax_sbh_ffi.py:805-830).
+ * points / normals are n x 3, leaf_out n * 32 bytes, records as above. */
+size_t sbh_build_adaptive_octree_workspace_bytes(int64_t n);
+int sbh_build_adaptive_octree(cudaStream_t stream, const float* points, const float* normals,
+                              const float* masses, int64_t n, const float* min_corner,
+                              const float* max_corner, float alpha, void* leaf_out,
+                              size_t leaf_bytes, void* node_out, size_t node_capacity_bytes,
+                              void* contrib_out, size_t contrib_capacity_bytes,
+                              uint64_t* num_nodes, void* workspace, size_t workspace_bytes);
+
 /* Query-side VJPs on Node2/Node3 trees: out[nq*dim] = J(q)^T cotangent of the
  * force (softened = 0: gravityGrad, 1: softened force), with the opening
  * decisions of the forward traversal. No handler counterpart: the

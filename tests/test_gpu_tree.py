@@ -227,3 +227,34 @@ def test_quadtree_buffers_drive_the_2d_targets(cuda):
     assert rel_l2(bh, want) < 2e-2
     s = B.stochastic_barnes_hut_force(leaf, node, contrib, q, samples_per_subdomain=2, seed=1, threads=64)
     assert torch.isfinite(s).all()
+
+
+@pytest.mark.parametrize("dist", ["uniform", "plummer", "clustered", "one"])
+def test_adaptive_octree_build_matches_reference_cpu_builder(cuda, dist):
+    """build_octree_buffers(backend="cpu"): the GPU builder of the adaptive
+    Tree3D<1,3> gives the bytes of the reference's CPU builder sbh.Octree3."""
+    rng = np.random.default_rng(62)
+    if dist == "uniform":
+        p, m = W.uniform_cube(3000, seed=71)
+    elif dist == "plummer":
+        p, m = W.plummer(6000, seed=72)
+    elif dist == "clustered":
+        p, m = W.plummer(1500, seed=73)
+        p = p * np.float32(1e-3)
+    else:
+        p, m = W.uniform_cube(1, seed=74)
+    nrm = rng.normal(size=p.shape).astype(np.float32)
+    mn = (p.min(0) - np.float32(1e-3)).astype(np.float32)
+    mx = (p.max(0) + np.float32(1e-3)).astype(np.float32)
+    t = O.RefTree3D(p, m, normals=nrm, min_corner=mn, max_corner=mx, variant=2, alpha=1.0)
+    leaf, node, contrib = B.build_octree_buffers_with_contrib(p, nrm, m, mn, mx, backend="cpu")
+    size = B.node3_size()
+    assert node.numel() == t.num_nodes * size
+    np.testing.assert_array_equal(leaf.cpu().numpy(), t.leaf_bytes())
+    keep = np.ones(size, bool)
+    keep[92:96] = False  # padding after the contrib record
+    keep[4269:4272] = False  # padding after is_leaf
+    a = node.cpu().numpy().reshape(-1, size)[:, keep]
+    b = t.node_bytes().reshape(-1, size)[:, keep]
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(contrib.cpu().numpy(), t.contrib_bytes())
