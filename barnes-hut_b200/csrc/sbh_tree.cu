@@ -290,7 +290,8 @@ enum TreeKernel {
   TK_SOFT = 2,
   TK_WINDING = 3,
   TK_GRAVITY_GRAD_VJP = 4,
-  TK_SOFT_VJP = 5
+  TK_SOFT_VJP = 5,
+  TK_SMOOTHDIST = 6  // smoothDistExp (include/kernel.h:82-87): exp(-alpha |p - q|)
 };
 
 constexpr bool is_vjp(int K) { return K == TK_GRAVITY_GRAD_VJP || K == TK_SOFT_VJP; }
@@ -299,7 +300,7 @@ template <int N, int K>
 __device__ __forceinline__ void tree_kernel(const LeafT<N>& d, const Vec<N>& q, const Vec<N>& g, const Soft& s,
                                             const Periodic& per, float* acc) {
   float r[N];
-  if (K == TK_POTENTIAL || K == TK_WINDING) {
+  if (K == TK_POTENTIAL || K == TK_WINDING || K == TK_SMOOTHDIST) {
     for (int k = 0; k < N; k++) r[k] = min_image_floor(d.pos[k] - q.v[k], per);
   } else {
     for (int k = 0; k < N; k++) r[k] = min_image_floor(q.v[k] - d.pos[k], per);
@@ -308,6 +309,8 @@ __device__ __forceinline__ void tree_kernel(const LeafT<N>& d, const Vec<N>& q, 
   for (int k = 0; k < N; k++) r2 += r[k] * r[k];
   if (K == TK_POTENTIAL) {
     acc[0] += -d.mass / (sqrtf(r2) + 1e-1f);
+  } else if (K == TK_SMOOTHDIST) {
+    acc[0] += expf(-d.alpha * sqrtf(r2));
   } else if (K == TK_WINDING) {
     float nd = 0.f;
     for (int k = 0; k < N; k++) nd += d.nrm[k] * r[k];
@@ -364,7 +367,7 @@ __device__ __forceinline__ float far_ratio(const NodeT<N>& nd, const Vec<N>& q) 
   return sqrtf(d2) / nd.diameter;
 }
 
-constexpr int kOut(int N, int K) { return (K == TK_POTENTIAL || K == TK_WINDING) ? 1 : N; }
+constexpr int kOut(int N, int K) { return (K == TK_POTENTIAL || K == TK_WINDING || K == TK_SMOOTHDIST) ? 1 : N; }
 
 // evaluateBarnesHutGPUVote (include/barnes_hut_gpu.h:19-72).
 template <int N, int K>
@@ -444,8 +447,9 @@ template <int N, int K>
 // exact sum's query-side VJP.
 __global__ void mlpcv_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* __restrict__ nodes,
                              const LeafT<N>* __restrict__ contrib, const float* __restrict__ queries,
-                             const float* __restrict__ cot, int64_t nq, int samples, int seed, Soft s, Periodic per,
-                             float* __restrict__ out, Bounds bd, uint64_t num_contrib, uint32_t* status) {
+                             const float* __restrict__ cot, int64_t nq, int samples, int seed, int seed_stride,
+                             Soft s, Periodic per, float* __restrict__ out, Bounds bd, uint64_t num_contrib,
+                             uint32_t* status) {
   int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (qi >= nq) return;
   Vec<N> q, g;
@@ -453,7 +457,9 @@ __global__ void mlpcv_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* 
   for (int k = 0; k < N; k++) g.v[k] = is_vjp(K) ? cot[N * qi + k] : 0.0f;
   constexpr int NO = kOut(N, K);
   curandState st, st2;
-  int sq = seed + static_cast<int>(qi);
+  // the FFI handlers seed each query with seed + q (src/sbh_ffi.cu:1553-1680);
+  // the pybind module passes 0 to every query (src/sbh_gpu.cu:143-208)
+  int sq = seed + seed_stride * static_cast<int>(qi);
   curand_init(static_cast<unsigned long long>(static_cast<long long>(sq)), 0, 0, &st);
   curand_init(static_cast<unsigned long long>(blockIdx.x), 0, 0, &st2);
   float bh[NO], mlcv[NO];
@@ -536,6 +542,44 @@ __global__ void mlpcv_kernel(const LeafT<N>* __restrict__ leaf, const NodeT<N>* 
   for (int k = 0; k < NO; k++) out[NO * qi + k] = bh[k] + mlcv[k];
 }
 
+// bruteForceSummationGPU (include/brute_force_gpu.h:19-65): every leaf record
+// in leaf order with Kahan compensation, the block staging a tile of
+// records in shared memory at a time.
+template <int N, int K>
+__global__ void brute_kernel(const LeafT<N>* __restrict__ leaf, int64_t n, const float* __restrict__ queries,
+                             int64_t nq, float* __restrict__ out) {
+  extern __shared__ unsigned char smem[];
+  LeafT<N>* tile = reinterpret_cast<LeafT<N>*>(smem);
+  int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  bool active = qi < nq;
+  Vec<N> q, g;
+  for (int k = 0; k < N; k++) {
+    q.v[k] = active ? queries[N * qi + k] : 0.0f;
+    g.v[k] = 0.0f;
+  }
+  Soft s{0.0f, 0.0f};
+  Periodic per{0, 1.0f};
+  float total = 0.0f, c = 0.0f;
+  for (int64_t i = 0; i < n; i += blockDim.x) {
+    int64_t j = i + threadIdx.x;
+    if (j < n) tile[threadIdx.x] = leaf[j];
+    __syncthreads();
+    if (active) {
+      int64_t lim = n - i < static_cast<int64_t>(blockDim.x) ? n - i : static_cast<int64_t>(blockDim.x);
+      for (int64_t b = 0; b < lim; b++) {
+        float v = 0.0f;
+        tree_kernel<N, K>(tile[b], q, g, s, per, &v);
+        float y = v - c;
+        float t = total + y;
+        c = (t - total) - y;
+        total = t;
+      }
+    }
+    __syncthreads();
+  }
+  if (active) out[qi] = total;
+}
+
 }  // namespace tr
 }  // namespace sbh
 
@@ -598,6 +642,9 @@ int launch_tree(int kernel, cudaStream_t stream, const void* leaf, size_t leaf_b
     case TK_SOFT_VJP:
       vote_launch<N, TK_SOFT_VJP>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
       break;
+    case TK_SMOOTHDIST:
+      vote_launch<N, TK_SMOOTHDIST>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
+      break;
     default:
       vote_launch<N, TK_WINDING>(g, threads, stream, L, T, queries, cot, nq, beta, s, per, out, bd, status);
       break;
@@ -607,47 +654,36 @@ int launch_tree(int kernel, cudaStream_t stream, const void* leaf, size_t leaf_b
 
 template <int N, int K>
 void mlpcv_launch(unsigned g, int threads, cudaStream_t stream, const LeafT<N>* L, const NodeT<N>* T,
-                  const LeafT<N>* C, const float* queries, const float* cot, int64_t nq, int samples, int seed, Soft s,
-                  Periodic per, float* out, Bounds bd, uint64_t nc, uint32_t* status) {
-  mlpcv_kernel<N, K><<<g, threads, 0, stream>>>(L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc, status);
+                  const LeafT<N>* C, const float* queries, const float* cot, int64_t nq, int samples, int seed,
+                  int seed_stride, Soft s, Periodic per, float* out, Bounds bd, uint64_t nc, uint32_t* status) {
+  mlpcv_kernel<N, K><<<g, threads, 0, stream>>>(L, T, C, queries, cot, nq, samples, seed, seed_stride, s, per, out, bd,
+                                                nc, status);
 }
 
 template <int N>
 int launch_mlpcv(int kernel, cudaStream_t stream, const void* leaf, size_t leaf_bytes, const void* nodes,
                  size_t node_bytes, const void* contrib, size_t contrib_bytes, const float* queries, const float* cot,
-                 int64_t nq, float* out, int samples, int seed, Soft s, Periodic per, int threads, uint32_t* status) {
+                 int64_t nq, float* out, int samples, int seed, int seed_stride, Soft s, Periodic per, int threads,
+                 uint32_t* status) {
   Bounds bd{node_bytes / sizeof(NodeT<N>), leaf_bytes / sizeof(LeafT<N>)};
   uint64_t nc = contrib_bytes / sizeof(LeafT<N>);
   unsigned g = static_cast<unsigned>((nq + threads - 1) / threads);
   auto L = static_cast<const LeafT<N>*>(leaf);
   auto T = static_cast<const NodeT<N>*>(nodes);
   auto C = static_cast<const LeafT<N>*>(contrib);
+#define SBH_MLPCV(KIND)                                                                                            \
+  mlpcv_launch<N, KIND>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, seed_stride, s, per, out, bd, \
+                        nc, status)
   switch (kernel) {
-    case TK_POTENTIAL:
-      mlpcv_launch<N, TK_POTENTIAL>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
-                                    status);
-      break;
-    case TK_GRAVITY_GRAD:
-      mlpcv_launch<N, TK_GRAVITY_GRAD>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd,
-                                       nc, status);
-      break;
-    case TK_SOFT:
-      mlpcv_launch<N, TK_SOFT>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
-                               status);
-      break;
-    case TK_GRAVITY_GRAD_VJP:
-      mlpcv_launch<N, TK_GRAVITY_GRAD_VJP>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out,
-                                           bd, nc, status);
-      break;
-    case TK_SOFT_VJP:
-      mlpcv_launch<N, TK_SOFT_VJP>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
-                                   status);
-      break;
-    default:
-      mlpcv_launch<N, TK_WINDING>(g, threads, stream, L, T, C, queries, cot, nq, samples, seed, s, per, out, bd, nc,
-                                  status);
-      break;
+    case TK_POTENTIAL: SBH_MLPCV(TK_POTENTIAL); break;
+    case TK_GRAVITY_GRAD: SBH_MLPCV(TK_GRAVITY_GRAD); break;
+    case TK_SOFT: SBH_MLPCV(TK_SOFT); break;
+    case TK_GRAVITY_GRAD_VJP: SBH_MLPCV(TK_GRAVITY_GRAD_VJP); break;
+    case TK_SOFT_VJP: SBH_MLPCV(TK_SOFT_VJP); break;
+    case TK_SMOOTHDIST: SBH_MLPCV(TK_SMOOTHDIST); break;
+    default: SBH_MLPCV(TK_WINDING); break;
   }
+#undef SBH_MLPCV
   return check_launch("stochastic_bh_tree");
 }
 
@@ -737,8 +773,8 @@ int tree_entry(cudaStream_t stream, int dim, int kernel, const void* leaf, size_
 int stochastic_entry(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes, const void* nodes,
                      size_t node_bytes, const void* contrib, size_t contrib_bytes, const float* queries,
                      const float* cot, int64_t nq, float* out, int samples_per_subdomain, int seed,
-                     float softening_scale, float cutoff_scale, int periodic, float box_length, int threads,
-                     void* workspace, size_t workspace_bytes) {
+                     int seed_stride, float softening_scale, float cutoff_scale, int periodic, float box_length,
+                     int threads, void* workspace, size_t workspace_bytes) {
   if (dim != 2 && dim != 3) return invalid("dim must be 2 or 3");
   size_t ls = dim == 3 ? sizeof(Leaf3) : sizeof(Leaf2), ns = dim == 3 ? sizeof(Node3) : sizeof(Node2);
   if (leaf_bytes % ls != 0) return invalid("leaf_bytes size mismatch");
@@ -757,9 +793,9 @@ int stochastic_entry(cudaStream_t stream, int dim, int kernel, const void* leaf,
   Periodic per{periodic, box_length};
   if (dim == 3)
     return launch_mlpcv<3>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries, cot,
-                           nq, out, samples_per_subdomain, seed, s, per, threads, status);
+                           nq, out, samples_per_subdomain, seed, seed_stride, s, per, threads, status);
   return launch_mlpcv<2>(kernel, stream, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries, cot, nq,
-                         out, samples_per_subdomain, seed, s, per, threads, status);
+                         out, samples_per_subdomain, seed, seed_stride, s, per, threads, status);
 }
 
 }  // namespace
@@ -770,8 +806,9 @@ int sbh_barnes_hut_tree(cudaStream_t stream, int dim, int kernel, const void* le
                         const void* nodes, size_t node_bytes, const float* queries, int64_t nq, float* out, float beta,
                         float softening_scale, float cutoff_scale, int periodic, float box_length, int threads,
                         void* workspace, size_t workspace_bytes) {
-  if (kernel < 0 || kernel > 3)
-    return invalid("kernel must be 0 (potential), 1 (force), 2 (softened force) or 3 (winding number)");
+  if (kernel < 0 || (kernel > 3 && kernel != TK_SMOOTHDIST))
+    return invalid("kernel must be 0 (potential), 1 (force), 2 (softened force), 3 (winding number) or 6 (smooth "
+                   "distance)");
   return tree_entry(stream, dim, kernel, leaf, leaf_bytes, nodes, node_bytes, queries, nullptr, nq, out, beta,
                     softening_scale, cutoff_scale, periodic, box_length, threads, workspace, workspace_bytes);
 }
@@ -792,7 +829,7 @@ int sbh_stochastic_bh_tree(cudaStream_t stream, int dim, int kernel, const void*
                            void* workspace, size_t workspace_bytes) {
   if (kernel < 0 || kernel > 3) return invalid("kernel must be in [0, 3]");
   return stochastic_entry(stream, dim, kernel, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries,
-                          nullptr, nq, out, samples_per_subdomain, seed, softening_scale, cutoff_scale, periodic,
+                          nullptr, nq, out, samples_per_subdomain, seed, 1, softening_scale, cutoff_scale, periodic,
                           box_length, threads, workspace, workspace_bytes);
 }
 
@@ -803,7 +840,48 @@ int sbh_stochastic_bh_tree_vjp(cudaStream_t stream, int dim, int softened, const
                                int periodic, float box_length, int threads, void* workspace, size_t workspace_bytes) {
   return stochastic_entry(stream, dim, softened ? TK_SOFT_VJP : TK_GRAVITY_GRAD_VJP, leaf, leaf_bytes, nodes,
                           node_bytes, contrib, contrib_bytes, queries, cotangent, nq, out, samples_per_subdomain, seed,
-                          softening_scale, cutoff_scale, periodic, box_length, threads, workspace, workspace_bytes);
+                          1, softening_scale, cutoff_scale, periodic, box_length, threads, workspace, workspace_bytes);
+}
+
+int sbh_stochastic_bh_tree_shared_seed(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes,
+                                       const void* nodes, size_t node_bytes, const void* contrib,
+                                       size_t contrib_bytes, const float* queries, int64_t nq, float* out,
+                                       int samples_per_subdomain, int seed, int threads, void* workspace,
+                                       size_t workspace_bytes) {
+  if (kernel != TK_POTENTIAL && kernel != TK_WINDING && kernel != TK_SMOOTHDIST)
+    return invalid("kernel must be 0 (potential), 3 (winding number) or 6 (smooth distance)");
+  return stochastic_entry(stream, dim, kernel, leaf, leaf_bytes, nodes, node_bytes, contrib, contrib_bytes, queries,
+                          nullptr, nq, out, samples_per_subdomain, seed, 0, 0.0f, 1.0f, 0, 1.0f, threads, workspace,
+                          workspace_bytes);
+}
+
+int sbh_brute_force_tree(cudaStream_t stream, int dim, int kernel, const void* leaf, size_t leaf_bytes,
+                         const float* queries, int64_t nq, float* out, int threads) {
+  if (dim != 2 && dim != 3) return invalid("dim must be 2 or 3");
+  if (kernel != TK_POTENTIAL && kernel != TK_WINDING && kernel != TK_SMOOTHDIST)
+    return invalid("kernel must be 0 (potential), 3 (winding number) or 6 (smooth distance)");
+  size_t ls = dim == 3 ? sizeof(Leaf3) : sizeof(Leaf2);
+  if (leaf_bytes % ls != 0) return invalid("leaf_bytes size mismatch");
+  if (threads <= 0 || threads > 1024) return invalid("threads must be in [1, 1024]");
+  if (nq < 0) return invalid("num_queries must be >= 0");
+  if (nq == 0) return SBH_OK;
+  if (!queries || !out || (leaf_bytes > 0 && !leaf)) return invalid("leaf, queries and out must be non-null");
+  int64_t n = static_cast<int64_t>(leaf_bytes / ls);
+  unsigned g = static_cast<unsigned>((nq + threads - 1) / threads);
+  size_t sm = threads * ls;
+#define SBH_BRUTE(D, KIND) \
+  brute_kernel<D, KIND><<<g, threads, sm, stream>>>(static_cast<const LeafT<D>*>(leaf), n, queries, nq, out)
+  if (dim == 3) {
+    if (kernel == TK_POTENTIAL) SBH_BRUTE(3, TK_POTENTIAL);
+    else if (kernel == TK_WINDING) SBH_BRUTE(3, TK_WINDING);
+    else SBH_BRUTE(3, TK_SMOOTHDIST);
+  } else {
+    if (kernel == TK_POTENTIAL) SBH_BRUTE(2, TK_POTENTIAL);
+    else if (kernel == TK_WINDING) SBH_BRUTE(2, TK_WINDING);
+    else SBH_BRUTE(2, TK_SMOOTHDIST);
+  }
+#undef SBH_BRUTE
+  return check_launch("brute_force_tree");
 }
 
 }  // extern "C"

@@ -118,6 +118,9 @@ _SIGS = {
                                  _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_stochastic_bh_tree": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_i, _c_i,
                                 _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
+    "sbh_brute_force_tree": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_i], _c_i),
+    "sbh_stochastic_bh_tree_shared_seed": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p,
+                                            _c_i, _c_i, _c_i, _c_p, _c_sz], _c_i),
     "sbh_stochastic_bh_tree_vjp": ([_c_p, _c_i, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p,
                                     _c_i, _c_i, _c_f, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_build_quadtree_workspace_bytes": ([_c_i64], _c_sz),
@@ -915,6 +918,7 @@ def native_force_recompute_vjp(points, masses, *, beta: float = 2.0, softening: 
 # 963-1334)
 # ---------------------------------------------------------------------------
 TREE_POTENTIAL, TREE_FORCE, TREE_SOFT_FORCE, TREE_WINDING = 0, 1, 2, 3
+TREE_SMOOTHDIST = 6
 
 
 def build_octree_buffers_with_contrib(points, normals, masses, min_corner=None, max_corner=None, *,
@@ -1207,3 +1211,91 @@ def stochastic_barnes_hut_winding_number(leaf_bytes, node_bytes, contrib_bytes, 
                                          samples_per_subdomain: int = 1, seed: int = 0, threads: int = 256):
     return _stochastic_tree_call(TREE_WINDING, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain,
                                  seed, 0.0, 1.0, False, 1.0, threads)
+
+
+# ---------------------------------------------------------------------------
+# the reference's pybind module sbh_gpu (src/sbh_gpu.cu:566-661): scalar
+# kernels on Node2/Node3 trees by brute force, warp-vote BH and MLPCV. The
+# module wraps a CPU-built tree object; here the tree is its buffers (from
+# build_quadtree_buffers_with_contrib or build_octree_buffers_with_contrib).
+# Each returns (values, milliseconds on the GPU), as the module does.
+# ---------------------------------------------------------------------------
+def _timed(fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = fn()
+    e1.record()
+    e1.synchronize()
+    return out, e0.elapsed_time(e1)
+
+
+def _brute(kind, leaf_bytes, queries):
+    dev = _device()
+    leaf, queries = _u8(leaf_bytes, dev), _f32(queries, dev)
+    if queries.ndim != 2 or queries.shape[1] not in (2, 3):
+        raise ValueError("queries must be (M, 2) or (M, 3)")
+    out = torch.empty(queries.shape[0], dtype=torch.float32, device=dev)
+
+    def run():
+        _check(lib().sbh_brute_force_tree(_stream_ptr(dev), queries.shape[1], kind, _p(leaf), leaf.numel(),
+                                          _p(queries), queries.shape[0], _p(out), 32), "brute_force_tree")
+        return out
+    return _timed(run)
+
+
+def eval_brute_force_gravity(leaf_bytes, queries):
+    return _brute(TREE_POTENTIAL, leaf_bytes, queries)
+
+
+def eval_brute_force_wn(leaf_bytes, queries):
+    return _brute(TREE_WINDING, leaf_bytes, queries)
+
+
+def eval_brute_force_smoothdist(leaf_bytes, queries):
+    return _brute(TREE_SMOOTHDIST, leaf_bytes, queries)
+
+
+def eval_barnes_hut_gravity(leaf_bytes, node_bytes, queries, beta: float):
+    return _timed(lambda: _tree_call(TREE_POTENTIAL, leaf_bytes, node_bytes, queries, beta, 0.0, 1.0, False, 1.0, 32))
+
+
+def eval_barnes_hut_wn(leaf_bytes, node_bytes, queries, beta: float):
+    return _timed(lambda: _tree_call(TREE_WINDING, leaf_bytes, node_bytes, queries, beta, 0.0, 1.0, False, 1.0, 32))
+
+
+def eval_barnes_hut_smoothdist(leaf_bytes, node_bytes, queries, beta: float):
+    return _timed(lambda: _tree_call(TREE_SMOOTHDIST, leaf_bytes, node_bytes, queries, beta, 0.0, 1.0, False, 1.0,
+                                     32))
+
+
+def _mlpcv_shared_seed(kind, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain):
+    dev = _device()
+    leaf, node, contrib = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _u8(contrib_bytes, dev)
+    queries = _f32(queries, dev)
+    if queries.ndim != 2 or queries.shape[1] not in (2, 3):
+        raise ValueError("queries must be (M, 2) or (M, 3)")
+    out = torch.empty(queries.shape[0], dtype=torch.float32, device=dev)
+    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+
+    def run():
+        _check(lib().sbh_stochastic_bh_tree_shared_seed(_stream_ptr(dev), queries.shape[1], kind, _p(leaf),
+                                                        leaf.numel(), _p(node), node.numel(), _p(contrib),
+                                                        contrib.numel(), _p(queries), queries.shape[0], _p(out),
+                                                        int(samples_per_subdomain), 0, 32, _p(ws), ws.numel()),
+               "stochastic_bh_tree_shared_seed")
+        return out
+    return _timed(run)
+
+
+def multi_level_prefix_control_variate_gravity(leaf_bytes, node_bytes, contrib_bytes, queries,
+                                               samples_per_subdomain: int):
+    return _mlpcv_shared_seed(TREE_POTENTIAL, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain)
+
+
+def multi_level_prefix_control_variate_wn(leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain: int):
+    return _mlpcv_shared_seed(TREE_WINDING, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain)
+
+
+def multi_level_prefix_control_variate_smoothdist(leaf_bytes, node_bytes, contrib_bytes, queries,
+                                                  samples_per_subdomain: int):
+    return _mlpcv_shared_seed(TREE_SMOOTHDIST, leaf_bytes, node_bytes, contrib_bytes, queries, samples_per_subdomain)

@@ -223,7 +223,9 @@ int sbh_build_octree_level3(cudaStream_t stream, const float* points, const floa
  *         1 = gravityGrad force (BarnesHutForce{,3D}, out[nq*dim]),
  *         2 = softened force (SoftenedBarnesHutForce{,3D}, out[nq*dim]),
  *         3 = winding number (new target; the reference only has it in the
- *             pybind module, src/sbh_gpu.cu:100-120), out[nq].
+ *             pybind module, src/sbh_gpu.cu:100-120), out[nq],
+ *         6 = smoothDistExp, exp(-alpha |p - q|) (pybind module only,
+ *             src/sbh_gpu.cu:122-141), out[nq].
  * dim 2 -> Node2/Leaf2 bytes, dim 3 -> Node3/Leaf3 bytes. Warp-vote opening
  * exactly as evaluateBarnesHutGPUVote (include/barnes_hut_gpu.h:19-72), with
  * warps formed from `threads`-sized blocks as the reference launches them. */
@@ -275,6 +277,25 @@ int sbh_build_adaptive_octree(cudaStream_t stream, const float* points, const fl
                               size_t leaf_bytes, void* node_out, size_t node_capacity_bytes,
                               void* contrib_out, size_t contrib_capacity_bytes,
                               uint64_t* num_nodes, void* workspace, size_t workspace_bytes);
+
+/* The pybind module sbh_gpu's evaluations (src/sbh_gpu.cu:36-661; no FFI
+ * handler) on Node2/Node3 buffers, for the scalar kernels kernel = 0
+ * (gravityPotential), 3 (signedSolidAngle) or 6 (smoothDistExp,
+ * include/kernel.h:82-87). Barnes-Hut is sbh_barnes_hut_tree with these
+ * kernel ids. sbh_brute_force_tree sums every leaf record in leaf order with
+ * Kahan compensation (bruteForceSummationGPU, include/brute_force_gpu.h);
+ * sbh_stochastic_bh_tree_shared_seed is the MLPCV estimate with one seed
+ * for every query, as the module passes it (0), instead of the FFI's
+ * seed + query index. */
+int sbh_brute_force_tree(cudaStream_t stream, int dim, int kernel, const void* leaf,
+                         size_t leaf_bytes, const float* queries, int64_t nq, float* out,
+                         int threads);
+int sbh_stochastic_bh_tree_shared_seed(cudaStream_t stream, int dim, int kernel, const void* leaf,
+                                       size_t leaf_bytes, const void* nodes, size_t node_bytes,
+                                       const void* contrib, size_t contrib_bytes,
+                                       const float* queries, int64_t nq, float* out,
+                                       int samples_per_subdomain, int seed, int threads,
+                                       void* workspace, size_t workspace_bytes);
 
 /* Query-side VJPs on Node2/Node3 trees: out[nq*dim] = J(q)^T cotangent of the
  * force (softened = 0: gravityGrad, 1: softened force), with the opening

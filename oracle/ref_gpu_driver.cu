@@ -229,3 +229,111 @@ int ref_stochastic_bh_force_octree8_vjp(void* s, int softened, const void* leaf,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The reference's pybind module sbh_gpu (src/sbh_gpu.cu:36-208) evaluates the
+// scalar kernels (gravityPotential, signedSolidAngle, smoothDistExp) by brute
+// force, warp-vote BH and MLPCV with seed 0, 32 threads per block. These
+// test-only kernels call the same reference templates on Node2/Node3
+// buffers so that the parity tests can compare against them.
+// ---------------------------------------------------------------------------
+#include "brute_force_gpu.h"
+
+namespace {
+
+template <typename TREE>
+__global__ void ref_vote_scalar(const LeafData<TREE::N>* leaf, const TREE* nodes, const float* q, int nq,
+                                float beta, int kind, float* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  VectorNd<TREE::N> p;
+  for (int d = 0; d < TREE::N; d++) p(d) = q[TREE::N * i + d];
+  if (kind == 0)
+    out[i] = evaluateBarnesHutGPUVote<FLOAT>(leaf, nodes, nodes, p, beta, gravityPotential<TREE::N>);
+  else if (kind == 3)
+    out[i] = evaluateBarnesHutGPUVote<FLOAT>(leaf, nodes, nodes, p, beta, signedSolidAngle<TREE::N>);
+  else
+    out[i] = evaluateBarnesHutGPUVote<FLOAT>(leaf, nodes, nodes, p, beta, smoothDistExp<TREE::N>);
+}
+
+template <typename TREE>
+__global__ void ref_mlpcv_scalar(const LeafData<TREE::N>* leaf, int n, const TREE* nodes,
+                                 const LeafData<TREE::N>* contrib, const float* q, int nq, int samples,
+                                 int kind, float* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  VectorNd<TREE::N> p;
+  for (int d = 0; d < TREE::N; d++) p(d) = q[TREE::N * i + d];
+  if (kind == 0)
+    out[i] = multiLevelPrefixControlVariateSampleGPUQuery<FLOAT>(leaf, n, nodes, nodes, contrib, p,
+                                                                 gravityPotential<TREE::N>, samples, 0);
+  else if (kind == 3)
+    out[i] = multiLevelPrefixControlVariateSampleGPUQuery<FLOAT>(leaf, n, nodes, nodes, contrib, p,
+                                                                 signedSolidAngle<TREE::N>, samples, 0);
+  else
+    out[i] = multiLevelPrefixControlVariateSampleGPUQuery<FLOAT>(leaf, n, nodes, nodes, contrib, p,
+                                                                 smoothDistExp<TREE::N>, samples, 0);
+}
+
+// q_soa: the queries axis by axis (the column-major layout the module reads).
+template <int N>
+__global__ void ref_brute_scalar(const LeafData<N>* leaf, int n, const float* q_soa, int nq, int kind,
+                                 float* out) {
+  int i = blockDim.x * blockIdx.x + threadIdx.x;
+  float r;
+  if (kind == 0)
+    r = bruteForceSummationGPU<FLOAT>(leaf, n, q_soa, nq, gravityPotential<N>, i);
+  else if (kind == 3)
+    r = bruteForceSummationGPU<FLOAT>(leaf, n, q_soa, nq, signedSolidAngle<N>, i);
+  else
+    r = bruteForceSummationGPU<FLOAT>(leaf, n, q_soa, nq, smoothDistExp<N>, i);
+  if (i < nq) out[i] = r;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_sbhgpu_barnes_hut(void* s, int dim, int kind, const void* leaf, const void* node, const float* q,
+                          int64_t nq, float beta, float* out) {
+  int g = static_cast<int>((nq + 31) / 32);
+  if (dim == 3)
+    ref_vote_scalar<Node3><<<g, 32, 0, S(s)>>>(static_cast<const Leaf3*>(leaf), static_cast<const Node3*>(node), q,
+                                               static_cast<int>(nq), beta, kind, out);
+  else
+    ref_vote_scalar<Node2><<<g, 32, 0, S(s)>>>(static_cast<const Leaf2*>(leaf), static_cast<const Node2*>(node), q,
+                                               static_cast<int>(nq), beta, kind, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int ref_sbhgpu_mlpcv(void* s, int dim, int kind, const void* leaf, int64_t n, const void* node,
+                     const void* contrib, const float* q, int64_t nq, int samples, float* out) {
+  int g = static_cast<int>((nq + 31) / 32);
+  if (dim == 3)
+    ref_mlpcv_scalar<Node3><<<g, 32, 0, S(s)>>>(static_cast<const Leaf3*>(leaf), static_cast<int>(n),
+                                                static_cast<const Node3*>(node),
+                                                static_cast<const Leaf3*>(contrib), q, static_cast<int>(nq),
+                                                samples, kind, out);
+  else
+    ref_mlpcv_scalar<Node2><<<g, 32, 0, S(s)>>>(static_cast<const Leaf2*>(leaf), static_cast<int>(n),
+                                                static_cast<const Node2*>(node),
+                                                static_cast<const Leaf2*>(contrib), q, static_cast<int>(nq),
+                                                samples, kind, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+int ref_sbhgpu_brute(void* s, int dim, int kind, const void* leaf, int64_t n, const float* q_soa, int64_t nq,
+                     float* out) {
+  int g = static_cast<int>((nq + 31) / 32);
+  if (dim == 3)
+    ref_brute_scalar<3><<<g, 32, 32 * sizeof(Leaf3), S(s)>>>(static_cast<const Leaf3*>(leaf),
+                                                             static_cast<int>(n), q_soa, static_cast<int>(nq),
+                                                             kind, out);
+  else
+    ref_brute_scalar<2><<<g, 32, 32 * sizeof(Leaf2), S(s)>>>(static_cast<const Leaf2*>(leaf),
+                                                             static_cast<int>(n), q_soa, static_cast<int>(nq),
+                                                             kind, out);
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+}  // extern "C"

@@ -433,6 +433,9 @@ def refgpu() -> ctypes.CDLL:
         for nm in ("ref_gpu_leaf3_size", "ref_gpu_node3_size", "ref_gpu_octree8_node_size", "ref_gpu_level3_max_nodes"):
             getattr(lib, nm).restype = _c_sz
         lib.ref_bruteforce_gravity.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_i64, _c_p, _c_i, _c_f, _c_i]
+        lib.ref_sbhgpu_barnes_hut.argtypes = [_c_p, _c_i, _c_i, _c_p, _c_p, _c_p, _c_i64, _c_f, _c_p]
+        lib.ref_sbhgpu_mlpcv.argtypes = [_c_p, _c_i, _c_i, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_i64, _c_i, _c_p]
+        lib.ref_sbhgpu_brute.argtypes = [_c_p, _c_i, _c_i, _c_p, _c_i64, _c_p, _c_i64, _c_p]
         lib.ref_direct_force_soft.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_i, _c_f, _c_i]
         lib.ref_direct_force_soft_vjp.argtypes = [_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f, _c_i,
                                                   _c_f, _c_i]

@@ -258,3 +258,50 @@ def test_adaptive_octree_build_matches_reference_cpu_builder(cuda, dist):
     b = t.node_bytes().reshape(-1, size)[:, keep]
     np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(contrib.cpu().numpy(), t.contrib_bytes())
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_sbh_gpu_module_evaluations_match_reference(cuda, dim):
+    """The pybind module sbh_gpu's scalar evaluations (brute force, warp-vote
+    BH and MLPCV with seed 0 for every query; gravity potential, winding
+    number, smooth distance) against the reference's own templates on the
+    same Node2/Node3 buffers."""
+    if not HAVE_REF:
+        pytest.skip("reference GPU build missing (make -C oracle ref)")
+    rng = np.random.default_rng(81)
+    p, m = W.uniform_cube(2000, seed=82)
+    p = np.ascontiguousarray(p[:, :dim])
+    nrm = rng.normal(size=p.shape).astype(np.float32)
+    alpha = 3.0
+    if dim == 2:
+        leaf, node, contrib = B.build_quadtree_buffers_with_contrib(p, nrm, m, alpha=alpha)
+    else:
+        t = O.RefTree3D(p, m, normals=nrm, variant=2, alpha=alpha)
+        leaf, node, contrib = _u8(t.leaf_bytes(), cuda), _u8(t.node_bytes(), cuda), _u8(t.contrib_bytes(), cuda)
+    q = rng.uniform(-0.2, 1.2, (300, dim)).astype(np.float32)
+    Q = _t(q, cuda)
+    L = O.refgpu()
+    n = p.shape[0]
+    for kind, name in ((0, "gravity"), (3, "wn"), (6, "smoothdist")):
+        out = torch.zeros(300, device=cuda)
+        O.refgpu_check(L.ref_sbhgpu_brute(_S(), dim, kind, leaf.data_ptr(), n, _t(q.T.copy(), cuda).data_ptr(), 300,
+                                          out.data_ptr()))
+        torch.cuda.synchronize()
+        got, ms = getattr(B, f"eval_brute_force_{name}")(leaf, q)
+        assert ms >= 0
+        np.testing.assert_allclose(got.cpu().numpy(), out.cpu().numpy(), rtol=1e-6, atol=1e-7)
+        for beta in (2.0, 0.5):
+            out = torch.zeros(300, device=cuda)
+            O.refgpu_check(L.ref_sbhgpu_barnes_hut(_S(), dim, kind, leaf.data_ptr(), node.data_ptr(), Q.data_ptr(),
+                                                   300, beta, out.data_ptr()))
+            torch.cuda.synchronize()
+            got, _ = getattr(B, f"eval_barnes_hut_{name}")(leaf, node, q, beta)
+            assert rel_l2(got.cpu().numpy(), out.cpu().numpy()) < 1e-6
+        out = torch.zeros(300, device=cuda)
+        O.refgpu_check(L.ref_sbhgpu_mlpcv(_S(), dim, kind, leaf.data_ptr(), n, node.data_ptr(), contrib.data_ptr(),
+                                          Q.data_ptr(), 300, 2, out.data_ptr()))
+        torch.cuda.synchronize()
+        got, _ = getattr(B, f"multi_level_prefix_control_variate_{name}")(leaf, node, contrib, q, 2)
+        want = out.cpu().numpy()
+        row = np.abs(got.cpu().numpy() - want) / np.maximum(np.abs(want), 1e-30)
+        assert (row < 1e-4).mean() > 0.99
