@@ -540,9 +540,50 @@ constexpr int kForceWalkMinBlocks = SBH_FORCE_WALK_MIN_BLOCKS;
 
 struct WalkParams {
   float beta;
-  float eps2;    // softening^2 + 1e-12
-  float cutoff;  // <= 0: no attenuation
+  float eps2;      // softening^2 + 1e-12
+  float cutoff;    // <= 0: no attenuation
+  float box;       // periodic box length (periodic walks)
+  float inv_box;   // 1 / box
+  float prune_r2;  // > 0: skip nodes whose cell is farther than sqrt(prune_r2) from the group box
 };
+
+// Minimum-image displacement of a periodic box (minImageDisplacement,
+// include/kernel.h:27-39).
+__device__ __forceinline__ float min_image(float d, const WalkParams& P) {
+  return d - P.box * floorf(d * P.inv_box + 0.5f);
+}
+
+// The periodic image of a cell's centre nearest the group box's centre, per
+// axis (IEEE operations, the oracle's order).
+__device__ __forceinline__ float4 cell_image(const float4& cell, const float* gmin, const float* gmax,
+                                             const WalkParams& P) {
+  float c[3] = {cell.x, cell.y, cell.z};
+  for (int d = 0; d < 3; d++) {
+    float bc = __fmul_rn(__fadd_rn(gmin[d], gmax[d]), 0.5f);
+    float k = rintf(__fmul_rn(__fsub_rn(bc, c[d]), P.inv_box));
+    c[d] = __fadd_rn(c[d], __fmul_rn(P.box, k));
+  }
+  return make_float4(c[0], c[1], c[2], cell.w);
+}
+
+// AABB prune of the short-range split (the group form of
+// octree8_should_prune, src/sbh_ffi.cu:1903-1948): the node is skipped when
+// the distance from the group box to its cell exceeds the prune radius. The
+// half side is taken a little above diag / (2 sqrt 3), so the test errs on
+// the side of keeping a node.
+__device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin, const float* gmax, float r2) {
+  float half = __fmul_rn(cell.w, 0.2887f);
+  float x[3] = {cell.x, cell.y, cell.z};
+  float t[3];
+  for (int d = 0; d < 3; d++) {
+    float a = __fsub_rn(gmin[d], __fadd_rn(x[d], half));
+    float b = __fsub_rn(__fsub_rn(x[d], half), gmax[d]);
+    float m = a > b ? a : b;
+    t[d] = m > 0.0f ? m : 0.0f;
+  }
+  float d2 = __fadd_rn(__fadd_rn(__fmul_rn(t[0], t[0]), __fmul_rn(t[1], t[1])), __fmul_rn(t[2], t[2]));
+  return d2 > r2;
+}
 
 // Targets of one group as a lane holds them: slots lane and lane + 32.
 // Inactive slots carry the group's first target (inside the group box) and
@@ -622,7 +663,7 @@ __device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, f
 // node 55 (monopole + quadrupole); adjoint walk (force + adjoint) near pair
 // 55, far node 200 including the share of the warp reductions.
 
-template <bool QUAD, bool CUT>
+template <bool QUAD, bool CUT, bool PER>
 __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
                       unsigned long long* __restrict__ counters) {
@@ -656,8 +697,10 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     }
     while (k < rt.y) {
       const NodeRec* nd = T.nodes + k;
-      const bool live = A.w != 0.0f;  // mass-zero nodes are skipped
-      const bool acc = live && accept_node(C, gmin, gmax, P.beta);
+      const float4 Ci = PER ? cell_image(C, gmin, gmax, P) : C;
+      const bool live = A.w != 0.0f &&  // mass-zero and pruned nodes are skipped
+                        !(CUT && P.prune_r2 > 0.0f && prune_node(Ci, gmin, gmax, P.prune_r2));
+      const bool acc = live && accept_node(Ci, gmin, gmax, P.beta);
       const bool leaf = (tp.w & kLeafFlag) != 0;
       const int next = (!live || acc || leaf) ? tp.z : k + 1;
       int4 tpn = tp;
@@ -677,6 +720,11 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
         for (int t = 0; t < kTPL; t++) {
           if (t > 0 && !two) break;
           float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+          if (PER) {
+            rx = min_image(rx, P);
+            ry = min_image(ry, P);
+            rz = min_image(rz, P);
+          }
           float r2 = rx * rx + ry * ry + rz * rz;
           float ir = rsqrtf(r2 + P.eps2);
           float ih = ir * ir;
@@ -717,6 +765,11 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
           for (int t = 0; t < kTPL; t++) {
             if (t > 0 && !two) break;
             float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
+            if (PER) {
+              rx = min_image(rx, P);
+              ry = min_image(ry, P);
+              rz = min_image(rz, P);
+            }
             float r2 = rx * rx + ry * ry + rz * rz;
             float ir = rsqrtf(r2 + P.eps2);
             float ir3 = ir * ir * ir;
@@ -847,7 +900,7 @@ __device__ __forceinline__ int reduce10_index(int lane) {
 // a3 = 15 ir^7 (r.Sw) - 52.5 ir^9 (rSr)(r.w), and the node-side terms are
 // A_X = -(that gradient), A_M = -lin (r.w) and
 // G = 1.5 ir^5 (w r^T + r w^T) + 1.5 ir^5 (r.w) I - 7.5 ir^7 (r.w) r r^T.
-template <bool QUAD, bool CUT>
+template <bool QUAD, bool CUT, bool PER>
 __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
                         float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
@@ -884,11 +937,13 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
       const NodeRec* nd = T.nodes + k;
       int4 tp = __ldg(&nd->topo);
       float4 A = __ldg(&nd->com);
-      if (A.w == 0.0f) {
-        k = tp.z;
+      float4 C = __ldg(&nd->cell);
+      if (PER) C = cell_image(C, gmin, gmax, P);
+      if (A.w == 0.0f || (CUT && P.prune_r2 > 0.0f && prune_node(C, gmin, gmax, P.prune_r2))) {
+        k = tp.z;  // mass-zero and pruned nodes are skipped
         continue;
       }
-      if (accept_node(__ldg(&nd->cell), gmin, gmax, P.beta)) {
+      if (accept_node(C, gmin, gmax, P.beta)) {
         float4 Qd = make_float4(0.f, 0.f, 0.f, 0.f), X = Qd;
         if (QUAD) {
           Qd = __ldg(&nd->quad);
@@ -904,6 +959,11 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
         for (int t = 0; t < kTPL; t++) {
           if (t > 0 && !two) break;
           float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+          if (PER) {
+            rx = min_image(rx, P);
+            ry = min_image(ry, P);
+            rz = min_image(rz, P);
+          }
           float r2 = rx * rx + ry * ry + rz * rz;
           float ir = rsqrtf(r2 + P.eps2);
           float ih = ir * ir;
@@ -995,6 +1055,11 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
           for (int t = 0; t < kTPL; t++) {
             if (t > 0 && !two) break;
             float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
+            if (PER) {
+              rx = min_image(rx, P);
+              ry = min_image(ry, P);
+              rz = min_image(rz, P);
+            }
             float r2 = rx * rx + ry * ry + rz * rz;
             float ir = rsqrtf(r2 + P.eps2);
             float ih = ir * ir;
@@ -1603,12 +1668,17 @@ int check_params(const sbh_native_params* p) {
   if (!(p->beta > 0.0f)) return invalid("beta must be > 0");
   if (p->softening < 0.0f) return invalid("softening must be >= 0");
   if (p->quadrupole && p->cutoff > 0.0f) return invalid("the quadrupole far field needs cutoff <= 0 (Plummer)");
+  if (p->periodic && !(p->box_length > 0.0f)) return invalid("box_length must be > 0 when periodic is set");
+  if (p->periodic && p->quadrupole) return invalid("the periodic walk uses the monopole far field (quadrupole = 0)");
+  if (p->prune_radius < 0.0f) return invalid("prune_radius must be >= 0");
+  if (p->prune_radius > 0.0f && !(p->cutoff > 0.0f)) return invalid("prune_radius needs an erfc cutoff (cutoff > 0)");
   return SBH_OK;
 }
 
 WalkParams walk_params(const sbh_native_params* p) {
   float eps = fmaxf(p->softening, 0.0f);
-  return WalkParams{p->beta, eps * eps + 1e-12f, p->cutoff};
+  float box = p->periodic ? p->box_length : 1.0f;
+  return WalkParams{p->beta, eps * eps + 1e-12f, p->cutoff, box, 1.0f / box, p->prune_radius * p->prune_radius};
 }
 
 }  // namespace
@@ -1628,8 +1698,10 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   WalkParams wp = walk_params(params);
   int64_t mg = h.n + h.nseg;
   bool cut = params->cutoff > 0.0f;
-  auto k = params->quadrupole ? force_walk_kernel<true, false>
-                              : (cut ? force_walk_kernel<false, true> : force_walk_kernel<false, false>);
+  bool per = params->periodic != 0;
+  auto k = params->quadrupole ? force_walk_kernel<true, false, false>
+           : per ? (cut ? force_walk_kernel<false, true, true> : force_walk_kernel<false, false, true>)
+                 : (cut ? force_walk_kernel<false, true, false> : force_walk_kernel<false, false, false>);
   e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h.n, h.nseg), wp, force_out, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_force");
@@ -1651,8 +1723,10 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
   WalkParams wp = walk_params(params);
   bool cut = params->cutoff > 0.0f;
-  auto k = params->quadrupole ? adjoint_walk_kernel<true, false>
-                              : (cut ? adjoint_walk_kernel<false, true> : adjoint_walk_kernel<false, false>);
+  bool per = params->periodic != 0;
+  auto k = params->quadrupole ? adjoint_walk_kernel<true, false, false>
+           : per ? (cut ? adjoint_walk_kernel<false, true, true> : adjoint_walk_kernel<false, false, true>)
+                 : (cut ? adjoint_walk_kernel<false, true, false> : adjoint_walk_kernel<false, false, false>);
   e = launch_walk(stream, L.work, n + h.nseg, k, tree_view(L), self_targets(L, h.n, h.nseg), wp, cotangent, force_out, L.gq,
                   L.node_adj, L.part_adj, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));

@@ -147,7 +147,8 @@ class NativeParams(ctypes.Structure):
     """sbh_native_params of include/sbh_b200.h."""
 
     _fields_ = [("beta", ctypes.c_float), ("softening", ctypes.c_float), ("cutoff", ctypes.c_float),
-                ("quadrupole", ctypes.c_int)]
+                ("quadrupole", ctypes.c_int), ("periodic", ctypes.c_int), ("box_length", ctypes.c_float),
+                ("prune_radius", ctypes.c_float)]
 
 _lib_handle = None
 _lib_lock = threading.Lock()
@@ -800,21 +801,28 @@ class NativeTree:
         return self
 
     @staticmethod
-    def params(beta=2.0, softening=1e-3, cutoff=0.0, quadrupole=True) -> NativeParams:
-        return NativeParams(float(beta), float(softening), float(cutoff), int(bool(quadrupole)))
+    def params(beta=2.0, softening=1e-3, cutoff=0.0, quadrupole=True, periodic=False, box_length=1.0,
+               prune_radius=0.0) -> NativeParams:
+        return NativeParams(float(beta), float(softening), float(cutoff), int(bool(quadrupole)), int(bool(periodic)),
+                            float(box_length), float(prune_radius))
 
     def force(self, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0, quadrupole: bool = True,
+              periodic: bool = False, box_length: float = 1.0, prune_radius: float = 0.0,
               out: Optional[torch.Tensor] = None) -> torch.Tensor:
-        prm = self.params(beta, softening, cutoff, quadrupole)
+        """Softened self-gravity. periodic: minimum image in a cube of side
+        box_length (monopole far field); cutoff > 0: the erfc short-range
+        split; prune_radius > 0: skip cells beyond it (TreePM short range)."""
+        prm = self.params(beta, softening, cutoff, quadrupole, periodic, box_length, prune_radius)
         out = out if out is not None else torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
         _check(lib().sbh_native_force(_stream_ptr(self.device), ctypes.byref(prm), _p(out), _p(self.ws),
                                       self.ws.numel()), "native_force")
         return out
 
     def force_vjp(self, cotangent, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,
-                  quadrupole: bool = True, want_force: bool = True):
+                  quadrupole: bool = True, periodic: bool = False, box_length: float = 1.0,
+                  prune_radius: float = 0.0, want_force: bool = True):
         """(force or None, d/d points, d/d masses) of sum(cotangent * force)."""
-        prm = self.params(beta, softening, cutoff, quadrupole)
+        prm = self.params(beta, softening, cutoff, quadrupole, periodic, box_length, prune_radius)
         cot = _f32(cotangent, self.device)
         if cot.shape != (self.n, 3):
             raise ValueError("cotangent must have shape (N, 3)")

@@ -340,6 +340,11 @@ typedef struct sbh_native_params {
   float softening; /* Plummer softening epsilon, >= 0 */
   float cutoff;    /* erfc attenuation scale of the short-range split; <= 0 disables */
   int quadrupole;  /* 1: monopole + quadrupole far field (needs cutoff <= 0), 0: monopole */
+  int periodic;    /* 1: minimum-image displacements in a cube of side box_length (monopole only);
+                      the opening test uses the cell's image nearest the group */
+  float box_length;
+  float prune_radius; /* > 0 (with cutoff > 0): skip nodes whose cell lies farther than this from
+                         every target of the group (the short-range split of TreePM) */
 } sbh_native_params;
 
 /* Most targets one group holds (one warp walks a group). */

@@ -942,17 +942,65 @@ static void com_float(const double* mom, int64_t k, float* X, float* M) {
 }
 
 /*
+ * Periodic and short-range settings of the native walk (the CUDA walk's
+ * sbh_native_params.periodic / box_length / prune_radius):
+ *   periodic: displacements take the minimum image in a cube of side box
+ *     (minImageDisplacement, include/kernel.h:27-39), and the opening test
+ *     and prune use the cell centre's image nearest the group box's centre;
+ *   prune_r2 > 0: a node whose cell lies farther than sqrt(prune_r2) from
+ *     the group box is skipped (octree8_should_prune, src/sbh_ffi.cu:1903-1948,
+ *     for a group), with the half side taken as diag * 0.2887.
+ */
+static int g_orc_periodic = 0;
+static float g_orc_box = 1.0f, g_orc_inv_box = 1.0f, g_orc_prune_r2 = 0.0f;
+void orc_native_set_periodic(int on, float box, float prune_radius) {
+  g_orc_periodic = on;
+  g_orc_box = on ? box : 1.0f;
+  g_orc_inv_box = 1.0f / g_orc_box;
+  g_orc_prune_r2 = prune_radius * prune_radius;
+}
+
+static void native_mi(double* r) {
+  if (!g_orc_periodic) return;
+  double L = (double)g_orc_box;
+  for (int d = 0; d < 3; d++) r[d] -= L * floor(r[d] / L + 0.5);
+}
+
+/* The cell centre of node k (its image nearest the group box when periodic). */
+static void native_cell(const NativeTree* t, int64_t k, const float* gmin, const float* gmax, float* C) {
+  for (int d = 0; d < 3; d++) {
+    C[d] = t->center[3 * k + d];
+    if (g_orc_periodic) {
+      float bc = (gmin[d] + gmax[d]) * 0.5f;
+      float kk = rintf((bc - C[d]) * g_orc_inv_box);
+      C[d] = C[d] + g_orc_box * kk;
+    }
+  }
+}
+
+static int native_prune(const NativeTree* t, int64_t k, const float* C, const float* gmin, const float* gmax) {
+  if (!(g_orc_prune_r2 > 0.0f)) return 0;
+  float half = (t->side[k] * 1.7320508f) * 0.2887f;
+  float tt[3];
+  for (int d = 0; d < 3; d++) {
+    float a = gmin[d] - (C[d] + half), b = (C[d] - half) - gmax[d];
+    float m = a > b ? a : b;
+    tt[d] = m > 0.0f ? m : 0.0f;
+  }
+  float d2 = tt[0] * tt[0] + tt[1] * tt[1] + tt[2] * tt[2];
+  return d2 > g_orc_prune_r2;
+}
+
+/*
  * Multipole acceptance for target group box [gmin, gmax] (float, no fused
  * operations): the reference's rule |q - cell centre| / diag >= beta
  * (include/tree3d.h:134-153, src/sbh_ffi.cu:1878-1893; beta = 1/theta) made
  * to hold for every target in the box:
- *   accept node k iff dist^2(box, cell centre) > (side * sqrt(3) * beta)^2.
- * X (the COM) is not used by the rule; the multipole is expanded about it.
+ *   accept node k iff dist^2(box, cell centre C) > (side * sqrt(3) * beta)^2.
+ * The multipole is expanded about the COM.
  */
-static int native_accept(const NativeTree* t, int64_t k, const float* X, const float* gmin,
+static int native_accept(const NativeTree* t, int64_t k, const float* C, const float* gmin,
                          const float* gmax, float beta) {
-  (void)X;
-  const float* C = t->center + 3 * k;
   float rc = t->side[k] * 1.7320508f * beta;
   float tt[3];
   for (int d = 0; d < 3; d++) {
@@ -964,13 +1012,6 @@ static int native_accept(const NativeTree* t, int64_t k, const float* X, const f
   return d2 > rc * rc;
 }
 
-/*
- * Record the traversal plan for beta: targets are consecutive runs of
- * group_size sorted particles; each group walks the pre-order tree,
- * accepting nodes by native_accept and summing near-field leaves directly.
- * Mass-zero nodes are skipped. Returns the total interaction count
- * (sum over groups of active targets x (accepted nodes + near particles)).
- */
 /*
  * Target groups cut from the tree. For every node holding more than G
  * particles its children are taken in order; each maximal run of
@@ -1067,14 +1108,15 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
       }
     int64_t k = 0, cnt_int = 0;
     while (k < t->nn) {
-      float X[3], M;
+      float X[3], M, C[3];
       com_float(mom, k, X, &M);
-      if (M == 0.0f) {
+      native_cell(t, k, gmin, gmax, C);
+      if (M == 0.0f || native_prune(t, k, C, gmin, gmax)) {
         k = t->skip[k];
         continue;
       }
       int is_leaf = (k + 1 >= t->nn) || (t->skip[k] == k + 1);
-      if (native_accept(t, k, X, gmin, gmax, fbeta)) {
+      if (native_accept(t, k, C, gmin, gmax, fbeta)) {
         if (nf == fcap) {
           fcap *= 2;
           t->far_idx = (int32_t*)realloc(t->far_idx, sizeof(int32_t) * fcap);
@@ -1128,6 +1170,7 @@ void orc_native_eval(void* h, const float* pts, const float* masses, double eps,
         int32_t k = t->far_idx[e];
         const double* o = &mom[MOM * k];
         double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
+        native_mi(r);
         soft_force_pair(r, o[0], &sp, acc);
         if (quad) quad_force(r, o + 4, eps, acc);
       }
@@ -1136,6 +1179,7 @@ void orc_native_eval(void* h, const float* pts, const float* masses, double eps,
         for (int32_t j = t->start[k]; j < t->end[k]; j++) {
           int64_t sj = t->perm[j];
           double r[3] = {q[0] - pts[3 * sj], q[1] - pts[3 * sj + 1], q[2] - pts[3 * sj + 2]};
+          native_mi(r);
           soft_force_pair(r, masses[sj], &sp, acc);
         }
       }
@@ -1186,6 +1230,7 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
         int32_t k = t->far_idx[e];
         const double* o = &mom[MOM * k];
         double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
+        native_mi(r);
         double jt[3] = {0, 0, 0}, f[3] = {0, 0, 0};
         soft_force_pair_vjp(r, o[0], wi, &sp, jt);
         soft_force_pair(r, 1.0, &sp, f);
@@ -1201,6 +1246,7 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
         for (int32_t j = t->start[k]; j < t->end[k]; j++) {
           int64_t sj = t->perm[j];
           double r[3] = {q[0] - pts[3 * sj], q[1] - pts[3 * sj + 1], q[2] - pts[3 * sj + 2]};
+          native_mi(r);
           double jt[3] = {0, 0, 0}, f[3] = {0, 0, 0};
           soft_force_pair_vjp(r, 1.0, wi, &sp, jt);
           soft_force_pair(r, 1.0, &sp, f);

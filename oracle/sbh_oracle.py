@@ -93,6 +93,7 @@ def _orc() -> ctypes.CDLL:
         lib.orc_native_plan.restype = _c_i64
         lib.orc_native_plan.argtypes = [_c_p, _c_p, _c_p, _c_d, _c_i]
         lib.orc_native_eval.argtypes = [_c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p, _c_p]
+        lib.orc_native_set_periodic.argtypes = [_c_i, _c_f, _c_f]
         lib.orc_native_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p]
         lib.orc_native_plan_stats.argtypes = [_c_p, _c_p, _c_p, _c_p]
         lib._typed = True
@@ -262,6 +263,23 @@ class NativeTree:
         self._lib.orc_native_adjoint(self._h, _ptr(p), _ptr(m), _ptr(_f32(w)), float(eps), float(cutoff), int(quad),
                                      _ptr(dx), _ptr(dm))
         return dx, dm
+
+
+class native_periodic:
+    """Context manager: the native plan and sums of the oracle use periodic
+    minimum images in a cube of side box and skip cells beyond prune_radius
+    of a group (0: no pruning), as the CUDA walk does with those params."""
+
+    def __init__(self, box: float, prune_radius: float = 0.0, periodic: bool = True):
+        self.args = (int(bool(periodic)), float(box), float(prune_radius))
+
+    def __enter__(self):
+        _orc().orc_native_set_periodic(*self.args)
+        return self
+
+    def __exit__(self, *exc):
+        _orc().orc_native_set_periodic(0, 1.0, 0.0)
+        return False
 
 
 # ---------------------------------------------------------------------------

@@ -151,3 +151,68 @@ def test_native_empty_and_invalid(cuda):
         B.NativeTree().build(np.zeros((4, 3), np.float32), np.zeros(4, np.float32), leaf_size=0)
     with pytest.raises(ValueError):
         B.NativeTree().build(np.zeros((4, 3), np.float32), np.zeros(4, np.float32)).force(beta=-1.0)
+
+
+def _periodic_direct(p, m, q, eps, cutoff):
+    from scipy.special import erfc
+    r = q[:, None, :].astype(np.float64) - p[None, :, :].astype(np.float64)
+    r -= np.floor(r + 0.5)
+    r2 = (r * r).sum(-1)
+    d = np.sqrt(r2 + 1e-12)
+    u = d / (2.0 * cutoff)
+    att = erfc(u) + 2.0 / np.sqrt(np.pi) * u * np.exp(-u * u)
+    return (-m[None, :, None] * (att * (r2 + eps * eps + 1e-12) ** -1.5)[..., None] * r).sum(1)
+
+
+def test_native_periodic_short_range_matches_oracle(cuda):
+    """TreePM short range on the native tree: minimum image in the unit box,
+    erfc cutoff 0.05, cells beyond 0.3 of a group skipped. Same plan as the
+    oracle (groups, pruned and accepted cells), forces and the full adjoint
+    within FP32 tolerance, and the periodic FP64 direct sum within the
+    opening-angle error."""
+    rng = np.random.default_rng(21)
+    p, m = W.uniform_cube(20000, seed=22)
+    w = rng.normal(size=p.shape).astype(np.float32)
+    kw = dict(beta=2.0, softening=1e-3, cutoff=0.05, quadrupole=False, periodic=True, box_length=1.0,
+              prune_radius=0.3)
+    t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True)
+    f, gx, gm = t.force_vjp(w, **kw)
+    st = t.stats()
+    T = O.NativeTree(p, m, leaf_size=16)
+    with O.native_periodic(1.0, 0.3):
+        inter = T.plan(2.0, B.native_group_size())
+        want_f, _ = T.force(1e-3, cutoff=0.05)
+        dx, dm = T.adjoint(w, 1e-3, cutoff=0.05)
+    assert abs((st["far"] + st["near"]) - inter) <= 1e-4 * inter
+    assert rel_l2(f.cpu().numpy(), want_f) < 1e-5
+    assert rel_l2(gx.cpu().numpy(), dx) < 1e-4
+    assert rel_l2(gm.cpu().numpy(), dm) < 1e-4
+    idx = rng.choice(p.shape[0], 512, replace=False)
+    # monopole-only at theta = 0.5 on a uniform cube: a few 1e-4
+    assert rel_l2(f.cpu().numpy()[idx], _periodic_direct(p, m, p[idx], 1e-3, 0.05)) < 1e-3
+    # the force walk sums in another order than the adjoint walk
+    f2 = t.force(**kw).cpu().numpy()
+    assert rel_l2(f2, want_f) < 1e-5
+
+
+def test_native_periodic_direct_limit_and_shift_invariance(cuda):
+    p, m = W.uniform_cube(6000, seed=23)
+    kw = dict(beta=1e30, softening=2e-3, cutoff=0.1, quadrupole=False, periodic=True, box_length=1.0)
+    f = B.NativeTree().build(p, m, leaf_size=16).force(**kw).cpu().numpy()
+    want = _periodic_direct(p, m, p, 2e-3, 0.1)
+    assert rel_l2(f, want) < 2e-6
+    shifted = np.mod(p + np.array([0.31, 0.77, 0.05], np.float32), np.float32(1.0)).astype(np.float32)
+    fs = B.NativeTree().build(shifted, m, leaf_size=16).force(**kw).cpu().numpy()
+    assert rel_l2(fs, _periodic_direct(shifted, m, shifted, 2e-3, 0.1)) < 2e-6
+    # the shifted coordinates are rounded to FP32 anew: close pairs move by an ulp
+    assert rel_l2(fs, f) < 1e-4
+
+
+def test_native_periodic_invalid_params(cuda):
+    t = B.NativeTree().build(*W.uniform_cube(100, seed=24))
+    with pytest.raises(ValueError):
+        t.force(periodic=True, box_length=0.0, quadrupole=False)
+    with pytest.raises(ValueError):
+        t.force(periodic=True, box_length=1.0, quadrupole=True)
+    with pytest.raises(ValueError):
+        t.force(cutoff=0.0, prune_radius=0.3, quadrupole=False)
