@@ -545,6 +545,8 @@ struct WalkParams {
   float box;       // periodic box length (periodic walks)
   float inv_box;   // 1 / box
   float prune_r2;  // > 0: skip nodes whose cell is farther than sqrt(prune_r2) from the group box
+  float quad_g;    // > 0: an accepted node takes the quadrupole only when its opening distance^2 is
+                   // below quad_g * (beta * diagonal)^2; 0: every accepted node takes it
 };
 
 // Minimum-image displacement of a periodic box (minImageDisplacement,
@@ -634,6 +636,30 @@ __device__ __forceinline__ void group_box(const LaneTargets& Q, float* gmin, flo
 // (include/tree3d.h:134-153, src/sbh_ffi.cu:1878-1893) made to hold for every
 // target of the group: dist(group box, cell centre) > beta * diag. IEEE
 // operations in the oracle's order (no contraction).
+__device__ __forceinline__ bool accept_node(const float4& cell, const float* gmin, const float* gmax, float beta,
+                                            float& d2, float& rc2) {
+  float rc = __fmul_rn(cell.w, beta);
+  float x[3] = {cell.x, cell.y, cell.z};
+  float t[3];
+  for (int d = 0; d < 3; d++) {
+    float a = __fsub_rn(gmin[d], x[d]);
+    float b = __fsub_rn(x[d], gmax[d]);
+    float m = a > b ? a : b;
+    t[d] = m > 0.0f ? m : 0.0f;
+  }
+  d2 = __fadd_rn(__fadd_rn(__fmul_rn(t[0], t[0]), __fmul_rn(t[1], t[1])), __fmul_rn(t[2], t[2]));
+  rc2 = __fmul_rn(rc, rc);
+  return d2 > rc2;
+}
+
+// Far-field order of an accepted node (warp-uniform: the inputs are the
+// group box and the node). The quadrupole's share of the error falls off
+// one power of the distance faster than the monopole's, so beyond
+// sqrt(quad_g) opening radii the monopole alone is kept.
+__device__ __forceinline__ bool quad_order(float d2, float rc2, const WalkParams& P) {
+  return !(P.quad_g > 0.0f) || d2 < __fmul_rn(P.quad_g, rc2);
+}
+
 __device__ __forceinline__ bool accept_node(const float4& cell, const float* gmin, const float* gmax, float beta) {
   float rc = __fmul_rn(cell.w, beta);
   float x[3] = {cell.x, cell.y, cell.z};
@@ -656,6 +682,64 @@ __device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, f
   float e = expf(-(u * u));
   att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
   cc = ir3 * dist * e / (2.0f * 1.772453850905516f * cutoff * cutoff * cutoff);
+}
+
+// One accepted node's monopole (with the erfc attenuation when CUT, minimum
+// image when PER) added to the lane's far-field accumulators.
+template <bool CUT, bool PER>
+__device__ __forceinline__ void far_mono_force(const float4& A, const LaneTargets& Q, bool two, const WalkParams& P,
+                                               float* fx, float* fy, float* fz) {
+#pragma unroll
+  for (int t = 0; t < kTPL; t++) {
+    if (t > 0 && !two) break;
+    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+    if (PER) {
+      rx = min_image(rx, P);
+      ry = min_image(ry, P);
+      rz = min_image(rz, P);
+    }
+    float r2 = rx * rx + ry * ry + rz * rz;
+    float ir = rsqrtf(r2 + P.eps2);
+    float ir3 = ir * ir * ir;
+    float c = -A.w * ir3;
+    if (CUT) {
+      float att, cc;
+      attenuation(r2, ir3, P.cutoff, att, cc);
+      c *= att;
+    }
+    fx[t] += c * rx;
+    fy[t] += c * ry;
+    fz[t] += c * rz;
+  }
+}
+
+// One accepted node's monopole + quadrupole (Plummer softening):
+// a_q = ir5 (3 S r + 1.5 tr(S) r) - 7.5 (r.S.r) ir7 r.
+__device__ __forceinline__ void far_quad_force(const NodeRec* nd, const float4& A, const LaneTargets& Q, bool two,
+                                               const WalkParams& P, float* fx, float* fy, float* fz) {
+  const float4 Qd = __ldg(&nd->quad);
+  const float4 X = __ldg(&nd->quad2);
+  const float tr15 = 1.5f * (Qd.x + Qd.y + Qd.z);
+#pragma unroll
+  for (int t = 0; t < kTPL; t++) {
+    if (t > 0 && !two) break;
+    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+    float r2 = rx * rx + ry * ry + rz * rz;
+    float ir = rsqrtf(r2 + P.eps2);
+    float ih = ir * ir;
+    float ir3 = ir * ih;
+    float c = -A.w * ir3;
+    float sx = Qd.x * rx + Qd.w * ry + X.x * rz;
+    float sy = Qd.w * rx + Qd.y * ry + X.y * rz;
+    float sz = X.x * rx + X.y * ry + Qd.z * rz;
+    float rsr = rx * sx + ry * sy + rz * sz;
+    float ir5 = ir3 * ih;
+    float cr = c + ir5 * (tr15 - 7.5f * rsr * ih);
+    float c3 = 3.0f * ir5;
+    fx[t] += cr * rx + c3 * sx;
+    fy[t] += cr * ry + c3 * sy;
+    fz[t] += cr * rz + c3 * sz;
+  }
 }
 
 // Flop accounting used by the roofline (FP32 operations counted from the
@@ -683,7 +767,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     float nx[kTPL], ny[kTPL], nz[kTPL], cx[kTPL], cy[kTPL], cz[kTPL];       // near field, compensated
 #pragma unroll
     for (int t = 0; t < kTPL; t++) fx[t] = fy[t] = fz[t] = nx[t] = ny[t] = nz[t] = cx[t] = cy[t] = cz[t] = 0.f;
-    unsigned long long nfar = 0, nnear = 0;
+    unsigned long long nfar = 0, nnear = 0, nquad = 0;
     // Pre-order walk. The next node is known once this node's opening test
     // is done, so its opening data is loaded before this node's terms are
     // evaluated and the load latency hides behind that arithmetic.
@@ -700,7 +784,9 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
       const float4 Ci = PER ? cell_image(C, gmin, gmax, P) : C;
       const bool live = A.w != 0.0f &&  // mass-zero and pruned nodes are skipped
                         !(CUT && P.prune_r2 > 0.0f && prune_node(Ci, gmin, gmax, P.prune_r2));
-      const bool acc = live && accept_node(Ci, gmin, gmax, P.beta);
+      float d2 = 0.0f, rc2 = 0.0f;
+      const bool acc = live && accept_node(Ci, gmin, gmax, P.beta, d2, rc2);
+      const bool qh = QUAD && quad_order(d2, rc2, P);
       const bool leaf = (tp.w & kLeafFlag) != 0;
       const int next = (!live || acc || leaf) ? tp.z : k + 1;
       int4 tpn = tp;
@@ -711,50 +797,13 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
         Cn = __ldg(&T.nodes[next].cell);
       }
       if (acc) {
-        float4 Qd = make_float4(0.f, 0.f, 0.f, 0.f), X = Qd;
-        if (QUAD) {
-          Qd = __ldg(&nd->quad);
-          X = __ldg(&nd->quad2);
-        }
-#pragma unroll
-        for (int t = 0; t < kTPL; t++) {
-          if (t > 0 && !two) break;
-          float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
-          if (PER) {
-            rx = min_image(rx, P);
-            ry = min_image(ry, P);
-            rz = min_image(rz, P);
-          }
-          float r2 = rx * rx + ry * ry + rz * rz;
-          float ir = rsqrtf(r2 + P.eps2);
-          float ih = ir * ir;
-          float ir3 = ir * ih;
-          float c = -A.w * ir3;
-          if (CUT) {
-            float att, cc;
-            attenuation(r2, ir3, P.cutoff, att, cc);
-            c *= att;
-          }
-          if (QUAD) {
-            // a_q = ir5 (3 S r + 1.5 tr(S) r) - 7.5 (r.S.r) ir7 r
-            float sx = Qd.x * rx + Qd.w * ry + X.x * rz;
-            float sy = Qd.w * rx + Qd.y * ry + X.y * rz;
-            float sz = X.x * rx + X.y * ry + Qd.z * rz;
-            float rsr = rx * sx + ry * sy + rz * sz;
-            float ir5 = ir3 * ih;
-            float tr = Qd.x + Qd.y + Qd.z;
-            float cr = c + ir5 * (1.5f * tr - 7.5f * rsr * ih);
-            float c3 = 3.0f * ir5;
-            fx[t] += cr * rx + c3 * sx;
-            fy[t] += cr * ry + c3 * sy;
-            fz[t] += cr * rz + c3 * sz;
-          } else {
-            fx[t] += c * rx;
-            fy[t] += c * ry;
-            fz[t] += c * rz;
-          }
+        if (qh) {
+          far_quad_force(nd, A, Q, two, P, fx, fy, fz);
+        } else {
+          far_mono_force<CUT, PER>(A, Q, two, P, fx, fy, fz);
         }
         nfar++;
+        nquad += qh;
       } else if (live && leaf) {
         float ax[kTPL], ay[kTPL], az[kTPL];
 #pragma unroll
@@ -810,6 +859,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
       unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
       atomicAdd(&counters[0], nfar * na);
       atomicAdd(&counters[1], nnear * na);
+      atomicAdd(&counters[2], nquad * na);
     }
   }
 }
@@ -885,6 +935,136 @@ __device__ __forceinline__ int reduce10_index(int lane) {
   return hj + 5 * ((lane >> 4) & 1);
 }
 
+// One accepted node, monopole far field, for the lane's targets: query-side
+// gradient and force into the lane's accumulators, the node-side adjoint
+// (A_X, A_M) reduced over the warp and added to the node's slots.
+template <bool CUT, bool PER>
+__device__ __forceinline__ void far_mono_adjoint(const float4& A, const LaneTargets& Q, const float* wx,
+                                                 const float* wy, const float* wz, bool two, const WalkParams& P,
+                                                 bool want_force, float* gx, float* gy, float* gz, float* fx,
+                                                 float* fy, float* fz, float* __restrict__ na, int lane, int r4) {
+  const float M = A.w;
+  float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
+#pragma unroll
+  for (int t = 0; t < kTPL; t++) {
+    if (t > 0 && !two) break;
+    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+    if (PER) {
+      rx = min_image(rx, P);
+      ry = min_image(ry, P);
+      rz = min_image(rz, P);
+    }
+    float r2 = rx * rx + ry * ry + rz * rz;
+    float ir = rsqrtf(r2 + P.eps2);
+    float ih = ir * ir;
+    float ir3 = ir * ih;
+    float ir5 = ir3 * ih;
+    float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
+    float att = 1.0f, cc = 0.0f;
+    if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
+    float lin = att * ir3;
+    float mlin = M * lin, mrad = M * (rw * (3.0f * att * ir5 + cc));
+    v3 -= lin * rw;  // A_M
+    float qx_ = mrad * rx - mlin * wx[t];
+    float qy_ = mrad * ry - mlin * wy[t];
+    float qz_ = mrad * rz - mlin * wz[t];
+    if (want_force) {
+      fx[t] -= mlin * rx;
+      fy[t] -= mlin * ry;
+      fz[t] -= mlin * rz;
+    }
+    gx[t] += qx_;
+    gy[t] += qy_;
+    gz[t] += qz_;
+    v0 -= qx_;
+    v1 -= qy_;
+    v2 -= qz_;
+  }
+  float tot = reduce4(v0, v1, v2, v3);
+  if ((lane & 7) == 0) atomicAdd(&na[r4], tot);
+}
+
+// One accepted node with the quadrupole (Plummer softening, no cutoff, not
+// periodic): as far_mono_adjoint plus the quadrupole's terms and the node's
+// G = sym d(w . a_q)/dS, ten values reduced over the warp.
+__device__ __forceinline__ void far_quad_adjoint(const NodeRec* nd, const float4& A, const LaneTargets& Q,
+                                                 const float* wx, const float* wy, const float* wz, bool two,
+                                                 const WalkParams& P, bool want_force, float* gx, float* gy,
+                                                 float* gz, float* fx, float* fy, float* fz, float* __restrict__ na,
+                                                 int r10) {
+  const float4 Qd = __ldg(&nd->quad);
+  const float4 X = __ldg(&nd->quad2);
+  const float M = A.w;
+  const float Sxx = Qd.x, Syy = Qd.y, Szz = Qd.z, Sxy = Qd.w, Sxz = X.x, Syz = X.y;
+  const float tr15 = 1.5f * (Sxx + Syy + Szz);
+  float v[10], vb = 0.f;  // vb: the (r.w) I part of G, added to its diagonal once
+#pragma unroll
+  for (int j = 0; j < 10; j++) v[j] = 0.f;
+#pragma unroll
+  for (int t = 0; t < kTPL; t++) {
+    if (t > 0 && !two) break;
+    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
+    float r2 = rx * rx + ry * ry + rz * rz;
+    float ir = rsqrtf(r2 + P.eps2);
+    float ih = ir * ir;
+    float ir3 = ir * ih;
+    float ir5 = ir3 * ih;
+    float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
+    float mlin = M * ir3, mrad = M * (rw * (3.0f * ir5));
+    v[3] -= ir3 * rw;  // A_M
+    float sx = Sxx * rx + Sxy * ry + Sxz * rz;
+    float sy = Sxy * rx + Syy * ry + Syz * rz;
+    float sz = Sxz * rx + Syz * ry + Szz * rz;
+    float swx = Sxx * wx[t] + Sxy * wy[t] + Sxz * wz[t];
+    float swy = Sxy * wx[t] + Syy * wy[t] + Syz * wz[t];
+    float swz = Sxz * wx[t] + Syz * wy[t] + Szz * wz[t];
+    float rsr = rx * sx + ry * sy + rz * sz;
+    float rsw = rx * swx + ry * swy + rz * swz;
+    float ir7 = ir5 * ih, ir9 = ir7 * ih;
+    float c1 = 3.0f * ir5;
+    float a1 = 5.0f * ir7 * rw;
+    float a3 = 15.0f * ir7 * rsw - 52.5f * ir9 * rsr * rw;
+    float cw = tr15 * ir5 - 7.5f * ir7 * rsr - mlin;
+    float cr = mrad - tr15 * a1 - a3;
+    float c2 = 3.0f * a1;
+    float qx_ = c1 * swx - c2 * sx + cw * wx[t] + cr * rx;
+    float qy_ = c1 * swy - c2 * sy + cw * wy[t] + cr * ry;
+    float qz_ = c1 * swz - c2 * sz + cw * wz[t] + cr * rz;
+    // G, off-diagonals doubled (halved once below)
+    float al = 1.5f * ir5, ga = 7.5f * ir7 * rw;
+    vb += al * rw;
+    float ux = 2.0f * al * wx[t] - ga * rx;
+    float uy = 2.0f * al * wy[t] - ga * ry;
+    float uz = 2.0f * al * wz[t] - ga * rz;
+    v[4] += ux * rx;
+    v[5] += uy * ry;
+    v[6] += uz * rz;
+    v[7] += ux * ry + uy * rx;
+    v[8] += ux * rz + uz * rx;
+    v[9] += uy * rz + uz * ry;
+    if (want_force) {
+      float cf = ir5 * (tr15 - 7.5f * rsr * ih) - mlin;
+      fx[t] += cf * rx + c1 * sx;
+      fy[t] += cf * ry + c1 * sy;
+      fz[t] += cf * rz + c1 * sz;
+    }
+    gx[t] += qx_;
+    gy[t] += qy_;
+    gz[t] += qz_;
+    v[0] -= qx_;
+    v[1] -= qy_;
+    v[2] -= qz_;
+  }
+  v[4] += vb;
+  v[5] += vb;
+  v[6] += vb;
+  v[7] *= 0.5f;
+  v[8] *= 0.5f;
+  v[9] *= 0.5f;
+  float tot = reduce10(v);
+  if (r10 >= 0) atomicAdd(&na[r10], tot);
+}
+
 // Fused force + adjoint walk. Per target slot: the query-side gradient
 // (written to gq in sorted order); per accepted node: A_X, A_M, G summed over
 // the group and added to node_adj; per near source particle: (dx, dm) summed
@@ -931,7 +1111,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     float fx[kTPL], fy[kTPL], fz[kTPL];  // force
 #pragma unroll
     for (int t = 0; t < kTPL; t++) gx[t] = gy[t] = gz[t] = fx[t] = fy[t] = fz[t] = 0.f;
-    unsigned long long nfar = 0, nnear = 0;
+    unsigned long long nfar = 0, nnear = 0, nquad = 0;
     int k = rt.x;
     while (k < rt.y) {
       const NodeRec* nd = T.nodes + k;
@@ -943,105 +1123,15 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
         k = tp.z;  // mass-zero and pruned nodes are skipped
         continue;
       }
-      if (accept_node(C, gmin, gmax, P.beta)) {
-        float4 Qd = make_float4(0.f, 0.f, 0.f, 0.f), X = Qd;
-        if (QUAD) {
-          Qd = __ldg(&nd->quad);
-          X = __ldg(&nd->quad2);
-        }
-        const float M = A.w;
-        const float Sxx = Qd.x, Syy = Qd.y, Szz = Qd.z, Sxy = Qd.w, Sxz = X.x, Syz = X.y;
-        const float tr15 = 1.5f * (Sxx + Syy + Szz);
-        float v[10], vb = 0.f;  // vb: the (r.w) I part of G, added to its diagonal once
-#pragma unroll
-        for (int j = 0; j < 10; j++) v[j] = 0.f;
-#pragma unroll
-        for (int t = 0; t < kTPL; t++) {
-          if (t > 0 && !two) break;
-          float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
-          if (PER) {
-            rx = min_image(rx, P);
-            ry = min_image(ry, P);
-            rz = min_image(rz, P);
-          }
-          float r2 = rx * rx + ry * ry + rz * rz;
-          float ir = rsqrtf(r2 + P.eps2);
-          float ih = ir * ir;
-          float ir3 = ir * ih;
-          float ir5 = ir3 * ih;
-          float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
-          float att = 1.0f, cc = 0.0f;
-          if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
-          float lin = att * ir3;
-          float mlin = M * lin, mrad = M * (rw * (3.0f * att * ir5 + cc));
-          v[3] -= lin * rw;  // A_M
-          float qx_, qy_, qz_;
-          if (QUAD) {
-            float sx = Sxx * rx + Sxy * ry + Sxz * rz;
-            float sy = Sxy * rx + Syy * ry + Syz * rz;
-            float sz = Sxz * rx + Syz * ry + Szz * rz;
-            float swx = Sxx * wx[t] + Sxy * wy[t] + Sxz * wz[t];
-            float swy = Sxy * wx[t] + Syy * wy[t] + Syz * wz[t];
-            float swz = Sxz * wx[t] + Syz * wy[t] + Szz * wz[t];
-            float rsr = rx * sx + ry * sy + rz * sz;
-            float rsw = rx * swx + ry * swy + rz * swz;
-            float ir7 = ir5 * ih, ir9 = ir7 * ih;
-            float c1 = 3.0f * ir5;
-            float a1 = 5.0f * ir7 * rw;
-            float a3 = 15.0f * ir7 * rsw - 52.5f * ir9 * rsr * rw;
-            float cw = tr15 * ir5 - 7.5f * ir7 * rsr - mlin;
-            float cr = mrad - tr15 * a1 - a3;
-            float c2 = 3.0f * a1;
-            qx_ = c1 * swx - c2 * sx + cw * wx[t] + cr * rx;
-            qy_ = c1 * swy - c2 * sy + cw * wy[t] + cr * ry;
-            qz_ = c1 * swz - c2 * sz + cw * wz[t] + cr * rz;
-            // G, off-diagonals doubled (halved once below)
-            float al = 1.5f * ir5, ga = 7.5f * ir7 * rw;
-            vb += al * rw;
-            float ux = 2.0f * al * wx[t] - ga * rx;
-            float uy = 2.0f * al * wy[t] - ga * ry;
-            float uz = 2.0f * al * wz[t] - ga * rz;
-            v[4] += ux * rx;
-            v[5] += uy * ry;
-            v[6] += uz * rz;
-            v[7] += ux * ry + uy * rx;
-            v[8] += ux * rz + uz * rx;
-            v[9] += uy * rz + uz * ry;
-            if (out) {
-              float cf = ir5 * (tr15 - 7.5f * rsr * ih) - mlin;
-              fx[t] += cf * rx + c1 * sx;
-              fy[t] += cf * ry + c1 * sy;
-              fz[t] += cf * rz + c1 * sz;
-            }
-          } else {
-            qx_ = mrad * rx - mlin * wx[t];
-            qy_ = mrad * ry - mlin * wy[t];
-            qz_ = mrad * rz - mlin * wz[t];
-            if (out) {
-              fx[t] -= mlin * rx;
-              fy[t] -= mlin * ry;
-              fz[t] -= mlin * rz;
-            }
-          }
-          gx[t] += qx_;
-          gy[t] += qy_;
-          gz[t] += qz_;
-          v[0] -= qx_;
-          v[1] -= qy_;
-          v[2] -= qz_;
-        }
-        if (QUAD) {
-          v[4] += vb;
-          v[5] += vb;
-          v[6] += vb;
-          v[7] *= 0.5f;
-          v[8] *= 0.5f;
-          v[9] *= 0.5f;
-          float tot = reduce10(v);
-          if (r10 >= 0) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r10], tot);
+      float d2, rc2;
+      if (accept_node(C, gmin, gmax, P.beta, d2, rc2)) {
+        float* na = node_adj + static_cast<int64_t>(k) * kNodeAdj;
+        if (QUAD && quad_order(d2, rc2, P)) {
+          far_quad_adjoint(nd, A, Q, wx, wy, wz, two, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, r10);
+          nquad++;
         } else {
-          float tot = reduce4(v[0], v[1], v[2], v[3]);
-          if ((lane & 7) == 0) atomicAdd(&node_adj[static_cast<int64_t>(k) * kNodeAdj + r4], tot);
+          far_mono_adjoint<CUT, PER>(A, Q, wx, wy, wz, two, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, lane,
+                                     r4);
         }
         nfar++;
         k = tp.z;
@@ -1100,6 +1190,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
       unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
       atomicAdd(&counters[0], nfar * na);
       atomicAdd(&counters[1], nnear * na);
+      atomicAdd(&counters[2], nquad * na);
     }
 #pragma unroll
     for (int t = 0; t < kTPL; t++) {
@@ -1226,7 +1317,6 @@ __global__ void __launch_bounds__(128, 4)
       C = __ldg(&T.nodes[k].cell);
     }
     while (k < rt.y) {
-      const NodeRec* nd = T.nodes + k;
       const bool live = A.w != 0.0f;  // mass-zero nodes are skipped
       const bool acc = live && accept_node(C, gmin, gmax, beta);
       const bool leaf = (tp.w & kLeafFlag) != 0;
@@ -1672,13 +1762,16 @@ int check_params(const sbh_native_params* p) {
   if (p->periodic && p->quadrupole) return invalid("the periodic walk uses the monopole far field (quadrupole = 0)");
   if (p->prune_radius < 0.0f) return invalid("prune_radius must be >= 0");
   if (p->prune_radius > 0.0f && !(p->cutoff > 0.0f)) return invalid("prune_radius needs an erfc cutoff (cutoff > 0)");
+  if (!(p->quadrupole_radius >= 0.0f)) return invalid("quadrupole_radius must be >= 0");
   return SBH_OK;
 }
 
 WalkParams walk_params(const sbh_native_params* p) {
   float eps = fmaxf(p->softening, 0.0f);
   float box = p->periodic ? p->box_length : 1.0f;
-  return WalkParams{p->beta, eps * eps + 1e-12f, p->cutoff, box, 1.0f / box, p->prune_radius * p->prune_radius};
+  float qr = p->quadrupole_radius;
+  return WalkParams{p->beta, eps * eps + 1e-12f, p->cutoff, box, 1.0f / box, p->prune_radius * p->prune_radius,
+                    qr > 0.0f ? qr * qr : 0.0f};
 }
 
 }  // namespace
@@ -1693,7 +1786,7 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   if (h.n == 0) return SBH_OK;
   if (!force_out) return invalid("force_out must be non-null");
-  cudaError_t e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
+  cudaError_t e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   WalkParams wp = walk_params(params);
   int64_t mg = h.n + h.nseg;
@@ -1718,7 +1811,7 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   if (!cotangent) return invalid("cotangent must be non-null");
   int64_t n = h.n;
   cudaError_t e = cudaMemsetAsync(L.part_adj, 0, n * kPartAdj * sizeof(float), stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
   WalkParams wp = walk_params(params);
@@ -1812,7 +1905,7 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   const uint32_t* qperm = which == 0 ? v0 : v1;
   query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
-  e = cudaMemsetAsync(L.counters, 0, 2 * sizeof(unsigned long long), stream);
+  e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1)};
   e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
@@ -1827,7 +1920,7 @@ int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspac
   Layout L;
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   uint32_t meta[8];
-  unsigned long long cnt[2];
+  unsigned long long cnt[3];
   cudaError_t e = cudaMemcpyAsync(meta, L.meta, sizeof(meta), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, L.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -1837,6 +1930,20 @@ int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspac
   out4[2] = cnt[0];
   out4[3] = cnt[1];
   if (meta[3]) return fail(SBH_ERR_LIMIT, "node capacity exceeded");
+  return SBH_OK;
+}
+
+int sbh_native_quadrupole_count(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
+                                uint64_t* far_quadrupole) {
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!far_quadrupole) return invalid("far_quadrupole must be non-null");
+  unsigned long long c = 0;
+  cudaError_t e = cudaMemcpyAsync(&c, L.counters + 2, sizeof(c), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  *far_quadrupole = c;
   return SBH_OK;
 }
 

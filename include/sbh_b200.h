@@ -345,6 +345,10 @@ typedef struct sbh_native_params {
   float box_length;
   float prune_radius; /* > 0 (with cutoff > 0): skip nodes whose cell lies farther than this from
                          every target of the group (the short-range split of TreePM) */
+  float quadrupole_radius; /* with quadrupole = 1: > 0 adds the quadrupole only for accepted nodes
+                              closer to the group box than quadrupole_radius opening radii
+                              (beta * diagonal), the monopole alone beyond; 0: for every
+                              accepted node */
 } sbh_native_params;
 
 /* Most targets one group holds (one warp walks a group). */
@@ -403,6 +407,11 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
  * interactions} of the last build / evaluation on this workspace. */
 int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
                      uint64_t* out4);
+
+/* Synchronises; *far_quadrupole = the far interactions (per target) of the
+ * last force or adjoint walk on this workspace that took the quadrupole. */
+int sbh_native_quadrupole_count(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
+                                uint64_t* far_quadrupole);
 
 /* Synchronises; copies sorted keys (n x u64), the permutation (n x u32,
  * sorted slot -> input index) and the 80-byte node records to device buffers

@@ -754,6 +754,7 @@ typedef struct {
   int64_t ngroups;
   int64_t* far_off; /* ngroups + 1 */
   int32_t* far_idx;
+  uint8_t* far_quad; /* per far entry: 1 when the node takes the quadrupole */
   int64_t* near_off;
   int32_t* near_idx; /* near-field leaf node ids */
   int64_t* gstart;
@@ -809,6 +810,7 @@ void orc_native_free(void* h) {
   free(t->side);
   free(t->far_off);
   free(t->far_idx);
+  free(t->far_quad);
   free(t->near_off);
   free(t->near_idx);
   free(t->gstart);
@@ -1000,7 +1002,7 @@ static int native_prune(const NativeTree* t, int64_t k, const float* C, const fl
  * The multipole is expanded about the COM.
  */
 static int native_accept(const NativeTree* t, int64_t k, const float* C, const float* gmin,
-                         const float* gmax, float beta) {
+                         const float* gmax, float beta, float* d2_out, float* rc2_out) {
   float rc = t->side[k] * 1.7320508f * beta;
   float tt[3];
   for (int d = 0; d < 3; d++) {
@@ -1009,7 +1011,22 @@ static int native_accept(const NativeTree* t, int64_t k, const float* C, const f
     tt[d] = m > 0.0f ? m : 0.0f;
   }
   float d2 = tt[0] * tt[0] + tt[1] * tt[1] + tt[2] * tt[2];
-  return d2 > rc * rc;
+  float rc2 = rc * rc;
+  *d2_out = d2;
+  *rc2_out = rc2;
+  return d2 > rc2;
+}
+
+/*
+ * Far-field order of an accepted node (the CUDA walk's quad_order): with a
+ * quadrupole radius q > 0 the quadrupole is added only when the opening
+ * distance^2 is below (q*q) * rc^2, in float; q = 0 adds it everywhere.
+ */
+static float g_orc_quad_g = 0.0f;
+void orc_native_set_quadrupole_radius(float q) { g_orc_quad_g = q > 0.0f ? q * q : 0.0f; }
+
+static int native_quad_order(float d2, float rc2) {
+  return !(g_orc_quad_g > 0.0f) || d2 < g_orc_quad_g * rc2;
 }
 
 /*
@@ -1068,6 +1085,7 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
   int64_t n = t->n;
   free(t->far_off);
   free(t->far_idx);
+  free(t->far_quad);
   free(t->near_off);
   free(t->near_idx);
   t->group_size = group_size;
@@ -1091,6 +1109,7 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
   float fbeta = (float)beta;
   int64_t fcap = 1 << 20, ncap = 1 << 18;
   t->far_idx = (int32_t*)malloc(sizeof(int32_t) * fcap);
+  t->far_quad = (uint8_t*)malloc(fcap);
   t->near_idx = (int32_t*)malloc(sizeof(int32_t) * ncap);
   t->far_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
   t->near_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
@@ -1116,11 +1135,14 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
         continue;
       }
       int is_leaf = (k + 1 >= t->nn) || (t->skip[k] == k + 1);
-      if (native_accept(t, k, C, gmin, gmax, fbeta)) {
+      float d2, rc2;
+      if (native_accept(t, k, C, gmin, gmax, fbeta, &d2, &rc2)) {
         if (nf == fcap) {
           fcap *= 2;
           t->far_idx = (int32_t*)realloc(t->far_idx, sizeof(int32_t) * fcap);
+          t->far_quad = (uint8_t*)realloc(t->far_quad, fcap);
         }
+        t->far_quad[nf] = (uint8_t)native_quad_order(d2, rc2);
         t->far_idx[nf++] = (int32_t)k;
         cnt_int += 1;
         k = t->skip[k];
@@ -1172,7 +1194,7 @@ void orc_native_eval(void* h, const float* pts, const float* masses, double eps,
         double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
         native_mi(r);
         soft_force_pair(r, o[0], &sp, acc);
-        if (quad) quad_force(r, o + 4, eps, acc);
+        if (quad && t->far_quad[e]) quad_force(r, o + 4, eps, acc);
       }
       for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
         int32_t k = t->near_idx[e];
@@ -1234,7 +1256,7 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
         double jt[3] = {0, 0, 0}, f[3] = {0, 0, 0};
         soft_force_pair_vjp(r, o[0], wi, &sp, jt);
         soft_force_pair(r, 1.0, &sp, f);
-        if (quad) quad_vjp(r, o + 4, wi, eps, jt, &AX[MOM * k + 4]);
+        if (quad && t->far_quad[e]) quad_vjp(r, o + 4, wi, eps, jt, &AX[MOM * k + 4]);
         for (int d = 0; d < 3; d++) {
           gq[d] += jt[d];
           AX[MOM * k + 1 + d] -= jt[d];
@@ -1285,6 +1307,18 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
 }
 
 /* Plan statistics: number of groups and list lengths. */
+/* Far interactions (per target) of the recorded plan that take the quadrupole. */
+int64_t orc_native_quadrupole_interactions(void* h) {
+  NativeTree* t = (NativeTree*)h;
+  int64_t total = 0;
+  for (int64_t g = 0; g < t->ngroups; g++) {
+    int64_t c = 0;
+    for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) c += t->far_quad[e];
+    total += c * (t->gend[g] - t->gstart[g]);
+  }
+  return total;
+}
+
 void orc_native_plan_stats(void* h, int64_t* ngroups, int64_t* nfar, int64_t* nnear) {
   NativeTree* t = (NativeTree*)h;
   *ngroups = t->ngroups;

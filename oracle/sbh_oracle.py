@@ -94,6 +94,9 @@ def _orc() -> ctypes.CDLL:
         lib.orc_native_plan.argtypes = [_c_p, _c_p, _c_p, _c_d, _c_i]
         lib.orc_native_eval.argtypes = [_c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p, _c_p]
         lib.orc_native_set_periodic.argtypes = [_c_i, _c_f, _c_f]
+        lib.orc_native_set_quadrupole_radius.argtypes = [_c_f]
+        lib.orc_native_quadrupole_interactions.argtypes = [_c_p]
+        lib.orc_native_quadrupole_interactions.restype = _c_i64
         lib.orc_native_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p]
         lib.orc_native_plan_stats.argtypes = [_c_p, _c_p, _c_p, _c_p]
         lib._typed = True
@@ -240,6 +243,10 @@ class NativeTree:
         return int(self._lib.orc_native_plan(self._h, _ptr(self.points), _ptr(self.masses), float(beta),
                                              int(group_size)))
 
+    def quadrupole_interactions(self) -> int:
+        """Far interactions (per target) of the plan that take the quadrupole."""
+        return int(self._lib.orc_native_quadrupole_interactions(self._h))
+
     def plan_stats(self):
         a, b, c = _c_i64(), _c_i64(), _c_i64()
         self._lib.orc_native_plan_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
@@ -279,6 +286,23 @@ class native_periodic:
 
     def __exit__(self, *exc):
         _orc().orc_native_set_periodic(0, 1.0, 0.0)
+        return False
+
+
+class native_quadrupole_radius:
+    """Context manager: plans recorded inside it give an accepted node the
+    quadrupole only within q opening radii of the group (q = 0: every
+    accepted node), as the CUDA walk does with quadrupole_radius = q."""
+
+    def __init__(self, q: float):
+        self.q = float(q)
+
+    def __enter__(self):
+        _orc().orc_native_set_quadrupole_radius(self.q)
+        return self
+
+    def __exit__(self, *exc):
+        _orc().orc_native_set_quadrupole_radius(0.0)
         return False
 
 

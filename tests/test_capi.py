@@ -54,6 +54,12 @@ def test_host_validation_without_device():
     prm = B.NativeParams(2.0, 1e-3, 0.0, 1)
     rc = L.sbh_native_force(null, ctypes.byref(prm), null, ctypes.c_void_p(12345), 1 << 20)
     assert rc == B.SBH_ERR_INVALID_ARGUMENT and "no native tree" in B.last_error()
+    prm = B.NativeTree.params(quadrupole_radius=-1.0)
+    rc = L.sbh_native_force(null, ctypes.byref(prm), null, ctypes.c_void_p(12345), 1 << 20)
+    assert rc == B.SBH_ERR_INVALID_ARGUMENT and "quadrupole_radius" in B.last_error()
+    prm = B.NativeTree.params(cutoff=0.05, quadrupole=False, prune_radius=0.3, periodic=True, box_length=0.0)
+    rc = L.sbh_native_force(null, ctypes.byref(prm), null, ctypes.c_void_p(12345), 1 << 20)
+    assert rc == B.SBH_ERR_INVALID_ARGUMENT and "box_length" in B.last_error()
     rc = L.sbh_barnes_hut_tree(null, 4, 0, null, 0, null, 616, null, 1, null, 2.0, 0.0, 1.0, 0, 1.0, 64, null, 0)
     assert rc == B.SBH_ERR_INVALID_ARGUMENT and "dim" in B.last_error()
 

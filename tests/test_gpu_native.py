@@ -53,46 +53,63 @@ def test_native_tree_bit_exact_vs_oracle(cuda, dist, leaf):
     np.testing.assert_allclose(nd["com"][:, 3].sum() >= 0, True)
 
 
-def test_native_force_matches_oracle_same_plan(cuda):
+@pytest.mark.parametrize("quad,qradius", [(True, 0.0), (True, 1.6), (False, 0.0)])
+def test_native_force_matches_oracle_same_plan(cuda, quad, qradius):
+    """qradius 0: every accepted node takes the quadrupole; 1.6: only those
+    within 1.6 opening radii of the group (the default)."""
     p, m = W.plummer(30000, seed=5)
-    for quad in (True, False):
-        t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=False)
-        f = t.force(beta=2.0, softening=1e-3, quadrupole=quad).cpu().numpy()
-        st = t.stats()
-        T = O.NativeTree(p, m, leaf_size=16)
+    t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=False)
+    f = t.force(beta=2.0, softening=1e-3, quadrupole=quad, quadrupole_radius=qradius).cpu().numpy()
+    st = t.stats()
+    T = O.NativeTree(p, m, leaf_size=16)
+    with O.native_quadrupole_radius(qradius):
         inter = T.plan(2.0, B.native_group_size())
-        want, _ = T.force(1e-3, quad=quad)
-        assert rel_l2(f, want) < 1e-5, quad
-        # same node-packed target groups
-        assert st["groups"] == T.plan_stats()[0]
-        # same opening decisions up to ulp-level ties
-        assert abs((st["far"] + st["near"]) - inter) <= 1e-4 * inter
+    want, _ = T.force(1e-3, quad=quad)
+    assert rel_l2(f, want) < 1e-5
+    # same node-packed target groups
+    assert st["groups"] == T.plan_stats()[0]
+    # same opening decisions up to ulp-level ties
+    assert abs((st["far"] + st["near"]) - inter) <= 1e-4 * inter
+    if quad:
+        # and the same far-field orders
+        nq = T.quadrupole_interactions()
+        assert abs(st["far_quadrupole"] - nq) <= 1e-4 * st["far"]
+        assert (nq == st["far"]) == (qradius == 0.0)
+    else:
+        assert st["far_quadrupole"] == 0
 
 
 def test_native_force_accuracy_vs_fp64_direct(cuda):
     p, m = W.plummer(200000, seed=6)
     t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=False)
-    f = t.force(beta=2.0, softening=1e-3, quadrupole=True).cpu().numpy()
     idx = np.random.default_rng(0).choice(p.shape[0], 4096, replace=False)
     want = O.direct_force_soft(p, m, p[idx], 1e-3)
-    assert rel_l2(f[idx], want) < 1e-4
+    err = {}
+    for q in (0.0, B.QUADRUPOLE_RADIUS):
+        f = t.force(beta=2.0, softening=1e-3, quadrupole=True, quadrupole_radius=q).cpu().numpy()
+        err[q] = rel_l2(f[idx], want)
+    f = t.force(beta=2.0, softening=1e-3, quadrupole=False).cpu().numpy()
+    err["mono"] = rel_l2(f[idx], want)
+    assert err[0.0] < err[B.QUADRUPOLE_RADIUS] < err["mono"]
+    assert err[B.QUADRUPOLE_RADIUS] < 8e-5
 
 
-def test_native_adjoint_matches_oracle(cuda):
+@pytest.mark.parametrize("quad,qradius", [(True, 0.0), (True, 1.6), (False, 0.0)])
+def test_native_adjoint_matches_oracle(cuda, quad, qradius):
     rng = np.random.default_rng(7)
     p, m = W.plummer(20000, seed=7)
     m = (m * rng.uniform(0.5, 1.5, m.shape)).astype(np.float32)
     w = rng.normal(size=p.shape).astype(np.float32)
-    for quad in (True, False):
-        t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True)
-        f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=quad)
-        T = O.NativeTree(p, m, leaf_size=16)
+    t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True)
+    f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=quad, quadrupole_radius=qradius)
+    T = O.NativeTree(p, m, leaf_size=16)
+    with O.native_quadrupole_radius(qradius):
         T.plan(2.0, B.native_group_size())
-        want_f, _ = T.force(1e-3, quad=quad)
-        dx, dm = T.adjoint(w, 1e-3, quad=quad)
-        assert rel_l2(f.cpu().numpy(), want_f) < 1e-5
-        assert rel_l2(gx.cpu().numpy(), dx) < 1e-4, quad
-        assert rel_l2(gm.cpu().numpy(), dm) < 1e-4, quad
+    want_f, _ = T.force(1e-3, quad=quad)
+    dx, dm = T.adjoint(w, 1e-3, quad=quad)
+    assert rel_l2(f.cpu().numpy(), want_f) < 1e-5
+    assert rel_l2(gx.cpu().numpy(), dx) < 1e-4
+    assert rel_l2(gm.cpu().numpy(), dm) < 1e-4
 
 
 def test_native_forest_equals_separate_systems(cuda):

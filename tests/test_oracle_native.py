@@ -56,15 +56,21 @@ def test_native_infinite_beta_is_direct():
     assert rel_l2(f, want) < 1e-12
 
 
-@pytest.mark.parametrize("quad", [False, True])
-def test_native_adjoint_matches_finite_differences(quad):
+@pytest.mark.parametrize("quad,qradius", [(False, 0.0), (True, 0.0), (True, 1.6)])
+def test_native_adjoint_matches_finite_differences(quad, qradius):
     rng = np.random.default_rng(6)
     p, m = W.plummer(600, seed=6)
     m = (m * rng.uniform(0.5, 1.5, m.shape)).astype(np.float32)
     w = rng.normal(size=p.shape).astype(np.float32)
     eps = 1e-2
     T = O.NativeTree(p, m, leaf_size=8)
-    T.plan(2.0, 32)
+    with O.native_quadrupole_radius(qradius):
+        T.plan(2.0, 32)
+    if qradius > 0:
+        # a mixed plan: some far nodes with the quadrupole, some without
+        T0 = O.NativeTree(p, m, leaf_size=8)
+        T0.plan(2.0, 32)
+        assert 0 < T.quadrupole_interactions() < T0.quadrupole_interactions()
     dx, dm = T.adjoint(w, eps, quad=quad)
     p64 = p.astype(np.float64)
     h = 1e-4
@@ -86,6 +92,30 @@ def test_native_adjoint_matches_finite_differences(quad):
         lm = T.force(eps, points=p, masses=mm.astype(np.float32), w=w, quad=quad)[1]
         fd = (lp - lm) / (2 * dh)
         assert abs(fd - dm[k]) <= 2e-3 * (abs(fd) + 1.0), (k, fd, dm[k])
+
+
+def test_native_quadrupole_radius_trades_order_for_accuracy():
+    """The quadrupole radius keeps the plan (same far and near lists) and
+    only drops the quadrupole of distant nodes: the error sits between the
+    monopole's and the full quadrupole's."""
+    p, m = W.plummer(20000, seed=9)
+    idx = np.random.default_rng(1).choice(p.shape[0], 256, replace=False)
+    want = O.direct_force_soft(p, m, p[idx], 1e-3)
+    err, counts = {}, {}
+    for q in (0.0, 1.6):
+        T = O.NativeTree(p, m, leaf_size=16)
+        with O.native_quadrupole_radius(q):
+            counts[q] = T.plan(2.0, 64)
+        err[q] = rel_l2(T.force(1e-3, quad=True)[0][idx], want)
+        if q == 0.0:
+            err["mono"] = rel_l2(T.force(1e-3, quad=False)[0][idx], want)
+            nfar_total = T.quadrupole_interactions()
+        else:
+            frac = T.quadrupole_interactions() / nfar_total
+    assert counts[0.0] == counts[1.6]
+    assert 0.2 < frac < 0.8
+    assert err[0.0] < err[1.6] < err["mono"]
+    assert err[1.6] < 1e-4
 
 
 def test_native_adjoint_approximates_exact_gradient():
