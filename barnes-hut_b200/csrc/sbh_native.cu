@@ -526,11 +526,12 @@ __device__ __forceinline__ uint32_t next_group(const WalkTargets& G) {
 
 // Resident blocks of 128 threads per SM the walks are compiled for (this
 // caps their registers at 65536 / (128 x blocks)). Measured on a B200 with
-// 2 x 2^20 Plummer particles: the adjoint walk takes 145 ms at 4 blocks (96
-// registers), 138 ms at 6 (80 registers, no spills), 136 ms at 7 (72
-// registers, 24 bytes of spills); the force walk 63 ms at 5, 60 ms at 6.
+// 8 x 2^20 Plummer particles, quadrupole radius 1.6: the adjoint walk takes
+// 477 ms at 5 blocks (88 registers), 445 ms at 6 (80 registers), 429 ms at 7
+// (72 registers, 48 bytes of spills) and 430 ms at 8 (64 registers); the
+// force walk 219 ms at 5, 211 ms at 6, 213 ms at 7 and 218 ms at 8.
 #ifndef SBH_ADJOINT_WALK_MIN_BLOCKS
-#define SBH_ADJOINT_WALK_MIN_BLOCKS 6
+#define SBH_ADJOINT_WALK_MIN_BLOCKS 7
 #endif
 #ifndef SBH_FORCE_WALK_MIN_BLOCKS
 #define SBH_FORCE_WALK_MIN_BLOCKS 6
@@ -767,7 +768,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     float nx[kTPL], ny[kTPL], nz[kTPL], cx[kTPL], cy[kTPL], cz[kTPL];       // near field, compensated
 #pragma unroll
     for (int t = 0; t < kTPL; t++) fx[t] = fy[t] = fz[t] = nx[t] = ny[t] = nz[t] = cx[t] = cy[t] = cz[t] = 0.f;
-    unsigned long long nfar = 0, nnear = 0, nquad = 0;
+    uint32_t nfar = 0, nnear = 0, nquad = 0;  // per group (a group's counts stay below n)
     // Pre-order walk. The next node is known once this node's opening test
     // is done, so its opening data is loaded before this node's terms are
     // evaluated and the load latency hides behind that arithmetic.
@@ -839,7 +840,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
           kahan_add(ny[t], cy[t], ay[t]);
           kahan_add(nz[t], cz[t], az[t]);
         }
-        nnear += static_cast<unsigned long long>(tp.y - tp.x);
+        nnear += static_cast<uint32_t>(tp.y - tp.x);
       }
       k = next;
       tp = tpn;
@@ -1096,13 +1097,12 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     load_targets(G, gr, lane, Q);
     const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
     float wx[kTPL], wy[kTPL], wz[kTPL];
-    uint32_t o[kTPL];
 #pragma unroll
     for (int t = 0; t < kTPL; t++) {
-      o[t] = Q.act[t] ? G.perm[Q.idx[t]] : 0u;
-      wx[t] = Q.act[t] ? cot[3 * o[t]] : 0.f;
-      wy[t] = Q.act[t] ? cot[3 * o[t] + 1] : 0.f;
-      wz[t] = Q.act[t] ? cot[3 * o[t] + 2] : 0.f;
+      const uint32_t o = Q.act[t] ? G.perm[Q.idx[t]] : 0u;
+      wx[t] = Q.act[t] ? cot[3 * o] : 0.f;
+      wy[t] = Q.act[t] ? cot[3 * o + 1] : 0.f;
+      wz[t] = Q.act[t] ? cot[3 * o + 2] : 0.f;
     }
     float gmin[3], gmax[3];
     group_box(Q, gmin, gmax);
@@ -1111,7 +1111,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     float fx[kTPL], fy[kTPL], fz[kTPL];  // force
 #pragma unroll
     for (int t = 0; t < kTPL; t++) gx[t] = gy[t] = gz[t] = fx[t] = fy[t] = fz[t] = 0.f;
-    unsigned long long nfar = 0, nnear = 0, nquad = 0;
+    uint32_t nfar = 0, nnear = 0, nquad = 0;  // per group (a group's counts stay below n)
     int k = rt.x;
     while (k < rt.y) {
       const NodeRec* nd = T.nodes + k;
@@ -1180,7 +1180,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
           float tot = reduce4(a0, a1, a2, a3);
           if ((lane & 7) == 0) atomicAdd(&part_adj[static_cast<int64_t>(j) * kPartAdj + r4], tot);
         }
-        nnear += static_cast<unsigned long long>(tp.y - tp.x);
+        nnear += static_cast<uint32_t>(tp.y - tp.x);
         k = tp.z;
       } else {
         k++;
@@ -1200,9 +1200,10 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
         gq[3 * i + 1] = gy[t];
         gq[3 * i + 2] = gz[t];
         if (out) {
-          out[3 * o[t]] = fx[t];
-          out[3 * o[t] + 1] = fy[t];
-          out[3 * o[t] + 2] = fz[t];
+          const uint32_t o = G.perm[i];  // reloaded: not kept live through the walk
+          out[3 * o] = fx[t];
+          out[3 * o + 1] = fy[t];
+          out[3 * o + 2] = fz[t];
         }
       }
     }
@@ -1304,7 +1305,7 @@ __global__ void __launch_bounds__(128, 4)
     float far[kTPL], near[kTPL], comp[kTPL];
 #pragma unroll
     for (int t = 0; t < kTPL; t++) far[t] = near[t] = comp[t] = 0.f;
-    unsigned long long nfar = 0, nnear = 0;
+    uint32_t nfar = 0, nnear = 0;  // per group (a group's counts stay below n)
     // Pre-order walk. The next node is known once this node's opening test
     // is done, so its opening data is loaded before this node's terms are
     // evaluated and the load latency hides behind that arithmetic.
@@ -1357,7 +1358,7 @@ __global__ void __launch_bounds__(128, 4)
         }
 #pragma unroll
         for (int t = 0; t < kTPL; t++) kahan_add(near[t], comp[t], a[t]);
-        nnear += static_cast<unsigned long long>(tp.y - tp.x);
+        nnear += static_cast<uint32_t>(tp.y - tp.x);
       }
       k = next;
       tp = tpn;
