@@ -478,6 +478,9 @@ def run_ours(args):
     idx = torch.tensor(np.random.default_rng(5).choice(n, 1024, replace=False), device=dev)
     ref = fp64_direct_subset(P[:n], M[:n], idx, EPS)
     rel = float(torch.linalg.norm(F[idx].double() - ref) / torch.linalg.norm(ref))
+    # rows whose own relative error exceeds 5% (outlier_frac of unified_force_benchmark.py:316-328)
+    row_rel = torch.linalg.norm(F[idx].double() - ref, dim=1) / torch.linalg.norm(ref, dim=1).clamp_min(1e-12)
+    outlier_frac = float((row_rel > 0.05).double().mean())
     st = tree.stats()
 
     for _ in range(args.warmup):
@@ -624,7 +627,8 @@ def run_ours(args):
                        "batched": f"{K} systems in one forest: one build, one walk, one finalize per step",
                        "l2": "flushed between steps (256 MB write, outside the timed events)",
                        "parallelism": "replicas" if world > 1 else "single"},
-            "accuracy": {"rel_l2_vs_fp64_direct": rel, "subset": 1024, "system": 0},
+            "accuracy": {"rel_l2_vs_fp64_direct": rel, "outlier_frac": outlier_frac,
+                         "max_row_rel": float(row_rel.max()), "subset": 1024, "system": 0},
             "batched_vs_plain": {"batched_evals_per_s": value / world, "plain_evals_per_s": plain_eps,
                                  "ratio": value / world / plain_eps, "plain_ms_per_eval": plain_ms,
                                  "graph_ms_per_step": graph_ms, "eager_ms_per_step": ms_per_step,
