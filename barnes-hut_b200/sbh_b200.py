@@ -140,6 +140,9 @@ _SIGS = {
     "sbh_native_winding_number": ([_c_p, _c_f, _c_p, _c_i64, _c_p, _c_p, _c_sz, _c_p, _c_sz], _c_i),
     "sbh_native_stats": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_quadrupole_count": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
+    "sbh_mesh_sample_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_sample_mesh_surface": ([_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_i64, _c_u64, _c_p, _c_p, _c_p, _c_p, _c_sz],
+                                _c_i),
     "sbh_native_export": ([_c_p, _c_p, _c_sz, _c_p, _c_p, _c_p, _c_sz, _c_p], _c_i),
 }
 
@@ -746,6 +749,60 @@ for _name in ("register_bruteforce_gravity", "register_softened_direct_force", "
               "register_stochastic_barnes_hut_force_octree8_vjp",
               "register_softened_stochastic_barnes_hut_force_octree8_vjp"):
     globals()[_name] = _register
+
+
+# ---------------------------------------------------------------------------
+# mesh surface sampling (python/old_interface/sampler.py:45-78,
+# python/old_interface/source.py:119-155)
+# ---------------------------------------------------------------------------
+def sample_points_on_mesh(num_particles: int, V, F, *, seed: int = 0, device=None):
+    """(points (n, 3), normals (n, 3), weights (n,)) on the device: points
+    uniform on the surface of the triangle mesh (V: (nv, 3) vertices, F:
+    (nf, 3) vertex indices), each with its face's unit normal e1 x e2 / |e1 x
+    e2| and the weight total area / n. Same distribution as the reference's
+    sample_points_on_mesh; the stream is the counter-based splitmix64 of
+    sbh_sample_mesh_surface, so (seed, sample index) fixes every sample.
+    Raises SbhError when a face references a missing vertex or the mesh has
+    no area (read back from the device status word, which synchronises)."""
+    device = device or (V.device if isinstance(V, torch.Tensor) and V.is_cuda else _device())
+    v = _f32(V, device)
+    f = F.to(device=device, dtype=torch.int32).contiguous() if isinstance(F, torch.Tensor) else \
+        torch.as_tensor(np.asarray(F, dtype=np.int32), device=device).contiguous()
+    if v.ndim != 2 or v.shape[1] != 3 or f.ndim != 2 or f.shape[1] != 3:
+        raise ValueError("V must be (nv, 3) and F (nf, 3)")
+    n = int(num_particles)
+    if n < 0:
+        raise ValueError("num_particles must be >= 0")
+    pts = torch.empty((n, 3), dtype=torch.float32, device=device)
+    nrm = torch.empty((n, 3), dtype=torch.float32, device=device)
+    w = torch.empty(n, dtype=torch.float32, device=device)
+    ws = workspace(int(lib().sbh_mesh_sample_workspace_bytes(f.shape[0])), device)
+    _check(lib().sbh_sample_mesh_surface(_stream_ptr(device), _p(v), v.shape[0], _p(f), f.shape[0], n,
+                                         int(seed) & 0xFFFFFFFFFFFFFFFF, _p(pts), _p(nrm), _p(w), _p(ws),
+                                         ws.numel()), "sample_mesh_surface")
+    if n > 0 and read_device_status(ws) & DEV_BAD_BOUNDS:
+        raise SbhError("sample_mesh_surface: a face references a missing vertex, or the mesh has no area")
+    return pts, nrm, w
+
+
+class MeshSurface:
+    """Winding-number sources sampled on a triangle mesh (the reference's
+    MeshSurface source, python/old_interface/source.py:119-155): the mesh is
+    centred and scaled so its largest extent is `scale`, then sample() draws
+    points, face normals and area weights on the device."""
+
+    def __init__(self, V, F, scale: float = 1.0, device=None):
+        V = np.asarray(V.cpu() if isinstance(V, torch.Tensor) else V, dtype=np.float64)
+        vmin, vmax = V.min(axis=0), V.max(axis=0)
+        width = float(np.max(vmax - vmin))
+        if not width > 0:
+            raise ValueError("the mesh has zero extent")
+        self.V = ((V - (vmax + vmin) / 2) / width * scale).astype(np.float32)
+        self.F = np.asarray(F.cpu() if isinstance(F, torch.Tensor) else F, dtype=np.int32)
+        self.device = device
+
+    def sample(self, num_points: int, seed: int = 0):
+        return sample_points_on_mesh(num_points, self.V, self.F, seed=seed, device=self.device)
 
 
 # ---------------------------------------------------------------------------

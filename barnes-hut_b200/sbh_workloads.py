@@ -87,6 +87,31 @@ def ellipsoid_inside(q, axes=(1.0, 0.7, 0.5)):
     return (q[:, 0] / a) ** 2 + (q[:, 1] / b) ** 2 + (q[:, 2] / c) ** 2 < 1.0
 
 
+def torus_mesh(R: float = 1.0, r: float = 0.4, nu: int = 128, nv: int = 64):
+    """Closed triangle mesh of the torus (sqrt(x^2 + y^2) - R)^2 + z^2 = r^2:
+    vertices on an nu x nv grid of the angles around the z axis (u) and
+    around the tube (v), two triangles per grid cell, ordered so that
+    e1 x e2 points outward. Returns (V (nu*nv, 3) float32, F (2*nu*nv, 3)
+    int32)."""
+    u = 2 * np.pi * np.arange(nu) / nu
+    v = 2 * np.pi * np.arange(nv) / nv
+    U, Vv = np.meshgrid(u, v, indexing="ij")
+    ring = R + r * np.cos(Vv)
+    V = np.stack([ring * np.cos(U), ring * np.sin(U), r * np.sin(Vv)], axis=-1).reshape(-1, 3)
+    i, j = np.meshgrid(np.arange(nu), np.arange(nv), indexing="ij")
+    a = i * nv + j
+    b = ((i + 1) % nu) * nv + j
+    c = ((i + 1) % nu) * nv + (j + 1) % nv
+    d = i * nv + (j + 1) % nv
+    F = np.concatenate([np.stack([a, b, c], -1).reshape(-1, 3), np.stack([a, c, d], -1).reshape(-1, 3)])
+    return V.astype(np.float32), F.astype(np.int32)
+
+
+def torus_inside(q, R: float = 1.0, r: float = 0.4):
+    q = np.asarray(q, np.float64)
+    return (np.sqrt(q[:, 0] ** 2 + q[:, 1] ** 2) - R) ** 2 + q[:, 2] ** 2 < r * r
+
+
 def uniform_box_queries(m: int, seed: int = 1, half: float = 1.5):
     rng = np.random.default_rng(seed)
     return rng.uniform(-half, half, (m, 3)).astype(np.float32)

@@ -423,6 +423,27 @@ int sbh_native_export(cudaStream_t stream, const void* workspace, size_t workspa
                       uint64_t* keys_out, uint32_t* perm_out, void* nodes_out,
                       size_t nodes_capacity, uint64_t* num_nodes);
 
+/* ---------------------------------------------------------------------- */
+/* Mesh surface sampling (winding-number sources from a triangle mesh)     */
+/* ---------------------------------------------------------------------- */
+/* Replaces the host-side sampler of the reference's mesh sources
+ * (python/old_interface/sampler.py:45-78 sample_points_on_mesh;
+ * python/old_interface/source.py:119-155 MeshSurface): n points, each on a
+ * face chosen with probability area / total area and uniform inside it, with
+ * the face's unit normal (e1 x e2 / |e1 x e2| for the face's vertex order)
+ * and the weight total area / n. The random numbers are outputs 3i+1..3i+3 of
+ * splitmix64 seeded with `seed` for sample i, so results depend on
+ * (seed, i) only. Faces that reference a vertex outside [0, nv) set
+ * SBH_DEV_BAD_BOUNDS in the device status word and count as zero area; a mesh
+ * without positive area sets it too and yields zeros.
+ * vertices: nv x 3 f32, faces: nf x 3 i32 (device). Outputs: points n x 3,
+ * normals n x 3, weights n (device, f32). */
+size_t sbh_mesh_sample_workspace_bytes(int64_t nf);
+int sbh_sample_mesh_surface(cudaStream_t stream, const float* vertices, int64_t nv,
+                            const int32_t* faces, int64_t nf, int64_t n, uint64_t seed,
+                            float* points_out, float* normals_out, float* weights_out,
+                            void* workspace, size_t workspace_bytes);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -519,3 +519,77 @@ def refgpu() -> ctypes.CDLL:
 def refgpu_check(rc: int) -> None:
     if rc != 0:
         raise RuntimeError("reference handler failed: " + refgpu().ref_gpu_last_error().decode())
+
+
+# ---------------------------------------------------------------------------
+# mesh surface sampling (pure numpy restatement of sbh_sample_mesh_surface)
+# ---------------------------------------------------------------------------
+_SPLITMIX_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+
+
+def splitmix64_mix(z: np.ndarray) -> np.ndarray:
+    """The splitmix64 output function (S. Vigna, 2015) on uint64 arrays; the
+    generator's k-th output from seed s is splitmix64_mix(s + k * gamma)."""
+    z = np.asarray(z, dtype=np.uint64)
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def mesh_face_geometry(V, F):
+    """(twice the face areas (float64), unit normals (float32)) in the order
+    of operations of the sampler's face pass: e1 = v1 - v0, e2 = v2 - v0 and
+    c = e1 x e2 in float64 from the float32 vertices, |c| =
+    sqrt((c0^2 + c1^2) + c2^2), normal = c / |c| rounded to float32.
+    Degenerate and NaN faces get zero area and a zero normal (the reference
+    zeroes NaN areas, python/old_interface/sampler.py:67-68)."""
+    V = np.asarray(V, dtype=np.float32).astype(np.float64)
+    F = np.asarray(F, dtype=np.int64)
+    v0, v1, v2 = V[F[:, 0]], V[F[:, 1]], V[F[:, 2]]
+    e1, e2 = v1 - v0, v2 - v0
+    c = np.stack([e1[:, 1] * e2[:, 2] - e1[:, 2] * e2[:, 1],
+                  e1[:, 2] * e2[:, 0] - e1[:, 0] * e2[:, 2],
+                  e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0]], axis=1)
+    with np.errstate(invalid="ignore"):
+        ln = np.sqrt((c[:, 0] * c[:, 0] + c[:, 1] * c[:, 1]) + c[:, 2] * c[:, 2])
+    ok = (ln > 0) & np.isfinite(ln)
+    ln = np.where(ok, ln, 0.0)
+    nrm = np.zeros_like(c)
+    nrm[ok] = c[ok] / ln[ok, None]
+    return ln, nrm.astype(np.float32)
+
+
+def sample_points_on_mesh(num_particles: int, V, F, seed: int = 0):
+    """Restatement of sbh_sample_mesh_surface (same distribution as the
+    reference's sample_points_on_mesh, python/old_interface/sampler.py:63-78):
+    sample i draws u0, u1, u2 = outputs 3i+1, 3i+2, 3i+3 of splitmix64 seeded
+    with `seed` (top 53 bits / 2^53); its face is the first face whose
+    cumulative doubled area exceeds min(u0 * total, the double below total);
+    (u1, u2) is reflected to (1 - u1, 1 - u2) when u1 + u2 > 1; the point is
+    (v0 + u1 e1) + u2 e2 in float64 rounded to float32; its normal the face's
+    unit normal; its weight (total / 2) / n as float32. Returns (points,
+    normals, weights, faces)."""
+    n = int(num_particles)
+    V64 = np.asarray(V, dtype=np.float32).astype(np.float64)
+    F = np.asarray(F, dtype=np.int64)
+    area2, nrm = mesh_face_geometry(V, F)
+    cdf = np.concatenate([[0.0], np.cumsum(area2)])
+    total = cdf[-1]
+    i = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):  # uint64 arithmetic wraps modulo 2^64, as on the device
+        base = np.uint64(seed) + (np.uint64(3) * i + np.uint64(1)) * _SPLITMIX_GAMMA
+        u = [(splitmix64_mix(base + np.full(n, k, np.uint64) * _SPLITMIX_GAMMA) >> np.uint64(11)).astype(np.float64)
+             * 2.0 ** -53 for k in range(3)]
+    top = np.nextafter(total, 0.0)
+    target = np.minimum(u[0] * total, top)
+    face = np.searchsorted(cdf[1:], target, side="right")
+    u1, u2 = u[1], u[2]
+    flip = (u1 + u2) > 1.0
+    u1 = np.where(flip, 1.0 - u1, u1)
+    u2 = np.where(flip, 1.0 - u2, u2)
+    v0 = V64[F[face, 0]]
+    e1 = V64[F[face, 1]] - v0
+    e2 = V64[F[face, 2]] - v0
+    pts = ((v0 + u1[:, None] * e1) + u2[:, None] * e2).astype(np.float32)
+    w = np.full(n, np.float32((total * 0.5) / n) if n else 0.0, dtype=np.float32)
+    return pts, nrm[face], w, face
