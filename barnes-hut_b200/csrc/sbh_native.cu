@@ -409,34 +409,35 @@ __global__ void roots_kernel(const int64_t* __restrict__ sorted_seg_off, int nse
   if (threadIdx.x == 0) roots[s] = make_int2(static_cast<int>(r0), static_cast<int>(a < b ? r1 : r0));
 }
 
-// Target groups cut from the tree. For every node holding more than kGroup
-// particles its children are taken in order; each maximal run of consecutive
-// children that hold at most kGroup particles each is one range of sorted
-// particles, cut into chunks of kGroup (the last one shorter). Children with
-// more particles are handled the same way one level down; a leaf with more
-// than kGroup particles (coincident points at level 21) and a system root
-// holding at most kGroup are cut into chunks directly. Every group lies
-// inside the cell of a node with more than kGroup particles, so its bounding
-// box is compact (runs of consecutive Morton positions can straddle distant
-// cells), and the chunks fill the lanes better than one group per child run.
-// Slots come from an atomic counter: the group order varies between runs,
-// each group's result does not.
+// Target groups cut from the tree, at most G (<= kGroup) targets each. For
+// every node holding more than G particles its children are taken in order;
+// each maximal run of consecutive children that hold at most G particles
+// each is one range of sorted particles, cut into chunks of G (the last one
+// shorter). Children with more particles are handled the same way one level
+// down; a leaf with more than G particles (coincident points at level 21)
+// and a system root holding at most G are cut into chunks directly. Every
+// group lies inside the cell of a node with more than G particles, so its
+// bounding box is compact (runs of consecutive Morton positions can straddle
+// distant cells), and the chunks fill the lanes better than one group per
+// child run. Slots come from an atomic counter: the group order varies
+// between runs, each group's result does not. Every group holds at least one
+// particle, so n + systems + 1 slots always suffice.
 __device__ __forceinline__ void emit_chunks(int4* groups, uint32_t* count, int64_t cap, int s0, int s1, int sys,
-                                            uint32_t* status) {
-  int ng = (s1 - s0 + kGroup - 1) / kGroup;
+                                            int G, uint32_t* status) {
+  int ng = (s1 - s0 + G - 1) / G;
   if (ng <= 0) return;
   uint32_t slot = atomicAdd(count, static_cast<uint32_t>(ng));
   for (int g = 0; g < ng; g++) {
-    int s = s0 + g * kGroup;
+    int s = s0 + g * G;
     if (slot + g < cap)
-      groups[slot + g] = make_int4(s, min(s + kGroup, s1), sys, 0);
+      groups[slot + g] = make_int4(s, min(s + G, s1), sys, 0);
     else
       raise_status(status, SBH_DEV_ITER_LIMIT);
   }
 }
 
 __global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
-                                   const uint32_t* __restrict__ sseg, int4* __restrict__ groups, int64_t cap,
+                                   const uint32_t* __restrict__ sseg, int4* __restrict__ groups, int64_t cap, int G,
                                    uint32_t* __restrict__ count, uint32_t* status) {
   uint32_t nn = *nn_ptr;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
@@ -445,15 +446,15 @@ __global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint
     bool leaf = (t.w & kLeafFlag) != 0;
     bool root = (t.w & 0xFF) == 0;
     int sys = sseg ? static_cast<int>(sseg[t.x]) : 0;
-    if (leaf || cnt <= kGroup) {
-      if (root || (leaf && cnt > kGroup)) emit_chunks(groups, count, cap, t.x, t.y, sys, status);
+    if (leaf || cnt <= G) {
+      if (root || (leaf && cnt > G)) emit_chunks(groups, count, cap, t.x, t.y, sys, G, status);
       continue;
     }
     int run_s = -1, run_e = -1;
     for (uint32_t c = k + 1; c < static_cast<uint32_t>(t.z) && c < nn;) {
       int4 tc = nodes[c].topo;
-      if (tc.y - tc.x > kGroup) {
-        if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, status);
+      if (tc.y - tc.x > G) {
+        if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, G, status);
         run_s = -1;
       } else {
         if (run_s < 0) run_s = tc.x;
@@ -462,7 +463,7 @@ __global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint
       if (static_cast<uint32_t>(tc.z) <= c) break;  // malformed skip: never loop
       c = static_cast<uint32_t>(tc.z);
     }
-    if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, status);
+    if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, G, status);
   }
 }
 
@@ -548,6 +549,8 @@ struct WalkParams {
   float prune_r2;  // > 0: skip nodes whose cell is farther than sqrt(prune_r2) from the group box
   float quad_g;    // > 0: an accepted node takes the quadrupole only when its opening distance^2 is
                    // below quad_g * (beta * diagonal)^2; 0: every accepted node takes it
+  float inv_2cut;  // 1 / (2 cutoff) (cutoff walks)
+  float cc_coef;   // 1 / (2 sqrt(pi) cutoff^3) (cutoff walks)
 };
 
 // Minimum-image displacement of a periodic box (minImageDisplacement,
@@ -676,13 +679,24 @@ __device__ __forceinline__ bool accept_node(const float4& cell, const float* gmi
 }
 
 // erfc attenuation of the short-range force and its radial derivative term
-// (src/sbh_ffi.cu:142-160, 2062-2090); att = 1, cc = 0 without cutoff.
-__device__ __forceinline__ void attenuation(float r2, float ir3, float cutoff, float& att, float& cc) {
-  float dist = sqrtf(r2 + 1e-12f);
-  float u = dist / (2.0f * cutoff);
-  float e = expf(-(u * u));
-  att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
-  cc = ir3 * dist * e / (2.0f * 1.772453850905516f * cutoff * cutoff * cutoff);
+// (src/sbh_ffi.cu:142-160, 2062-2090), with u = r / (2 cutoff):
+//   att = erfc(u) + (2 / sqrt(pi)) u e^{-u^2},
+//   cc  = ir3 r e^{-u^2} / (2 sqrt(pi) cutoff^3);
+// att = 1, cc = 0 without cutoff. erfc(u) is the rational approximation of
+// Abramowitz & Stegun 7.1.26 (after Hastings): (a1 t + a2 t^2 + a3 t^3 +
+// a4 t^4 + a5 t^5) e^{-u^2} with t = 1 / (1 + p u), absolute error at most
+// 1.5e-7 for u >= 0. It shares e^{-u^2} with the second term, so one
+// exponential serves a pair; the divisions by the cutoff are precomputed.
+__device__ __forceinline__ void attenuation(float r2, float ir3, const WalkParams& P, float& att, float& cc) {
+  const float r2p = r2 + 1e-12f;
+  const float dist = r2p * rsqrtf(r2p);
+  const float u = dist * P.inv_2cut;
+  const float e = expf(-(u * u));
+  const float t = __fdividef(1.0f, fmaf(0.3275911f, u, 1.0f));
+  const float poly =
+      t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f), 0.254829592f);
+  att = e * fmaf(1.1283791671f, u, poly);  // 2 / sqrt(pi) = 1.1283791671
+  cc = ir3 * dist * e * P.cc_coef;
 }
 
 // One accepted node's monopole (with the erfc attenuation when CUT, minimum
@@ -705,7 +719,7 @@ __device__ __forceinline__ void far_mono_force(const float4& A, const LaneTarget
     float c = -A.w * ir3;
     if (CUT) {
       float att, cc;
-      attenuation(r2, ir3, P.cutoff, att, cc);
+      attenuation(r2, ir3, P, att, cc);
       c *= att;
     }
     fx[t] += c * rx;
@@ -826,7 +840,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
             float c = -s.w * ir3;
             if (CUT) {
               float att, cc;
-              attenuation(r2, ir3, P.cutoff, att, cc);
+              attenuation(r2, ir3, P, att, cc);
               c *= att;
             }
             ax[t] += c * rx;
@@ -962,7 +976,7 @@ __device__ __forceinline__ void far_mono_adjoint(const float4& A, const LaneTarg
     float ir5 = ir3 * ih;
     float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
     float att = 1.0f, cc = 0.0f;
-    if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
+    if (CUT) attenuation(r2, ir3, P, att, cc);
     float lin = att * ir3;
     float mlin = M * lin, mrad = M * (rw * (3.0f * att * ir5 + cc));
     v3 -= lin * rw;  // A_M
@@ -1157,7 +1171,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
             float ir5 = ir3 * ih;
             float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
             float att = 1.0f, cc = 0.0f;
-            if (CUT) attenuation(r2, ir3, P.cutoff, att, cc);
+            if (CUT) attenuation(r2, ir3, P, att, cc);
             float lin = att * ir3;
             float m = (selfchk && j == Q.idx[t]) ? 0.0f : s.w;
             float mlin = m * lin, mrad = m * (rw * (3.0f * att * ir5 + cc));
@@ -1675,7 +1689,7 @@ int sbh_native_build(cudaStream_t stream, const float* points, const float* mass
   roots_kernel<<<nseg, 32, 0, stream>>>(L.seg_off, nseg, L.base, L.cap, L.roots);
   if (n > 0)
     group_nodes_kernel<<<gs(static_cast<int64_t>(L.cap)), 256, 0, stream>>>(
-        L.nodes, L.meta, nseg > 1 ? L.sseg : nullptr, L.groups, n + nseg + 1, L.meta + 1, status);
+        L.nodes, L.meta, nseg > 1 ? L.sseg : nullptr, L.groups, n + nseg + 1, kGroup, L.meta + 1, status);
   if (int rc = check_launch("sbh_native_build")) return rc;
   return register_tree(workspace, h);
 }
@@ -1771,13 +1785,38 @@ WalkParams walk_params(const sbh_native_params* p) {
   float eps = fmaxf(p->softening, 0.0f);
   float box = p->periodic ? p->box_length : 1.0f;
   float qr = p->quadrupole_radius;
-  return WalkParams{p->beta, eps * eps + 1e-12f, p->cutoff, box, 1.0f / box, p->prune_radius * p->prune_radius,
-                    qr > 0.0f ? qr * qr : 0.0f};
+  double c = p->cutoff > 0.0f ? static_cast<double>(p->cutoff) : 1.0;
+  return WalkParams{p->beta,
+                    eps * eps + 1e-12f,
+                    p->cutoff,
+                    box,
+                    1.0f / box,
+                    p->prune_radius * p->prune_radius,
+                    qr > 0.0f ? qr * qr : 0.0f,
+                    static_cast<float>(0.5 / c),
+                    static_cast<float>(1.0 / (2.0 * 1.7724538509055160 * c * c * c))};
 }
 
 }  // namespace
 
 extern "C" {
+
+// Re-cuts the target groups of the tree in `workspace` with at most
+// group_size targets each (the build cuts groups of kGroup).
+int sbh_native_set_group_size(cudaStream_t stream, void* workspace, size_t workspace_bytes, int group_size) {
+  if (group_size < 1 || group_size > kGroup)
+    return invalid("group_size must be in [1, " + std::to_string(kGroup) + "]");
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (h.n == 0) return SBH_OK;
+  cudaError_t e = cudaMemsetAsync(L.meta + 1, 0, sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  group_nodes_kernel<<<gs(static_cast<int64_t>(L.cap)), 256, 0, stream>>>(
+      L.nodes, L.meta, h.nseg > 1 ? L.sseg : nullptr, L.groups, h.n + h.nseg + 1, group_size, L.meta + 1,
+      static_cast<uint32_t*>(workspace));
+  return check_launch("sbh_native_set_group_size");
+}
 
 int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float* force_out, void* workspace,
                      size_t workspace_bytes) {

@@ -140,6 +140,7 @@ _SIGS = {
     "sbh_native_winding_number": ([_c_p, _c_f, _c_p, _c_i64, _c_p, _c_p, _c_sz, _c_p, _c_sz], _c_i),
     "sbh_native_stats": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_quadrupole_count": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
+    "sbh_native_set_group_size": ([_c_p, _c_p, _c_sz, _c_i], _c_i),
     "sbh_mesh_sample_workspace_bytes": ([_c_i64], _c_sz),
     "sbh_sample_mesh_surface": ([_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_i64, _c_u64, _c_p, _c_p, _c_p, _c_p, _c_sz],
                                 _c_i),
@@ -832,7 +833,12 @@ class NativeTree:
         self.adjoint = False
 
     def build(self, points, masses, normals=None, system_offsets=None, *, leaf_size: int = 16,
-              with_adjoint: bool = True):
+              with_adjoint: bool = True, group_size: Optional[int] = None):
+        """Builds the tree (or forest) into this object's workspace.
+        group_size: most targets per walk group (default native_group_size();
+        32 suits walks bounded by a prune radius)."""
+        if group_size is not None and not 1 <= int(group_size) <= native_group_size():
+            raise ValueError(f"group_size must be in [1, {native_group_size()}]")
         dev = self.device
         points, masses = _f32(points, dev), _f32(masses, dev)
         if points.ndim != 2 or points.shape[1] != 3:
@@ -864,7 +870,14 @@ class NativeTree:
                "native_build")
         self.n, self.num_systems, self.leaf_size = n, nsys, int(leaf_size)
         self.normals, self.adjoint = nrm is not None, bool(with_adjoint)
+        if group_size is not None and int(group_size) != native_group_size():
+            self.set_group_size(int(group_size))
         return self
+
+    def set_group_size(self, group_size: int) -> None:
+        """Re-cuts the target groups with at most group_size targets each."""
+        _check(lib().sbh_native_set_group_size(_stream_ptr(self.device), _p(self.ws), self.ws.numel(),
+                                               int(group_size)), "native_set_group_size")
 
     @staticmethod
     def params(beta=2.0, softening=1e-3, cutoff=0.0, quadrupole=True, periodic=False, box_length=1.0,

@@ -354,6 +354,15 @@ typedef struct sbh_native_params {
 /* Most targets one group holds (one warp walks a group). */
 int sbh_native_group_size(void);
 
+/* Re-cuts the target groups of the tree built in `workspace` with at most
+ * group_size (1 .. sbh_native_group_size()) targets each; later walks use
+ * them. The build cuts groups of sbh_native_group_size(). Smaller groups have
+ * tighter boxes: fewer interactions per target where the walk is bounded by
+ * a prune radius (the TreePM short range), more per-node overhead per target
+ * elsewhere. */
+int sbh_native_set_group_size(cudaStream_t stream, void* workspace, size_t workspace_bytes,
+                              int group_size);
+
 /* Workspace for a tree of n points in num_systems independent systems. */
 size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int with_normals,
                                   int with_adjoint);

@@ -212,6 +212,42 @@ def test_native_periodic_short_range_matches_oracle(cuda):
     assert rel_l2(f2, want_f) < 1e-5
 
 
+@pytest.mark.parametrize("group_size", [32, 17])
+def test_native_smaller_groups_match_oracle(cuda, group_size):
+    """Groups re-cut with fewer targets (sbh_native_set_group_size): the same
+    groups and plan as the oracle's with that group size, the forces and the
+    adjoint within FP32 tolerance; on the periodic short-range walk and on the
+    plain softened walk."""
+    rng = np.random.default_rng(31)
+    p, m = W.uniform_cube(12000, seed=32)
+    w = rng.normal(size=p.shape).astype(np.float32)
+    t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True, group_size=group_size)
+    kw = dict(beta=2.0, softening=1e-3, cutoff=0.05, quadrupole=False, periodic=True, box_length=1.0,
+              prune_radius=0.2)
+    f, gx, gm = t.force_vjp(w, **kw)
+    st = t.stats()
+    T = O.NativeTree(p, m, leaf_size=16)
+    with O.native_periodic(1.0, 0.2):
+        inter = T.plan(2.0, group_size)
+        want_f, _ = T.force(1e-3, cutoff=0.05)
+        dx, dm = T.adjoint(w, 1e-3, cutoff=0.05)
+    assert st["groups"] == T.plan_stats()[0]
+    assert abs((st["far"] + st["near"]) - inter) <= 1e-4 * inter
+    assert rel_l2(f.cpu().numpy(), want_f) < 1e-5
+    assert rel_l2(gx.cpu().numpy(), dx) < 1e-4
+    assert rel_l2(gm.cpu().numpy(), dm) < 1e-4
+    # back to full groups on the same tree: the oracle's plan with full groups
+    t.set_group_size(B.native_group_size())
+    f64 = t.force(**kw).cpu().numpy()
+    assert t.stats()["groups"] < st["groups"]
+    with O.native_periodic(1.0, 0.2):
+        T.plan(2.0, B.native_group_size())
+        want64, _ = T.force(1e-3, cutoff=0.05)
+    assert rel_l2(f64, want64) < 1e-5
+    with pytest.raises(ValueError):
+        t.set_group_size(B.native_group_size() + 1)
+
+
 def test_native_periodic_direct_limit_and_shift_invariance(cuda):
     p, m = W.uniform_cube(6000, seed=23)
     kw = dict(beta=1e30, softening=2e-3, cutoff=0.1, quadrupole=False, periodic=True, box_length=1.0)
