@@ -1,7 +1,15 @@
 // Native adaptive Morton octree ("ntree"): build, group traversal for the
 // softened force with monopole + quadrupole far field, the full adjoint
 // (w.r.t. positions and masses), the winding number, and the batched forest
-// (many independent systems in one build and one launch).
+// (many independent systems in one build and one launch). The walks also
+// take a periodic box with minimum images, the erfc short-range cutoff and a
+// prune radius (the short range of TreePM), and a quadrupole radius beyond
+// which accepted nodes keep the monopole alone.
+//
+// Traversal: one warp per target group of at most 64 targets (two per
+// lane), cut from the tree so its box is compact; every opening decision is
+// taken on the group's box, so it is warp-uniform; warps take groups from an
+// atomic counter (persistent grid).
 //
 // Tree definition (the CPU oracle restates it; integer fields are pinned
 // bit-exactly):
