@@ -432,9 +432,10 @@ __global__ void __launch_bounds__(256)
     o8_bh_kernel(const Leaf3* __restrict__ leaf, const OctreeNode8* __restrict__ nodes,
                  const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq, float beta,
                  Soft s, int prune_on, float r_cut_sq, Periodic per, float* __restrict__ out,
-                 uint32_t* status, O8Bounds bd) {
-  int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (qi >= nq) return;
+                 uint32_t* status, O8Bounds bd, const uint32_t* __restrict__ order) {
+  int64_t ti = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (ti >= nq) return;
+  const int64_t qi = order ? static_cast<int64_t>(order[ti]) : ti;
   float qx = queries[3 * qi], qy = queries[3 * qi + 1], qz = queries[3 * qi + 2];
   float gx = 0.f, gy = 0.f, gz = 0.f;
   if (KERNEL == O8_SOFT_VJP || KERNEL == O8_GRAV_GRAD_VJP) {
@@ -510,9 +511,11 @@ __global__ void __launch_bounds__(256)
     o8_stochastic_kernel(const Leaf3* __restrict__ leaf, const OctreeNode8* __restrict__ nodes,
                          const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq,
                          int samples, int seed, float beta, Soft s, int prune_on, float r_cut_sq,
-                         Periodic per, float* __restrict__ out, uint32_t* status, O8Bounds bd) {
-  int64_t qi = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (qi >= nq) return;
+                         Periodic per, float* __restrict__ out, uint32_t* status, O8Bounds bd,
+                         const uint32_t* __restrict__ order) {
+  int64_t ti = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (ti >= nq) return;
+  const int64_t qi = order ? static_cast<int64_t>(order[ti]) : ti;
   float qx = queries[3 * qi], qy = queries[3 * qi + 1], qz = queries[3 * qi + 2];
   float gx = 0.f, gy = 0.f, gz = 0.f;
   if (KERNEL == O8_SOFT_VJP || KERNEL == O8_GRAV_GRAD_VJP) {
@@ -692,6 +695,66 @@ static void o8_carve(C& c, int64_t n, int depth, O8Params** prm, uint32_t** k0, 
 
 using namespace sbh;
 
+// Query order of the per-query octree8 traversals. Each query walks the
+// tree on its own (the deterministic kernels) or with curand streams seeded
+// by its own index (the stochastic ones), so the order in which threads take
+// queries changes no result; it only decides which queries share a warp.
+// With a large enough workspace the queries are sorted by the 30-bit Morton
+// code of their position in the root cell, so a warp's threads walk nearby
+// paths and the per-thread traversal diverges far less than for queries in
+// random order.
+constexpr int64_t kOrderMinQueries = 4096;
+
+template <typename C>
+static void order_carve(C& c, int64_t nq, uint32_t** k0, uint32_t** v0, uint32_t** k1, uint32_t** v1,
+                        uint32_t** hist, uint32_t** tmp) {
+  *k0 = c.template take<uint32_t>(static_cast<size_t>(nq));
+  *v0 = c.template take<uint32_t>(static_cast<size_t>(nq));
+  *k1 = c.template take<uint32_t>(static_cast<size_t>(nq));
+  *v1 = c.template take<uint32_t>(static_cast<size_t>(nq));
+  int64_t h = radix_hist_elems(nq);
+  *hist = c.template take<uint32_t>(static_cast<size_t>(h));
+  *tmp = c.template take<uint32_t>(static_cast<size_t>(scan_tiles<uint32_t>(h)));
+}
+
+// 10 bits per axis of the query's position in the root cell (clamped; NaN
+// goes to 0), interleaved x, y, z from bit 0.
+__global__ void o8_query_codes_kernel(const OctreeNode8* __restrict__ nodes, const float* __restrict__ q,
+                                      int64_t nq, uint32_t* __restrict__ codes) {
+  const float h = nodes[0].half_size;
+  const float lo[3] = {nodes[0].cx - h, nodes[0].cy - h, nodes[0].cz - h};
+  const float scale = h > 0.0f ? 512.0f / h : 0.0f;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nq;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t c = 0;
+    for (int d = 0; d < 3; d++) {
+      float t = (q[3 * i + d] - lo[d]) * scale;
+      uint32_t v = t > 0.0f ? (t < 1023.0f ? static_cast<uint32_t>(t) : 1023u) : 0u;
+      for (int b = 0; b < 10; b++) c |= ((v >> b) & 1u) << (3 * b + d);
+    }
+    codes[i] = c;
+  }
+}
+
+// The sorted query order, or null (input order) when nq is small or the
+// workspace has no room for the sort.
+static const uint32_t* o8_query_order(cudaStream_t stream, const OctreeNode8* nodes, const float* queries,
+                                      int64_t nq, void* workspace, size_t workspace_bytes, int* rc) {
+  *rc = SBH_OK;
+  if (nq < kOrderMinQueries || workspace_bytes < sbh_traversal_ordered_workspace_bytes(nq)) return nullptr;
+  Carver c(workspace, workspace_bytes);
+  uint32_t *k0, *v0, *k1, *v1, *hist, *tmp;
+  order_carve(c, nq, &k0, &v0, &k1, &v1, &hist, &tmp);
+  o8_query_codes_kernel<<<grid_stride(nq, 256), 256, 0, stream>>>(nodes, queries, nq, k0);
+  int which = 0;
+  cudaError_t e = radix_sort<uint32_t>(stream, k0, v0, k1, v1, nq, 30, false, hist, tmp, &which);
+  if (e != cudaSuccess) {
+    *rc = fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    return nullptr;
+  }
+  return which == 0 ? v0 : v1;
+}
+
 extern "C" {
 
 int sbh_bruteforce_gravity(cudaStream_t stream, const float* points, const float* masses, int64_t n, int dim,
@@ -806,22 +869,26 @@ static int o8_launch_bh(int kernel, cudaStream_t stream, const void* leaf, size_
   const Leaf3* L = static_cast<const Leaf3*>(leaf);
   const OctreeNode8* N = static_cast<const OctreeNode8*>(nodes);
   O8Bounds bd{static_cast<uint32_t>(node_bytes / sizeof(OctreeNode8)), static_cast<uint32_t>(leaf_bytes / sizeof(Leaf3))};
+  int orc = SBH_OK;
+  const uint32_t* order = o8_query_order(stream, N, queries, nq, workspace, workspace_bytes, &orc);
+  if (orc != SBH_OK) return orc;
   unsigned g = grid_for(nq, 256);
   switch (kernel) {
     case O8_GRAV_GRAD:
-      o8_bh_kernel<O8_GRAV_GRAD><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out, status, bd);
+      o8_bh_kernel<O8_GRAV_GRAD><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out, status, bd,
+                                                        order);
       break;
     case O8_SOFT:
       o8_bh_kernel<O8_SOFT><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per, out,
-                                                   status, bd);
+                                                   status, bd, order);
       break;
     case O8_GRAV_GRAD_VJP:
       o8_bh_kernel<O8_GRAV_GRAD_VJP><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out, status,
-                                                            bd);
+                                                            bd, order);
       break;
     default:
       o8_bh_kernel<O8_SOFT_VJP><<<g, 256, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per,
-                                                       out, status, bd);
+                                                       out, status, bd, order);
       break;
   }
   return check_launch("barnes_hut_force_octree8");
@@ -908,24 +975,37 @@ static int o8_launch_stochastic(bool vjp, int softened, cudaStream_t stream, con
   const OctreeNode8* N = static_cast<const OctreeNode8*>(nodes);
   O8Bounds bd{static_cast<uint32_t>(node_bytes / sizeof(OctreeNode8)), static_cast<uint32_t>(leaf_bytes / sizeof(Leaf3))};
   // The reference's kernel reads a curand state per query, independent of
-  // the block size, so any launch shape gives the same numbers.
+  // the block size and of which thread takes the query, so any launch shape
+  // and query order give the same numbers.
+  int orc = SBH_OK;
+  const uint32_t* order = o8_query_order(stream, N, queries, nq, workspace, workspace_bytes, &orc);
+  if (orc != SBH_OK) return orc;
   unsigned g = grid_for(nq, 128);
   if (!vjp) {
     if (softened)
       o8_stochastic_kernel<O8_SOFT, true><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed, beta, s, on,
-                                                                 rsq, per, out, status, bd);
+                                                                 rsq, per, out, status, bd, order);
     else
       o8_stochastic_kernel<O8_GRAV_GRAD, false><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed, beta,
-                                                                       s, 0, 0.f, per, out, status, bd);
+                                                                       s, 0, 0.f, per, out, status, bd, order);
   } else {
     if (softened)
       o8_stochastic_kernel<O8_SOFT_VJP, true><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed, beta, s,
-                                                                     on, rsq, per, out, status, bd);
+                                                                     on, rsq, per, out, status, bd, order);
     else
       o8_stochastic_kernel<O8_GRAV_GRAD_VJP, false><<<g, 128, 0, stream>>>(L, N, queries, cot, nq, samples, seed,
-                                                                           beta, s, 0, 0.f, per, out, status, bd);
+                                                                           beta, s, 0, 0.f, per, out, status, bd,
+                                                                           order);
   }
   return check_launch("stochastic_bh_force_octree8");
+}
+
+size_t sbh_traversal_ordered_workspace_bytes(int64_t nq) {
+  if (nq < 0) return 0;
+  Sizer z;
+  uint32_t *k0, *v0, *k1, *v1, *hist, *tmp;
+  order_carve(z, nq, &k0, &v0, &k1, &v1, &hist, &tmp);
+  return z.off;
 }
 
 int sbh_stochastic_bh_force_octree8(cudaStream_t stream, int softened, const void* leaf, size_t leaf_bytes,

@@ -86,6 +86,7 @@ _SIGS = {
     "sbh_node2_size": ([], _c_sz),
     "sbh_octree8_total_nodes": ([_c_i], _c_u64),
     "sbh_traversal_workspace_bytes": ([], _c_sz),
+    "sbh_traversal_ordered_workspace_bytes": ([_c_i64], _c_sz),
     "sbh_bruteforce_gravity": ([_c_p, _c_p, _c_p, _c_i64, _c_i, _c_p, _c_i64, _c_p, _c_i, _c_f, _c_i], _c_i),
     "sbh_direct_force_soft": ([_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_f, _c_f, _c_i, _c_f, _c_i], _c_i),
     "sbh_direct_force_soft_vjp": ([_c_p, _c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_f, _c_i, _c_f, _c_i],
@@ -461,13 +462,19 @@ def _status_after(ws, what, check_status):
             raise SbhError(f"{what}: device traversal limit reached (status 0x{st:x})")
 
 
+def _octree8_ws_bytes(nq: int) -> int:
+    """Workspace with room to take the queries in Morton order (the results
+    do not depend on the order; the per-thread traversal diverges less)."""
+    return int(lib().sbh_traversal_ordered_workspace_bytes(int(nq)))
+
+
 def barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: float = 2.0, periodic: bool = False,
                              box_length: float = 1.0, threads: int = 256, check_status: bool = False):
     dev = _device()
     leaf, node, queries = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
     _check_traversal(queries, periodic, box_length, threads)
     out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
-    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    ws = workspace(_octree8_ws_bytes(queries.shape[0]), dev)
     _check(lib().sbh_barnes_hut_force_octree8(_stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(),
                                               _p(queries), queries.shape[0], _p(out), float(beta), int(bool(periodic)),
                                               float(box_length), int(threads), _p(ws), ws.numel()),
@@ -489,7 +496,7 @@ def barnes_hut_force_octree8_vjp(leaf_bytes, node_bytes, queries, cotangent, *, 
     if cot.shape != queries.shape:
         raise ValueError("cotangent must have same shape as queries")
     out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
-    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    ws = workspace(_octree8_ws_bytes(queries.shape[0]), dev)
     _check(lib().sbh_barnes_hut_force_octree8_vjp(_stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(),
                                                   _p(queries), queries.shape[0], _p(cot), _p(out), float(beta),
                                                   int(bool(periodic)), float(box_length), int(threads), _p(ws),
@@ -510,7 +517,7 @@ def softened_barnes_hut_force_octree8(leaf_bytes, node_bytes, queries, *, beta: 
     if prune_enabled and prune_r_cut_mult <= 0:
         raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
     out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
-    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    ws = workspace(_octree8_ws_bytes(queries.shape[0]), dev)
     _check(lib().sbh_barnes_hut_force_octree8_soft(
         _stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(), _p(queries), queries.shape[0], _p(out),
         float(beta), float(softening_scale), float(cutoff_scale), int(bool(prune_enabled)), float(prune_r_cut_mult),
@@ -534,7 +541,7 @@ def softened_barnes_hut_force_octree8_vjp(leaf_bytes, node_bytes, queries, cotan
     if prune_enabled and prune_r_cut_mult <= 0:
         raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
     out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
-    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    ws = workspace(_octree8_ws_bytes(queries.shape[0]), dev)
     _check(lib().sbh_barnes_hut_force_octree8_soft_vjp(
         _stream_ptr(dev), _p(leaf), leaf.numel(), _p(node), node.numel(), _p(queries), queries.shape[0],
         _p(cotangent), _p(out), float(beta), float(softening_scale), float(cutoff_scale), int(bool(prune_enabled)),
@@ -555,7 +562,7 @@ def _stochastic_octree8(vjp, softened, leaf_bytes, node_bytes, queries, cotangen
         if prune_enabled and prune_r_cut_mult <= 0:
             raise ValueError("prune_r_cut_mult must be > 0 when prune_enabled=True")
     out = torch.empty((queries.shape[0], 3), dtype=torch.float32, device=dev)
-    ws = workspace(int(lib().sbh_traversal_workspace_bytes()), dev)
+    ws = workspace(_octree8_ws_bytes(queries.shape[0]), dev)
     common = (float(beta), float(softening_scale), float(cutoff_scale), int(bool(prune_enabled)),
               float(prune_r_cut_mult), int(bool(periodic)), float(box_length), int(threads), _p(ws), ws.numel())
     if vjp:

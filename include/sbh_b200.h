@@ -206,6 +206,14 @@ int sbh_probe_fp32(cudaStream_t stream, float* out, int blocks, int iters);
  * (the device status word). */
 size_t sbh_traversal_workspace_bytes(void);
 
+/* Workspace with which the per-query octree8 traversals (classic, softened,
+ * their VJPs and the stochastic ones) of nq queries take the queries in
+ * Morton order of their positions: a warp's threads then walk nearby paths.
+ * Every query's result is the same in either order (each query is
+ * traversed on its own, its curand streams seeded by its own index); with a
+ * smaller workspace, or below 4,096 queries, they run in input order. */
+size_t sbh_traversal_ordered_workspace_bytes(int64_t nq);
+
 /* ---------------------------------------------------------------------- */
 /* Level-3 tree (Tree3DNode<1,3> layout) and Node2 / Node3 traversals     */
 /* ---------------------------------------------------------------------- */

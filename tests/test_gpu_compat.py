@@ -388,3 +388,48 @@ def test_octree8_large_build_and_force_sanity(cuda):
                                               check_status=True).cpu().numpy()
     want = O.direct_force_soft(p, m, q, 1e-3, 1e6)
     assert rel_l2(got, want) < 5e-3  # octree8's geometric-centre criterion (reference README: ~1e-2)
+
+
+def test_octree8_query_order_changes_no_result(cuda):
+    """With the ordered workspace the per-query octree8 traversals take the
+    queries in Morton order; every output row must equal the input-order
+    run bit for bit (classic, softened with prune, both VJPs, stochastic and
+    its VJP)."""
+    p, m = W.plummer(30000, seed=41)
+    nrm = np.zeros_like(p)
+    leaf, node = B.build_octree8_buffers(p, nrm, m, p.min(0) - 1e-3, p.max(0) + 1e-3, max_depth=6)
+    rng = np.random.default_rng(42)
+    q = p[rng.permutation(p.shape[0])[:20000]]
+    cot = rng.normal(size=q.shape).astype(np.float32)
+    Q, C = torch.tensor(q, device=cuda), torch.tensor(cot, device=cuda)
+    nq = q.shape[0]
+    L = B.lib()
+    big = torch.empty(int(L.sbh_traversal_ordered_workspace_bytes(nq)), dtype=torch.uint8, device=cuda)
+    small = torch.empty(int(L.sbh_traversal_workspace_bytes()), dtype=torch.uint8, device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    lp, lb, np_, nb = leaf.data_ptr(), leaf.numel(), node.data_ptr(), node.numel()
+
+    def both(call):
+        outs = []
+        for ws in (big, small):
+            out = torch.full((nq, 3), float("nan"), device=cuda)
+            assert call(out.data_ptr(), ws.data_ptr(), ws.numel()) == 0, B.last_error()
+            outs.append(out)
+        torch.cuda.synchronize()
+        assert torch.equal(outs[0], outs[1])
+        return outs[0]
+
+    both(lambda o, w, wb: L.sbh_barnes_hut_force_octree8(s, lp, lb, np_, nb, Q.data_ptr(), nq, o, 2.0, 0, 1.0, 256,
+                                                         w, wb))
+    both(lambda o, w, wb: L.sbh_barnes_hut_force_octree8_vjp(s, lp, lb, np_, nb, Q.data_ptr(), nq, C.data_ptr(), o,
+                                                             2.0, 0, 1.0, 256, w, wb))
+    both(lambda o, w, wb: L.sbh_barnes_hut_force_octree8_soft(s, lp, lb, np_, nb, Q.data_ptr(), nq, o, 2.0, 1e-2, 0.5,
+                                                              1, 4.0, 0, 1.0, 256, w, wb))
+    both(lambda o, w, wb: L.sbh_barnes_hut_force_octree8_soft_vjp(s, lp, lb, np_, nb, Q.data_ptr(), nq, C.data_ptr(),
+                                                                  o, 2.0, 1e-2, 0.5, 1, 4.0, 0, 1.0, 256, w, wb))
+    for soft in (0, 1):
+        both(lambda o, w, wb: L.sbh_stochastic_bh_force_octree8(s, soft, lp, lb, np_, nb, Q.data_ptr(), nq, o, 2, 7,
+                                                                2.0, 1e-2, 0.5, 1, 4.0, 0, 1.0, 256, w, wb))
+        both(lambda o, w, wb: L.sbh_stochastic_bh_force_octree8_vjp(s, soft, lp, lb, np_, nb, Q.data_ptr(), nq,
+                                                                    C.data_ptr(), o, 2, 7, 2.0, 1e-2, 0.5, 1, 4.0, 0,
+                                                                    1.0, 256, w, wb))
