@@ -155,6 +155,14 @@ struct Soft {
   float cutoff;  // <= 0 disables the erfc attenuation
 };
 
+// Below this u = r / (2 cutoff) the attenuation erfc(u) + (2/sqrt(pi)) u
+// e^{-u^2} = 1 - (4 / (3 sqrt(pi))) u^3 + O(u^5) is within 6e-9 of 1, under
+// half an FP32 ulp of 1, so it is taken as 1 without evaluating erfc and exp.
+// The reference's "Plummer softening, no cutoff" convention passes a cutoff
+// of 1e6 box lengths (python/unified_force_benchmark.py:364-374), which
+// puts every pair here.
+constexpr float kAttUnityU = 1.0f / 512.0f;
+
 // coefficient c with f = c * r for the softened force; r = q - p.
 __device__ __forceinline__ float soft_coeff(float r2, float mass, const Soft& s) {
   float inv_r = rsqrtf(r2 + s.eps * s.eps + 1e-12f);
@@ -163,8 +171,10 @@ __device__ __forceinline__ float soft_coeff(float r2, float mass, const Soft& s)
   if (s.cutoff > 0.0f) {
     float dist = sqrtf(r2 + 1e-12f);
     float u = dist / (2.0f * s.cutoff);
-    float e = expf(-(u * u));
-    att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+    if (u >= kAttUnityU) {
+      float e = expf(-(u * u));
+      att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+    }
   }
   return -mass * att * inv_r3;
 }
@@ -182,8 +192,12 @@ __device__ __forceinline__ void soft_vjp_accum(float rx, float ry, float rz, flo
   if (s.cutoff > 0.0f) {
     float dist = sqrtf(r2 + 1e-12f);
     float u = dist / (2.0f * s.cutoff);
-    float e = expf(-(u * u));
-    att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+    // below kAttUnityU: att = 1 and e^{-u^2} = 1 to FP32 precision
+    float e = 1.0f;
+    if (u >= kAttUnityU) {
+      e = expf(-(u * u));
+      att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+    }
     cc = inv_r3 * dist * e / (2.0f * 1.772453850905516f * s.cutoff * s.cutoff * s.cutoff);
   }
   float rg = rx * gx + ry * gy + rz * gz;

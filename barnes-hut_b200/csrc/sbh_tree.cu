@@ -345,8 +345,11 @@ __device__ __forceinline__ void tree_kernel(const LeafT<N>& d, const Vec<N>& q, 
     if (s.cutoff > 0.0f) {
       float dist = sqrtf(r2 + 1e-12f);
       float u = dist / (2.0f * s.cutoff);
-      float e = expf(-(u * u));
-      att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+      float e = 1.0f;  // att = 1, e^{-u^2} = 1 to FP32 precision below kAttUnityU
+      if (u >= kAttUnityU) {
+        e = expf(-(u * u));
+        att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+      }
       cc = ir3 * dist * e / (2.0f * 1.772453850905516f * s.cutoff * s.cutoff * s.cutoff);
     }
     float rg = 0.f;
