@@ -33,6 +33,7 @@
 // oracle reproduces them bit for bit; the pair kernels use rsqrtf.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -520,6 +521,7 @@ struct WalkTargets {
   int self;                  // targets are the sources (skip i == j pairs)
   uint32_t* counter;         // work counter, zero at launch
   uint32_t capacity;         // entries of groups (bounds the device-side count)
+  int64_t tbeg, tend;        // groups whose first sorted target lies outside [tbeg, tend) are skipped
 };
 
 // Persistent walks: the grid holds as many warps as the SMs keep resident,
@@ -780,6 +782,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     uint32_t gw = next_group(G);
     if (gw >= ng) break;
     int4 gr = G.groups[gw];
+    if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
     const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
@@ -1115,6 +1118,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     uint32_t gw = next_group(G);
     if (gw >= ng) break;
     int4 gr = G.groups[gw];
+    if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
     const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
@@ -1318,6 +1322,7 @@ __global__ void __launch_bounds__(128, 4)
     uint32_t gw = next_group(G);
     if (gw >= ng) break;
     int4 gr = G.groups[gw];
+    if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
     const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
@@ -1557,6 +1562,7 @@ struct Header {
   int32_t leaf_size;
   int32_t normals;
   int32_t adjoint;
+  int64_t tbeg = 0, tend = INT64_MAX;  // sorted target range the walks serve
 };
 constexpr uint64_t kMagic = 0x5342483230304e54ull;  // "SBH200NT"
 
@@ -1728,9 +1734,12 @@ __global__ void zero_node_adj_kernel(float* adj, const uint32_t* meta) {
 
 WalkTree tree_view(const Layout& L) { return WalkTree{L.nodes, L.sp, L.sn, L.nnrm, L.roots}; }
 
-WalkTargets self_targets(const Layout& L, int64_t n, int nseg) {
-  return WalkTargets{L.sp, L.v0, L.groups, L.meta + 1, 1, L.work, static_cast<uint32_t>(n + nseg + 1)};
+WalkTargets self_targets(const Layout& L, const Header& h) {
+  return WalkTargets{L.sp,      L.v0, L.groups, L.meta + 1, 1, L.work, static_cast<uint32_t>(h.n + h.nseg + 1),
+                     h.tbeg, h.tend};
 }
+
+bool partial_range(const Header& h) { return h.tbeg > 0 || h.tend < h.n; }
 
 // Blocks of a persistent walk: resident blocks per SM x SMs, and no more
 // than one warp per possible group. Occupancy is queried per kernel and
@@ -1826,6 +1835,27 @@ int sbh_native_set_group_size(cudaStream_t stream, void* workspace, size_t works
   return check_launch("sbh_native_set_group_size");
 }
 
+// Restricts the force and adjoint walks on the tree in `workspace` to the
+// target groups whose first target lies at sorted positions [begin, end).
+// Ranks holding the same tree and a partition of [0, n) into such ranges
+// serve every target exactly once; each rank's forces are zero outside its
+// targets and its gradients are partial sums, so summing the ranks' outputs
+// gives the full force and gradient. A new build resets the range to [0, n).
+int sbh_native_set_target_range(cudaStream_t stream, void* workspace, size_t workspace_bytes, int64_t begin,
+                                int64_t end) {
+  (void)stream;  // host-side state only
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (begin < 0 || end < begin || end > h.n) return invalid("target range must satisfy 0 <= begin <= end <= n");
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  auto it = g_registry.find(workspace);
+  if (it == g_registry.end()) return invalid("workspace holds no native tree; call sbh_native_build first");
+  it->second.tbeg = begin;
+  it->second.tend = end;
+  return SBH_OK;
+}
+
 int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float* force_out, void* workspace,
                      size_t workspace_bytes) {
   if (int rc = check_params(params)) return rc;
@@ -1835,6 +1865,8 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   if (h.n == 0) return SBH_OK;
   if (!force_out) return invalid("force_out must be non-null");
   cudaError_t e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
+  // with a partial target range the other targets' rows are zero (ranks sum their outputs)
+  if (e == cudaSuccess && partial_range(h)) e = cudaMemsetAsync(force_out, 0, h.n * 3 * sizeof(float), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   WalkParams wp = walk_params(params);
   int64_t mg = h.n + h.nseg;
@@ -1843,7 +1875,7 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   auto k = params->quadrupole ? force_walk_kernel<true, false, false>
            : per ? (cut ? force_walk_kernel<false, true, true> : force_walk_kernel<false, false, true>)
                  : (cut ? force_walk_kernel<false, true, false> : force_walk_kernel<false, false, false>);
-  e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h.n, h.nseg), wp, force_out, L.counters);
+  e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h), wp, force_out, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_force");
 }
@@ -1860,6 +1892,11 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   int64_t n = h.n;
   cudaError_t e = cudaMemsetAsync(L.part_adj, 0, n * kPartAdj * sizeof(float), stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
+  // with a partial target range the query-side gradient (added for every particle by the
+  // finalize) and the force rows of the other targets are zero
+  if (e == cudaSuccess && partial_range(h)) e = cudaMemsetAsync(L.gq, 0, n * 3 * sizeof(float), stream);
+  if (e == cudaSuccess && partial_range(h) && force_out)
+    e = cudaMemsetAsync(force_out, 0, n * 3 * sizeof(float), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
   WalkParams wp = walk_params(params);
@@ -1868,7 +1905,7 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   auto k = params->quadrupole ? adjoint_walk_kernel<true, false, false>
            : per ? (cut ? adjoint_walk_kernel<false, true, true> : adjoint_walk_kernel<false, false, true>)
                  : (cut ? adjoint_walk_kernel<false, true, false> : adjoint_walk_kernel<false, false, false>);
-  e = launch_walk(stream, L.work, n + h.nseg, k, tree_view(L), self_targets(L, h.n, h.nseg), wp, cotangent, force_out, L.gq,
+  e = launch_walk(stream, L.work, n + h.nseg, k, tree_view(L), self_targets(L, h), wp, cotangent, force_out, L.gq,
                   L.node_adj, L.part_adj, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_adjoint_walk");
@@ -1955,7 +1992,7 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
   e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1)};
+  WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1), 0, INT64_MAX};
   e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   return check_launch("sbh_native_winding_number");

@@ -142,6 +142,7 @@ _SIGS = {
     "sbh_native_stats": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_quadrupole_count": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_set_group_size": ([_c_p, _c_p, _c_sz, _c_i], _c_i),
+    "sbh_native_set_target_range": ([_c_p, _c_p, _c_sz, _c_i64, _c_i64], _c_i),
     "sbh_mesh_sample_workspace_bytes": ([_c_i64], _c_sz),
     "sbh_sample_mesh_surface": ([_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_i64, _c_u64, _c_p, _c_p, _c_p, _c_p, _c_sz],
                                 _c_i),
@@ -880,6 +881,13 @@ class NativeTree:
         if group_size is not None and int(group_size) != native_group_size():
             self.set_group_size(int(group_size))
         return self
+
+    def set_target_range(self, begin: int, end: int) -> None:
+        """Walk only the target groups starting at sorted positions
+        [begin, end); other targets' force rows are zero and the gradients
+        are this share's partial sums (sbh_native_set_target_range)."""
+        _check(lib().sbh_native_set_target_range(_stream_ptr(self.device), _p(self.ws), self.ws.numel(),
+                                                 int(begin), int(end)), "native_set_target_range")
 
     def set_group_size(self, group_size: int) -> None:
         """Re-cuts the target groups with at most group_size targets each."""

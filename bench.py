@@ -496,6 +496,52 @@ def treepm_measurement(B, torch, dev, flush):
                 speedup_vs_reference_algorithm=ref_ms / ours_ms)
 
 
+def sharded_measurement(B, torch, dev, rank, world, n):
+    """Strong scaling of one system (runs when world > 1): n Plummer
+    particles split by target across the ranks (sbh_dist.sharded_force_vjp).
+    Every rank builds the same tree, walks its share of the target groups,
+    and one all-reduce of forces and gradients (n x 28 bytes) completes the
+    result on every rank. Timed per evaluation (build + walk + finalize +
+    all-reduce, max over ranks) beside the same evaluation on one rank."""
+    import sbh_dist
+
+    p, m = W.plummer(n, seed=999)
+    w = np.random.default_rng(998).normal(size=p.shape).astype(np.float32)
+    P, M, Wt = (torch.tensor(a, device=dev) for a in (p, m, w))
+    tree = B.NativeTree(dev)
+
+    def sharded():
+        tree.build(P, M, leaf_size=LEAF, with_adjoint=True)
+        return sbh_dist.sharded_force_vjp(tree, Wt, beta=BETA, softening=EPS)
+
+    def single():
+        tree.build(P, M, leaf_size=LEAF, with_adjoint=True)
+        return tree.force_vjp(Wt, beta=BETA, softening=EPS)
+
+    def timed(fn, reps):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    for _ in range(2):
+        sharded()
+    single()
+    sh_ms = sbh_dist.max_over_ranks(timed(sharded, 5), dev)
+    one_ms = timed(single, 3)
+    f, gx, _ = sharded()
+    f1, gx1, _ = single()
+    torch.cuda.synchronize()
+    rel_f = sbh_dist.max_over_ranks(float(torch.linalg.norm(f - f1) / torch.linalg.norm(f1)), dev)
+    rel_g = sbh_dist.max_over_ranks(float(torch.linalg.norm(gx - gx1) / torch.linalg.norm(gx1)), dev)
+    return dict(particles=n, ranks=world, sharded_ms=sh_ms, single_rank_ms=one_ms, speedup=one_ms / sh_ms,
+                allreduce_bytes=int(n * 28), rel_force_vs_single=rel_f, rel_grad_vs_single=rel_g)
+
+
 def measure_fp32_peak(B, torch, dev):
     buf = torch.zeros(1024, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
@@ -723,6 +769,8 @@ def run_ours(args):
         if world == 1:
             extras["octree8_plain"] = octree8_plain_measurement(B, torch, P0, M0, W0, idx, ref, flush)
         extras["forest"] = forest_measurement(B, torch, dev, rank, world, flush)
+        if world > 1:
+            extras["sharded_single_system"] = sharded_measurement(B, torch, dev, rank, world, n)
         if world == 1:
             extras["winding_number"] = winding_measurement(B, torch, dev, flush)
             extras["winding_number_mesh"] = winding_mesh_measurement(B, torch, dev, flush)

@@ -371,6 +371,16 @@ int sbh_native_group_size(void);
 int sbh_native_set_group_size(cudaStream_t stream, void* workspace, size_t workspace_bytes,
                               int group_size);
 
+/* Restricts the force and adjoint walks on the tree in `workspace` to the
+ * target groups whose first target lies at sorted positions [begin, end)
+ * (0 <= begin <= end <= n). Ranks holding the same tree and a partition of
+ * [0, n) serve every target exactly once: each rank's force rows are zero
+ * outside its targets and its gradients are partial sums, so the sum over
+ * ranks (an all-reduce of N x 16 bytes) is the full result. Host-side state;
+ * a new build resets the range to [0, n). */
+int sbh_native_set_target_range(cudaStream_t stream, void* workspace, size_t workspace_bytes,
+                                int64_t begin, int64_t end);
+
 /* Workspace for a tree of n points in num_systems independent systems. */
 size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int with_normals,
                                   int with_adjoint);

@@ -269,3 +269,41 @@ def test_native_periodic_invalid_params(cuda):
         t.force(periodic=True, box_length=1.0, quadrupole=True)
     with pytest.raises(ValueError):
         t.force(cutoff=0.0, prune_radius=0.3, quadrupole=False)
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_native_target_ranges_sum_to_full(cuda, world):
+    """Ranks emulated one after another on one GPU (no collective): each
+    walks its share of the sorted targets (sbh_native_set_target_range); the
+    shares' forces are disjoint and their sum, like the sum of the partial
+    gradients, equals the unsharded result."""
+    import sbh_dist
+
+    rng = np.random.default_rng(51)
+    systems = [W.plummer(n, seed=52 + i) for i, n in enumerate((15000, 4000))]
+    p = np.concatenate([s[0] + np.float32(40.0 * i) for i, s in enumerate(systems)])
+    m = np.concatenate([s[1] for s in systems])
+    offs = np.array([0, 15000, 19000], np.int64)
+    w = rng.normal(size=p.shape).astype(np.float32)
+    t = B.NativeTree().build(p, m, system_offsets=offs, leaf_size=16, with_adjoint=True)
+    f_all, gx_all, gm_all = t.force_vjp(w, beta=2.0, softening=1e-3)
+    f_all, gx_all, gm_all = f_all.cpu().numpy(), gx_all.cpu().numpy(), gm_all.cpu().numpy()
+    fs, gxs, gms, nonzero = 0, 0, 0, np.zeros(p.shape[0], np.int64)
+    for r in range(world):
+        t.set_target_range(*sbh_dist.shard_targets(t.n, world, r))
+        f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3)
+        f = f.cpu().numpy()
+        nonzero += np.any(f != 0, axis=1)
+        fs, gxs, gms = fs + f, gxs + gx.cpu().numpy(), gms + gm.cpu().numpy()
+        ff = t.force(beta=2.0, softening=1e-3).cpu().numpy()
+        np.testing.assert_array_equal(ff != 0, f != 0)
+    t.set_target_range(0, t.n)
+    assert (nonzero == 1).all()  # every target served by exactly one share
+    assert rel_l2(fs, f_all) < 1e-6
+    assert rel_l2(gxs, gx_all) < 1e-5
+    assert rel_l2(gms, gm_all) < 1e-5
+    with pytest.raises(ValueError):
+        t.set_target_range(5, 4)
+    with pytest.raises(ValueError):
+        t.set_target_range(0, t.n + 1)
+
