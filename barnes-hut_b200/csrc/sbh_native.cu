@@ -774,8 +774,7 @@ __device__ __forceinline__ void far_quad_force(const NodeRec* nd, const float4& 
 
 template <bool QUAD, bool CUT, bool PER>
 __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
-    force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out,
-                      unsigned long long* __restrict__ counters) {
+    force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out) {
   const int lane = threadIdx.x & 31;
   const uint32_t ng = min(*G.ngroups, G.capacity);
   for (;;) {
@@ -793,7 +792,6 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     float nx[kTPL], ny[kTPL], nz[kTPL], cx[kTPL], cy[kTPL], cz[kTPL];       // near field, compensated
 #pragma unroll
     for (int t = 0; t < kTPL; t++) fx[t] = fy[t] = fz[t] = nx[t] = ny[t] = nz[t] = cx[t] = cy[t] = cz[t] = 0.f;
-    uint32_t nfar = 0, nnear = 0, nquad = 0;  // per group (a group's counts stay below n)
     // Pre-order walk. The next node is known once this node's opening test
     // is done, so its opening data is loaded before this node's terms are
     // evaluated and the load latency hides behind that arithmetic.
@@ -828,8 +826,6 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
         } else {
           far_mono_force<CUT, PER>(A, Q, two, P, fx, fy, fz);
         }
-        nfar++;
-        nquad += qh;
       } else if (live && leaf) {
         float ax[kTPL], ay[kTPL], az[kTPL];
 #pragma unroll
@@ -865,7 +861,6 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
           kahan_add(ny[t], cy[t], ay[t]);
           kahan_add(nz[t], cz[t], az[t]);
         }
-        nnear += static_cast<uint32_t>(tp.y - tp.x);
       }
       k = next;
       tp = tpn;
@@ -880,12 +875,6 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
         out[3 * o + 1] = fy[t] + ny[t];
         out[3 * o + 2] = fz[t] + nz[t];
       }
-    }
-    if (counters && lane == 0) {
-      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
-      atomicAdd(&counters[0], nfar * na);
-      atomicAdd(&counters[1], nnear * na);
-      atomicAdd(&counters[2], nquad * na);
     }
   }
 }
@@ -1110,7 +1099,7 @@ template <bool QUAD, bool CUT, bool PER>
 __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
                         float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
-                        float* __restrict__ part_adj, unsigned long long* __restrict__ counters) {
+                        float* __restrict__ part_adj) {
   const int lane = threadIdx.x & 31;
   const uint32_t ng = min(*G.ngroups, G.capacity);
   const int r4 = reduce4_index(lane), r10 = reduce10_index(lane);
@@ -1137,7 +1126,6 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     float fx[kTPL], fy[kTPL], fz[kTPL];  // force
 #pragma unroll
     for (int t = 0; t < kTPL; t++) gx[t] = gy[t] = gz[t] = fx[t] = fy[t] = fz[t] = 0.f;
-    uint32_t nfar = 0, nnear = 0, nquad = 0;  // per group (a group's counts stay below n)
     int k = rt.x;
     while (k < rt.y) {
       const NodeRec* nd = T.nodes + k;
@@ -1154,12 +1142,10 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
         float* na = node_adj + static_cast<int64_t>(k) * kNodeAdj;
         if (QUAD && quad_order(d2, rc2, P)) {
           far_quad_adjoint(nd, A, Q, wx, wy, wz, two, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, r10);
-          nquad++;
         } else {
           far_mono_adjoint<CUT, PER>(A, Q, wx, wy, wz, two, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, lane,
                                      r4);
         }
-        nfar++;
         k = tp.z;
       } else if (tp.w & kLeafFlag) {
         // the self pair (r = 0) only occurs when the leaf overlaps the group
@@ -1206,17 +1192,10 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
           float tot = reduce4(a0, a1, a2, a3);
           if ((lane & 7) == 0) atomicAdd(&part_adj[static_cast<int64_t>(j) * kPartAdj + r4], tot);
         }
-        nnear += static_cast<uint32_t>(tp.y - tp.x);
         k = tp.z;
       } else {
         k++;
       }
-    }
-    if (counters && lane == 0) {
-      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
-      atomicAdd(&counters[0], nfar * na);
-      atomicAdd(&counters[1], nnear * na);
-      atomicAdd(&counters[2], nquad * na);
     }
 #pragma unroll
     for (int t = 0; t < kTPL; t++) {
@@ -1232,6 +1211,58 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
           out[3 * o + 2] = fz[t];
         }
       }
+    }
+  }
+}
+
+// Interaction counts of the force and adjoint walks: the same traversal and
+// the same decisions without the sums, so the hot walks carry no counters.
+// Per group: accepted nodes (and those that take the quadrupole) and near
+// source particles, each times the group's targets.
+template <bool QUAD, bool CUT, bool PER>
+__global__ void __launch_bounds__(128)
+    count_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, unsigned long long* __restrict__ counters) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t ng = min(*G.ngroups, G.capacity);
+  for (;;) {
+    uint32_t gw = next_group(G);
+    if (gw >= ng) break;
+    int4 gr = G.groups[gw];
+    if (gr.x < G.tbeg || gr.x >= G.tend) continue;
+    LaneTargets Q;
+    load_targets(G, gr, lane, Q);
+    float gmin[3], gmax[3];
+    group_box(Q, gmin, gmax);
+    int2 rt = T.roots[gr.z];
+    unsigned long long nfar = 0, nnear = 0, nquad = 0;
+    int k = rt.x;
+    while (k < rt.y) {
+      const NodeRec* nd = T.nodes + k;
+      const int4 tp = __ldg(&nd->topo);
+      const float4 A = __ldg(&nd->com);
+      float4 C = __ldg(&nd->cell);
+      if (PER) C = cell_image(C, gmin, gmax, P);
+      if (A.w == 0.0f || (CUT && P.prune_r2 > 0.0f && prune_node(C, gmin, gmax, P.prune_r2))) {
+        k = tp.z;
+        continue;
+      }
+      float d2, rc2;
+      if (accept_node(C, gmin, gmax, P.beta, d2, rc2)) {
+        nfar++;
+        if (QUAD && quad_order(d2, rc2, P)) nquad++;
+        k = tp.z;
+      } else if (tp.w & kLeafFlag) {
+        nnear += static_cast<unsigned long long>(tp.y - tp.x);
+        k = tp.z;
+      } else {
+        k++;
+      }
+    }
+    if (lane == 0) {
+      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
+      atomicAdd(&counters[0], nfar * na);
+      atomicAdd(&counters[1], nnear * na);
+      atomicAdd(&counters[2], nquad * na);
     }
   }
 }
@@ -1563,6 +1594,12 @@ struct Header {
   int32_t normals;
   int32_t adjoint;
   int64_t tbeg = 0, tend = INT64_MAX;  // sorted target range the walks serve
+  // the last evaluation: 0 none, 1 a force or adjoint walk (its interaction
+  // counts are recounted on demand), 2 the winding number (counted in-walk)
+  int32_t last_walk = 0;
+  bool counts_fresh = true;
+  sbh_native_params last_params{};
+  int64_t last_tbeg = 0, last_tend = INT64_MAX;
 };
 constexpr uint64_t kMagic = 0x5342483230304e54ull;  // "SBH200NT"
 
@@ -1725,6 +1762,19 @@ int lookup(const void* ws, size_t ws_bytes, Header& h, Layout& L) {
   return native_layout(const_cast<void*>(ws), ws_bytes, h, L);
 }
 
+// Records which evaluation last ran on the tree in `ws` (Header::last_walk).
+void remember_walk(const void* ws, int kind, const sbh_native_params* p) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  auto it = g_registry.find(ws);
+  if (it == g_registry.end()) return;
+  Header& h = it->second;
+  h.last_walk = kind;
+  if (p) h.last_params = *p;
+  h.last_tbeg = h.tbeg;
+  h.last_tend = h.tend;
+  h.counts_fresh = kind != 1;
+}
+
 __global__ void zero_node_adj_kernel(float* adj, const uint32_t* meta) {
   int64_t total = static_cast<int64_t>(meta[0]) * kNodeAdj;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
@@ -1814,6 +1864,31 @@ WalkParams walk_params(const sbh_native_params* p) {
                     static_cast<float>(1.0 / (2.0 * 1.7724538509055160 * c * c * c))};
 }
 
+// Recounts the interactions of the last force or adjoint walk (same tree,
+// parameters and target range) into the counters, once per walk.
+int refresh_counts(cudaStream_t stream, const void* ws, const Header& h, const Layout& L) {
+  if (h.last_walk != 1 || h.counts_fresh) return SBH_OK;
+  cudaError_t e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  const sbh_native_params& p = h.last_params;
+  Header hr = h;
+  hr.tbeg = h.last_tbeg;
+  hr.tend = h.last_tend;
+  WalkParams wp = walk_params(&p);
+  bool cut = p.cutoff > 0.0f;
+  bool per = p.periodic != 0;
+  auto k = p.quadrupole ? count_walk_kernel<true, false, false>
+           : per ? (cut ? count_walk_kernel<false, true, true> : count_walk_kernel<false, false, true>)
+                 : (cut ? count_walk_kernel<false, true, false> : count_walk_kernel<false, false, false>);
+  e = launch_walk(stream, L.work, h.n + h.nseg, k, tree_view(L), self_targets(L, hr), wp, L.counters);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  auto it = g_registry.find(ws);
+  if (it != g_registry.end()) it->second.counts_fresh = true;
+  return SBH_OK;
+}
+
+
 }  // namespace
 
 extern "C" {
@@ -1864,9 +1939,9 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   if (h.n == 0) return SBH_OK;
   if (!force_out) return invalid("force_out must be non-null");
-  cudaError_t e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
+  cudaError_t e = cudaSuccess;
   // with a partial target range the other targets' rows are zero (ranks sum their outputs)
-  if (e == cudaSuccess && partial_range(h)) e = cudaMemsetAsync(force_out, 0, h.n * 3 * sizeof(float), stream);
+  if (partial_range(h)) e = cudaMemsetAsync(force_out, 0, h.n * 3 * sizeof(float), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   WalkParams wp = walk_params(params);
   int64_t mg = h.n + h.nseg;
@@ -1875,8 +1950,9 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   auto k = params->quadrupole ? force_walk_kernel<true, false, false>
            : per ? (cut ? force_walk_kernel<false, true, true> : force_walk_kernel<false, false, true>)
                  : (cut ? force_walk_kernel<false, true, false> : force_walk_kernel<false, false, false>);
-  e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h), wp, force_out, L.counters);
+  e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h), wp, force_out);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  remember_walk(workspace, 1, params);
   return check_launch("sbh_native_force");
 }
 
@@ -1891,7 +1967,6 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   if (!cotangent) return invalid("cotangent must be non-null");
   int64_t n = h.n;
   cudaError_t e = cudaMemsetAsync(L.part_adj, 0, n * kPartAdj * sizeof(float), stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
   // with a partial target range the query-side gradient (added for every particle by the
   // finalize) and the force rows of the other targets are zero
   if (e == cudaSuccess && partial_range(h)) e = cudaMemsetAsync(L.gq, 0, n * 3 * sizeof(float), stream);
@@ -1906,8 +1981,9 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
            : per ? (cut ? adjoint_walk_kernel<false, true, true> : adjoint_walk_kernel<false, false, true>)
                  : (cut ? adjoint_walk_kernel<false, true, false> : adjoint_walk_kernel<false, false, false>);
   e = launch_walk(stream, L.work, n + h.nseg, k, tree_view(L), self_targets(L, h), wp, cotangent, force_out, L.gq,
-                  L.node_adj, L.part_adj, L.counters);
+                  L.node_adj, L.part_adj);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  remember_walk(workspace, 1, params);
   return check_launch("sbh_native_adjoint_walk");
 }
 
@@ -1995,6 +2071,7 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1), 0, INT64_MAX};
   e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  remember_walk(workspace, 2, nullptr);
   return check_launch("sbh_native_winding_number");
 }
 
@@ -2006,6 +2083,7 @@ int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspac
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   uint32_t meta[8];
   unsigned long long cnt[3];
+  if (int rc = refresh_counts(stream, workspace, h, L)) return rc;
   cudaError_t e = cudaMemcpyAsync(meta, L.meta, sizeof(meta), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, L.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
@@ -2024,6 +2102,7 @@ int sbh_native_quadrupole_count(cudaStream_t stream, const void* workspace, size
   Layout L;
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   if (!far_quadrupole) return invalid("far_quadrupole must be non-null");
+  if (int rc = refresh_counts(stream, workspace, h, L)) return rc;
   unsigned long long c = 0;
   cudaError_t e = cudaMemcpyAsync(&c, L.counters + 2, sizeof(c), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);

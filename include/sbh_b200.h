@@ -431,7 +431,10 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
                               void* query_workspace, size_t query_workspace_bytes);
 
 /* Synchronises; out4 = {nodes, target groups, far interactions, near
- * interactions} of the last build / evaluation on this workspace. */
+ * interactions} of the last build / evaluation on this workspace. The walks
+ * themselves carry no counters: after a force or adjoint walk the counts
+ * come from one count-only traversal with that walk's parameters and target
+ * range (the same decisions), run here once per walk. */
 int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
                      uint64_t* out4);
 
