@@ -537,15 +537,15 @@ __device__ __forceinline__ uint32_t next_group(const WalkTargets& G) {
 
 // Resident blocks of 128 threads per SM the walks are compiled for (this
 // caps their registers at 65536 / (128 x blocks)). Measured on a B200 with
-// 8 x 2^20 Plummer particles, quadrupole radius 1.6: the adjoint walk takes
-// 477 ms at 5 blocks (88 registers), 445 ms at 6 (80 registers), 429 ms at 7
-// (72 registers, 48 bytes of spills) and 430 ms at 8 (64 registers); the
-// force walk 219 ms at 5, 211 ms at 6, 213 ms at 7 and 218 ms at 8.
+// 8 x 2^20 Plummer particles, quadrupole radius 1.6, walks without in-walk
+// counters: the adjoint walk takes 410 ms at 7 blocks (72 registers, 4
+// bytes of spills) and 416 ms at 8 (64 registers, 56 bytes of spills); the
+// force walk 197 ms at 6 (80 registers) and 194.5 ms at 7 (72 registers).
 #ifndef SBH_ADJOINT_WALK_MIN_BLOCKS
 #define SBH_ADJOINT_WALK_MIN_BLOCKS 7
 #endif
 #ifndef SBH_FORCE_WALK_MIN_BLOCKS
-#define SBH_FORCE_WALK_MIN_BLOCKS 6
+#define SBH_FORCE_WALK_MIN_BLOCKS 7
 #endif
 constexpr int kAdjointWalkMinBlocks = SBH_ADJOINT_WALK_MIN_BLOCKS;
 constexpr int kForceWalkMinBlocks = SBH_FORCE_WALK_MIN_BLOCKS;
