@@ -735,24 +735,65 @@ def run_ours(args):
     force_ms = timed(plain_force, 2)
     plain_force_rel = float(torch.linalg.norm(F0[idx].double() - ref) / torch.linalg.norm(ref))
 
-    # e2e: host buffers in, host buffers out, through the public API
+    # e2e: host buffers in, host buffers out, through the public API. Every
+    # step uploads its own inputs from pinned host memory and reads its own
+    # results back, inside the timed region; as a serving loop would, the
+    # copies run on two side streams against two device buffer sets, so the
+    # upload of step s + 1 and the download of step s - 1 overlap the walk of
+    # step s. The inputs (235 MB) are larger than L2, so no flush is needed.
     Ph, Mh, Wh = (torch.tensor(a_).pin_memory() for a_ in (p, m, w))
-    Fh = torch.empty(P.shape).pin_memory()
-    GXh = torch.empty(P.shape).pin_memory()
-    GMh = torch.empty(M.shape).pin_memory()
+    Fh = [torch.empty(P.shape).pin_memory() for _ in range(2)]
+    GXh = [torch.empty(P.shape).pin_memory() for _ in range(2)]
+    GMh = [torch.empty(M.shape).pin_memory() for _ in range(2)]
+    Pd = [torch.empty_like(P) for _ in range(2)]
+    Md = [torch.empty_like(M) for _ in range(2)]
+    Wd = [torch.empty_like(Wt) for _ in range(2)]
+    Fd = [torch.empty_like(F) for _ in range(2)]
+    GXd = [torch.empty_like(GX) for _ in range(2)]
+    GMd = [torch.empty_like(GM) for _ in range(2)]
+    comp = torch.cuda.current_stream(dev)
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
 
-    def e2e_step():
-        Pd = Ph.to(dev, non_blocking=True)
-        Md = Mh.to(dev, non_blocking=True)
-        Wd = Wh.to(dev, non_blocking=True)
-        tree.build(Pd, Md, system_offsets=OFFS, leaf_size=LEAF, with_adjoint=True)
-        tree.adjoint_walk(Wd, prm, F)
-        tree.adjoint_finalize(GX, GM)
-        Fh.copy_(F, non_blocking=True)
-        GXh.copy_(GX, non_blocking=True)
-        GMh.copy_(GM, non_blocking=True)
+    def e2e_run(steps):
+        free = [None, None]  # events: compute done with buffer set b
+        done = [None, None]
+        t0, t1 = ev(), ev()
+        t0.record(comp)
+        up.wait_stream(comp)
+        down.wait_stream(comp)
+        for s_ in range(steps):
+            b = s_ % 2
+            with torch.cuda.stream(up):
+                if free[b] is not None:
+                    up.wait_event(free[b])
+                Pd[b].copy_(Ph, non_blocking=True)
+                Md[b].copy_(Mh, non_blocking=True)
+                Wd[b].copy_(Wh, non_blocking=True)
+                loaded = torch.cuda.Event()
+                loaded.record(up)
+            comp.wait_event(loaded)
+            if done[b] is not None:
+                comp.wait_event(done[b])  # the previous download from these outputs has finished
+            tree.build(Pd[b], Md[b], system_offsets=OFFS, leaf_size=LEAF, with_adjoint=True)
+            tree.adjoint_walk(Wd[b], prm, Fd[b])
+            tree.adjoint_finalize(GXd[b], GMd[b])
+            free[b] = torch.cuda.Event()
+            free[b].record(comp)
+            with torch.cuda.stream(down):
+                down.wait_event(free[b])
+                Fh[b].copy_(Fd[b], non_blocking=True)
+                GXh[b].copy_(GXd[b], non_blocking=True)
+                GMh[b].copy_(GMd[b], non_blocking=True)
+                done[b] = torch.cuda.Event()
+                done[b].record(down)
+        comp.wait_stream(down)
+        comp.wait_stream(up)
+        t1.record(comp)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / steps
 
-    e_ms = timed(e2e_step, args.steps)
+    e2e_run(2)
+    e_ms = e2e_run(args.steps)
     if world > 1:
         t = torch.tensor([e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -813,7 +854,9 @@ def run_ours(args):
                          "interactions": {"far": st["far"], "far_quadrupole": st["far_quadrupole"], "near": st["near"]}},
             "cpu_baseline": cpu,
             "e2e": {"value": world * K * 1000.0 / e_ms, "unit": "evals/s",
-                    "h2d_bytes_per_step": int(K * n * 28), "d2h_bytes_per_step": int(K * n * 28)},
+                    "h2d_bytes_per_step": int(K * n * 28), "d2h_bytes_per_step": int(K * n * 28),
+                    "copies": "each step uploads its inputs and reads its results back from pinned host memory "
+                              "on two side streams, overlapping the walks of the neighbouring steps"},
             "gpu_launches": launches,
             "clocks": clocks,
             "tree": {"nodes": st["nodes"], "groups": st["groups"]},
