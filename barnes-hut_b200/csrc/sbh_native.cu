@@ -6,7 +6,7 @@
 // prune radius (the short range of TreePM), and a quadrupole radius beyond
 // which accepted nodes keep the monopole alone.
 //
-// Traversal: one warp per target group of at most 64 targets (two per
+// Traversal: one warp per target group of at most kGroup targets (kTPL per
 // lane), cut from the tree so its box is compact; every opening decision is
 // taken on the group's box, so it is warp-uniform; warps take groups from an
 // atomic counter (persistent grid).
@@ -537,15 +537,16 @@ __device__ __forceinline__ uint32_t next_group(const WalkTargets& G) {
 
 // Resident blocks of 128 threads per SM the walks are compiled for (this
 // caps their registers at 65536 / (128 x blocks)). Measured on a B200 with
-// 8 x 2^20 Plummer particles, quadrupole radius 1.6, walks without in-walk
-// counters: the adjoint walk takes 410 ms at 7 blocks (72 registers, 4
-// bytes of spills) and 416 ms at 8 (64 registers, 56 bytes of spills); the
-// force walk 197 ms at 6 (80 registers) and 194.5 ms at 7 (72 registers).
+// 8 x 2^20 Plummer particles, quadrupole radius 1.6, three targets per
+// lane: the adjoint walk takes 412 ms at 5 blocks (96 registers) and 389 ms
+// at 6 (80 registers, 56 bytes of spills), where 7 blocks leave 72
+// registers and 128 bytes of spills; the force walk 182.5 ms at 5 and 177 ms
+// at 6.
 #ifndef SBH_ADJOINT_WALK_MIN_BLOCKS
-#define SBH_ADJOINT_WALK_MIN_BLOCKS 7
+#define SBH_ADJOINT_WALK_MIN_BLOCKS 6
 #endif
 #ifndef SBH_FORCE_WALK_MIN_BLOCKS
-#define SBH_FORCE_WALK_MIN_BLOCKS 7
+#define SBH_FORCE_WALK_MIN_BLOCKS 6
 #endif
 constexpr int kAdjointWalkMinBlocks = SBH_ADJOINT_WALK_MIN_BLOCKS;
 constexpr int kForceWalkMinBlocks = SBH_FORCE_WALK_MIN_BLOCKS;
@@ -712,11 +713,11 @@ __device__ __forceinline__ void attenuation(float r2, float ir3, const WalkParam
 // One accepted node's monopole (with the erfc attenuation when CUT, minimum
 // image when PER) added to the lane's far-field accumulators.
 template <bool CUT, bool PER>
-__device__ __forceinline__ void far_mono_force(const float4& A, const LaneTargets& Q, bool two, const WalkParams& P,
+__device__ __forceinline__ void far_mono_force(const float4& A, const LaneTargets& Q, int nslot, const WalkParams& P,
                                                float* fx, float* fy, float* fz) {
 #pragma unroll
   for (int t = 0; t < kTPL; t++) {
-    if (t > 0 && !two) break;
+    if (t >= nslot) break;
     float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
     if (PER) {
       rx = min_image(rx, P);
@@ -740,14 +741,14 @@ __device__ __forceinline__ void far_mono_force(const float4& A, const LaneTarget
 
 // One accepted node's monopole + quadrupole (Plummer softening):
 // a_q = ir5 (3 S r + 1.5 tr(S) r) - 7.5 (r.S.r) ir7 r.
-__device__ __forceinline__ void far_quad_force(const NodeRec* nd, const float4& A, const LaneTargets& Q, bool two,
+__device__ __forceinline__ void far_quad_force(const NodeRec* nd, const float4& A, const LaneTargets& Q, int nslot,
                                                const WalkParams& P, float* fx, float* fy, float* fz) {
   const float4 Qd = __ldg(&nd->quad);
   const float4 X = __ldg(&nd->quad2);
   const float tr15 = 1.5f * (Qd.x + Qd.y + Qd.z);
 #pragma unroll
   for (int t = 0; t < kTPL; t++) {
-    if (t > 0 && !two) break;
+    if (t >= nslot) break;
     float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
     float r2 = rx * rx + ry * ry + rz * rz;
     float ir = rsqrtf(r2 + P.eps2);
@@ -784,7 +785,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
     if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
-    const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
+    const int nslot = (gr.y - gr.x + 31) / 32;  // warp-uniform: the target slots in use
     float gmin[3], gmax[3];
     group_box(Q, gmin, gmax);
     int2 rt = T.roots[gr.z];
@@ -822,9 +823,9 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
       }
       if (acc) {
         if (qh) {
-          far_quad_force(nd, A, Q, two, P, fx, fy, fz);
+          far_quad_force(nd, A, Q, nslot, P, fx, fy, fz);
         } else {
-          far_mono_force<CUT, PER>(A, Q, two, P, fx, fy, fz);
+          far_mono_force<CUT, PER>(A, Q, nslot, P, fx, fy, fz);
         }
       } else if (live && leaf) {
         float ax[kTPL], ay[kTPL], az[kTPL];
@@ -834,7 +835,7 @@ __global__ void __launch_bounds__(128, kForceWalkMinBlocks)
           float4 s = __ldg(&T.sp[j]);
 #pragma unroll
           for (int t = 0; t < kTPL; t++) {
-            if (t > 0 && !two) break;
+            if (t >= nslot) break;
             float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
             if (PER) {
               rx = min_image(rx, P);
@@ -955,14 +956,14 @@ __device__ __forceinline__ int reduce10_index(int lane) {
 // (A_X, A_M) reduced over the warp and added to the node's slots.
 template <bool CUT, bool PER>
 __device__ __forceinline__ void far_mono_adjoint(const float4& A, const LaneTargets& Q, const float* wx,
-                                                 const float* wy, const float* wz, bool two, const WalkParams& P,
+                                                 const float* wy, const float* wz, int nslot, const WalkParams& P,
                                                  bool want_force, float* gx, float* gy, float* gz, float* fx,
                                                  float* fy, float* fz, float* __restrict__ na, int lane, int r4) {
   const float M = A.w;
   float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
 #pragma unroll
   for (int t = 0; t < kTPL; t++) {
-    if (t > 0 && !two) break;
+    if (t >= nslot) break;
     float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
     if (PER) {
       rx = min_image(rx, P);
@@ -1003,7 +1004,7 @@ __device__ __forceinline__ void far_mono_adjoint(const float4& A, const LaneTarg
 // periodic): as far_mono_adjoint plus the quadrupole's terms and the node's
 // G = sym d(w . a_q)/dS, ten values reduced over the warp.
 __device__ __forceinline__ void far_quad_adjoint(const NodeRec* nd, const float4& A, const LaneTargets& Q,
-                                                 const float* wx, const float* wy, const float* wz, bool two,
+                                                 const float* wx, const float* wy, const float* wz, int nslot,
                                                  const WalkParams& P, bool want_force, float* gx, float* gy,
                                                  float* gz, float* fx, float* fy, float* fz, float* __restrict__ na,
                                                  int r10) {
@@ -1017,7 +1018,7 @@ __device__ __forceinline__ void far_quad_adjoint(const NodeRec* nd, const float4
   for (int j = 0; j < 10; j++) v[j] = 0.f;
 #pragma unroll
   for (int t = 0; t < kTPL; t++) {
-    if (t > 0 && !two) break;
+    if (t >= nslot) break;
     float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
     float r2 = rx * rx + ry * ry + rz * rz;
     float ir = rsqrtf(r2 + P.eps2);
@@ -1110,7 +1111,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
     if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
-    const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
+    const int nslot = (gr.y - gr.x + 31) / 32;  // warp-uniform: the target slots in use
     float wx[kTPL], wy[kTPL], wz[kTPL];
 #pragma unroll
     for (int t = 0; t < kTPL; t++) {
@@ -1141,9 +1142,9 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
       if (accept_node(C, gmin, gmax, P.beta, d2, rc2)) {
         float* na = node_adj + static_cast<int64_t>(k) * kNodeAdj;
         if (QUAD && quad_order(d2, rc2, P)) {
-          far_quad_adjoint(nd, A, Q, wx, wy, wz, two, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, r10);
+          far_quad_adjoint(nd, A, Q, wx, wy, wz, nslot, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, r10);
         } else {
-          far_mono_adjoint<CUT, PER>(A, Q, wx, wy, wz, two, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, lane,
+          far_mono_adjoint<CUT, PER>(A, Q, wx, wy, wz, nslot, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, lane,
                                      r4);
         }
         k = tp.z;
@@ -1155,7 +1156,7 @@ __global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
           float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
 #pragma unroll
           for (int t = 0; t < kTPL; t++) {
-            if (t > 0 && !two) break;
+            if (t >= nslot) break;
             float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
             if (PER) {
               rx = min_image(rx, P);
@@ -1356,7 +1357,7 @@ __global__ void __launch_bounds__(128, 4)
     if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
     LaneTargets Q;
     load_targets(G, gr, lane, Q);
-    const bool two = gr.y - gr.x > 32;  // warp-uniform: the second slots hold targets
+    const int nslot = (gr.y - gr.x + 31) / 32;  // warp-uniform: the target slots in use
     float gmin[3], gmax[3];
     group_box(Q, gmin, gmax);
     int2 rt = T.roots[gr.z];
@@ -1391,7 +1392,7 @@ __global__ void __launch_bounds__(128, 4)
         float4 N = __ldg(&T.nnrm[k]);
 #pragma unroll
         for (int t = 0; t < kTPL; t++) {
-          if (t > 0 && !two) break;
+          if (t >= nslot) break;
           float dx = A.x - Q.x[t], dy = A.y - Q.y[t], dz = A.z - Q.z[t];
           float dist = sqrtf(dx * dx + dy * dy + dz * dz);
           float nd_ = N.x * dx + N.y * dy + N.z * dz;
@@ -1407,7 +1408,7 @@ __global__ void __launch_bounds__(128, 4)
           float4 nrm = __ldg(&T.sn[j]);
 #pragma unroll
           for (int t = 0; t < kTPL; t++) {
-            if (t > 0 && !two) break;
+            if (t >= nslot) break;
             float dx = s.x - Q.x[t], dy = s.y - Q.y[t], dz = s.z - Q.z[t];
             float dist = sqrtf(dx * dx + dy * dy + dz * dz);
             float nd_ = nrm.x * dx + nrm.y * dy + nrm.z * dz;
