@@ -602,7 +602,7 @@ __device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin
   return d2 > r2;
 }
 
-// Targets of one group as a lane holds them: slots lane and lane + 32.
+// Targets of one group as a lane holds them: slots lane + 32 t, t < kTPL.
 // Inactive slots carry the group's first target (inside the group box) and
 // a zero cotangent or mass, so they add nothing to the sums over the warp.
 struct LaneTargets {
