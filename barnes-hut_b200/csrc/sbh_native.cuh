@@ -35,7 +35,11 @@ constexpr int kLeafFlag = 0x100;
 #endif
 constexpr int kTPL = SBH_TARGETS_PER_LANE;
 constexpr int kGroup = 32 * kTPL;  // targets per group (one warp)
-constexpr int kQueryGroup = 32;    // targets per group of external queries
+#ifndef SBH_QUERY_GROUP
+#define SBH_QUERY_GROUP 32
+#endif
+constexpr int kQueryGroup = SBH_QUERY_GROUP;  // targets per group of external queries (<= 32 * kTPL)
+static_assert(kQueryGroup <= 32 * kTPL, "a query group must fit the lanes' target slots");
 constexpr int kNodeAdj = 12;    // per-node adjoint floats: A_X(3) A_M(1) G(6) pad(2)
 constexpr int kPartAdj = 4;     // per-particle adjoint floats: dx(3) dm(1)
 
