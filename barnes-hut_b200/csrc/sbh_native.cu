@@ -341,7 +341,7 @@ struct NormalMomentLoad {
   }
 };
 
-// Node records from topology + moments + cell geometry (NodeRec, 64 B).
+// Node records from topology + moments + cell geometry (NodeRec, 80 B).
 // The topology fields were written by emit_nodes_kernel into nodes[k].topo.
 __global__ void finalize_nodes_kernel(NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
                                       const uint64_t* __restrict__ keys, const uint32_t* __restrict__ sseg,
