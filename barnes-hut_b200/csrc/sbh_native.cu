@@ -110,46 +110,72 @@ __global__ void bbox_init_kernel(uint32_t* bb, int nseg) {
   }
 }
 
+// Per-system bounding boxes (order-preserving uint encoding, min/max by
+// atomics). Each block scans a contiguous chunk; a lane keeps running
+// min/max for the system its warp is in and the warp reduces and flushes
+// them only when that system changes, so the atomics per system are few
+// (contiguous systems: about one flush per warp) instead of six per 32
+// points. A warp whose 32 points straddle a system boundary adds them with
+// per-lane atomics.
+__device__ __forceinline__ void bbox_flush(uint32_t* bb, int s, uint32_t* mn, uint32_t* mx, int lane) {
+  for (int d = 0; d < 3; d++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+      mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+    }
+  }
+  if (lane == 0 && mn[0] <= mx[0]) {
+    for (int d = 0; d < 3; d++) {
+      atomicMin(&bb[6 * s + d], mn[d]);
+      atomicMax(&bb[6 * s + 3 + d], mx[d]);
+    }
+  }
+}
+
 __global__ void bbox_kernel(const float* __restrict__ pts, int64_t n, const int64_t* __restrict__ seg_off, int nseg,
                             uint32_t* bb) {
-  int lane = threadIdx.x & 31;
-  int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < n; base += stride) {
-    int64_t i = base + threadIdx.x;
-    bool ok = i < n;
-    uint32_t mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0u, 0u, 0u};
+  const int lane = threadIdx.x & 31;
+  const int64_t per_block = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t chunk = (per_block + blockDim.x - 1) / blockDim.x * blockDim.x;
+  const int64_t lo = static_cast<int64_t>(blockIdx.x) * chunk;
+  const int64_t hi = lo + chunk < n ? lo + chunk : n;
+  int run = -1;  // the warp's current system (warp-uniform)
+  uint32_t mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0u, 0u, 0u};
+  for (int64_t base = lo; base < hi; base += blockDim.x) {
+    const int64_t i = base + threadIdx.x;
+    const bool ok = i < hi;
     int s = 0;
+    uint32_t o[3] = {0u, 0u, 0u};
     if (ok) {
       s = nseg > 1 ? seg_of(seg_off, nseg, i) : 0;
-      for (int d = 0; d < 3; d++) {
-        uint32_t o = float_to_ordered(pts[3 * i + d]);
-        mn[d] = o;
-        mx[d] = o;
-      }
+      for (int d = 0; d < 3; d++) o[d] = float_to_ordered(pts[3 * i + d]);
     }
-    int s0 = __shfl_sync(0xffffffffu, s, 0);
-    bool uniform = __all_sync(0xffffffffu, !ok || s == s0);
-    if (uniform) {
-      for (int d = 0; d < 3; d++) {
-        for (int o = 16; o > 0; o >>= 1) {
-          mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
-          mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+    const int first = __ffs(__ballot_sync(0xffffffffu, ok)) - 1;
+    if (first < 0) continue;  // no point of this warp in range
+    const int s0 = __shfl_sync(0xffffffffu, s, first);
+    if (__all_sync(0xffffffffu, !ok || s == s0)) {
+      if (s0 != run) {
+        if (run >= 0) bbox_flush(bb, run, mn, mx, lane);
+        run = s0;
+        for (int d = 0; d < 3; d++) {
+          mn[d] = 0xFFFFFFFFu;
+          mx[d] = 0u;
         }
       }
-      bool any = __any_sync(0xffffffffu, ok);
-      if (lane == 0 && any) {
+      if (ok) {
         for (int d = 0; d < 3; d++) {
-          atomicMin(&bb[6 * s0 + d], mn[d]);
-          atomicMax(&bb[6 * s0 + 3 + d], mx[d]);
+          mn[d] = min(mn[d], o[d]);
+          mx[d] = max(mx[d], o[d]);
         }
       }
     } else if (ok) {
       for (int d = 0; d < 3; d++) {
-        atomicMin(&bb[6 * s + d], mn[d]);
-        atomicMax(&bb[6 * s + 3 + d], mx[d]);
+        atomicMin(&bb[6 * s + d], o[d]);
+        atomicMax(&bb[6 * s + 3 + d], o[d]);
       }
     }
   }
+  if (run >= 0) bbox_flush(bb, run, mn, mx, lane);
 }
 
 // SegBox: lo (float3), span (float), scale (double) per system.
