@@ -561,21 +561,6 @@ __device__ __forceinline__ uint32_t next_group(const WalkTargets& G) {
   return __shfl_sync(0xffffffffu, s, 0);
 }
 
-// Resident blocks of 128 threads per SM the walks are compiled for (this
-// caps their registers at 65536 / (128 x blocks)). Measured on a B200 with
-// 8 x 2^20 Plummer particles, quadrupole radius 1.6, three targets per
-// lane: the adjoint walk takes 412 ms at 5 blocks (96 registers) and 389 ms
-// at 6 (80 registers, 56 bytes of spills), where 7 blocks leave 72
-// registers and 128 bytes of spills; the force walk 182.5 ms at 5 and 177 ms
-// at 6.
-#ifndef SBH_ADJOINT_WALK_MIN_BLOCKS
-#define SBH_ADJOINT_WALK_MIN_BLOCKS 6
-#endif
-#ifndef SBH_FORCE_WALK_MIN_BLOCKS
-#define SBH_FORCE_WALK_MIN_BLOCKS 6
-#endif
-constexpr int kAdjointWalkMinBlocks = SBH_ADJOINT_WALK_MIN_BLOCKS;
-constexpr int kForceWalkMinBlocks = SBH_FORCE_WALK_MIN_BLOCKS;
 
 struct WalkParams {
   float beta;
@@ -628,671 +613,38 @@ __device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin
   return d2 > r2;
 }
 
-// Targets of one group as a lane holds them: slots lane + 32 t, t < kTPL.
-// Inactive slots carry the group's first target (inside the group box) and
-// a zero cotangent or mass, so they add nothing to the sums over the warp.
-struct LaneTargets {
-  float x[kTPL], y[kTPL], z[kTPL];
-  int idx[kTPL];
-  bool act[kTPL];
-};
+// The walks are compiled twice: three targets per lane (groups of up to 96)
+// and two (up to 64), each for the occupancy that suits it. Measured on a
+// B200 over 8 x 2^20 Plummer particles at quadrupole radius 1.6, the adjoint
+// walk takes 410 ms with two targets per lane at 7 blocks per SM (72
+// registers) and 389 ms with three at 6 blocks (80 registers); 4 per lane at
+// 4 blocks takes 411 ms. Clustered systems gain from the larger groups;
+// near-uniform ones and walks bounded by a prune radius gain from smaller
+// groups (a 2^21 lattice trajectory: 3.76 s with groups of 64, 4.46 s with
+// 96), which the two-slot kernels serve. A tree walks with the kernels of its
+// current group size (sbh_native_set_group_size).
+namespace tpl2 {
+constexpr int kTPL = 2;
+constexpr int kForceWalkMinBlocks = 7;
+constexpr int kAdjointWalkMinBlocks = 7;
+#define SBH_NT_WITH_WN_WALK  // the winding-number walk (groups of 32 queries) only here
+#include "sbh_native_walks.inc"
+#undef SBH_NT_WITH_WN_WALK
+}  // namespace tpl2
 
-__device__ __forceinline__ void load_targets(const WalkTargets& G, const int4& gr, int lane, LaneTargets& Q) {
-#pragma unroll
-  for (int t = 0; t < kTPL; t++) {
-    int i = gr.x + lane + 32 * t;
-    Q.act[t] = i < gr.y;
-    Q.idx[t] = i;
-    float4 q = G.tp[Q.act[t] ? i : gr.x];
-    Q.x[t] = q.x;
-    Q.y[t] = q.y;
-    Q.z[t] = q.z;
-  }
-}
+namespace tpl3 {
+constexpr int kTPL = 3;
+constexpr int kForceWalkMinBlocks = 6;
+constexpr int kAdjointWalkMinBlocks = 6;
+#include "sbh_native_walks.inc"
+}  // namespace tpl3
 
-// Group bounding box: min/max over every slot of the warp.
-__device__ __forceinline__ void group_box(const LaneTargets& Q, float* gmin, float* gmax) {
-  float lo[3] = {Q.x[0], Q.y[0], Q.z[0]}, hi[3] = {Q.x[0], Q.y[0], Q.z[0]};
-#pragma unroll
-  for (int t = 1; t < kTPL; t++) {
-    lo[0] = fminf(lo[0], Q.x[t]);
-    lo[1] = fminf(lo[1], Q.y[t]);
-    lo[2] = fminf(lo[2], Q.z[t]);
-    hi[0] = fmaxf(hi[0], Q.x[t]);
-    hi[1] = fmaxf(hi[1], Q.y[t]);
-    hi[2] = fmaxf(hi[2], Q.z[t]);
-  }
-#pragma unroll
-  for (int d = 0; d < 3; d++) {
-    for (int o = 16; o > 0; o >>= 1) {
-      lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-      hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
-    }
-    gmin[d] = lo[d];
-    gmax[d] = hi[d];
-  }
-}
-
-// Acceptance test: the reference's rule |q - cell centre| / diag >= beta
-// (include/tree3d.h:134-153, src/sbh_ffi.cu:1878-1893) made to hold for every
-// target of the group: dist(group box, cell centre) > beta * diag. IEEE
-// operations in the oracle's order (no contraction).
-__device__ __forceinline__ bool accept_node(const float4& cell, const float* gmin, const float* gmax, float beta,
-                                            float& d2, float& rc2) {
-  float rc = __fmul_rn(cell.w, beta);
-  float x[3] = {cell.x, cell.y, cell.z};
-  float t[3];
-  for (int d = 0; d < 3; d++) {
-    float a = __fsub_rn(gmin[d], x[d]);
-    float b = __fsub_rn(x[d], gmax[d]);
-    float m = a > b ? a : b;
-    t[d] = m > 0.0f ? m : 0.0f;
-  }
-  d2 = __fadd_rn(__fadd_rn(__fmul_rn(t[0], t[0]), __fmul_rn(t[1], t[1])), __fmul_rn(t[2], t[2]));
-  rc2 = __fmul_rn(rc, rc);
-  return d2 > rc2;
-}
-
-// Far-field order of an accepted node (warp-uniform: the inputs are the
-// group box and the node). The quadrupole's share of the error falls off
-// one power of the distance faster than the monopole's, so beyond
-// sqrt(quad_g) opening radii the monopole alone is kept.
-__device__ __forceinline__ bool quad_order(float d2, float rc2, const WalkParams& P) {
-  return !(P.quad_g > 0.0f) || d2 < __fmul_rn(P.quad_g, rc2);
-}
-
-__device__ __forceinline__ bool accept_node(const float4& cell, const float* gmin, const float* gmax, float beta) {
-  float rc = __fmul_rn(cell.w, beta);
-  float x[3] = {cell.x, cell.y, cell.z};
-  float t[3];
-  for (int d = 0; d < 3; d++) {
-    float a = __fsub_rn(gmin[d], x[d]);
-    float b = __fsub_rn(x[d], gmax[d]);
-    float m = a > b ? a : b;
-    t[d] = m > 0.0f ? m : 0.0f;
-  }
-  float d2 = __fadd_rn(__fadd_rn(__fmul_rn(t[0], t[0]), __fmul_rn(t[1], t[1])), __fmul_rn(t[2], t[2]));
-  return d2 > __fmul_rn(rc, rc);
-}
-
-// erfc attenuation of the short-range force and its radial derivative term
-// (src/sbh_ffi.cu:142-160, 2062-2090), with u = r / (2 cutoff):
-//   att = erfc(u) + (2 / sqrt(pi)) u e^{-u^2},
-//   cc  = ir3 r e^{-u^2} / (2 sqrt(pi) cutoff^3);
-// att = 1, cc = 0 without cutoff. erfc(u) is the rational approximation of
-// Abramowitz & Stegun 7.1.26 (after Hastings): (a1 t + a2 t^2 + a3 t^3 +
-// a4 t^4 + a5 t^5) e^{-u^2} with t = 1 / (1 + p u), absolute error at most
-// 1.5e-7 for u >= 0. It shares e^{-u^2} with the second term, so one
-// exponential serves a pair; the divisions by the cutoff are precomputed.
-__device__ __forceinline__ void attenuation(float r2, float ir3, const WalkParams& P, float& att, float& cc) {
-  const float r2p = r2 + 1e-12f;
-  const float dist = r2p * rsqrtf(r2p);
-  const float u = dist * P.inv_2cut;
-  const float e = expf(-(u * u));
-  const float t = __fdividef(1.0f, fmaf(0.3275911f, u, 1.0f));
-  const float poly =
-      t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, 1.061405429f, -1.453152027f), 1.421413741f), -0.284496736f), 0.254829592f);
-  att = e * fmaf(1.1283791671f, u, poly);  // 2 / sqrt(pi) = 1.1283791671
-  cc = ir3 * dist * e * P.cc_coef;
-}
-
-// One accepted node's monopole (with the erfc attenuation when CUT, minimum
-// image when PER) added to the lane's far-field accumulators.
-template <bool CUT, bool PER>
-__device__ __forceinline__ void far_mono_force(const float4& A, const LaneTargets& Q, int nslot, const WalkParams& P,
-                                               float* fx, float* fy, float* fz) {
-#pragma unroll
-  for (int t = 0; t < kTPL; t++) {
-    if (t >= nslot) break;
-    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
-    if (PER) {
-      rx = min_image(rx, P);
-      ry = min_image(ry, P);
-      rz = min_image(rz, P);
-    }
-    float r2 = rx * rx + ry * ry + rz * rz;
-    float ir = rsqrtf(r2 + P.eps2);
-    float ir3 = ir * ir * ir;
-    float c = -A.w * ir3;
-    if (CUT) {
-      float att, cc;
-      attenuation(r2, ir3, P, att, cc);
-      c *= att;
-    }
-    fx[t] += c * rx;
-    fy[t] += c * ry;
-    fz[t] += c * rz;
-  }
-}
-
-// One accepted node's monopole + quadrupole (Plummer softening):
-// a_q = ir5 (3 S r + 1.5 tr(S) r) - 7.5 (r.S.r) ir7 r.
-__device__ __forceinline__ void far_quad_force(const NodeRec* nd, const float4& A, const LaneTargets& Q, int nslot,
-                                               const WalkParams& P, float* fx, float* fy, float* fz) {
-  const float4 Qd = __ldg(&nd->quad);
-  const float4 X = __ldg(&nd->quad2);
-  const float tr15 = 1.5f * (Qd.x + Qd.y + Qd.z);
-#pragma unroll
-  for (int t = 0; t < kTPL; t++) {
-    if (t >= nslot) break;
-    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
-    float r2 = rx * rx + ry * ry + rz * rz;
-    float ir = rsqrtf(r2 + P.eps2);
-    float ih = ir * ir;
-    float ir3 = ir * ih;
-    float c = -A.w * ir3;
-    float sx = Qd.x * rx + Qd.w * ry + X.x * rz;
-    float sy = Qd.w * rx + Qd.y * ry + X.y * rz;
-    float sz = X.x * rx + X.y * ry + Qd.z * rz;
-    float rsr = rx * sx + ry * sy + rz * sz;
-    float ir5 = ir3 * ih;
-    float cr = c + ir5 * (tr15 - 7.5f * rsr * ih);
-    float c3 = 3.0f * ir5;
-    fx[t] += cr * rx + c3 * sx;
-    fy[t] += cr * ry + c3 * sy;
-    fz[t] += cr * rz + c3 * sz;
-  }
-}
-
-// Flop accounting used by the roofline (FP32 operations counted from the
-// formulas below, an FMA as 2, per target): force walk near pair 20, far
-// node 55 (monopole + quadrupole); adjoint walk (force + adjoint) near pair
-// 55, far node 200 including the share of the warp reductions.
-
-template <bool QUAD, bool CUT, bool PER>
-__global__ void __launch_bounds__(128, kForceWalkMinBlocks)
-    force_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, float* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t ng = min(*G.ngroups, G.capacity);
-  for (;;) {
-    uint32_t gw = next_group(G);
-    if (gw >= ng) break;
-    int4 gr = G.groups[gw];
-    if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
-    LaneTargets Q;
-    load_targets(G, gr, lane, Q);
-    const int nslot = (gr.y - gr.x + 31) / 32;  // warp-uniform: the target slots in use
-    float gmin[3], gmax[3];
-    group_box(Q, gmin, gmax);
-    int2 rt = T.roots[gr.z];
-    float fx[kTPL], fy[kTPL], fz[kTPL];                                     // far field
-    float nx[kTPL], ny[kTPL], nz[kTPL], cx[kTPL], cy[kTPL], cz[kTPL];       // near field, compensated
-#pragma unroll
-    for (int t = 0; t < kTPL; t++) fx[t] = fy[t] = fz[t] = nx[t] = ny[t] = nz[t] = cx[t] = cy[t] = cz[t] = 0.f;
-    // Pre-order walk. The next node is known once this node's opening test
-    // is done, so its opening data is loaded before this node's terms are
-    // evaluated and the load latency hides behind that arithmetic.
-    int k = rt.x;
-    int4 tp = make_int4(0, 0, rt.y, 0);
-    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), C = A;
-    if (k < rt.y) {
-      tp = __ldg(&T.nodes[k].topo);
-      A = __ldg(&T.nodes[k].com);
-      C = __ldg(&T.nodes[k].cell);
-    }
-    while (k < rt.y) {
-      const NodeRec* nd = T.nodes + k;
-      const float4 Ci = PER ? cell_image(C, gmin, gmax, P) : C;
-      const bool live = A.w != 0.0f &&  // mass-zero and pruned nodes are skipped
-                        !(CUT && P.prune_r2 > 0.0f && prune_node(Ci, gmin, gmax, P.prune_r2));
-      float d2 = 0.0f, rc2 = 0.0f;
-      const bool acc = live && accept_node(Ci, gmin, gmax, P.beta, d2, rc2);
-      const bool qh = QUAD && quad_order(d2, rc2, P);
-      const bool leaf = (tp.w & kLeafFlag) != 0;
-      const int next = (!live || acc || leaf) ? tp.z : k + 1;
-      int4 tpn = tp;
-      float4 An = A, Cn = C;
-      if (next < rt.y) {
-        tpn = __ldg(&T.nodes[next].topo);
-        An = __ldg(&T.nodes[next].com);
-        Cn = __ldg(&T.nodes[next].cell);
-      }
-      if (acc) {
-        if (qh) {
-          far_quad_force(nd, A, Q, nslot, P, fx, fy, fz);
-        } else {
-          far_mono_force<CUT, PER>(A, Q, nslot, P, fx, fy, fz);
-        }
-      } else if (live && leaf) {
-        float ax[kTPL], ay[kTPL], az[kTPL];
-#pragma unroll
-        for (int t = 0; t < kTPL; t++) ax[t] = ay[t] = az[t] = 0.f;
-        for (int j = tp.x; j < tp.y; j++) {
-          float4 s = __ldg(&T.sp[j]);
-#pragma unroll
-          for (int t = 0; t < kTPL; t++) {
-            if (t >= nslot) break;
-            float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
-            if (PER) {
-              rx = min_image(rx, P);
-              ry = min_image(ry, P);
-              rz = min_image(rz, P);
-            }
-            float r2 = rx * rx + ry * ry + rz * rz;
-            float ir = rsqrtf(r2 + P.eps2);
-            float ir3 = ir * ir * ir;
-            float c = -s.w * ir3;
-            if (CUT) {
-              float att, cc;
-              attenuation(r2, ir3, P, att, cc);
-              c *= att;
-            }
-            ax[t] += c * rx;
-            ay[t] += c * ry;
-            az[t] += c * rz;
-          }
-        }
-#pragma unroll
-        for (int t = 0; t < kTPL; t++) {
-          kahan_add(nx[t], cx[t], ax[t]);
-          kahan_add(ny[t], cy[t], ay[t]);
-          kahan_add(nz[t], cz[t], az[t]);
-        }
-      }
-      k = next;
-      tp = tpn;
-      A = An;
-      C = Cn;
-    }
-#pragma unroll
-    for (int t = 0; t < kTPL; t++) {
-      if (Q.act[t]) {
-        uint32_t o = G.perm[Q.idx[t]];
-        out[3 * o] = fx[t] + nx[t];
-        out[3 * o + 1] = fy[t] + ny[t];
-        out[3 * o + 2] = fz[t] + nz[t];
-      }
-    }
-  }
-}
-
-// Sum 4 values over the warp with 6 shuffles: afterwards lane 8*v holds the
-// warp total of value v (v = 0..3).
-__device__ __forceinline__ float reduce4(float v0, float v1, float v2, float v3) {
-  int lane = threadIdx.x & 31;
-  bool b4 = lane & 16;
-  float s0 = b4 ? v0 : v2, s1 = b4 ? v1 : v3;
-  float k0 = b4 ? v2 : v0, k1 = b4 ? v3 : v1;
-  k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
-  k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
-  bool b3 = lane & 8;
-  float s = b3 ? k0 : k1;
-  float v = b3 ? k1 : k0;
-  v += __shfl_xor_sync(0xffffffffu, s, 8);
-  v += __shfl_xor_sync(0xffffffffu, v, 4);
-  v += __shfl_xor_sync(0xffffffffu, v, 2);
-  v += __shfl_xor_sync(0xffffffffu, v, 1);
-  return v;  // lane with bits (b4, b3): value 2*b4 + b3
-}
-
-__device__ __forceinline__ int reduce4_index(int lane) { return ((lane >> 4) & 1) * 2 + ((lane >> 3) & 1); }
-
-// Sum 10 values over the warp with 12 shuffles (a transposed butterfly: at
-// each step a lane keeps one half of its values and receives its partner's
-// share of that half). Afterwards lane l holds the warp total of value
-// reduce10_index(l); lanes where that is -1 hold padding.
-__device__ __forceinline__ float reduce10(const float* v) {
-  int lane = threadIdx.x & 31;
-  bool b = lane & 16;
-  float h[6];
-#pragma unroll
-  for (int j = 0; j < 5; j++) {
-    float send = b ? v[j] : v[j + 5];
-    float keep = b ? v[j + 5] : v[j];
-    h[j] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-  }
-  h[5] = 0.f;
-  b = lane & 8;
-  float g[4];
-#pragma unroll
-  for (int j = 0; j < 3; j++) {
-    float send = b ? h[j] : h[j + 3];
-    float keep = b ? h[j + 3] : h[j];
-    g[j] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-  }
-  g[3] = 0.f;
-  b = lane & 4;
-  float e[2];
-#pragma unroll
-  for (int j = 0; j < 2; j++) {
-    float send = b ? g[j] : g[j + 2];
-    float keep = b ? g[j + 2] : g[j];
-    e[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-  }
-  b = lane & 2;
-  float send = b ? e[0] : e[1];
-  float d = (b ? e[1] : e[0]) + __shfl_xor_sync(0xffffffffu, send, 2);
-  d += __shfl_xor_sync(0xffffffffu, d, 1);
-  return d;
-}
-
-// Value index held by lane l after reduce10: value (c + 3 b3) + 5 b4 with
-// c = b1 + 2 b2, for even lanes with c < 3 and c + 3 b3 < 5; otherwise -1.
-__device__ __forceinline__ int reduce10_index(int lane) {
-  if (lane & 1) return -1;
-  int c = ((lane >> 1) & 1) + 2 * ((lane >> 2) & 1);
-  if (c >= 3) return -1;
-  int hj = c + 3 * ((lane >> 3) & 1);
-  if (hj >= 5) return -1;
-  return hj + 5 * ((lane >> 4) & 1);
-}
-
-// One accepted node, monopole far field, for the lane's targets: query-side
-// gradient and force into the lane's accumulators, the node-side adjoint
-// (A_X, A_M) reduced over the warp and added to the node's slots.
-template <bool CUT, bool PER>
-__device__ __forceinline__ void far_mono_adjoint(const float4& A, const LaneTargets& Q, const float* wx,
-                                                 const float* wy, const float* wz, int nslot, const WalkParams& P,
-                                                 bool want_force, float* gx, float* gy, float* gz, float* fx,
-                                                 float* fy, float* fz, float* __restrict__ na, int lane, int r4) {
-  const float M = A.w;
-  float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
-#pragma unroll
-  for (int t = 0; t < kTPL; t++) {
-    if (t >= nslot) break;
-    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
-    if (PER) {
-      rx = min_image(rx, P);
-      ry = min_image(ry, P);
-      rz = min_image(rz, P);
-    }
-    float r2 = rx * rx + ry * ry + rz * rz;
-    float ir = rsqrtf(r2 + P.eps2);
-    float ih = ir * ir;
-    float ir3 = ir * ih;
-    float ir5 = ir3 * ih;
-    float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
-    float att = 1.0f, cc = 0.0f;
-    if (CUT) attenuation(r2, ir3, P, att, cc);
-    float lin = att * ir3;
-    float mlin = M * lin, mrad = M * (rw * (3.0f * att * ir5 + cc));
-    v3 -= lin * rw;  // A_M
-    float qx_ = mrad * rx - mlin * wx[t];
-    float qy_ = mrad * ry - mlin * wy[t];
-    float qz_ = mrad * rz - mlin * wz[t];
-    if (want_force) {
-      fx[t] -= mlin * rx;
-      fy[t] -= mlin * ry;
-      fz[t] -= mlin * rz;
-    }
-    gx[t] += qx_;
-    gy[t] += qy_;
-    gz[t] += qz_;
-    v0 -= qx_;
-    v1 -= qy_;
-    v2 -= qz_;
-  }
-  float tot = reduce4(v0, v1, v2, v3);
-  if ((lane & 7) == 0) atomicAdd(&na[r4], tot);
-}
-
-// One accepted node with the quadrupole (Plummer softening, no cutoff, not
-// periodic): as far_mono_adjoint plus the quadrupole's terms and the node's
-// G = sym d(w . a_q)/dS, ten values reduced over the warp.
-__device__ __forceinline__ void far_quad_adjoint(const NodeRec* nd, const float4& A, const LaneTargets& Q,
-                                                 const float* wx, const float* wy, const float* wz, int nslot,
-                                                 const WalkParams& P, bool want_force, float* gx, float* gy,
-                                                 float* gz, float* fx, float* fy, float* fz, float* __restrict__ na,
-                                                 int r10) {
-  const float4 Qd = __ldg(&nd->quad);
-  const float4 X = __ldg(&nd->quad2);
-  const float M = A.w;
-  const float Sxx = Qd.x, Syy = Qd.y, Szz = Qd.z, Sxy = Qd.w, Sxz = X.x, Syz = X.y;
-  const float tr15 = 1.5f * (Sxx + Syy + Szz);
-  float v[10], vb = 0.f;  // vb: the (r.w) I part of G, added to its diagonal once
-#pragma unroll
-  for (int j = 0; j < 10; j++) v[j] = 0.f;
-#pragma unroll
-  for (int t = 0; t < kTPL; t++) {
-    if (t >= nslot) break;
-    float rx = Q.x[t] - A.x, ry = Q.y[t] - A.y, rz = Q.z[t] - A.z;
-    float r2 = rx * rx + ry * ry + rz * rz;
-    float ir = rsqrtf(r2 + P.eps2);
-    float ih = ir * ir;
-    float ir3 = ir * ih;
-    float ir5 = ir3 * ih;
-    float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
-    float mlin = M * ir3, mrad = M * (rw * (3.0f * ir5));
-    v[3] -= ir3 * rw;  // A_M
-    float sx = Sxx * rx + Sxy * ry + Sxz * rz;
-    float sy = Sxy * rx + Syy * ry + Syz * rz;
-    float sz = Sxz * rx + Syz * ry + Szz * rz;
-    float swx = Sxx * wx[t] + Sxy * wy[t] + Sxz * wz[t];
-    float swy = Sxy * wx[t] + Syy * wy[t] + Syz * wz[t];
-    float swz = Sxz * wx[t] + Syz * wy[t] + Szz * wz[t];
-    float rsr = rx * sx + ry * sy + rz * sz;
-    float rsw = rx * swx + ry * swy + rz * swz;
-    float ir7 = ir5 * ih, ir9 = ir7 * ih;
-    float c1 = 3.0f * ir5;
-    float a1 = 5.0f * ir7 * rw;
-    float a3 = 15.0f * ir7 * rsw - 52.5f * ir9 * rsr * rw;
-    float cw = tr15 * ir5 - 7.5f * ir7 * rsr - mlin;
-    float cr = mrad - tr15 * a1 - a3;
-    float c2 = 3.0f * a1;
-    float qx_ = c1 * swx - c2 * sx + cw * wx[t] + cr * rx;
-    float qy_ = c1 * swy - c2 * sy + cw * wy[t] + cr * ry;
-    float qz_ = c1 * swz - c2 * sz + cw * wz[t] + cr * rz;
-    // G, off-diagonals doubled (halved once below)
-    float al = 1.5f * ir5, ga = 7.5f * ir7 * rw;
-    vb += al * rw;
-    float ux = 2.0f * al * wx[t] - ga * rx;
-    float uy = 2.0f * al * wy[t] - ga * ry;
-    float uz = 2.0f * al * wz[t] - ga * rz;
-    v[4] += ux * rx;
-    v[5] += uy * ry;
-    v[6] += uz * rz;
-    v[7] += ux * ry + uy * rx;
-    v[8] += ux * rz + uz * rx;
-    v[9] += uy * rz + uz * ry;
-    if (want_force) {
-      float cf = ir5 * (tr15 - 7.5f * rsr * ih) - mlin;
-      fx[t] += cf * rx + c1 * sx;
-      fy[t] += cf * ry + c1 * sy;
-      fz[t] += cf * rz + c1 * sz;
-    }
-    gx[t] += qx_;
-    gy[t] += qy_;
-    gz[t] += qz_;
-    v[0] -= qx_;
-    v[1] -= qy_;
-    v[2] -= qz_;
-  }
-  v[4] += vb;
-  v[5] += vb;
-  v[6] += vb;
-  v[7] *= 0.5f;
-  v[8] *= 0.5f;
-  v[9] *= 0.5f;
-  float tot = reduce10(v);
-  if (r10 >= 0) atomicAdd(&na[r10], tot);
-}
-
-// Fused force + adjoint walk. Per target slot: the query-side gradient
-// (written to gq in sorted order); per accepted node: A_X, A_M, G summed over
-// the group and added to node_adj; per near source particle: (dx, dm) summed
-// over the group and added to part_adj. Forces are written when out != null.
-// Every node-side term is linear in the cotangent, so inactive slots (zero
-// cotangent) add nothing.
-//
-// Per (target, node) pair with r = q - X, h = |r|^2 + eps^2, ir = h^-1/2,
-// lin = att ir^3, rad = (3 att ir^5 + cc)(r.w), and S the node's second
-// moment, the query-side gradient is
-//   M (rad r - lin w) + 3 ir^5 S w - 15 ir^7 (r.w) S r
-//     + (1.5 tr(S) ir^5 - 7.5 ir^7 rSr) w - (7.5 tr(S) ir^7 (r.w) + a3) r,
-// a3 = 15 ir^7 (r.Sw) - 52.5 ir^9 (rSr)(r.w), and the node-side terms are
-// A_X = -(that gradient), A_M = -lin (r.w) and
-// G = 1.5 ir^5 (w r^T + r w^T) + 1.5 ir^5 (r.w) I - 7.5 ir^7 (r.w) r r^T.
-template <bool QUAD, bool CUT, bool PER>
-__global__ void __launch_bounds__(128, kAdjointWalkMinBlocks)
-    adjoint_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, const float* __restrict__ cot,
-                        float* __restrict__ out, float* __restrict__ gq, float* __restrict__ node_adj,
-                        float* __restrict__ part_adj) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t ng = min(*G.ngroups, G.capacity);
-  const int r4 = reduce4_index(lane), r10 = reduce10_index(lane);
-  for (;;) {
-    uint32_t gw = next_group(G);
-    if (gw >= ng) break;
-    int4 gr = G.groups[gw];
-    if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
-    LaneTargets Q;
-    load_targets(G, gr, lane, Q);
-    const int nslot = (gr.y - gr.x + 31) / 32;  // warp-uniform: the target slots in use
-    float wx[kTPL], wy[kTPL], wz[kTPL];
-#pragma unroll
-    for (int t = 0; t < kTPL; t++) {
-      const uint32_t o = Q.act[t] ? G.perm[Q.idx[t]] : 0u;
-      wx[t] = Q.act[t] ? cot[3 * o] : 0.f;
-      wy[t] = Q.act[t] ? cot[3 * o + 1] : 0.f;
-      wz[t] = Q.act[t] ? cot[3 * o + 2] : 0.f;
-    }
-    float gmin[3], gmax[3];
-    group_box(Q, gmin, gmax);
-    int2 rt = T.roots[gr.z];
-    float gx[kTPL], gy[kTPL], gz[kTPL];  // query-side gradient
-    float fx[kTPL], fy[kTPL], fz[kTPL];  // force
-#pragma unroll
-    for (int t = 0; t < kTPL; t++) gx[t] = gy[t] = gz[t] = fx[t] = fy[t] = fz[t] = 0.f;
-    int k = rt.x;
-    while (k < rt.y) {
-      const NodeRec* nd = T.nodes + k;
-      int4 tp = __ldg(&nd->topo);
-      float4 A = __ldg(&nd->com);
-      float4 C = __ldg(&nd->cell);
-      if (PER) C = cell_image(C, gmin, gmax, P);
-      if (A.w == 0.0f || (CUT && P.prune_r2 > 0.0f && prune_node(C, gmin, gmax, P.prune_r2))) {
-        k = tp.z;  // mass-zero and pruned nodes are skipped
-        continue;
-      }
-      float d2, rc2;
-      if (accept_node(C, gmin, gmax, P.beta, d2, rc2)) {
-        float* na = node_adj + static_cast<int64_t>(k) * kNodeAdj;
-        if (QUAD && quad_order(d2, rc2, P)) {
-          far_quad_adjoint(nd, A, Q, wx, wy, wz, nslot, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, r10);
-        } else {
-          far_mono_adjoint<CUT, PER>(A, Q, wx, wy, wz, nslot, P, out != nullptr, gx, gy, gz, fx, fy, fz, na, lane,
-                                     r4);
-        }
-        k = tp.z;
-      } else if (tp.w & kLeafFlag) {
-        // the self pair (r = 0) only occurs when the leaf overlaps the group
-        const bool selfchk = G.self && tp.x < gr.y && gr.x < tp.y;
-        for (int j = tp.x; j < tp.y; j++) {
-          float4 s = __ldg(&T.sp[j]);
-          float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll
-          for (int t = 0; t < kTPL; t++) {
-            if (t >= nslot) break;
-            float rx = Q.x[t] - s.x, ry = Q.y[t] - s.y, rz = Q.z[t] - s.z;
-            if (PER) {
-              rx = min_image(rx, P);
-              ry = min_image(ry, P);
-              rz = min_image(rz, P);
-            }
-            float r2 = rx * rx + ry * ry + rz * rz;
-            float ir = rsqrtf(r2 + P.eps2);
-            float ih = ir * ir;
-            float ir3 = ir * ih;
-            float ir5 = ir3 * ih;
-            float rw = rx * wx[t] + ry * wy[t] + rz * wz[t];
-            float att = 1.0f, cc = 0.0f;
-            if (CUT) attenuation(r2, ir3, P, att, cc);
-            float lin = att * ir3;
-            float m = (selfchk && j == Q.idx[t]) ? 0.0f : s.w;
-            float mlin = m * lin, mrad = m * (rw * (3.0f * att * ir5 + cc));
-            float qx_ = mrad * rx - mlin * wx[t];
-            float qy_ = mrad * ry - mlin * wy[t];
-            float qz_ = mrad * rz - mlin * wz[t];
-            gx[t] += qx_;
-            gy[t] += qy_;
-            gz[t] += qz_;
-            if (out) {
-              fx[t] -= mlin * rx;
-              fy[t] -= mlin * ry;
-              fz[t] -= mlin * rz;
-            }
-            a0 -= qx_;
-            a1 -= qy_;
-            a2 -= qz_;
-            a3 -= lin * rw;  // zero for the self pair (r = 0) and inactive slots (w = 0)
-          }
-          float tot = reduce4(a0, a1, a2, a3);
-          if ((lane & 7) == 0) atomicAdd(&part_adj[static_cast<int64_t>(j) * kPartAdj + r4], tot);
-        }
-        k = tp.z;
-      } else {
-        k++;
-      }
-    }
-#pragma unroll
-    for (int t = 0; t < kTPL; t++) {
-      if (Q.act[t]) {
-        int64_t i = Q.idx[t];
-        gq[3 * i] = gx[t];
-        gq[3 * i + 1] = gy[t];
-        gq[3 * i + 2] = gz[t];
-        if (out) {
-          const uint32_t o = G.perm[i];  // reloaded: not kept live through the walk
-          out[3 * o] = fx[t];
-          out[3 * o + 1] = fy[t];
-          out[3 * o + 2] = fz[t];
-        }
-      }
-    }
-  }
-}
-
-// Interaction counts of the force and adjoint walks: the same traversal and
-// the same decisions without the sums, so the hot walks carry no counters.
-// Per group: accepted nodes (and those that take the quadrupole) and near
-// source particles, each times the group's targets.
-template <bool QUAD, bool CUT, bool PER>
-__global__ void __launch_bounds__(128)
-    count_walk_kernel(WalkTree T, WalkTargets G, WalkParams P, unsigned long long* __restrict__ counters) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t ng = min(*G.ngroups, G.capacity);
-  for (;;) {
-    uint32_t gw = next_group(G);
-    if (gw >= ng) break;
-    int4 gr = G.groups[gw];
-    if (gr.x < G.tbeg || gr.x >= G.tend) continue;
-    LaneTargets Q;
-    load_targets(G, gr, lane, Q);
-    float gmin[3], gmax[3];
-    group_box(Q, gmin, gmax);
-    int2 rt = T.roots[gr.z];
-    unsigned long long nfar = 0, nnear = 0, nquad = 0;
-    int k = rt.x;
-    while (k < rt.y) {
-      const NodeRec* nd = T.nodes + k;
-      const int4 tp = __ldg(&nd->topo);
-      const float4 A = __ldg(&nd->com);
-      float4 C = __ldg(&nd->cell);
-      if (PER) C = cell_image(C, gmin, gmax, P);
-      if (A.w == 0.0f || (CUT && P.prune_r2 > 0.0f && prune_node(C, gmin, gmax, P.prune_r2))) {
-        k = tp.z;
-        continue;
-      }
-      float d2, rc2;
-      if (accept_node(C, gmin, gmax, P.beta, d2, rc2)) {
-        nfar++;
-        if (QUAD && quad_order(d2, rc2, P)) nquad++;
-        k = tp.z;
-      } else if (tp.w & kLeafFlag) {
-        nnear += static_cast<unsigned long long>(tp.y - tp.x);
-        k = tp.z;
-      } else {
-        k++;
-      }
-    }
-    if (lane == 0) {
-      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
-      atomicAdd(&counters[0], nfar * na);
-      atomicAdd(&counters[1], nnear * na);
-      atomicAdd(&counters[2], nquad * na);
-    }
-  }
-}
+// One of the five variants (quadrupole; periodic and/or cutoff) of a walk
+// kernel of namespace NS.
+#define SBH_NT_SELECT(NS, KERNEL, QUADV, PERV, CUTV)                                          \
+  ((QUADV)  ? NS::KERNEL<true, false, false>                                                  \
+   : (PERV) ? ((CUTV) ? NS::KERNEL<false, true, true> : NS::KERNEL<false, false, true>)       \
+            : ((CUTV) ? NS::KERNEL<false, true, false> : NS::KERNEL<false, false, false>))
 
 // Node adjoints -> difference arrays over each node's particle range. Per
 // node (coordinates relative to the system's box centre c0, Xc = X - c0):
@@ -1364,100 +716,6 @@ __global__ void adjoint_combine_kernel(const float4* __restrict__ sp, const uint
                 (x[0] * Gx[0] + x[1] * Gx[1] + x[2] * Gx[2]) -
                 2.0 * (x[0] * c.v[10] + x[1] * c.v[11] + x[2] * c.v[12]) + c.v[13];
     dm[o] = static_cast<float>(static_cast<double>(part_adj[kPartAdj * i + 3]) + wq);
-  }
-}
-
-// Winding number (include/kernel.h:73-80): w(q) = sum m n.(p - q) / (4 pi (|p-q|^3 + 1e-5));
-// far field: node mass and mass-weighted mean normal at the COM, as the
-// reference's trees aggregate them (include/tree3d.h:255-264, 310-327).
-__global__ void __launch_bounds__(128, 4)
-    wn_walk_kernel(WalkTree T, WalkTargets G, float beta, float* __restrict__ out,
-                   unsigned long long* __restrict__ counters) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t ng = min(*G.ngroups, G.capacity);
-  const float k4pi = 0.07957747154594767f;  // 1 / (4 pi)
-  for (;;) {
-    uint32_t gw = next_group(G);
-    if (gw >= ng) break;
-    int4 gr = G.groups[gw];
-    if (gr.x < G.tbeg || gr.x >= G.tend) continue;  // another rank's targets (warp-uniform)
-    LaneTargets Q;
-    load_targets(G, gr, lane, Q);
-    const int nslot = (gr.y - gr.x + 31) / 32;  // warp-uniform: the target slots in use
-    float gmin[3], gmax[3];
-    group_box(Q, gmin, gmax);
-    int2 rt = T.roots[gr.z];
-    float far[kTPL], near[kTPL], comp[kTPL];
-#pragma unroll
-    for (int t = 0; t < kTPL; t++) far[t] = near[t] = comp[t] = 0.f;
-    uint32_t nfar = 0, nnear = 0;  // per group (a group's counts stay below n)
-    // Pre-order walk. The next node is known once this node's opening test
-    // is done, so its opening data is loaded before this node's terms are
-    // evaluated and the load latency hides behind that arithmetic.
-    int k = rt.x;
-    int4 tp = make_int4(0, 0, rt.y, 0);
-    float4 A = make_float4(0.f, 0.f, 0.f, 0.f), C = A;
-    if (k < rt.y) {
-      tp = __ldg(&T.nodes[k].topo);
-      A = __ldg(&T.nodes[k].com);
-      C = __ldg(&T.nodes[k].cell);
-    }
-    while (k < rt.y) {
-      const bool live = A.w != 0.0f;  // mass-zero nodes are skipped
-      const bool acc = live && accept_node(C, gmin, gmax, beta);
-      const bool leaf = (tp.w & kLeafFlag) != 0;
-      const int next = (!live || acc || leaf) ? tp.z : k + 1;
-      int4 tpn = tp;
-      float4 An = A, Cn = C;
-      if (next < rt.y) {
-        tpn = __ldg(&T.nodes[next].topo);
-        An = __ldg(&T.nodes[next].com);
-        Cn = __ldg(&T.nodes[next].cell);
-      }
-      if (acc) {
-        float4 N = __ldg(&T.nnrm[k]);
-#pragma unroll
-        for (int t = 0; t < kTPL; t++) {
-          if (t >= nslot) break;
-          float dx = A.x - Q.x[t], dy = A.y - Q.y[t], dz = A.z - Q.z[t];
-          float dist = sqrtf(dx * dx + dy * dy + dz * dz);
-          float nd_ = N.x * dx + N.y * dy + N.z * dz;
-          far[t] += A.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
-        }
-        nfar++;
-      } else if (live && leaf) {
-        float a[kTPL];
-#pragma unroll
-        for (int t = 0; t < kTPL; t++) a[t] = 0.f;
-        for (int j = tp.x; j < tp.y; j++) {
-          float4 s = __ldg(&T.sp[j]);
-          float4 nrm = __ldg(&T.sn[j]);
-#pragma unroll
-          for (int t = 0; t < kTPL; t++) {
-            if (t >= nslot) break;
-            float dx = s.x - Q.x[t], dy = s.y - Q.y[t], dz = s.z - Q.z[t];
-            float dist = sqrtf(dx * dx + dy * dy + dz * dz);
-            float nd_ = nrm.x * dx + nrm.y * dy + nrm.z * dz;
-            a[t] += s.w * nd_ * k4pi / (dist * dist * dist + 1e-5f);
-          }
-        }
-#pragma unroll
-        for (int t = 0; t < kTPL; t++) kahan_add(near[t], comp[t], a[t]);
-        nnear += static_cast<uint32_t>(tp.y - tp.x);
-      }
-      k = next;
-      tp = tpn;
-      A = An;
-      C = Cn;
-    }
-#pragma unroll
-    for (int t = 0; t < kTPL; t++)
-      if (Q.act[t]) out[G.perm[Q.idx[t]]] = far[t] + near[t];
-    if (counters && lane == 0) {
-      unsigned long long na = static_cast<unsigned long long>(gr.y - gr.x);
-      atomicAdd(&counters[0], nfar * na);
-      atomicAdd(&counters[1], nnear * na);
-    }
   }
 }
 
@@ -1623,6 +881,7 @@ struct Header {
   int32_t normals;
   int32_t adjoint;
   int64_t tbeg = 0, tend = INT64_MAX;  // sorted target range the walks serve
+  int32_t group_size = kGroup;         // most targets per group (selects the walk kernels)
   // the last evaluation: 0 none, 1 a force or adjoint walk (its interaction
   // counts are recounted on demand), 2 the winding number (counted in-walk)
   int32_t last_walk = 0;
@@ -1906,9 +1165,8 @@ int refresh_counts(cudaStream_t stream, const void* ws, const Header& h, const L
   WalkParams wp = walk_params(&p);
   bool cut = p.cutoff > 0.0f;
   bool per = p.periodic != 0;
-  auto k = p.quadrupole ? count_walk_kernel<true, false, false>
-           : per ? (cut ? count_walk_kernel<false, true, true> : count_walk_kernel<false, false, true>)
-                 : (cut ? count_walk_kernel<false, true, false> : count_walk_kernel<false, false, false>);
+  auto k = h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, count_walk_kernel, p.quadrupole, per, cut)
+                                         : SBH_NT_SELECT(tpl2, count_walk_kernel, p.quadrupole, per, cut);
   e = launch_walk(stream, L.work, h.n + h.nseg, k, tree_view(L), self_targets(L, hr), wp, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   std::lock_guard<std::mutex> lk(g_reg_mu);
@@ -1936,6 +1194,14 @@ int sbh_native_set_group_size(cudaStream_t stream, void* workspace, size_t works
   group_nodes_kernel<<<gs(static_cast<int64_t>(L.cap)), 256, 0, stream>>>(
       L.nodes, L.meta, h.nseg > 1 ? L.sseg : nullptr, L.groups, h.n + h.nseg + 1, group_size, L.meta + 1,
       static_cast<uint32_t*>(workspace));
+  {
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    auto it = g_registry.find(workspace);
+    if (it != g_registry.end()) {
+      it->second.group_size = group_size;
+      it->second.counts_fresh = it->second.last_walk != 1;
+    }
+  }
   return check_launch("sbh_native_set_group_size");
 }
 
@@ -1976,9 +1242,8 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   int64_t mg = h.n + h.nseg;
   bool cut = params->cutoff > 0.0f;
   bool per = params->periodic != 0;
-  auto k = params->quadrupole ? force_walk_kernel<true, false, false>
-           : per ? (cut ? force_walk_kernel<false, true, true> : force_walk_kernel<false, false, true>)
-                 : (cut ? force_walk_kernel<false, true, false> : force_walk_kernel<false, false, false>);
+  auto k = h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, force_walk_kernel, params->quadrupole, per, cut)
+                                         : SBH_NT_SELECT(tpl2, force_walk_kernel, params->quadrupole, per, cut);
   e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h), wp, force_out);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   remember_walk(workspace, 1, params);
@@ -2006,9 +1271,8 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   WalkParams wp = walk_params(params);
   bool cut = params->cutoff > 0.0f;
   bool per = params->periodic != 0;
-  auto k = params->quadrupole ? adjoint_walk_kernel<true, false, false>
-           : per ? (cut ? adjoint_walk_kernel<false, true, true> : adjoint_walk_kernel<false, false, true>)
-                 : (cut ? adjoint_walk_kernel<false, true, false> : adjoint_walk_kernel<false, false, false>);
+  auto k = h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, adjoint_walk_kernel, params->quadrupole, per, cut)
+                                         : SBH_NT_SELECT(tpl2, adjoint_walk_kernel, params->quadrupole, per, cut);
   e = launch_walk(stream, L.work, n + h.nseg, k, tree_view(L), self_targets(L, h), wp, cotangent, force_out, L.gq,
                   L.node_adj, L.part_adj);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
@@ -2098,7 +1362,8 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1), 0, INT64_MAX};
-  e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, wn_walk_kernel, tree_view(L), G, beta, out, L.counters);
+  e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, tpl2::wn_walk_kernel, tree_view(L), G, beta, out,
+                  L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   remember_walk(workspace, 2, nullptr);
   return check_launch("sbh_native_winding_number");

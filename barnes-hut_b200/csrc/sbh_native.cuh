@@ -24,22 +24,15 @@ struct NodeRec {
 static_assert(sizeof(NodeRec) == 80, "NodeRec must be 80 bytes");
 
 constexpr int kLeafFlag = 0x100;
-// Targets per lane in the walks (a group of 32 * kTPL targets per warp).
-// Measured on a B200, adjoint walk over 8 x 2^20 Plummer particles at
-// quadrupole radius 1.6: 410 ms with 2 per lane (7 blocks per SM), 389 ms
-// with 3 (6 blocks, 80 registers), 411 ms with 4 (4 blocks); larger groups
-// share each node's load, opening test and warp reduction among more
-// targets at the price of a larger box and more registers.
-#ifndef SBH_TARGETS_PER_LANE
-#define SBH_TARGETS_PER_LANE 3
-#endif
-constexpr int kTPL = SBH_TARGETS_PER_LANE;
-constexpr int kGroup = 32 * kTPL;  // targets per group (one warp)
+// Most targets per group: three per lane of a warp. Groups of at most
+// kGroupTwoSlots targets are walked by the two-slot kernels.
+constexpr int kGroupTwoSlots = 64;
+constexpr int kGroup = 96;  // targets per group built by default (one warp, three per lane)
 #ifndef SBH_QUERY_GROUP
 #define SBH_QUERY_GROUP 32
 #endif
-constexpr int kQueryGroup = SBH_QUERY_GROUP;  // targets per group of external queries (<= 32 * kTPL)
-static_assert(kQueryGroup <= 32 * kTPL, "a query group must fit the lanes' target slots");
+constexpr int kQueryGroup = SBH_QUERY_GROUP;  // targets per group of external queries
+static_assert(kQueryGroup <= kGroupTwoSlots, "query groups are walked by the two-slot kernels");
 constexpr int kNodeAdj = 12;    // per-node adjoint floats: A_X(3) A_M(1) G(6) pad(2)
 constexpr int kPartAdj = 4;     // per-particle adjoint floats: dx(3) dm(1)
 

@@ -34,21 +34,25 @@ import sbh_b200 as B
 
 @dataclass
 class Gravity:
+    """Softened self-gravity on the native tree. group_size: most targets per
+    walk group (None: the library's default of 96, best for clustered
+    systems; 64 suits near-uniform ones such as a perturbed lattice)."""
     beta: float = 1.0 / 0.6
     softening: float = 2e-3
     leaf_size: int = 16
     quadrupole: bool = True
+    group_size: int | None = None
 
     def __post_init__(self):
         self.tree = B.NativeTree()
 
     def accel(self, x: torch.Tensor, m: torch.Tensor) -> torch.Tensor:
-        self.tree.build(x, m, leaf_size=self.leaf_size, with_adjoint=False)
+        self.tree.build(x, m, leaf_size=self.leaf_size, with_adjoint=False, group_size=self.group_size)
         return self.tree.force(beta=self.beta, softening=self.softening, quadrupole=self.quadrupole)
 
     def accel_vjp(self, x: torch.Tensor, m: torch.Tensor, w: torch.Tensor):
         """(J_a(x)^T w, d(w . a)/dm)."""
-        self.tree.build(x, m, leaf_size=self.leaf_size, with_adjoint=True)
+        self.tree.build(x, m, leaf_size=self.leaf_size, with_adjoint=True, group_size=self.group_size)
         _, gx, gm = self.tree.force_vjp(w, beta=self.beta, softening=self.softening, quadrupole=self.quadrupole,
                                         want_force=False)
         return gx, gm

@@ -323,7 +323,7 @@ def trajectory_measurement(torch, dev, flush):
     v0 = torch.zeros_like(x0)
     mt = torch.tensor(m, device=dev)
     tgt = torch.tensor(target, device=dev)
-    grav = T.Gravity(beta=1.0 / 0.6, softening=2e-3, leaf_size=LEAF)
+    grav = T.Gravity(beta=1.0 / 0.6, softening=2e-3, leaf_size=LEAF, group_size=64)  # near-uniform lattice
     steps, dt, ck = 50, 1e-3, 10
     T.kdk(x0, v0, mt, 1, dt, grav)  # warm-up (workspaces)
     torch.cuda.synchronize()
@@ -426,7 +426,8 @@ def treepm_measurement(B, torch, dev, flush):
     a 128^3 perturbed lattice (2,097,152 particles, rms displacement 0.5
     cells) in a periodic box of 128 mesh cells, r_split 1 cell, softening 0.1,
     beta 1.7, cells beyond 4 r_split pruned. The native periodic walk (build +
-    force; also timed with target groups of 32) against the reference's algorithm on this GPU (dense octree8 of
+    force with target groups of 64, the size for walks bounded by a prune
+    radius; also timed with 32 and 96) against the reference's algorithm on this GPU (dense octree8 of
     depth 6, the reference's traversal with the same prune), both checked
     against the FP64 minimum-image erfc direct sum on 1,024 particles."""
     k = 128
@@ -483,13 +484,15 @@ def treepm_measurement(B, torch, dev, flush):
         return tot / reps, out
 
     ours32_ms, _ = timed(lambda: ours(32), 3)
-    ours_ms, _ = timed(ours, 3)
+    ours96_ms, _ = timed(lambda: ours(B.native_group_size()), 3)
+    ours_ms, _ = timed(lambda: ours(64), 3)
     st = tree.stats()
     rel = float(torch.linalg.norm(F[idx].double() - ref) / torch.linalg.norm(ref))
     ref_ms, o8 = timed(refalg, 1)
     rel_o8 = float(torch.linalg.norm(o8[idx].double() - ref) / torch.linalg.norm(ref))
     return dict(particles=int(pts.shape[0]), box_cells=k, r_split=rs, prune_radius=mult * rs, softening=eps,
-                beta=beta, ms=ours_ms, ms_with_32_target_groups=ours32_ms,
+                beta=beta, group_size=64, ms=ours_ms, ms_with_32_target_groups=ours32_ms,
+                ms_with_96_target_groups=ours96_ms,
                 rel_l2_vs_fp64_direct=rel,
                 interactions_per_particle=(st["far"] + st["near"]) / pts.shape[0],
                 octree8_reference_algorithm_ms=ref_ms, octree8_rel_l2_vs_fp64_direct=rel_o8,
