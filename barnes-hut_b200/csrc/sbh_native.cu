@@ -454,42 +454,59 @@ __global__ void roots_kernel(const int64_t* __restrict__ sorted_seg_off, int nse
 // group lies inside the cell of a node with more than G particles, so its
 // bounding box is compact (runs of consecutive Morton positions can straddle
 // distant cells), and the chunks fill the lanes better than one group per
-// child run. Slots come from an atomic counter: the group order varies
-// between runs, each group's result does not. Every group holds at least one
-// particle, so n + systems + 1 slots always suffice.
-__device__ __forceinline__ void emit_chunks(int4* groups, uint32_t* count, int64_t cap, int s0, int s1, int sys,
-                                            int G, uint32_t* status) {
+// child run. Every group holds at least one particle, so n + systems + 1
+// slots always suffice.
+//
+// The groups are stored deepest first: a counting pass (COUNT) tallies them
+// by the level of the cells they come from, group_bins_kernel turns the
+// tallies into cursors, and the emitting pass writes each group at its
+// level's cursor. Deeper cells lie in denser regions, where a group has more
+// interactions, so the persistent walks hand out the expensive groups first
+// and the cheap ones fill the tail. Within a level the order comes from
+// atomics and varies between runs; each group's result does not.
+constexpr int kGroupBins = 24;  // levels 0..22 (a run of children sits one level below its parent)
+
+template <bool COUNT>
+__device__ __forceinline__ void emit_chunks(int4* groups, uint32_t* bins, int64_t cap, int s0, int s1, int sys,
+                                            int G, int level, uint32_t* status) {
   int ng = (s1 - s0 + G - 1) / G;
   if (ng <= 0) return;
-  uint32_t slot = atomicAdd(count, static_cast<uint32_t>(ng));
+  const int bin = kGroupBins - 1 - min(level, kGroupBins - 1);
+  if (COUNT) {
+    atomicAdd(&bins[bin], static_cast<uint32_t>(ng));
+    return;
+  }
+  uint32_t slot = atomicAdd(&bins[bin], static_cast<uint32_t>(ng));
   for (int g = 0; g < ng; g++) {
     int s = s0 + g * G;
     if (slot + g < cap)
-      groups[slot + g] = make_int4(s, min(s + G, s1), sys, 0);
+      groups[slot + g] = make_int4(s, min(s + G, s1), sys, level);
     else
       raise_status(status, SBH_DEV_ITER_LIMIT);
   }
 }
 
+template <bool COUNT>
 __global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
                                    const uint32_t* __restrict__ sseg, int4* __restrict__ groups, int64_t cap, int G,
-                                   uint32_t* __restrict__ count, uint32_t* status) {
+                                   uint32_t* __restrict__ bins, uint32_t* status) {
   uint32_t nn = *nn_ptr;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
     int4 t = nodes[k].topo;
     int cnt = t.y - t.x;
     bool leaf = (t.w & kLeafFlag) != 0;
-    bool root = (t.w & 0xFF) == 0;
+    int level = t.w & 0xFF;
+    bool root = level == 0;
     int sys = sseg ? static_cast<int>(sseg[t.x]) : 0;
     if (leaf || cnt <= G) {
-      if (root || (leaf && cnt > G)) emit_chunks(groups, count, cap, t.x, t.y, sys, G, status);
+      if (root || (leaf && cnt > G)) emit_chunks<COUNT>(groups, bins, cap, t.x, t.y, sys, G, level, status);
       continue;
     }
     int run_s = -1, run_e = -1;
     for (uint32_t c = k + 1; c < static_cast<uint32_t>(t.z) && c < nn;) {
       int4 tc = nodes[c].topo;
       if (tc.y - tc.x > G) {
-        if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, G, status);
+        if (run_s >= 0) emit_chunks<COUNT>(groups, bins, cap, run_s, run_e, sys, G, level + 1, status);
         run_s = -1;
       } else {
         if (run_s < 0) run_s = tc.x;
@@ -498,8 +515,21 @@ __global__ void group_nodes_kernel(const NodeRec* __restrict__ nodes, const uint
       if (static_cast<uint32_t>(tc.z) <= c) break;  // malformed skip: never loop
       c = static_cast<uint32_t>(tc.z);
     }
-    if (run_s >= 0) emit_chunks(groups, count, cap, run_s, run_e, sys, G, status);
+    if (run_s >= 0) emit_chunks<COUNT>(groups, bins, cap, run_s, run_e, sys, G, level + 1, status);
   }
+}
+
+// Tallies per level -> cursors (exclusive offsets, deepest level first) and
+// the group count.
+__global__ void group_bins_kernel(uint32_t* bins, uint32_t* group_count) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t run = 0;
+  for (int b = 0; b < kGroupBins; b++) {
+    uint32_t c = bins[b];
+    bins[b] = run;
+    run += c;
+  }
+  *group_count = run;
 }
 
 __global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx, int64_t n,
@@ -797,6 +827,7 @@ struct Layout {
   int4* groups;
   uint32_t* work;  // persistent-walk work counters
   uint32_t* meta;  // [0] node count, [1] group count, [2] which ping-pong buffer holds perm
+  uint32_t* gbins;  // per-level group tallies, then cursors (group_nodes_kernel)
   unsigned long long* counters;
   // adjoint scratch
   float* node_adj;
@@ -815,6 +846,7 @@ void carve(C& c, int64_t n, int nseg, int S, bool normals, bool adjoint, Layout&
   int64_t cap = node_capacity(n, nseg, S);
   L.cap = cap;
   L.meta = c.template take<uint32_t>(8);
+  L.gbins = c.template take<uint32_t>(kGroupBins);
   L.counters = c.template take<unsigned long long>(4);
   L.boxes = c.template take<SegBox>(nseg);
   L.bb = c.template take<uint32_t>(6 * nseg);
@@ -914,6 +946,20 @@ namespace {
 // recover the workspace layout without reading device memory.
 std::mutex g_reg_mu;
 std::unordered_map<const void*, Header> g_registry;
+
+// Target groups of at most G targets, deepest cells first (group_nodes_kernel).
+cudaError_t cut_groups(cudaStream_t stream, const Layout& L, int64_t n, int nseg, int G, uint32_t* status) {
+  cudaError_t e = cudaMemsetAsync(L.gbins, 0, kGroupBins * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  const unsigned grid = gs(static_cast<int64_t>(L.cap));
+  const uint32_t* sseg = nseg > 1 ? L.sseg : nullptr;
+  group_nodes_kernel<true><<<grid, 256, 0, stream>>>(L.nodes, L.meta, sseg, L.groups, n + nseg + 1, G, L.gbins,
+                                                     status);
+  group_bins_kernel<<<1, 32, 0, stream>>>(L.gbins, L.meta + 1);
+  group_nodes_kernel<false><<<grid, 256, 0, stream>>>(L.nodes, L.meta, sseg, L.groups, n + nseg + 1, G, L.gbins,
+                                                      status);
+  return cudaGetLastError();
+}
 
 int register_tree(void* ws, const Header& h) {
   std::lock_guard<std::mutex> lk(g_reg_mu);
@@ -1026,9 +1072,10 @@ int sbh_native_build(cudaStream_t stream, const float* points, const float* mass
   }
   // system roots and target groups (meta[1] counts the groups)
   roots_kernel<<<nseg, 32, 0, stream>>>(L.seg_off, nseg, L.base, L.cap, L.roots);
-  if (n > 0)
-    group_nodes_kernel<<<gs(static_cast<int64_t>(L.cap)), 256, 0, stream>>>(
-        L.nodes, L.meta, nseg > 1 ? L.sseg : nullptr, L.groups, n + nseg + 1, kGroup, L.meta + 1, status);
+  if (n > 0) {
+    cudaError_t ge = cut_groups(stream, L, n, nseg, kGroup, status);
+    if (ge != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(ge));
+  }
   if (int rc = check_launch("sbh_native_build")) return rc;
   return register_tree(workspace, h);
 }
@@ -1189,11 +1236,8 @@ int sbh_native_set_group_size(cudaStream_t stream, void* workspace, size_t works
   Layout L;
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   if (h.n == 0) return SBH_OK;
-  cudaError_t e = cudaMemsetAsync(L.meta + 1, 0, sizeof(uint32_t), stream);
+  cudaError_t e = cut_groups(stream, L, h.n, h.nseg, group_size, static_cast<uint32_t*>(workspace));
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  group_nodes_kernel<<<gs(static_cast<int64_t>(L.cap)), 256, 0, stream>>>(
-      L.nodes, L.meta, h.nseg > 1 ? L.sseg : nullptr, L.groups, h.n + h.nseg + 1, group_size, L.meta + 1,
-      static_cast<uint32_t*>(workspace));
   {
     std::lock_guard<std::mutex> lk(g_reg_mu);
     auto it = g_registry.find(workspace);

@@ -876,15 +876,16 @@ def run_ours(args):
 # build of one system: offsets 1 + bbox 3 + keys 1 + 8 radix passes x
 #   (count 1 + scan 3 + scatter 1) + levels 1 + slots 1 + scan 3 + emit 1 +
 #   node count 1 + gather 1 + moment scan 3 + finalize 1 + roots 1 +
-#   groups 1 = 59; a forest of K > 1 systems copies its offsets instead of
-#   the offsets kernel and adds a stable pass on the system id (gather 1 +
-#   ceil(log2 K / 8) radix passes x 5 + gathers 2 + system ids 1)
+#   groups 3 (count pass, level cursors, emit pass) = 61; a forest of K > 1
+#   systems copies its offsets instead of the offsets kernel and adds a
+#   stable pass on the system id (gather 1 + ceil(log2 K / 8) radix passes
+#   x 5 + gathers 2 + system ids 1)
 # walk: zero adjoint 1 + walk 1 = 2; finalize: push 1 + scan 3 + combine 1 = 5
 def build_launches(k: int) -> int:
     if k <= 1:
-        return 59
+        return 61
     bits = max(1, (k - 1).bit_length())
-    return 59 - 1 + 1 + 5 * ((bits + 7) // 8) + 3
+    return 61 - 1 + 1 + 5 * ((bits + 7) // 8) + 3
 
 
 WALK_LAUNCHES = 2
