@@ -150,11 +150,6 @@ __device__ __forceinline__ float min_image_rint(float d, float inv_l, const Peri
   return d;
 }
 
-struct Soft {
-  float eps;     // max(softening, 0)
-  float cutoff;  // <= 0 disables the erfc attenuation
-};
-
 // Below this u = r / (2 cutoff) the attenuation erfc(u) + (2/sqrt(pi)) u
 // e^{-u^2} = 1 - (4 / (3 sqrt(pi))) u^3 + O(u^5) is within 6e-9 of 1, under
 // half an FP32 ulp of 1, so it is taken as 1 without evaluating erfc and exp.
@@ -163,12 +158,21 @@ struct Soft {
 // puts every pair here.
 constexpr float kAttUnityU = 1.0f / 512.0f;
 
+struct Soft {
+  float eps;       // max(softening, 0)
+  float cutoff;    // <= 0 disables the erfc attenuation
+  float unity_r2;  // (2 cutoff kAttUnityU)^2: pairs with r^2 + 1e-12 below it have att = 1
+  __host__ __device__ Soft(float e = 0.0f, float c = 0.0f)
+      : eps(e), cutoff(c), unity_r2(c > 0.0f ? (2.0f * c * kAttUnityU) * (2.0f * c * kAttUnityU) : 0.0f) {}
+};
+
 // coefficient c with f = c * r for the softened force; r = q - p.
 __device__ __forceinline__ float soft_coeff(float r2, float mass, const Soft& s) {
   float inv_r = rsqrtf(r2 + s.eps * s.eps + 1e-12f);
   float inv_r3 = inv_r * inv_r * inv_r;
   float att = 1.0f;
-  if (s.cutoff > 0.0f) {
+  // the square-root and division are only needed outside the att = 1 range
+  if (s.cutoff > 0.0f && r2 + 1e-12f >= s.unity_r2) {
     float dist = sqrtf(r2 + 1e-12f);
     float u = dist / (2.0f * s.cutoff);
     if (u >= kAttUnityU) {
@@ -189,10 +193,11 @@ __device__ __forceinline__ void soft_vjp_accum(float rx, float ry, float rz, flo
   float inv_r5 = inv_r3 * inv_r * inv_r;
   float att = 1.0f;
   float cc = 0.0f;
-  if (s.cutoff > 0.0f) {
+  // below kAttUnityU (r^2 under unity_r2): att = 1, and cc = ir3 r e / (2 sqrt(pi) cutoff^3) is
+  // below 1e-4 (r^2 + eps^2) / cutoff^2 of the 3 att ir^5 term it joins, so it is left out
+  if (s.cutoff > 0.0f && r2 + 1e-12f >= s.unity_r2) {
     float dist = sqrtf(r2 + 1e-12f);
     float u = dist / (2.0f * s.cutoff);
-    // below kAttUnityU: att = 1 and e^{-u^2} = 1 to FP32 precision
     float e = 1.0f;
     if (u >= kAttUnityU) {
       e = expf(-(u * u));

@@ -40,7 +40,7 @@ namespace sbh {
 // ---------------------------------------------------------------------------
 constexpr int kDirectThreads = 256;
 
-template <int VJP>
+template <int VJP, bool PER>
 __global__ void __launch_bounds__(kDirectThreads)
     direct_soft_kernel(const float* __restrict__ pts, const float* __restrict__ masses, int64_t n,
                        const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq,
@@ -68,11 +68,15 @@ __global__ void __launch_bounds__(kDirectThreads)
     __syncthreads();
     int cnt = static_cast<int>(n - base < kDirectThreads ? n - base : kDirectThreads);
     float ax = 0.f, ay = 0.f, az = 0.f;
+#pragma unroll 4
     for (int k = 0; k < cnt; k++) {
       float4 p = tile[k];
-      float rx = min_image_rint(qx - p.x, inv_l, per);
-      float ry = min_image_rint(qy - p.y, inv_l, per);
-      float rz = min_image_rint(qz - p.z, inv_l, per);
+      float rx = qx - p.x, ry = qy - p.y, rz = qz - p.z;
+      if (PER) {
+        rx = min_image_rint(rx, inv_l, per);
+        ry = min_image_rint(ry, inv_l, per);
+        rz = min_image_rint(rz, inv_l, per);
+      }
       if (VJP) {
         soft_vjp_accum(rx, ry, rz, p.w, gx, gy, gz, s, ax, ay, az);
       } else {
@@ -777,9 +781,11 @@ int sbh_direct_force_soft(cudaStream_t stream, const float* points, const float*
   if (!(cutoff_scale > 0.0f)) return invalid("cutoff_scale must be > 0");
   if (int rc = check_threads(threads)) return rc;
   if (nq == 0) return SBH_OK;
-  direct_soft_kernel<0><<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(
-      points, masses, n, queries, nullptr, nq, out, Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
-      Periodic{periodic, box_length});
+  const bool per = periodic && box_length > 0.0f;
+  auto k = per ? direct_soft_kernel<0, true> : direct_soft_kernel<0, false>;
+  k<<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(points, masses, n, queries, nullptr, nq, out,
+                                                                 Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
+                                                                 Periodic{periodic, box_length});
   return check_launch("direct_force_soft");
 }
 
@@ -792,9 +798,11 @@ int sbh_direct_force_soft_vjp(cudaStream_t stream, const float* points, const fl
   if (!(cutoff_scale > 0.0f)) return invalid("cutoff_scale must be > 0");
   if (int rc = check_threads(threads)) return rc;
   if (nq == 0) return SBH_OK;
-  direct_soft_kernel<1><<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(
-      points, masses, n, queries, cotangent, nq, out, Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
-      Periodic{periodic, box_length});
+  const bool per = periodic && box_length > 0.0f;
+  auto k = per ? direct_soft_kernel<1, true> : direct_soft_kernel<1, false>;
+  k<<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(points, masses, n, queries, cotangent, nq, out,
+                                                                 Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
+                                                                 Periodic{periodic, box_length});
   return check_launch("direct_force_soft_vjp");
 }
 

@@ -1236,15 +1236,14 @@ int sbh_native_set_group_size(cudaStream_t stream, void* workspace, size_t works
   Layout L;
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   if (h.n == 0) return SBH_OK;
+  // the stats keep describing the last walk: count it on its own groups first
+  if (int rc = refresh_counts(stream, workspace, h, L)) return rc;
   cudaError_t e = cut_groups(stream, L, h.n, h.nseg, group_size, static_cast<uint32_t*>(workspace));
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   {
     std::lock_guard<std::mutex> lk(g_reg_mu);
     auto it = g_registry.find(workspace);
-    if (it != g_registry.end()) {
-      it->second.group_size = group_size;
-      it->second.counts_fresh = it->second.last_walk != 1;
-    }
+    if (it != g_registry.end()) it->second.group_size = group_size;
   }
   return check_launch("sbh_native_set_group_size");
 }

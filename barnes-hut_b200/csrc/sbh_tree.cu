@@ -342,7 +342,7 @@ __device__ __forceinline__ void tree_kernel(const LeafT<N>& d, const Vec<N>& q, 
     float ir3 = ir * ir * ir;
     float ir5 = ir3 * ir * ir;
     float att = 1.0f, cc = 0.0f;
-    if (s.cutoff > 0.0f) {
+    if (s.cutoff > 0.0f && r2 + 1e-12f >= s.unity_r2) {
       float dist = sqrtf(r2 + 1e-12f);
       float u = dist / (2.0f * s.cutoff);
       float e = 1.0f;  // att = 1, e^{-u^2} = 1 to FP32 precision below kAttUnityU

@@ -545,6 +545,30 @@ def sharded_measurement(B, torch, dev, rank, world, n):
                 allreduce_bytes=int(n * 28), rel_force_vs_single=rel_f, rel_grad_vs_single=rel_g)
 
 
+def direct_measurement(B, torch, P0, M0, W0, flush):
+    """The direct sums (the reference's SoftenedDirectForce and its VJP,
+    src/sbh_ffi.cu:503-546): all 2^20 x 2^20 pairs of the first Plummer
+    system, softening 1e-3, no cutoff (the reference's convention: a cutoff
+    of 1e6 box lengths). One launch each."""
+    span = float((P0.max(0).values - P0.min(0).values).max())
+    kw = dict(softening_scale=1e-3, cutoff_scale=span * 1e6)
+    out = {}
+    for name, fn in (("force", lambda: B.softened_direct_force(P0, M0, P0, **kw)),
+                     ("vjp", lambda: B.softened_direct_force_vjp(P0, M0, P0, W0, **kw))):
+        fn()
+        torch.cuda.synchronize()
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        pairs = float(P0.shape[0]) ** 2
+        out[name] = dict(ms=ms, pair_interactions_per_s=pairs / (ms * 1e-3))
+    return dict(sources=int(P0.shape[0]), queries=int(P0.shape[0]), **out)
+
+
 def measure_fp32_peak(B, torch, dev):
     buf = torch.zeros(1024, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
@@ -820,6 +844,7 @@ def run_ours(args):
             extras["winding_number_mesh"] = winding_mesh_measurement(B, torch, dev, flush)
             extras["treepm_short_range"] = treepm_measurement(B, torch, dev, flush)
             extras["stochastic_octree8"] = stochastic_measurement(B, torch, P0, M0, idx, ref, flush)
+            extras["direct_sum"] = direct_measurement(B, torch, P0, M0, W0, flush)
             extras["trajectory"] = trajectory_measurement(torch, dev, flush)
 
     if rank == 0:
