@@ -371,8 +371,27 @@ def winding_measurement(B, torch, dev, flush):
     ms = tot / 3
     err_in = float((out[inside] - 1.0).abs().mean())
     err_out = float(out[~inside].abs().mean())
+    # the reference's algorithm on this GPU: its adaptive Tree3D<1,3> (leaf size 1, built here on the
+    # device with the reference CPU builder's bytes) and its warp-vote traversal (src/sbh_gpu.cu)
+    def ref_step():
+        leaf, node = B.build_octree_buffers(P, N, M, backend="cpu")
+        return B.eval_barnes_hut_wn(leaf, node, Q, beta=BETA)[0]
+
+    ref_step()
+    torch.cuda.synchronize()
+    flush.zero_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    rout = ref_step()
+    e1.record()
+    torch.cuda.synchronize()
+    ref_ms = e0.elapsed_time(e1)
     return dict(sources=262144, queries=1048576, ms=ms, queries_per_s=1048576 / (ms * 1e-3),
-                mean_abs_err_inside=err_in, mean_abs_err_outside=err_out)
+                mean_abs_err_inside=err_in, mean_abs_err_outside=err_out,
+                reference_algorithm_ms=ref_ms, speedup_vs_reference_algorithm=ref_ms / ms,
+                reference_algorithm_mean_abs_err_inside=float((rout[inside] - 1.0).abs().mean()),
+                reference_algorithm_mean_abs_err_outside=float(rout[~inside].abs().mean()),
+                reference_algorithm="Tree3D<1,3> (leaf size 1) + warp-vote Barnes-Hut, beta 2, both on this GPU")
 
 
 def winding_mesh_measurement(B, torch, dev, flush):
