@@ -307,3 +307,28 @@ def test_native_target_ranges_sum_to_full(cuda, world):
     with pytest.raises(ValueError):
         t.set_target_range(0, t.n + 1)
 
+
+
+@pytest.mark.parametrize("group_size", [64, 40])
+def test_native_two_slot_kernels_match_oracle(cuda, group_size):
+    """Groups of at most 64 run on the two-targets-per-lane walks: forces and
+    the full adjoint with the quadrupole (radius 1.6) against the oracle's
+    plan with the same group size, on a clustered and a uniform system."""
+    rng = np.random.default_rng(61)
+    for p, m in (W.plummer(20000, seed=62), W.uniform_cube(15000, seed=63)):
+        w = rng.normal(size=p.shape).astype(np.float32)
+        t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True, group_size=group_size)
+        f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=True, quadrupole_radius=1.6)
+        f2 = t.force(beta=2.0, softening=1e-3, quadrupole=True, quadrupole_radius=1.6).cpu().numpy()
+        st = t.stats()
+        T = O.NativeTree(p, m, leaf_size=16)
+        with O.native_quadrupole_radius(1.6):
+            inter = T.plan(2.0, group_size)
+        want_f, _ = T.force(1e-3, quad=True)
+        dx, dm = T.adjoint(w, 1e-3, quad=True)
+        assert st["groups"] == T.plan_stats()[0]
+        assert abs((st["far"] + st["near"]) - inter) <= 1e-4 * inter
+        assert rel_l2(f.cpu().numpy(), want_f) < 1e-5
+        assert rel_l2(f2, want_f) < 1e-5
+        assert rel_l2(gx.cpu().numpy(), dx) < 1e-4
+        assert rel_l2(gm.cpu().numpy(), dm) < 1e-4
