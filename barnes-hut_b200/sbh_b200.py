@@ -1007,6 +1007,48 @@ class _NativeGravity(torch.autograd.Function):
         return gx, gm, None
 
 
+# Candidate (leaf size, most targets per group) pairs of autotune_native:
+# groups of 96 suit clustered systems, 64 near-uniform ones; leaves of 12 to
+# 20 cost about the same on Plummer spheres.
+AUTOTUNE_CANDIDATES = ((16, 96), (16, 64), (12, 96), (24, 64))
+
+
+def autotune_native(points, masses, system_offsets=None, *, normals=None, adjoint: bool = True,
+                    candidates=AUTOTUNE_CANDIDATES, reps: int = 2, **walk_kw) -> dict:
+    """Times build + walk (force_vjp when adjoint, else force) of the given
+    system(s) for each (leaf_size, group_size) candidate and returns the
+    fastest as dict(leaf_size, group_size, ms, trials). Results do not
+    depend on the choice beyond FP32 rounding and the opening decisions a
+    group size implies; the walk parameters (beta, softening, ...) are the
+    caller's."""
+    dev = points.device if isinstance(points, torch.Tensor) and points.is_cuda else _device()
+    tree = NativeTree(dev)
+    cot = None
+    trials = []
+    for leaf, group in candidates:
+        def step():
+            tree.build(points, masses, normals, system_offsets, leaf_size=leaf, with_adjoint=adjoint,
+                       group_size=group)
+            if adjoint:
+                return tree.force_vjp(cot, **walk_kw)
+            return tree.force(**walk_kw)
+
+        if cot is None:
+            cot = torch.ones((int(points.shape[0]), 3), dtype=torch.float32, device=dev)
+        step()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            step()
+        b.record()
+        torch.cuda.synchronize(dev)
+        trials.append((a.elapsed_time(b) / reps, leaf, group))
+    ms, leaf, group = min(trials)
+    return dict(leaf_size=leaf, group_size=group, ms=ms,
+                trials=[dict(leaf_size=l_, group_size=g_, ms=m_) for m_, l_, g_ in trials])
+
+
 def native_force_recompute_vjp(points, masses, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,
                                leaf_size: int = 16, quadrupole: bool = True) -> torch.Tensor:
     """Differentiable native self-gravity (gradients w.r.t. points and masses)."""

@@ -217,9 +217,12 @@ def forest_measurement(B, torch, dev, rank, world, flush):
     F, GX, GM = torch.empty_like(pts), torch.empty_like(pts), torch.empty(n, device=dev)
     prm = B.NativeTree.params(BETA, EPS, 0.0, True)
     tree = B.NativeTree(dev)
+    # leaf and group size autotuned on this forest (outside the timed region)
+    tune = B.autotune_native(pts, ms, offs, adjoint=True, beta=BETA, softening=EPS)
+    leaf, group = tune["leaf_size"], tune["group_size"]
 
     def batched():
-        tree.build(pts, ms, system_offsets=offs, leaf_size=LEAF, with_adjoint=True)
+        tree.build(pts, ms, system_offsets=offs, leaf_size=leaf, with_adjoint=True, group_size=group)
         tree.adjoint_walk(w, prm, F)
         tree.adjoint_finalize(GX, GM)
 
@@ -228,9 +231,9 @@ def forest_measurement(B, torch, dev, rank, world, flush):
 
     def plain():
         for p_, m_, w_ in views:
-            trees[0].build(p_, m_, leaf_size=LEAF, with_adjoint=False)
+            trees[0].build(p_, m_, leaf_size=leaf, with_adjoint=False, group_size=group)
             trees[0].force(beta=BETA, softening=EPS)
-            trees[1].build(p_, m_, leaf_size=LEAF, with_adjoint=True)
+            trees[1].build(p_, m_, leaf_size=leaf, with_adjoint=True, group_size=group)
             trees[1].force_vjp(w_, beta=BETA, softening=EPS, want_force=False)
 
     # CUDA graph of the batched step (build + walk + finalize, no host sync inside)
@@ -266,7 +269,8 @@ def forest_measurement(B, torch, dev, rank, world, flush):
     del g
     return dict(systems=int(b - a), particles=int(n), plain_ms=t_plain, batched_ms=t_batched, graph_ms=t_graph,
                 batched_over_plain=t_plain / t_graph,
-                particle_evals_per_s_graph=n / (t_graph * 1e-3), particle_evals_per_s_plain=n / (t_plain * 1e-3))
+                particle_evals_per_s_graph=n / (t_graph * 1e-3), particle_evals_per_s_plain=n / (t_plain * 1e-3),
+                autotuned=dict(leaf_size=leaf, group_size=group, trials=tune["trials"]))
 
 
 def stochastic_measurement(B, torch, P0, M0, idx, ref, flush):
@@ -315,6 +319,7 @@ def trajectory_measurement(torch, dev, flush):
     gradient of the mean squared final-position error to a seeded target
     with respect to the initial displacements, checkpointing every 10 steps
     (sbh_trajectory: native force and full adjoint per step)."""
+    import sbh_b200 as B
     import sbh_trajectory as T
 
     p, m, disp = W.perturbed_lattice(128, seed=5, rms_cells=0.2)
@@ -323,7 +328,9 @@ def trajectory_measurement(torch, dev, flush):
     v0 = torch.zeros_like(x0)
     mt = torch.tensor(m, device=dev)
     tgt = torch.tensor(target, device=dev)
-    grav = T.Gravity(beta=1.0 / 0.6, softening=2e-3, leaf_size=LEAF, group_size=64)  # near-uniform lattice
+    # leaf and group size autotuned on the initial positions (outside the timed region)
+    tune = B.autotune_native(x0, mt, adjoint=True, beta=1.0 / 0.6, softening=2e-3)
+    grav = T.Gravity(beta=1.0 / 0.6, softening=2e-3, leaf_size=tune["leaf_size"], group_size=tune["group_size"])
     steps, dt, ck = 50, 1e-3, 10
     T.kdk(x0, v0, mt, 1, dt, grav)  # warm-up (workspaces)
     torch.cuda.synchronize()
@@ -341,7 +348,8 @@ def trajectory_measurement(torch, dev, flush):
     return dict(particles=int(n), steps=steps, checkpoint_every=ck, forward_ms=fwd, backward_ms=bwd,
                 total_s=(fwd + bwd) * 1e-3, force_evals=steps + 1, recomputed_forces=steps,
                 force_vjp_evals=steps + 1, grad_norm=float(torch.linalg.norm(gx0)),
-                loss=float(((xT - tgt) ** 2).mean()))
+                loss=float(((xT - tgt) ** 2).mean()),
+                autotuned=dict(leaf_size=tune["leaf_size"], group_size=tune["group_size"], trials=tune["trials"]))
 
 
 def winding_measurement(B, torch, dev, flush):

@@ -332,3 +332,13 @@ def test_native_two_slot_kernels_match_oracle(cuda, group_size):
         assert rel_l2(f2, want_f) < 1e-5
         assert rel_l2(gx.cpu().numpy(), dx) < 1e-4
         assert rel_l2(gm.cpu().numpy(), dm) < 1e-4
+
+
+def test_autotune_native_picks_a_candidate(cuda):
+    p, m = W.plummer(30000, seed=71)
+    cands = ((16, 96), (16, 64))
+    r = B.autotune_native(torch.tensor(p, device=cuda), torch.tensor(m, device=cuda), candidates=cands,
+                          beta=2.0, softening=1e-3)
+    assert (r["leaf_size"], r["group_size"]) in cands
+    assert len(r["trials"]) == 2 and all(t["ms"] > 0 for t in r["trials"])
+    assert r["ms"] == min(t["ms"] for t in r["trials"])
