@@ -2,9 +2,11 @@
  * sbh_b200 -- C ABI of the B200-native Barnes-Hut summation library.
  *
  * Every entry point takes a CUDA stream, raw device pointers and sizes, and
- * parameters by value. No entry point allocates device memory, synchronises
- * the stream or touches process-global parameter state, so all of them can
- * be called concurrently on different streams and captured in CUDA graphs.
+ * parameters by value. The builds, walks and direct sums allocate no device
+ * memory, do not synchronise the stream and touch no process-global
+ * parameter state, so they can be called concurrently on different streams
+ * and captured in CUDA graphs; the read-backs (status, stats, export) and the
+ * adaptive Tree2D/Tree3D builders synchronise, as their comments say.
  * Temporary storage comes from a caller-provided workspace whose size the
  * matching *_workspace_bytes() function reports.
  *
