@@ -41,6 +41,7 @@
 #include <unordered_map>
 
 #include "sbh_common.cuh"
+#include "sbh_f32x2.cuh"
 #include "sbh_native.cuh"
 #include "sbh_primitives.cuh"
 
@@ -648,7 +649,12 @@ __device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin
 // B200 over 8 x 2^20 Plummer particles at quadrupole radius 1.6, the adjoint
 // walk takes 410 ms with two targets per lane at 7 blocks per SM (72
 // registers) and 389 ms with three at 6 blocks (80 registers); 4 per lane at
-// 4 blocks takes 411 ms. Clustered systems gain from the larger groups;
+// 4 blocks takes 411 ms. The adjoint walk's packed form (two slots per FP32
+// instruction) then brought three per lane to 367 ms at 5 blocks (96
+// registers), against 374 ms for the scalar form at 6 blocks and 397 ms at 5;
+// packed at 4 blocks it takes 403 ms. Two per lane packed stays best at 7
+// blocks (the 2^21 lattice walk: 33.9 ms, 34.8 at 6, 36.9 at 5; scalar 36.9
+// at 7). Clustered systems gain from the larger groups;
 // near-uniform ones and walks bounded by a prune radius gain from smaller
 // groups (a 2^21 lattice trajectory: 3.76 s with groups of 64, 4.46 s with
 // 96), which the two-slot kernels serve. A tree walks with the kernels of its
@@ -665,7 +671,7 @@ constexpr int kAdjointWalkMinBlocks = 7;
 namespace tpl3 {
 constexpr int kTPL = 3;
 constexpr int kForceWalkMinBlocks = 6;
-constexpr int kAdjointWalkMinBlocks = 6;
+constexpr int kAdjointWalkMinBlocks = 5;
 #include "sbh_native_walks.inc"
 }  // namespace tpl3
 

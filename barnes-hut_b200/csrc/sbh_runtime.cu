@@ -87,6 +87,26 @@ __global__ void __launch_bounds__(256) fp32_probe_kernel(float* out, int iters, 
   float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
   if (s == 12345.678f) out[blockIdx.x] = s;  // keeps the chains alive
 }
+
+// The same chains two to an instruction (packed FFMA2 on sm_100): 4 float2
+// chains per thread, the same flops per launch.
+__global__ void __launch_bounds__(256) fp32x2_probe_kernel(float* out, int iters, float a, float b) {
+  const float x0 = threadIdx.x * 1e-7f;
+  float2 y0 = make_float2(x0, x0 + 1e-3f), y1 = make_float2(x0 + 2e-3f, x0 + 3e-3f);
+  float2 y2 = make_float2(x0 + 4e-3f, x0 + 5e-3f), y3 = make_float2(x0 + 6e-3f, x0 + 7e-3f);
+  const float2 a2 = make_float2(a, a), b2 = make_float2(b, b);
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      y0 = __ffma2_rn(y0, a2, b2);
+      y1 = __ffma2_rn(y1, a2, b2);
+      y2 = __ffma2_rn(y2, a2, b2);
+      y3 = __ffma2_rn(y3, a2, b2);
+    }
+  }
+  float s = y0.x + y0.y + y1.x + y1.y + y2.x + y2.y + y3.x + y3.y;
+  if (s == 12345.678f) out[blockIdx.x] = s;  // keeps the chains alive
+}
 }  // namespace
 
 extern "C" {
@@ -96,5 +116,12 @@ int sbh_probe_fp32(cudaStream_t stream, float* out, int blocks, int iters) {
   if (blocks <= 0 || iters <= 0 || !out) return sbh::invalid("blocks, iters > 0 and out non-null required");
   fp32_probe_kernel<<<blocks, 256, 0, stream>>>(out, iters, 0.999999f, 1e-7f);
   return sbh::check_launch("probe_fp32");
+}
+
+// As sbh_probe_fp32 with the FMAs issued two per instruction; same flops.
+int sbh_probe_fp32x2(cudaStream_t stream, float* out, int blocks, int iters) {
+  if (blocks <= 0 || iters <= 0 || !out) return sbh::invalid("blocks, iters > 0 and out non-null required");
+  fp32x2_probe_kernel<<<blocks, 256, 0, stream>>>(out, iters, 0.999999f, 1e-7f);
+  return sbh::check_launch("probe_fp32x2");
 }
 }

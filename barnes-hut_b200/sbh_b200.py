@@ -110,6 +110,7 @@ _SIGS = {
     "sbh_stochastic_bh_force_octree8_vjp": ([_c_p, _c_i, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_i64, _c_p, _c_p, _c_i,
                                              _c_i, _c_f, _c_f, _c_f, _c_i, _c_f, _c_i, _c_f, _c_i, _c_p, _c_sz], _c_i),
     "sbh_probe_fp32": ([_c_p, _c_p, _c_i, _c_i], _c_i),
+    "sbh_probe_fp32x2": ([_c_p, _c_p, _c_i, _c_i], _c_i),
     "sbh_build_octree_level3_workspace_bytes": ([_c_i64], _c_sz),
     "sbh_build_octree_level3": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz, _c_p,
                                  _c_sz], _c_i),

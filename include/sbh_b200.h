@@ -204,6 +204,10 @@ int sbh_stochastic_bh_force_octree8_vjp(cudaStream_t stream, int softened, const
  * the FP32 pipe peak that the traversal rooflines are reported against. */
 int sbh_probe_fp32(cudaStream_t stream, float* out, int blocks, int iters);
 
+/* As sbh_probe_fp32 with the FMAs issued two per instruction (packed FP32,
+ * sm_100); same flops per launch. */
+int sbh_probe_fp32x2(cudaStream_t stream, float* out, int blocks, int iters);
+
 /* Bytes of device workspace every octree8 / Node2 / Node3 traversal needs
  * (the device status word). */
 size_t sbh_traversal_workspace_bytes(void);
