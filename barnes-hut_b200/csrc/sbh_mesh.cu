@@ -154,6 +154,93 @@ void carve(C& c, int64_t nf, double** area2, double** cdf, double** tmp, float4*
   *normal = c.template take<float4>(static_cast<size_t>(nf));
 }
 
+// ---------------------------------------------------------------------------
+// Vertex sources (the reference's MeshVertices, python/old_interface/
+// source.py:85-115): every vertex is a source, with the area-weighted vertex
+// normal of igl.per_vertex_normals(V, F, 1) (the normalised sum of e1 x e2
+// over the incident faces) and, as its mass, the diagonal of libigl's
+// default (Voronoi) mass matrix: the mixed Voronoi area of Meyer, Desbrun,
+// Schroeder and Barr (2003). Per face P0 P1 P2 with cot_i the cotangent of
+// the angle at corner i:
+//   no obtuse angle: corner i takes (|Pi Pk|^2 cot_j + |Pi Pj|^2 cot_k) / 8;
+//   obtuse at corner i: corner i takes area / 2, the other two area / 4.
+// The three shares sum to the face's area, so the masses sum to the surface
+// area. Faces of zero area add nothing. FP64 throughout; the per-vertex sums
+// are FP64 atomics, so the FP32 outputs can differ from a sequential sum in
+// the last place.
+__global__ void vertex_face_kernel(const float* __restrict__ V, int64_t nv, const int32_t* __restrict__ F,
+                                   int64_t nf, double* __restrict__ acc, uint32_t* status) {
+  for (int64_t f = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; f < nf;
+       f += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t id[3] = {F[3 * f], F[3 * f + 1], F[3 * f + 2]};
+    bool ok = true;
+    for (int c = 0; c < 3; c++) ok = ok && id[c] >= 0 && id[c] < nv;
+    if (!ok) {
+      raise_status(status, SBH_DEV_BAD_BOUNDS);
+      continue;
+    }
+    double p[3][3];
+    for (int c = 0; c < 3; c++)
+      for (int d = 0; d < 3; d++) p[c][d] = V[3 * id[c] + d];
+    // e[c]: the edge from corner c to corner c + 1
+    double e[3][3];
+    for (int c = 0; c < 3; c++)
+      for (int d = 0; d < 3; d++) e[c][d] = __dsub_rn(p[(c + 1) % 3][d], p[c][d]);
+    double n[3];  // e0 x (P2 - P0) = -(e0 x e2)
+    n[0] = __dsub_rn(__dmul_rn(e[2][1], e[0][2]), __dmul_rn(e[2][2], e[0][1]));
+    n[1] = __dsub_rn(__dmul_rn(e[2][2], e[0][0]), __dmul_rn(e[2][0], e[0][2]));
+    n[2] = __dsub_rn(__dmul_rn(e[2][0], e[0][1]), __dmul_rn(e[2][1], e[0][0]));
+    const double dbl = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(n[0], n[0]), __dmul_rn(n[1], n[1])),
+                                            __dmul_rn(n[2], n[2])));
+    if (!(dbl > 0.0) || isinf(dbl)) continue;  // no area, no share
+    const double area = __dmul_rn(dbl, 0.5);
+    // squared edge lengths and the corner dot products: corner c sits
+    // between e[c] (outgoing) and e[c - 1] (incoming, reversed)
+    double l2[3], dot[3];
+    for (int c = 0; c < 3; c++) {
+      l2[c] = __dadd_rn(__dadd_rn(__dmul_rn(e[c][0], e[c][0]), __dmul_rn(e[c][1], e[c][1])),
+                        __dmul_rn(e[c][2], e[c][2]));
+      const int b = (c + 2) % 3;
+      dot[c] = -__dadd_rn(__dadd_rn(__dmul_rn(e[c][0], e[b][0]), __dmul_rn(e[c][1], e[b][1])),
+                          __dmul_rn(e[c][2], e[b][2]));
+    }
+    double share[3];
+    int obtuse = -1;
+    for (int c = 0; c < 3; c++)
+      if (dot[c] < 0.0) obtuse = c;
+    if (obtuse >= 0) {
+      for (int c = 0; c < 3; c++) share[c] = c == obtuse ? __dmul_rn(area, 0.5) : __dmul_rn(area, 0.25);
+    } else {
+      double cot[3];
+      for (int c = 0; c < 3; c++) cot[c] = __ddiv_rn(dot[c], dbl);
+      // corner c: the edge to c + 1 (l2[c]) faces corner c + 2, the edge to c + 2 (l2[c + 2]) faces c + 1
+      for (int c = 0; c < 3; c++)
+        share[c] = __dmul_rn(__dadd_rn(__dmul_rn(l2[c], cot[(c + 2) % 3]), __dmul_rn(l2[(c + 2) % 3], cot[(c + 1) % 3])),
+                             0.125);
+    }
+    for (int c = 0; c < 3; c++) {
+      double* a = acc + 4 * static_cast<int64_t>(id[c]);
+      atomicAdd(a, share[c]);
+      atomicAdd(a + 1, n[0]);
+      atomicAdd(a + 2, n[1]);
+      atomicAdd(a + 3, n[2]);
+    }
+  }
+}
+
+__global__ void vertex_finish_kernel(const double* __restrict__ acc, int64_t nv, float* __restrict__ normals,
+                                     float* __restrict__ masses) {
+  for (int64_t v = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; v < nv;
+       v += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double* a = acc + 4 * v;
+    const double len = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(a[1], a[1]), __dmul_rn(a[2], a[2])),
+                                            __dmul_rn(a[3], a[3])));
+    const bool unit = len > 0.0 && !isinf(len);
+    for (int d = 0; d < 3; d++) normals[3 * v + d] = unit ? __double2float_rn(__ddiv_rn(a[1 + d], len)) : 0.0f;
+    masses[v] = __double2float_rn(a[0]);
+  }
+}
+
 }  // namespace
 }  // namespace mesh
 }  // namespace sbh
@@ -196,6 +283,34 @@ int sbh_sample_mesh_surface(cudaStream_t stream, const float* vertices, int64_t 
   mesh::sample_kernel<<<mesh::grid_for(n), mesh::kThreads, 0, stream>>>(
       vertices, nv, faces, nf, cdf, normal, n, seed, points_out, normals_out, weights_out, status);
   return check_launch("sample_mesh_surface");
+}
+
+size_t sbh_mesh_vertex_workspace_bytes(int64_t nv) {
+  if (nv < 0) return 0;
+  Sizer s;
+  s.take<double>(4 * static_cast<size_t>(nv));
+  return s.off;
+}
+
+int sbh_mesh_vertex_sources(cudaStream_t stream, const float* vertices, int64_t nv, const int32_t* faces, int64_t nf,
+                            float* normals_out, float* masses_out, void* workspace, size_t workspace_bytes) {
+  if (nv < 0 || nf < 0) return invalid("sizes must be >= 0");
+  if (nv > 0 && (!vertices || !normals_out || !masses_out)) return invalid("vertices and outputs must be non-null");
+  if (nf > 0 && !faces) return invalid("faces must be non-null");
+  if (nv == 0) return nf == 0 ? SBH_OK : invalid("faces reference vertices of an empty mesh");
+  size_t need = sbh_mesh_vertex_workspace_bytes(nv);
+  if (!workspace || workspace_bytes < need)
+    return fail(SBH_ERR_WORKSPACE, "workspace too small: need " + std::to_string(need) + " bytes");
+  Carver c(workspace, workspace_bytes);
+  double* acc = c.take<double>(4 * static_cast<size_t>(nv));
+  uint32_t* status = static_cast<uint32_t*>(workspace);
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, 4 * sizeof(double) * static_cast<size_t>(nv), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  if (nf > 0)
+    mesh::vertex_face_kernel<<<mesh::grid_for(nf), mesh::kThreads, 0, stream>>>(vertices, nv, faces, nf, acc, status);
+  mesh::vertex_finish_kernel<<<mesh::grid_for(nv), mesh::kThreads, 0, stream>>>(acc, nv, normals_out, masses_out);
+  return check_launch("mesh_vertex_sources");
 }
 
 }  // extern "C"

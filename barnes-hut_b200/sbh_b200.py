@@ -145,6 +145,8 @@ _SIGS = {
     "sbh_native_set_group_size": ([_c_p, _c_p, _c_sz, _c_i], _c_i),
     "sbh_native_set_target_range": ([_c_p, _c_p, _c_sz, _c_i64, _c_i64], _c_i),
     "sbh_mesh_sample_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_mesh_vertex_workspace_bytes": ([_c_i64], _c_sz),
+    "sbh_mesh_vertex_sources": ([_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_sz], _c_i),
     "sbh_sample_mesh_surface": ([_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_i64, _c_u64, _c_p, _c_p, _c_p, _c_p, _c_sz],
                                 _c_i),
     "sbh_native_export": ([_c_p, _c_p, _c_sz, _c_p, _c_p, _c_p, _c_sz, _c_p], _c_i),
@@ -813,6 +815,52 @@ class MeshSurface:
 
     def sample(self, num_points: int, seed: int = 0):
         return sample_points_on_mesh(num_points, self.V, self.F, seed=seed, device=self.device)
+
+
+def mesh_vertex_sources(V, F, *, device=None):
+    """(points (nv, 3), normals (nv, 3), masses (nv,)) on the device: every
+    vertex of the triangle mesh as a winding-number source, with the
+    area-weighted vertex normal (igl.per_vertex_normals(V, F, 1)) and the
+    mixed Voronoi area (the diagonal of igl.massmatrix's default Voronoi mass
+    matrix) as its mass; the masses sum to the surface area. Raises SbhError
+    when a face references a missing vertex (read back from the device status
+    word, which synchronises)."""
+    device = device or (V.device if isinstance(V, torch.Tensor) and V.is_cuda else _device())
+    v = _f32(V, device)
+    f = F.to(device=device, dtype=torch.int32).contiguous() if isinstance(F, torch.Tensor) else \
+        torch.as_tensor(np.asarray(F, dtype=np.int32), device=device).contiguous()
+    if v.ndim != 2 or v.shape[1] != 3 or f.ndim != 2 or f.shape[1] != 3:
+        raise ValueError("V must be (nv, 3) and F (nf, 3)")
+    nv = v.shape[0]
+    nrm = torch.empty((nv, 3), dtype=torch.float32, device=device)
+    m = torch.empty(nv, dtype=torch.float32, device=device)
+    ws = workspace(int(lib().sbh_mesh_vertex_workspace_bytes(nv)), device)
+    _check(lib().sbh_mesh_vertex_sources(_stream_ptr(device), _p(v), nv, _p(f), f.shape[0], _p(nrm), _p(m), _p(ws),
+                                         ws.numel()), "mesh_vertex_sources")
+    if nv > 0 and read_device_status(ws) & DEV_BAD_BOUNDS:
+        raise SbhError("mesh_vertex_sources: a face references a missing vertex")
+    return v, nrm, m
+
+
+class MeshVertices:
+    """Winding-number sources at the vertices of a triangle mesh (the
+    reference's MeshVertices source, python/old_interface/source.py:85-115):
+    the mesh is centred and scaled so its largest extent is `scale`; sample()
+    returns the vertices, their area-weighted normals and their Voronoi
+    masses (the reference ignores the requested count, and so does this)."""
+
+    def __init__(self, V, F, scale: float = 1.0, device=None):
+        V = np.asarray(V.cpu() if isinstance(V, torch.Tensor) else V, dtype=np.float64)
+        vmin, vmax = V.min(axis=0), V.max(axis=0)
+        width = float(np.max(vmax - vmin))
+        if not width > 0:
+            raise ValueError("the mesh has zero extent")
+        self.V = ((V - (vmax + vmin) / 2) / width * scale).astype(np.float32)
+        self.F = np.asarray(F.cpu() if isinstance(F, torch.Tensor) else F, dtype=np.int32)
+        self.device = device
+
+    def sample(self, num_points: int = 0):
+        return mesh_vertex_sources(self.V, self.F, device=self.device)
 
 
 # ---------------------------------------------------------------------------

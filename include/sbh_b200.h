@@ -480,6 +480,23 @@ int sbh_sample_mesh_surface(cudaStream_t stream, const float* vertices, int64_t 
                             float* points_out, float* normals_out, float* weights_out,
                             void* workspace, size_t workspace_bytes);
 
+/* Vertex sources of a triangle mesh, replacing the host-side libigl calls of
+ * the reference's MeshVertices (python/old_interface/source.py:85-115:
+ * igl.per_vertex_normals(V, F, 1) and the diagonal of igl.massmatrix). Every
+ * vertex is a source; its normal is the normalised sum of e1 x e2 over the
+ * incident faces (area weighting; zero for a vertex without area), its mass
+ * the mixed Voronoi area of Meyer, Desbrun, Schroeder and Barr (2003): per
+ * face, corner i takes (|Pi Pk|^2 cot_j + |Pi Pj|^2 cot_k) / 8 when no angle
+ * is obtuse, else area / 2 at the obtuse corner and area / 4 at the others.
+ * Masses sum to the surface area. Faces that reference a vertex outside
+ * [0, nv) set SBH_DEV_BAD_BOUNDS in the device status word and add nothing.
+ * vertices: nv x 3 f32, faces: nf x 3 i32 (device). Outputs: normals nv x 3,
+ * masses nv (device, f32); the points are the vertices themselves. */
+size_t sbh_mesh_vertex_workspace_bytes(int64_t nv);
+int sbh_mesh_vertex_sources(cudaStream_t stream, const float* vertices, int64_t nv,
+                            const int32_t* faces, int64_t nf, float* normals_out,
+                            float* masses_out, void* workspace, size_t workspace_bytes);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -593,3 +593,46 @@ def sample_points_on_mesh(num_particles: int, V, F, seed: int = 0):
     pts = ((v0 + u1[:, None] * e1) + u2[:, None] * e2).astype(np.float32)
     w = np.full(n, np.float32((total * 0.5) / n) if n else 0.0, dtype=np.float32)
     return pts, nrm[face], w, face
+
+
+def mesh_vertex_sources(V, F):
+    """Restatement of sbh_mesh_vertex_sources (the reference's MeshVertices,
+    python/old_interface/source.py:85-115, whose libigl calls are
+    per_vertex_normals(V, F, 1) and the diagonal of massmatrix): per vertex,
+    the normalised sum of c = (v1 - v0) x (v2 - v0) over its faces (area
+    weighting), and the mixed Voronoi area of Meyer, Desbrun, Schroeder and
+    Barr (2003) summed over its faces. Per face with corner angles theta_i:
+    without an obtuse angle, corner i takes (|Pi Pk|^2 cot theta_j +
+    |Pi Pj|^2 cot theta_k) / 8; with one at corner i, corner i takes area / 2
+    and the others area / 4. float64 from the float32 vertices, faces of zero
+    area skipped; returns (normals float64, masses float64)."""
+    V = np.asarray(V, dtype=np.float32).astype(np.float64)
+    F = np.asarray(F, dtype=np.int64)
+    nv = V.shape[0]
+    P = [V[F[:, c]] for c in range(3)]
+    e = [P[(c + 1) % 3] - P[c] for c in range(3)]  # edge from corner c to c + 1
+    n = np.cross(e[0], P[2] - P[0])
+    dbl = np.linalg.norm(n, axis=1)
+    ok = (dbl > 0) & np.isfinite(dbl)
+    F, n, dbl = F[ok], n[ok], dbl[ok]
+    e = [x[ok] for x in e]
+    area = 0.5 * dbl
+    l2 = [np.einsum("ij,ij->i", x, x) for x in e]
+    dot = [-np.einsum("ij,ij->i", e[c], e[(c + 2) % 3]) for c in range(3)]  # corner c: P(c+1)-Pc . P(c-1)-Pc
+    cot = [d / dbl for d in dot]
+    share = np.stack([(l2[c] * cot[(c + 2) % 3] + l2[(c + 2) % 3] * cot[(c + 1) % 3]) / 8.0 for c in range(3)],
+                     axis=1)
+    for c in range(3):
+        ob = dot[c] < 0
+        share[ob] = 0.25 * area[ob, None]
+        share[ob, c] = 0.5 * area[ob]
+    mass = np.zeros(nv)
+    nsum = np.zeros((nv, 3))
+    for c in range(3):
+        np.add.at(mass, F[:, c], share[:, c])
+        np.add.at(nsum, F[:, c], n)
+    ln = np.linalg.norm(nsum, axis=1)
+    nrm = np.zeros_like(nsum)
+    good = ln > 0
+    nrm[good] = nsum[good] / ln[good, None]
+    return nrm, mass

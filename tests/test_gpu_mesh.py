@@ -71,3 +71,58 @@ def test_mesh_sampler_invalid(cuda):
     p, _, _ = s.sample(4096, seed=1)
     ext = p.max(0).values - p.min(0).values
     assert float(ext.max()) <= 2.0 + 1e-5
+
+
+def _perturbed_torus(seed):
+    """The torus mesh with jittered vertices: a mix of acute, right-ish and
+    obtuse faces."""
+    V, F = W.torus_mesh(1.0, 0.4, 48, 24)
+    V = V + np.random.default_rng(seed).normal(scale=0.01, size=V.shape).astype(np.float32)
+    return V, F
+
+
+@pytest.mark.parametrize("mesh", ["torus", "perturbed"])
+def test_mesh_vertex_sources_match_oracle(cuda, mesh):
+    V, F = W.torus_mesh(1.0, 0.4, 128, 64) if mesh == "torus" else _perturbed_torus(3)
+    pts, nrm, m = B.mesh_vertex_sources(V, F)
+    want_n, want_m = O.mesh_vertex_sources(V, F)
+    assert torch.equal(pts.cpu(), torch.tensor(V))
+    # FP64 sums in another order, rounded once to FP32
+    np.testing.assert_allclose(m.cpu().numpy(), want_m, rtol=2e-7, atol=0)
+    np.testing.assert_allclose(nrm.cpu().numpy(), want_n, rtol=0, atol=2e-7)
+    area2, _ = O.mesh_face_geometry(V, F)
+    assert abs(float(m.double().sum()) - 0.5 * area2.sum()) < 1e-5 * area2.sum()
+
+
+def test_mesh_vertex_sources_winding_number(cuda):
+    """The vertices of the closed torus mesh as winding-number sources on the
+    native tree: against the FP64 direct sum of the same sources, and the
+    analytic inside/outside away from the surface."""
+    V, F = W.torus_mesh(1.0, 0.4, 128, 64)
+    pts, nrm, m = B.MeshVertices(V, F, scale=2.8).sample()
+    q = W.uniform_box_queries(1 << 16, seed=7)
+    t = B.NativeTree().build(pts, m, normals=nrm, leaf_size=16, with_adjoint=False)
+    wn = t.winding_number(q, beta=2.0).cpu().numpy()
+    want = O.direct_winding_number(pts.cpu().numpy(), nrm.cpu().numpy(), m.cpu().numpy(), q)
+    assert np.abs(wn - want).max() < 2e-2
+    P = pts.cpu().numpy().astype(np.float64)
+    # MeshVertices rescales the torus (extent 2.8 = 2 (R + r)) back to R 1, r 0.4
+    inside = W.torus_inside(q)
+    d = np.abs(np.sqrt((np.sqrt(q[:, 0].astype(np.float64) ** 2 + q[:, 1] ** 2) - 1.0) ** 2 + q[:, 2] ** 2) - 0.4)
+    far = d > 0.1
+    assert np.abs(P).max() <= 1.4 + 1e-6
+    assert np.abs(wn[far & inside] - 1).mean() < 0.02
+    assert np.abs(wn[far & ~inside]).mean() < 0.01
+
+
+def test_mesh_vertex_sources_invalid(cuda):
+    V, F = W.torus_mesh(1.0, 0.4, 8, 4)
+    with pytest.raises(ValueError):
+        B.mesh_vertex_sources(V[:, :2], F)
+    bad = F.copy()
+    bad[2, 0] = -1
+    with pytest.raises(B.SbhError):
+        B.mesh_vertex_sources(V, bad)
+    # no faces: every vertex keeps mass 0 and a zero normal
+    _, nrm, m = B.mesh_vertex_sources(V, F[:0])
+    assert float(m.abs().max()) == 0.0 and float(nrm.abs().max()) == 0.0

@@ -83,3 +83,55 @@ def test_sampled_torus_winding_number(nu, nv):
     inside = W.torus_inside(q)
     assert np.abs(wn[inside] - 1).mean() < 0.05
     assert np.abs(wn[~inside]).mean() < 0.05
+
+
+def _one_face(p):
+    return np.asarray(p, np.float32), np.array([[0, 1, 2]])
+
+
+def test_vertex_sources_voronoi_known_answers():
+    """Mixed Voronoi areas (Meyer et al. 2003) on single faces: an equilateral
+    face splits evenly; a right angle takes the square up to the hypotenuse's
+    midpoint (1/4 of legs 1 x 1) and the other corners 1/8; an obtuse corner
+    takes half the area and the others a quarter."""
+    s3 = np.sqrt(3.0)
+    n, m = O.mesh_vertex_sources(*_one_face([[0, 0, 0], [1, 0, 0], [0.5, s3 / 2, 0]]))
+    np.testing.assert_allclose(m, np.full(3, s3 / 12), rtol=1e-6)
+    np.testing.assert_allclose(n, np.tile([0.0, 0.0, 1.0], (3, 1)), atol=1e-12)
+    _, m = O.mesh_vertex_sources(*_one_face([[0, 0, 0], [1, 0, 0], [0, 1, 0]]))
+    np.testing.assert_allclose(m, [0.25, 0.125, 0.125], rtol=1e-12)
+    V, F = _one_face([[0, 0, 0], [1, 0.1, 0], [-1, 0.1, 0]])
+    area = 0.5 * abs(np.cross(V[1].astype(np.float64) - V[0], V[2].astype(np.float64) - V[0])[2])
+    _, m = O.mesh_vertex_sources(V, F)
+    np.testing.assert_allclose(m, [area / 2, area / 4, area / 4], rtol=1e-12)
+    # corner order does not matter: the obtuse corner moved to position 2
+    _, m = O.mesh_vertex_sources(V[[1, 2, 0]], F)
+    np.testing.assert_allclose(m, [area / 4, area / 4, area / 2], rtol=1e-12)
+
+
+def test_vertex_sources_torus():
+    """On the closed torus mesh the masses sum to the surface area (the sum
+    of the face areas) and the area-weighted normals point along the
+    analytic torus normal."""
+    V, F = W.torus_mesh(1.0, 0.4, 64, 32)
+    n, m = O.mesh_vertex_sources(V, F)
+    area2, _ = O.mesh_face_geometry(V, F)
+    np.testing.assert_allclose(m.sum(), 0.5 * area2.sum(), rtol=1e-12)
+    assert (m > 0).all()
+    np.testing.assert_allclose(np.linalg.norm(n, axis=1), 1.0, rtol=1e-12)
+    p = V.astype(np.float64)
+    rho = np.hypot(p[:, 0], p[:, 1])
+    c = np.stack([p[:, 0] / rho, p[:, 1] / rho, np.zeros_like(rho)], axis=1)  # ring centre direction
+    radial = p - c * 1.0
+    radial /= np.linalg.norm(radial, axis=1, keepdims=True)
+    assert np.einsum("ij,ij->i", n, radial).min() > 0.99
+
+
+def test_vertex_sources_degenerate_and_unused():
+    """A zero-area face adds nothing; a vertex without faces keeps mass 0 and
+    a zero normal."""
+    V = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [2, 0, 0], [5, 5, 5]], np.float32)
+    F = np.array([[0, 1, 2], [0, 1, 3]])  # the second face is collinear
+    n, m = O.mesh_vertex_sources(V, F)
+    np.testing.assert_allclose(m, [0.25, 0.125, 0.125, 0.0, 0.0], rtol=1e-12)
+    assert np.all(n[3:] == 0.0)
