@@ -644,8 +644,9 @@ __device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin
   return d2 > r2;
 }
 
-// The walks are compiled twice: three targets per lane (groups of up to 96)
-// and two (up to 64), each for the occupancy that suits it. Measured on a
+// The walks are compiled three times: four targets per lane (groups of up
+// to 128), three (up to 96) and two (up to 64), each for the occupancy that
+// suits it. Measured on a
 // B200 over 8 x 2^20 Plummer particles at quadrupole radius 1.6, the adjoint
 // walk takes 410 ms with two targets per lane at 7 blocks per SM (72
 // registers) and 389 ms with three at 6 blocks (80 registers); 4 per lane at
@@ -654,7 +655,10 @@ __device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin
 // registers), against 374 ms for the scalar form at 6 blocks and 397 ms at 5;
 // packed at 4 blocks it takes 403 ms. Two per lane packed stays best at 7
 // blocks (the 2^21 lattice walk: 33.9 ms, 34.8 at 6, 36.9 at 5; scalar 36.9
-// at 7). Clustered systems gain from the larger groups;
+// at 7). Four per lane packed (two full pairs, groups of 128) at 4 blocks
+// (128 registers) takes 356 ms, and build + force of one 2^20 Plummer system
+// 23.2 against 24.1 ms with groups of 96. Clustered systems gain from the
+// larger groups;
 // near-uniform ones and walks bounded by a prune radius gain from smaller
 // groups (a 2^21 lattice trajectory: 3.76 s with groups of 64, 4.46 s with
 // 96), which the two-slot kernels serve. A tree walks with the kernels of its
@@ -674,6 +678,13 @@ constexpr int kForceWalkMinBlocks = 6;
 constexpr int kAdjointWalkMinBlocks = 5;
 #include "sbh_native_walks.inc"
 }  // namespace tpl3
+
+namespace tpl4 {
+constexpr int kTPL = 4;
+constexpr int kForceWalkMinBlocks = 4;
+constexpr int kAdjointWalkMinBlocks = 4;
+#include "sbh_native_walks.inc"
+}  // namespace tpl4
 
 // One of the five variants (quadrupole; periodic and/or cutoff) of a walk
 // kernel of namespace NS.
@@ -1218,8 +1229,9 @@ int refresh_counts(cudaStream_t stream, const void* ws, const Header& h, const L
   WalkParams wp = walk_params(&p);
   bool cut = p.cutoff > 0.0f;
   bool per = p.periodic != 0;
-  auto k = h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, count_walk_kernel, p.quadrupole, per, cut)
-                                         : SBH_NT_SELECT(tpl2, count_walk_kernel, p.quadrupole, per, cut);
+  auto k = h.group_size > kGroupThreeSlots ? SBH_NT_SELECT(tpl4, count_walk_kernel, p.quadrupole, per, cut)
+           : h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, count_walk_kernel, p.quadrupole, per, cut)
+                                           : SBH_NT_SELECT(tpl2, count_walk_kernel, p.quadrupole, per, cut);
   e = launch_walk(stream, L.work, h.n + h.nseg, k, tree_view(L), self_targets(L, hr), wp, L.counters);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   std::lock_guard<std::mutex> lk(g_reg_mu);
@@ -1291,8 +1303,9 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
   int64_t mg = h.n + h.nseg;
   bool cut = params->cutoff > 0.0f;
   bool per = params->periodic != 0;
-  auto k = h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, force_walk_kernel, params->quadrupole, per, cut)
-                                         : SBH_NT_SELECT(tpl2, force_walk_kernel, params->quadrupole, per, cut);
+  auto k = h.group_size > kGroupThreeSlots ? SBH_NT_SELECT(tpl4, force_walk_kernel, params->quadrupole, per, cut)
+           : h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, force_walk_kernel, params->quadrupole, per, cut)
+                                           : SBH_NT_SELECT(tpl2, force_walk_kernel, params->quadrupole, per, cut);
   e = launch_walk(stream, L.work, mg, k, tree_view(L), self_targets(L, h), wp, force_out);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   remember_walk(workspace, 1, params);
@@ -1320,8 +1333,9 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
   WalkParams wp = walk_params(params);
   bool cut = params->cutoff > 0.0f;
   bool per = params->periodic != 0;
-  auto k = h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, adjoint_walk_kernel, params->quadrupole, per, cut)
-                                         : SBH_NT_SELECT(tpl2, adjoint_walk_kernel, params->quadrupole, per, cut);
+  auto k = h.group_size > kGroupThreeSlots ? SBH_NT_SELECT(tpl4, adjoint_walk_kernel, params->quadrupole, per, cut)
+           : h.group_size > kGroupTwoSlots ? SBH_NT_SELECT(tpl3, adjoint_walk_kernel, params->quadrupole, per, cut)
+                                           : SBH_NT_SELECT(tpl2, adjoint_walk_kernel, params->quadrupole, per, cut);
   e = launch_walk(stream, L.work, n + h.nseg, k, tree_view(L), self_targets(L, h), wp, cotangent, force_out, L.gq,
                   L.node_adj, L.part_adj);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));

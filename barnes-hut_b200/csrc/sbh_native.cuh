@@ -24,10 +24,13 @@ struct NodeRec {
 static_assert(sizeof(NodeRec) == 80, "NodeRec must be 80 bytes");
 
 constexpr int kLeafFlag = 0x100;
-// Most targets per group: three per lane of a warp. Groups of at most
-// kGroupTwoSlots targets are walked by the two-slot kernels.
+// Most targets per group: four per lane of a warp. Groups of at most
+// kGroupTwoSlots targets are walked by the two-slot kernels, of at most
+// kGroupThreeSlots by the three-slot kernels, larger ones by the four-slot
+// kernels.
 constexpr int kGroupTwoSlots = 64;
-constexpr int kGroup = 96;  // targets per group built by default (one warp, three per lane)
+constexpr int kGroupThreeSlots = 96;
+constexpr int kGroup = 128;  // targets per group built by default (one warp, four per lane)
 #ifndef SBH_QUERY_GROUP
 #define SBH_QUERY_GROUP 32
 #endif

@@ -1057,9 +1057,9 @@ class _NativeGravity(torch.autograd.Function):
 
 
 # Candidate (leaf size, most targets per group) pairs of autotune_native:
-# groups of 96 suit clustered systems, 64 near-uniform ones; leaves of 12 to
-# 20 cost about the same on Plummer spheres.
-AUTOTUNE_CANDIDATES = ((16, 96), (16, 64), (12, 96), (24, 64))
+# groups of 128 or 96 suit clustered systems, 64 near-uniform ones; leaves of
+# 12 to 20 cost about the same on Plummer spheres.
+AUTOTUNE_CANDIDATES = ((16, 128), (16, 96), (16, 64), (24, 64))
 
 
 def autotune_native(points, masses, system_offsets=None, *, normals=None, adjoint: bool = True,

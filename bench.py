@@ -513,7 +513,8 @@ def treepm_measurement(B, torch, dev, flush):
         return tot / reps, out
 
     ours32_ms, _ = timed(lambda: ours(32), 3)
-    ours96_ms, _ = timed(lambda: ours(B.native_group_size()), 3)
+    ours96_ms, _ = timed(lambda: ours(96), 3)
+    ours128_ms, _ = timed(lambda: ours(B.native_group_size()), 3)
     ours_ms, _ = timed(lambda: ours(64), 3)
     st = tree.stats()
     rel = float(torch.linalg.norm(F[idx].double() - ref) / torch.linalg.norm(ref))
@@ -521,7 +522,7 @@ def treepm_measurement(B, torch, dev, flush):
     rel_o8 = float(torch.linalg.norm(o8[idx].double() - ref) / torch.linalg.norm(ref))
     return dict(particles=int(pts.shape[0]), box_cells=k, r_split=rs, prune_radius=mult * rs, softening=eps,
                 beta=beta, group_size=64, ms=ours_ms, ms_with_32_target_groups=ours32_ms,
-                ms_with_96_target_groups=ours96_ms,
+                ms_with_96_target_groups=ours96_ms, ms_with_128_target_groups=ours128_ms,
                 rel_l2_vs_fp64_direct=rel,
                 interactions_per_particle=(st["far"] + st["near"]) / pts.shape[0],
                 octree8_reference_algorithm_ms=ref_ms, octree8_rel_l2_vs_fp64_direct=rel_o8,

@@ -309,11 +309,12 @@ def test_native_target_ranges_sum_to_full(cuda, world):
 
 
 
-@pytest.mark.parametrize("group_size", [64, 40])
-def test_native_two_slot_kernels_match_oracle(cuda, group_size):
-    """Groups of at most 64 run on the two-targets-per-lane walks: forces and
-    the full adjoint with the quadrupole (radius 1.6) against the oracle's
-    plan with the same group size, on a clustered and a uniform system."""
+@pytest.mark.parametrize("group_size", [64, 40, 96, 72])
+def test_native_two_and_three_slot_kernels_match_oracle(cuda, group_size):
+    """Groups of at most 64 run on the two-targets-per-lane walks, of 65 to
+    96 on the three-per-lane walks: forces and the full adjoint with the
+    quadrupole (radius 1.6) against the oracle's plan with the same group
+    size, on a clustered and a uniform system."""
     rng = np.random.default_rng(61)
     for p, m in (W.plummer(20000, seed=62), W.uniform_cube(15000, seed=63)):
         w = rng.normal(size=p.shape).astype(np.float32)
@@ -336,7 +337,7 @@ def test_native_two_slot_kernels_match_oracle(cuda, group_size):
 
 def test_autotune_native_picks_a_candidate(cuda):
     p, m = W.plummer(30000, seed=71)
-    cands = ((16, 96), (16, 64))
+    cands = ((16, 128), (16, 64))
     r = B.autotune_native(torch.tensor(p, device=cuda), torch.tensor(m, device=cuda), candidates=cands,
                           beta=2.0, softening=1e-3)
     assert (r["leaf_size"], r["group_size"]) in cands
