@@ -952,11 +952,11 @@ WALK_LAUNCHES = 2
 
 # DRAM bytes (read + write) of one adjoint walk per particle, from one ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of the packed walk
-# over 4 Plummer systems of 262,144 particles at quadrupole radius 1.6:
-# 125.35 MB + 39.06 MB for 1,048,576 particles. The walk's DRAM traffic is
+# (four targets per lane) over 4 Plummer systems of 262,144 particles at
+# quadrupole radius 1.6: 124.39 MB + 33.80 MB for 1,048,576 particles. The walk's DRAM traffic is
 # its L2 misses on the tree, the particles and the adjoint arrays, which grow
 # with the particle count.
-WALK_DRAM_BYTES_PER_PARTICLE = 156.8
+WALK_DRAM_BYTES_PER_PARTICLE = 150.9
 FINALIZE_LAUNCHES = 5
 
 # FP32 flops per interaction of the adjoint walk (force + adjoint, counted
