@@ -656,8 +656,9 @@ __device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin
 // packed at 4 blocks it takes 403 ms. Two per lane packed stays best at 7
 // blocks (the 2^21 lattice walk: 33.9 ms, 34.8 at 6, 36.9 at 5; scalar 36.9
 // at 7). Four per lane packed (two full pairs, groups of 128) at 4 blocks
-// (128 registers) takes 356 ms, and build + force of one 2^20 Plummer system
-// 23.2 against 24.1 ms with groups of 96. Clustered systems gain from the
+// (128 registers) takes 356 ms; its force walk at 5 blocks (102 registers)
+// builds + forces one 2^20 Plummer system in 22.7 ms (23.2 at 4 blocks, 24.1
+// with groups of 96). Clustered systems gain from the
 // larger groups;
 // near-uniform ones and walks bounded by a prune radius gain from smaller
 // groups (a 2^21 lattice trajectory: 3.76 s with groups of 64, 4.46 s with
@@ -681,7 +682,7 @@ constexpr int kAdjointWalkMinBlocks = 5;
 
 namespace tpl4 {
 constexpr int kTPL = 4;
-constexpr int kForceWalkMinBlocks = 4;
+constexpr int kForceWalkMinBlocks = 5;
 constexpr int kAdjointWalkMinBlocks = 4;
 #include "sbh_native_walks.inc"
 }  // namespace tpl4
