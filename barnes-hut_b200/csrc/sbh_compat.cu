@@ -452,7 +452,15 @@ __global__ void __launch_bounds__(256)
   int top = 0;
   stack[top++] = 0;
   bool overflow = false;
+  // A well-formed tree reaches each node from the root exactly once, so one
+  // query pops at most num_nodes nodes. More pops mean that the caller's
+  // child indices form a cycle: stop, flag it and keep the partial sum.
+  uint32_t visits = 0;
   while (top > 0) {
+    if (++visits > bd.num_nodes) {
+      raise_status(status, SBH_DEV_ITER_LIMIT);
+      break;
+    }
     int idx = stack[--top];
     if (o8_mass(nodes, idx) == 0.0f) continue;
     const OctreeNode8& nd = nodes[idx];
@@ -494,6 +502,7 @@ __global__ void __launch_bounds__(256)
 // ---------------------------------------------------------------------------
 constexpr int kControlDepth = 3;
 constexpr int kMaxSubdomains = 512;
+constexpr int kO8MaxDescent = 64;
 
 template <int KERNEL>
 __device__ __forceinline__ void o8_contrib_pair(const OctreeNode8& nd, float qx, float qy, float qz, float gx,
@@ -541,7 +550,12 @@ __global__ void __launch_bounds__(256)
   uint32_t subs[kMaxSubdomains];
   int nsub = 0;
   bool overflow = false;
+  uint32_t visits = 0;  // bounded as in o8_bh_kernel
   while (top > 0) {
+    if (++visits > bd.num_nodes) {
+      raise_status(status, SBH_DEV_ITER_LIMIT);
+      break;
+    }
     int idx = stack[--top];
     const OctreeNode8& nd = nodes[idx];
     if (nd.contrib.mass == 0.0f) continue;
@@ -583,7 +597,14 @@ __global__ void __launch_bounds__(256)
       float dy = min_image_floor(qy - cur->cy, per);
       float dz = min_image_floor(qz - cur->cz, per);
       float cur_beta = fmaxf(beta, sqrtf(dx * dx + dy * dy + dz * dz) / cur->diameter);
+      // Each step goes one level down a tree of depth <= 10; a longer descent
+      // follows a cycle in the caller's child indices.
+      int steps = 0;
       while (!cur->is_leaf) {
+        if (++steps > kO8MaxDescent) {
+          raise_status(status, SBH_DEV_ITER_LIMIT);
+          break;
+        }
         if (SOFTENED && o8_prune(*cur, qx, qy, qz, prune_on, r_cut_sq, per)) break;
         float ex = min_image_floor(qx - cur->cx, per);
         float ey = min_image_floor(qy - cur->cy, per);

@@ -51,7 +51,8 @@ struct Face {
 
 __device__ __forceinline__ bool load_face(const float* __restrict__ V, int64_t nv, const int32_t* __restrict__ F,
                                           int64_t f, Face& out) {
-  int32_t a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
+  // 64-bit indices: 3 * a overflows int32 for vertex indices past ~7.2e8
+  const int64_t a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
   if (a < 0 || b < 0 || c < 0 || a >= nv || b >= nv || c >= nv) return false;
   for (int d = 0; d < 3; d++) {
     double x0 = V[3 * a + d], x1 = V[3 * b + d], x2 = V[3 * c + d];
@@ -172,7 +173,7 @@ __global__ void vertex_face_kernel(const float* __restrict__ V, int64_t nv, cons
                                    int64_t nf, double* __restrict__ acc, uint32_t* status) {
   for (int64_t f = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; f < nf;
        f += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int32_t id[3] = {F[3 * f], F[3 * f + 1], F[3 * f + 2]};
+    const int64_t id[3] = {F[3 * f], F[3 * f + 1], F[3 * f + 2]};  // 64-bit: 3 * id below
     bool ok = true;
     for (int c = 0; c < 3; c++) ok = ok && id[c] >= 0 && id[c] < nv;
     if (!ok) {

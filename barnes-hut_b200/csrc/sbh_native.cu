@@ -767,6 +767,16 @@ __global__ void adjoint_combine_kernel(const float4* __restrict__ sp, const uint
   }
 }
 
+// The query-side gradient of the last adjoint walk (sorted order) in input order.
+__global__ void query_side_kernel(const uint32_t* __restrict__ perm, int64_t n, const float* __restrict__ gq,
+                                  float* __restrict__ out) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    uint32_t o = perm[i];
+    for (int d = 0; d < 3; d++) out[3 * static_cast<int64_t>(o) + d] = gq[3 * i + d];
+  }
+}
+
 // Query targets: keys in the box of system 0 (clamped), sorted, grouped in
 // runs of kQueryGroup (one slot per lane: for queries spread evenly through
 // the box, wider groups only add interactions; 2^20 uniform queries over
@@ -960,8 +970,10 @@ using namespace sbh::nt;
 
 namespace {
 
-// Host registry: which tree (sizes) a workspace holds, so evaluation calls
-// recover the workspace layout without reading device memory.
+// Host registry: which tree (sizes, group size, target range) a workspace
+// holds, keyed by the workspace's address, so evaluation calls recover the
+// workspace layout without reading device memory. An entry lives until
+// sbh_native_release(workspace) or the next build on the same address.
 std::mutex g_reg_mu;
 std::unordered_map<const void*, Header> g_registry;
 
@@ -997,6 +1009,12 @@ int native_layout(void* ws, size_t ws_bytes, const Header& h, Layout& L) {
 extern "C" {
 
 int sbh_native_group_size(void) { return kGroup; }
+
+int sbh_native_release(const void* workspace) {
+  std::lock_guard<std::mutex> lk(g_reg_mu);
+  g_registry.erase(workspace);
+  return SBH_OK;
+}
 
 size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int with_normals, int with_adjoint) {
   if (n < 0 || num_systems < 1 || leaf_size < 1 || leaf_size > 32) return 0;
@@ -1362,6 +1380,18 @@ int sbh_native_adjoint_finalize(cudaStream_t stream, float* grad_points, float* 
   adjoint_combine_kernel<<<gs(n), 256, 0, stream>>>(L.sp, L.v0, sseg, L.boxes, n, L.gq, L.part_adj, L.D, grad_points,
                                                     grad_masses);
   return check_launch("sbh_native_adjoint_finalize");
+}
+
+int sbh_native_adjoint_query_side(cudaStream_t stream, float* grad_points, void* workspace,
+                                  size_t workspace_bytes) {
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!h.adjoint) return invalid("the tree was built without adjoint scratch (with_adjoint = 0)");
+  if (h.n == 0) return SBH_OK;
+  if (!grad_points) return invalid("grad_points must be non-null");
+  query_side_kernel<<<gs(h.n), 256, 0, stream>>>(L.v0, h.n, L.gq, grad_points);
+  return check_launch("sbh_native_adjoint_query_side");
 }
 
 int sbh_native_force_vjp(cudaStream_t stream, const sbh_native_params* params, const float* cotangent,

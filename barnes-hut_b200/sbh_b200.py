@@ -132,12 +132,14 @@ _SIGS = {
     "sbh_build_quadtree": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_p, _c_f, _c_p, _c_sz, _c_p, _c_sz, _c_p, _c_sz,
                             _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_group_size": ([], _c_i),
+    "sbh_native_release": ([_c_p], _c_i),
     "sbh_native_workspace_bytes": ([_c_i64, _c_i, _c_i, _c_i, _c_i], _c_sz),
     "sbh_native_build": ([_c_p, _c_p, _c_p, _c_p, _c_i64, _c_p, _c_i, _c_i, _c_i, _c_p, _c_sz], _c_i),
     "sbh_native_force": ([_c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_force_vjp": ([_c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_adjoint_walk": ([_c_p, _c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_adjoint_finalize": ([_c_p, _c_p, _c_p, _c_p, _c_sz], _c_i),
+    "sbh_native_adjoint_query_side": ([_c_p, _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_query_workspace_bytes": ([_c_i64], _c_sz),
     "sbh_native_winding_number": ([_c_p, _c_f, _c_p, _c_i64, _c_p, _c_p, _c_sz, _c_p, _c_sz], _c_i),
     "sbh_native_stats": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
@@ -920,6 +922,7 @@ class NativeTree:
         n = points.shape[0]
         need = int(lib().sbh_native_workspace_bytes(n, nsys, int(leaf_size), int(nrm is not None), int(with_adjoint)))
         if self.ws is None or self.ws.numel() < need:
+            self.release()
             self.ws = torch.empty(need, dtype=torch.uint8, device=dev)
         self._keep = (points, masses, nrm, offs)
         _check(lib().sbh_native_build(_stream_ptr(dev), _p(points), _p(masses), _p(nrm), n, _p(offs), nsys,
@@ -930,6 +933,19 @@ class NativeTree:
         if group_size is not None and int(group_size) != native_group_size():
             self.set_group_size(int(group_size))
         return self
+
+    def release(self) -> None:
+        """Drops this tree's entry in the library's host registry (before the
+        workspace memory goes back to the allocator, which may hand the same
+        address to another tree)."""
+        if self.ws is not None:
+            lib().sbh_native_release(_p(self.ws))
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:  # interpreter shutdown: the library may be gone
+            pass
 
     def set_target_range(self, begin: int, end: int) -> None:
         """Walk only the target groups starting at sorted positions
@@ -987,6 +1003,14 @@ class NativeTree:
         """Phase 2 of force_vjp (node adjoints to particles, input order)."""
         _check(lib().sbh_native_adjoint_finalize(_stream_ptr(self.device), _p(grad_points), _p(grad_masses),
                                                  _p(self.ws), self.ws.numel()), "native_adjoint_finalize")
+
+    def query_side_gradient(self) -> torch.Tensor:
+        """The query-side part J_i^T w_i of the last adjoint walk's gradient
+        (n x 3, input order): the reference octree8 VJP's convention."""
+        out = torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
+        _check(lib().sbh_native_adjoint_query_side(_stream_ptr(self.device), _p(out), _p(self.ws), self.ws.numel()),
+               "native_adjoint_query_side")
+        return out
 
     def winding_number(self, queries, *, beta: float = 2.0) -> torch.Tensor:
         q = _f32(queries, self.device)

@@ -3,10 +3,16 @@
  *
  * Every entry point takes a CUDA stream, raw device pointers and sizes, and
  * parameters by value. The builds, walks and direct sums allocate no device
- * memory, do not synchronise the stream and touch no process-global
- * parameter state, so they can be called concurrently on different streams
- * and captured in CUDA graphs; the read-backs (status, stats, export) and the
- * adaptive Tree2D/Tree3D builders synchronise, as their comments say.
+ * memory and do not synchronise the stream, so they can be called
+ * concurrently on different streams and captured in CUDA graphs; the
+ * read-backs (status, stats, export) and the adaptive Tree2D/Tree3D builders
+ * synchronise, as their comments say. The one piece of process-global state
+ * is the native tree's host registry: sbh_native_build records, per
+ * workspace address, the tree's sizes, its target-group size and its target
+ * range, which the later sbh_native_* calls on that workspace read (guarded
+ * by a mutex). sbh_native_release() drops a workspace's entry; call it
+ * before the workspace is freed, so that memory reused at the same address
+ * is not mistaken for the old tree.
  * Temporary storage comes from a caller-provided workspace whose size the
  * matching *_workspace_bytes() function reports.
  *
@@ -125,12 +131,20 @@ int sbh_build_octree8(cudaStream_t stream, const float* points, const float* nor
  * sbh_build_octree8_static_scratch_bytes() are rejected with
  * SBH_ERR_INVALID_ARGUMENT (for example n = 200,000 fits at max_depth 6,
  * n = 100,000 at max_depth 7). The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) and caches it. Each call
- * clears what must start at zero (status word, cell counters) itself. All
- * calls share the one array, so calls that may overlap on the GPU
- * (different streams, or several host threads) race and must be serialised
- * by the caller. An invalid bounds span is recorded in the array's status
- * word, which this entry point does not expose. */
+ * array's device address (cudaGetSymbolAddress) and caches it; under CUDA's
+ * default lazy module loading that lookup is also where the library's device
+ * code and this array are loaded onto the device, which can allocate device
+ * memory and synchronise. Make that first call before a framework reserves
+ * the rest of the GPU and before any stream capture, or set
+ * CUDA_MODULE_LOADING=EAGER. The cached address is not valid after
+ * cudaDeviceReset on that device. Each call clears what must start at zero
+ * (status word, cell counters) itself. All calls share the one array, so
+ * calls that may overlap on the GPU (different streams, or several host
+ * threads) race and must be serialised by the caller. An invalid bounds span
+ * (the largest of max_corner - min_corner over the axes not > 0) is recorded
+ * only in the array's own status word, which this entry point does not
+ * expose, and leaves a malformed tree: callers check their corners before
+ * the call. */
 size_t sbh_build_octree8_static_scratch_bytes(void);
 int sbh_build_octree8_static(cudaStream_t stream, const float* points, const float* normals,
                              const float* masses, int64_t n, const float* min_corner,
@@ -368,6 +382,13 @@ typedef struct sbh_native_params {
 /* Most targets one group holds (one warp walks a group). */
 int sbh_native_group_size(void);
 
+/* Forgets the tree recorded for `workspace` in the host registry (sizes,
+ * group size, target range). Later sbh_native_* evaluation calls on it fail
+ * with SBH_ERR_INVALID_ARGUMENT until the next sbh_native_build. Call it
+ * before freeing a workspace. Always returns SBH_OK; device memory is not
+ * touched. */
+int sbh_native_release(const void* workspace);
+
 /* Re-cuts the target groups of the tree built in `workspace` with at most
  * group_size (1 .. sbh_native_group_size()) targets each; later walks use
  * them. The build cuts groups of sbh_native_group_size(). Smaller groups have
@@ -424,6 +445,15 @@ int sbh_native_adjoint_walk(cudaStream_t stream, const sbh_native_params* params
                             size_t workspace_bytes);
 int sbh_native_adjoint_finalize(cudaStream_t stream, float* grad_points, float* grad_masses,
                                 void* workspace, size_t workspace_bytes);
+
+/* After sbh_native_adjoint_walk (or sbh_native_force_vjp) on this workspace:
+ * the query-side part of the gradient alone, J_i^T w_i of target i's own row
+ * (n x 3, input order). This is the quantity the reference's octree8 VJP
+ * returns (barnes_hut_force_octree8_soft_vjp_kernel, src/sbh_ffi.cu:2092-2144,
+ * which has no source-side terms). It reads the walk's scratch, so it comes
+ * before the next walk on the workspace. */
+int sbh_native_adjoint_query_side(cudaStream_t stream, float* grad_points, void* workspace,
+                                  size_t workspace_bytes);
 
 /* Query workspace of sbh_native_winding_number. */
 size_t sbh_native_query_workspace_bytes(int64_t nq);

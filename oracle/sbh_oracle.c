@@ -1339,3 +1339,259 @@ void orc_native_group_costs(void* h, int64_t* far, int64_t* near_particles) {
     near_particles[g] = np_;
   }
 }
+
+/*
+ * Central finite differences, in float64, of the frozen-plan loss
+ * L = sum_i w_i . a_i of orc_native_eval (the recorded plan: groups, accepted
+ * nodes with their quadrupole flags, near leaves) with respect to the
+ * position and the mass of each listed particle: step hx in each coordinate,
+ * hm_rel * m_k in the mass. Plummer softening only (cutoff 0, no periodic box
+ * or prune radius).
+ *
+ * Under a frozen plan particle k enters L only through
+ *   (1) its own row, target k (its far nodes and near pairs);
+ *   (2) the near pairs where it is the source, for every target of the groups
+ *       whose near list holds k's leaf;
+ *   (3) the mass, centroid and second moment of each node that contains it,
+ *       for every target of the groups that accept that node.
+ * Only these terms are evaluated, at the perturbed position or mass, and each
+ * term's difference f(+) - f(-) is taken before it is summed, so the sum does
+ * not lose the small per-particle signal to cancellation. A node's perturbed
+ * moments are updated about its unperturbed centroid X:
+ *   M' = M - m + m',  D = (m' d1 - m d0) / M',  X' = X + D,
+ *   S' = S - m d0 d0^T + m' d1 d1^T - M' D D^T,  d0 = x - X, d1 = x' - X.
+ * One particle costs about N far-field evaluations per perturbation instead
+ * of the whole loss. dx: nidx x 3 and dm: nidx, in the order of idx.
+ */
+#define FD_MAX_DEPTH 64
+static int native_is_leaf(const NativeTree* t, int64_t k) { return (k + 1 >= t->nn) || (t->skip[k] == k + 1); }
+
+/* nodes containing sorted position s, root first; returns their count */
+static int native_ancestors(const NativeTree* t, int64_t s, int32_t* anc) {
+  int na = 0;
+  int64_t a = 0;
+  while (na < FD_MAX_DEPTH) {
+    anc[na++] = (int32_t)a;
+    if (native_is_leaf(t, a)) break;
+    int64_t c = a + 1;
+    while (c < t->skip[a] && !(t->start[c] <= s && s < t->end[c])) c = t->skip[c];
+    if (c >= t->skip[a]) break;
+    a = c;
+  }
+  return na;
+}
+
+/* soft_force_pair (no cutoff) plus, with use_quad, quad_force: the same
+ * formulas sharing h = |r|^2 + eps^2 + 1e-12 and its inverse square root */
+static inline void far_term(const double* r, double M, const double* S, int use_quad, const SoftParams* sp,
+                            double* acc) {
+  const double h = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + sp->eps * sp->eps + 1e-12;
+  const double ir = 1.0 / sqrt(h), ih = ir * ir, ir3 = ir * ih;
+  const double c = -M * ir3;
+  if (!use_quad) {
+    for (int d = 0; d < 3; d++) acc[d] += c * r[d];
+    return;
+  }
+  const double ir5 = ir3 * ih;
+  double Sx[3];
+  sym_mul(S, r, Sx);
+  const double tr = S[0] + S[1] + S[2];
+  const double xSx = r[0] * Sx[0] + r[1] * Sx[1] + r[2] * Sx[2];
+  for (int d = 0; d < 3; d++) acc[d] += c * r[d] + ir5 * (3.0 * Sx[d] + 1.5 * tr * r[d]) - 7.5 * xSx * ir5 * ih * r[d];
+}
+
+void orc_native_fd(void* h, const float* pts, const float* masses, const float* w, double eps, int quad,
+                   const int64_t* idx, int64_t nidx, double hx, double hm_rel, double* dx, double* dm) {
+  NativeTree* t = (NativeTree*)h;
+  const int64_t n = t->n, nn = t->nn, ng = t->ngroups;
+  SoftParams sp = {eps, 0.0, 0, 1.0};
+  double* mom = (double*)malloc(sizeof(double) * MOM * (nn > 0 ? nn : 1));
+  native_moments(t, pts, masses, mom);
+  double* sx = (double*)malloc(sizeof(double) * 3 * (n > 0 ? n : 1));
+  double* sw = (double*)malloc(sizeof(double) * 3 * (n > 0 ? n : 1));
+  double* sm = (double*)malloc(sizeof(double) * (n > 0 ? n : 1));
+  int64_t* inv = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  for (int64_t s = 0; s < n; s++) {
+    int64_t j = t->perm[s];
+    for (int d = 0; d < 3; d++) {
+      sx[3 * s + d] = pts[3 * j + d];
+      sw[3 * s + d] = w[3 * j + d];
+    }
+    sm[s] = masses[j];
+    inv[j] = s;
+  }
+  int64_t* grp = (int64_t*)malloc(sizeof(int64_t) * (n > 0 ? n : 1));
+  for (int64_t g = 0; g < ng; g++)
+    for (int64_t s = t->gstart[g]; s < t->gend[g]; s++) grp[s] = g;
+  /* nodes that contain a listed particle */
+  uint8_t* mark = (uint8_t*)calloc(nn > 0 ? nn : 1, 1);
+  for (int64_t j = 0; j < nidx; j++) {
+    int32_t anc[FD_MAX_DEPTH];
+    int na = native_ancestors(t, inv[idx[j]], anc);
+    for (int a = 0; a < na; a++) mark[anc[a]] = 1;
+  }
+  /* for each marked node: the groups accepting it (with the quadrupole flag),
+   * and for each marked leaf: the groups whose near list holds it */
+  int64_t* foff = (int64_t*)calloc(nn + 1, sizeof(int64_t));
+  int64_t* noff = (int64_t*)calloc(nn + 1, sizeof(int64_t));
+  for (int64_t g = 0; g < ng; g++) {
+    for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++)
+      if (mark[t->far_idx[e]]) foff[t->far_idx[e] + 1]++;
+    for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++)
+      if (mark[t->near_idx[e]]) noff[t->near_idx[e] + 1]++;
+  }
+  for (int64_t k = 0; k < nn; k++) {
+    foff[k + 1] += foff[k];
+    noff[k + 1] += noff[k];
+  }
+  int32_t* fgrp = (int32_t*)malloc(sizeof(int32_t) * (foff[nn] > 0 ? foff[nn] : 1));
+  uint8_t* fq = (uint8_t*)malloc(foff[nn] > 0 ? foff[nn] : 1);
+  int32_t* ngrp = (int32_t*)malloc(sizeof(int32_t) * (noff[nn] > 0 ? noff[nn] : 1));
+  int64_t* fcur = (int64_t*)malloc(sizeof(int64_t) * (nn > 0 ? nn : 1));
+  int64_t* ncur = (int64_t*)malloc(sizeof(int64_t) * (nn > 0 ? nn : 1));
+  memcpy(fcur, foff, sizeof(int64_t) * nn);
+  memcpy(ncur, noff, sizeof(int64_t) * nn);
+  for (int64_t g = 0; g < ng; g++) {
+    for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) {
+      int32_t k = t->far_idx[e];
+      if (!mark[k]) continue;
+      fgrp[fcur[k]] = (int32_t)g;
+      fq[fcur[k]++] = t->far_quad[e];
+    }
+    for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
+      int32_t k = t->near_idx[e];
+      if (mark[k]) ngrp[ncur[k]++] = (int32_t)g;
+    }
+  }
+  free(fcur);
+  free(ncur);
+
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t j = 0; j < nidx; j++) {
+    const int64_t k = idx[j], sk = inv[k], gk = grp[sk];
+    int32_t anc[FD_MAX_DEPTH];
+    const int na = native_ancestors(t, sk, anc);
+    const double xk[3] = {sx[3 * sk], sx[3 * sk + 1], sx[3 * sk + 2]};
+    const double mk = sm[sk];
+    /* perturbation c (0..2: coordinate c, 3: mass), side p (0: +, 1: -) */
+    double xp[4][2][3], mp[4][2];
+    for (int c = 0; c < 4; c++)
+      for (int p = 0; p < 2; p++) {
+        const double sg = p == 0 ? 1.0 : -1.0;
+        for (int d = 0; d < 3; d++) xp[c][p][d] = xk[d];
+        mp[c][p] = mk;
+        if (c < 3)
+          xp[c][p][c] += sg * hx;
+        else
+          mp[c][p] = mk * (1.0 + sg * hm_rel);
+      }
+    /* perturbed moments of every ancestor: [ancestor][c][p][M, X(3), S(6)] */
+    double(*pm)[4][2][MOM] = malloc(sizeof(double) * (size_t)na * 4 * 2 * MOM);
+    for (int a = 0; a < na; a++) {
+      const double* o = &mom[MOM * anc[a]];
+      for (int c = 0; c < 4; c++)
+        for (int p = 0; p < 2; p++) {
+          double d0[3], d1[3], D[3];
+          const double M1 = o[0] - mk + mp[c][p];
+          for (int d = 0; d < 3; d++) {
+            d0[d] = xk[d] - o[1 + d];
+            d1[d] = xp[c][p][d] - o[1 + d];
+            D[d] = (mp[c][p] * d1[d] - mk * d0[d]) / M1;
+          }
+          double* q = pm[a][c][p];
+          q[0] = M1;
+          for (int d = 0; d < 3; d++) q[1 + d] = o[1 + d] + D[d];
+          static const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+          for (int e = 0; e < 6; e++)
+            q[4 + e] = o[4 + e] - mk * d0[ii[e]] * d0[jj[e]] + mp[c][p] * d1[ii[e]] * d1[jj[e]] -
+                       M1 * D[ii[e]] * D[jj[e]];
+        }
+    }
+    double D4[4] = {0, 0, 0, 0};
+    const double* wk = &sw[3 * sk];
+    /* (1) own row */
+    for (int64_t e = t->far_off[gk]; e < t->far_off[gk + 1]; e++) {
+      const int32_t K = t->far_idx[e];
+      int ai = -1;
+      for (int a = 0; a < na; a++)
+        if (anc[a] == K) ai = a;
+      const int uq = quad && t->far_quad[e];
+      for (int c = 0; c < 4; c++) {
+        double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        for (int p = 0; p < 2; p++) {
+          const double* o = ai >= 0 ? pm[ai][c][p] : &mom[MOM * K];
+          double r[3] = {xp[c][p][0] - o[1], xp[c][p][1] - o[2], xp[c][p][2] - o[3]};
+          far_term(r, o[0], o + 4, uq, &sp, f[p]);
+        }
+        D4[c] += wk[0] * (f[0][0] - f[1][0]) + wk[1] * (f[0][1] - f[1][1]) + wk[2] * (f[0][2] - f[1][2]);
+      }
+    }
+    for (int64_t e = t->near_off[gk]; e < t->near_off[gk + 1]; e++) {
+      const int32_t K = t->near_idx[e];
+      for (int64_t s = t->start[K]; s < t->end[K]; s++) {
+        if (s == sk) continue; /* the self pair is zero on both sides */
+        for (int c = 0; c < 3; c++) {
+          double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
+          for (int p = 0; p < 2; p++) {
+            double r[3] = {xp[c][p][0] - sx[3 * s], xp[c][p][1] - sx[3 * s + 1], xp[c][p][2] - sx[3 * s + 2]};
+            far_term(r, sm[s], NULL, 0, &sp, f[p]);
+          }
+          D4[c] += wk[0] * (f[0][0] - f[1][0]) + wk[1] * (f[0][1] - f[1][1]) + wk[2] * (f[0][2] - f[1][2]);
+        }
+      }
+    }
+    /* (2) near pairs with k as the source */
+    const int32_t leafk = anc[na - 1];
+    for (int64_t e = noff[leafk]; e < noff[leafk + 1]; e++) {
+      const int64_t g = ngrp[e];
+      for (int64_t s = t->gstart[g]; s < t->gend[g]; s++) {
+        if (s == sk) continue;
+        const double* ws = &sw[3 * s];
+        for (int c = 0; c < 4; c++) {
+          double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
+          for (int p = 0; p < 2; p++) {
+            double r[3] = {sx[3 * s] - xp[c][p][0], sx[3 * s + 1] - xp[c][p][1], sx[3 * s + 2] - xp[c][p][2]};
+            far_term(r, mp[c][p], NULL, 0, &sp, f[p]);
+          }
+          D4[c] += ws[0] * (f[0][0] - f[1][0]) + ws[1] * (f[0][1] - f[1][1]) + ws[2] * (f[0][2] - f[1][2]);
+        }
+      }
+    }
+    /* (3) the moments of k's ancestors, for the targets that accept them */
+    for (int a = 0; a < na; a++) {
+      const int32_t A = anc[a];
+      for (int64_t e = foff[A]; e < foff[A + 1]; e++) {
+        const int64_t g = fgrp[e];
+        const int uq = quad && fq[e];
+        for (int64_t s = t->gstart[g]; s < t->gend[g]; s++) {
+          if (s == sk) continue; /* target k's row is term (1) */
+          const double* ws = &sw[3 * s];
+          for (int c = 0; c < 4; c++) {
+            double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
+            for (int p = 0; p < 2; p++) {
+              const double* o = pm[a][c][p];
+              double r[3] = {sx[3 * s] - o[1], sx[3 * s + 1] - o[2], sx[3 * s + 2] - o[3]};
+              far_term(r, o[0], o + 4, uq, &sp, f[p]);
+            }
+            D4[c] += ws[0] * (f[0][0] - f[1][0]) + ws[1] * (f[0][1] - f[1][1]) + ws[2] * (f[0][2] - f[1][2]);
+          }
+        }
+      }
+    }
+    for (int c = 0; c < 3; c++) dx[3 * j + c] = D4[c] / (2.0 * hx);
+    dm[j] = mk != 0.0 ? D4[3] / (2.0 * hm_rel * mk) : 0.0;
+    free(pm);
+  }
+  free(fgrp);
+  free(fq);
+  free(ngrp);
+  free(foff);
+  free(noff);
+  free(mark);
+  free(grp);
+  free(inv);
+  free(sm);
+  free(sw);
+  free(sx);
+  free(mom);
+}

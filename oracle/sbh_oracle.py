@@ -99,6 +99,7 @@ def _orc() -> ctypes.CDLL:
         lib.orc_native_quadrupole_interactions.restype = _c_i64
         lib.orc_native_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p]
         lib.orc_native_plan_stats.argtypes = [_c_p, _c_p, _c_p, _c_p]
+        lib.orc_native_fd.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_i, _c_p, _c_i64, _c_d, _c_d, _c_p, _c_p]
         lib._typed = True
     return lib
 
@@ -261,6 +262,18 @@ class NativeTree:
         self._lib.orc_native_eval(self._h, _ptr(p), _ptr(m), float(eps), float(cutoff), int(quad), _ptr(out), _ptr(ww),
                                   ctypes.byref(loss))
         return out, loss.value
+
+    def finite_differences(self, w, eps, idx, hx=1e-4, hm_rel=1e-4, quad=False):
+        """Central FD in float64 of the recorded plan's loss sum_i w_i . a_i
+        with respect to the positions (step hx) and masses (step hm_rel * m)
+        of the particles idx (orc_native_fd: only the terms each particle
+        enters are re-evaluated). Returns (dx (len(idx), 3), dm (len(idx),))."""
+        ip = np.ascontiguousarray(np.asarray(idx, np.int64))
+        dx = np.zeros((ip.shape[0], 3), np.float64)
+        dm = np.zeros(ip.shape[0], np.float64)
+        self._lib.orc_native_fd(self._h, _ptr(self.points), _ptr(self.masses), _ptr(_f32(w)), float(eps), int(quad),
+                                _ptr(ip), ip.shape[0], float(hx), float(hm_rel), _ptr(dx), _ptr(dm))
+        return dx, dm
 
     def adjoint(self, w, eps, cutoff=0.0, points=None, masses=None, quad=False):
         p = self.points if points is None else _f32(points)

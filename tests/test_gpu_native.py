@@ -343,3 +343,15 @@ def test_autotune_native_picks_a_candidate(cuda):
     assert (r["leaf_size"], r["group_size"]) in cands
     assert len(r["trials"]) == 2 and all(t["ms"] > 0 for t in r["trials"])
     assert r["ms"] == min(t["ms"] for t in r["trials"])
+
+
+def test_native_release_forgets_the_workspace(cuda):
+    p, m = W.plummer(3000, seed=21)
+    t = B.NativeTree().build(p, m)
+    want = t.force().cpu().numpy()
+    t.release()
+    with pytest.raises(ValueError, match="no native tree"):
+        t.force()
+    t.release()  # idempotent
+    got = t.build(p, m).force().cpu().numpy()
+    np.testing.assert_array_equal(got, want)
