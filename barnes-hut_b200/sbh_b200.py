@@ -22,6 +22,7 @@ import torch
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libsbh_b200.so")
 HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "sbh_b200.h")
+FFI_HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "sbh_xla_ffi.h")
 
 # Target names of the reference FFI (python/jax_sbh_ffi.py:10-34).
 TARGETS = {
@@ -198,8 +199,8 @@ def lib() -> ctypes.CDLL:
 
 
 def header_symbols() -> list[str]:
-    """Function names declared in include/sbh_b200.h."""
-    text = open(HEADER_PATH).read()
+    """Function names declared in include/sbh_b200.h and include/sbh_xla_ffi.h."""
+    text = open(HEADER_PATH).read() + open(FFI_HEADER_PATH).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(sbh_[a-z0-9_]+)\s*\(", text)))
 
@@ -747,22 +748,73 @@ def softened_stochastic_barnes_hut_force_octree8_recompute_vjp(points, masses, *
     return _StochasticOctree8Recompute.apply(points, masses, True, cfg)
 
 
-# register_* exist in the reference to hand handler capsules to XLA; with
-# torch there is nothing to register, so they only load the library.
-def _register(*_a, **_k) -> None:
-    lib()
+# register_* (python/jax_sbh_ffi.py:99-338): hand this library's XLA
+# handlers (include/sbh_xla_ffi.h, the reference's symbol names) to XLA under
+# the reference's target names. With jax importable they register exactly as
+# the reference does (jax.ffi.pycapsule, platform "CUDA", api_version 1);
+# without jax there is no XLA to register with, and the torch functions of
+# this module call the same kernels through the C entry points.
+_FFI_TARGETS = {
+    "register_bruteforce_gravity": [("sbh_bruteforce_gravity", "sbh_bruteforce_gravity_ffi")],
+    "register_softened_direct_force": [("sbh_direct_force_soft", "sbh_direct_force_soft_ffi")],
+    "register_softened_direct_force_vjp": [("sbh_direct_force_soft_vjp", "sbh_direct_force_soft_vjp_ffi")],
+    "register_build_octree_level3_buffers": [("sbh_build_octree_level3_buffers",
+                                              "sbh_build_octree_level3_buffers_ffi")],
+    "register_build_octree8_buffers": [("sbh_build_octree8_buffers", "sbh_build_octree8_buffers_ffi")],
+    "register_barnes_hut_gravity": [("sbh_barnes_hut_gravity", "sbh_barnes_hut_gravity_ffi"),
+                                    ("sbh_barnes_hut_gravity_3d", "sbh_barnes_hut_gravity_ffi_3d")],
+    "register_stochastic_barnes_hut_gravity": [("sbh_stochastic_bh_gravity", "sbh_stochastic_bh_gravity_ffi"),
+                                               ("sbh_stochastic_bh_gravity_3d", "sbh_stochastic_bh_gravity_ffi_3d")],
+    "register_stochastic_barnes_hut_force": [("sbh_stochastic_bh_force", "sbh_stochastic_bh_force_ffi"),
+                                             ("sbh_stochastic_bh_force_3d", "sbh_stochastic_bh_force_ffi_3d")],
+    "register_softened_stochastic_barnes_hut_force": [
+        ("sbh_stochastic_bh_force_soft", "sbh_stochastic_bh_force_soft_ffi"),
+        ("sbh_stochastic_bh_force_soft_3d", "sbh_stochastic_bh_force_soft_ffi_3d")],
+    "register_barnes_hut_force": [("sbh_barnes_hut_force", "sbh_barnes_hut_force_ffi"),
+                                  ("sbh_barnes_hut_force_3d", "sbh_barnes_hut_force_ffi_3d")],
+    "register_softened_barnes_hut_force": [("sbh_barnes_hut_force_soft", "sbh_barnes_hut_force_soft_ffi"),
+                                           ("sbh_barnes_hut_force_soft_3d", "sbh_barnes_hut_force_soft_ffi_3d")],
+    "register_barnes_hut_force_octree8": [("sbh_barnes_hut_force_octree8", "sbh_barnes_hut_force_octree8_ffi")],
+    "register_softened_barnes_hut_force_octree8": [("sbh_barnes_hut_force_octree8_soft",
+                                                    "sbh_barnes_hut_force_octree8_soft_ffi")],
+    "register_softened_barnes_hut_force_octree8_vjp": [("sbh_barnes_hut_force_octree8_soft_vjp",
+                                                        "sbh_barnes_hut_force_octree8_soft_vjp_ffi")],
+    "register_stochastic_barnes_hut_force_octree8": [("sbh_stochastic_bh_force_octree8",
+                                                      "sbh_stochastic_bh_force_octree8_ffi")],
+    "register_softened_stochastic_barnes_hut_force_octree8": [("sbh_stochastic_bh_force_octree8_soft",
+                                                               "sbh_stochastic_bh_force_octree8_soft_ffi")],
+    "register_stochastic_barnes_hut_force_octree8_vjp": [("sbh_stochastic_bh_force_octree8_vjp",
+                                                          "sbh_stochastic_bh_force_octree8_vjp_ffi")],
+    "register_softened_stochastic_barnes_hut_force_octree8_vjp": [("sbh_stochastic_bh_force_octree8_soft_vjp",
+                                                                   "sbh_stochastic_bh_force_octree8_soft_vjp_ffi")],
+}
 
 
-for _name in ("register_bruteforce_gravity", "register_softened_direct_force", "register_softened_direct_force_vjp",
-              "register_build_octree_level3_buffers", "register_build_octree8_buffers",
-              "register_barnes_hut_gravity", "register_stochastic_barnes_hut_gravity",
-              "register_stochastic_barnes_hut_force", "register_softened_stochastic_barnes_hut_force",
-              "register_barnes_hut_force", "register_softened_barnes_hut_force", "register_barnes_hut_force_octree8",
-              "register_softened_barnes_hut_force_octree8", "register_softened_barnes_hut_force_octree8_vjp",
-              "register_stochastic_barnes_hut_force_octree8", "register_softened_stochastic_barnes_hut_force_octree8",
-              "register_stochastic_barnes_hut_force_octree8_vjp",
-              "register_softened_stochastic_barnes_hut_force_octree8_vjp"):
-    globals()[_name] = _register
+# the handlers' C signature: XLA_FFI_Error* handler(XLA_FFI_CallFrame*)
+for _pairs in _FFI_TARGETS.values():
+    for _target, _symbol in _pairs:
+        _SIGS[_symbol] = ([_c_p], _c_p)
+
+
+def _make_register(pairs):
+    def register(path: Optional[str] = None) -> None:
+        """Registers this library's XLA handlers for the reference's target
+        names when jax is importable (the reference's call, api_version 1);
+        otherwise only loads the library. `path` is accepted for the
+        reference's signature; this module always uses its in-tree build."""
+        handle = lib()
+        try:
+            import jax  # noqa: F401  (optional: only needed to hand the handlers to XLA)
+        except ImportError:
+            return
+        for target, symbol in pairs:
+            jax.ffi.register_ffi_target(target, jax.ffi.pycapsule(getattr(handle, symbol)), platform="CUDA",
+                                        api_version=1)
+    return register
+
+
+for _name, _pairs in _FFI_TARGETS.items():
+    globals()[_name] = _make_register(_pairs)
 
 
 # ---------------------------------------------------------------------------
