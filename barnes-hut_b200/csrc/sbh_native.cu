@@ -604,6 +604,8 @@ struct WalkParams {
                    // below quad_g * (beta * diagonal)^2; 0: every accepted node takes it
   float inv_2cut;  // 1 / (2 cutoff) (cutoff walks)
   float cc_coef;   // 1 / (2 sqrt(pi) cutoff^3) (cutoff walks)
+  float quad_lin;  // kappa^2 > 0: accepted quadrupole nodes with r_g^2 <= kappa^2 |c - cell centre|^2 take
+                   // the quadrupole to first order about the group centre c; 0: never
 };
 
 // Minimum-image displacement of a periodic box (minImageDisplacement,
@@ -642,6 +644,171 @@ __device__ __forceinline__ bool prune_node(const float4& cell, const float* gmin
   }
   float d2 = __fadd_rn(__fadd_rn(__fmul_rn(t[0], t[0]), __fmul_rn(t[1], t[1])), __fmul_rn(t[2], t[2]));
   return d2 > r2;
+}
+
+// ---------------------------------------------------------------------------
+// Linearized quadrupole. An accepted node whose cell lies far from the group
+// compared with the group's size (r_g^2 <= kappa^2 |c - cell centre|^2, c the
+// group box centre, r_g its half diagonal) takes its quadrupole field to
+// first order about c: a_q(x_t - X) ~ a_q(c - X) + J(c - X) (x_t - c), J the
+// field's (symmetric) Jacobian. The sum over such nodes of a_q(c - X) and
+// J(c - X) is then one 9-value expansion per group, applied to each target
+// once at the end of the walk, instead of one quadrupole evaluation per
+// (target, node) pair. The monopole stays exact at every target. With
+// h = |x|^2 + eps^2 and f_n = h^{-(2n+1)/2}:
+//   a_q = (1.5 tr S f2 - 7.5 (x.Sx) f3) x + 3 f2 Sx,
+//   J   = (52.5 (x.Sx) f4 - 7.5 tr S f3) x x^T - 15 f3 (Sx x^T + x (Sx)^T)
+//         + (1.5 tr S f2 - 7.5 (x.Sx) f3) I + 3 f2 S.
+// For the adjoint, a group's linearized terms contribute w_t . (a_q + J dx_t)
+// to L; per node that is W . a_q(x) + V : J(x) with W = sum_t w_t and
+// V = sym sum_t w_t (x_t - c)^T, whose gradients with respect to x = c - X
+// and S (contractions of the third to fifth derivatives of h^{-1/2}) are
+//   dL/dx = J W + 0.5 [ -945 f5 (x.Sx)(x.Vx) x
+//             + 105 f4 ((tr S (x.Vx) + tr V (x.Sx) + 4 Sx.Vx) x + 2 (x.Vx) Sx + 2 (x.Sx) Vx)
+//             - 15 f3 ((tr S tr V + 2 S:V) x + 4 V Sx + 4 S Vx + 2 tr V Sx + 2 tr S Vx) ],
+//   dL/dS = c1 x x^T + 1.5 f2 (W x^T + x W^T) - 15 f3 (Vx x^T + x (Vx)^T) + c2 I + 3 f2 V,
+//   c1 = -7.5 (W.x) f3 + 52.5 (x.Vx) f4 - 7.5 tr V f3, c2 = 1.5 (W.x) f2 - 7.5 (x.Vx) f3 + 1.5 tr V f2,
+// and dL/dX = -dL/dx. Symmetric 3x3 matrices are packed (xx, yy, zz, xy, xz, yz).
+
+__device__ __forceinline__ void lq_symv(const float* A, float x0, float x1, float x2, float* o) {
+  o[0] = fmaf(A[0], x0, fmaf(A[3], x1, A[4] * x2));
+  o[1] = fmaf(A[3], x0, fmaf(A[1], x1, A[5] * x2));
+  o[2] = fmaf(A[4], x0, fmaf(A[5], x1, A[2] * x2));
+}
+
+// a_q(x) and J(x) packed, for x = c - X (the second moment S packed).
+__device__ __forceinline__ void lq_field(const float* x, const float* S, float eps2, float* a, float* J, float* f) {
+  const float h = fmaf(x[0], x[0], fmaf(x[1], x[1], fmaf(x[2], x[2], eps2)));
+  const float ir = rsqrtf(h), ih = ir * ir;
+  f[0] = ir * ih * ih;  // f2
+  f[1] = f[0] * ih;     // f3
+  f[2] = f[1] * ih;     // f4
+  f[3] = f[2] * ih;     // f5
+  float Sx[3];
+  lq_symv(S, x[0], x[1], x[2], Sx);
+  const float trS = S[0] + S[1] + S[2];
+  const float xSx = fmaf(x[0], Sx[0], fmaf(x[1], Sx[1], x[2] * Sx[2]));
+  const float be = fmaf(1.5f * trS, f[0], -7.5f * xSx * f[1]);
+  const float al = fmaf(52.5f * xSx, f[2], -7.5f * trS * f[1]);
+  const float f2x3 = 3.0f * f[0], f3x15 = 15.0f * f[1];
+#pragma unroll
+  for (int d = 0; d < 3; d++) a[d] = fmaf(be, x[d], f2x3 * Sx[d]);
+  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int e = 0; e < 6; e++) {
+    const int i = ii[e], j = jj[e];
+    float v = fmaf(al * x[i], x[j], -f3x15 * fmaf(Sx[i], x[j], x[i] * Sx[j]));
+    v = fmaf(f2x3, S[e], v);
+    J[e] = i == j ? v + be : v;
+  }
+}
+
+// dL/dx (g) and dL/dS (G, packed) of L = W . a_q(x) + V : J(x), from
+// lq_field's J and radial factors f = (f2, f3, f4, f5).
+__device__ __forceinline__ void lq_node_adjoint(const float* x, const float* S, const float* J, const float* f,
+                                                const float* W, const float* V, float* g, float* G) {
+  float Sx[3], Vx[3], SVx[3], VSx[3];
+  lq_symv(S, x[0], x[1], x[2], Sx);
+  lq_symv(V, x[0], x[1], x[2], Vx);
+  lq_symv(S, Vx[0], Vx[1], Vx[2], SVx);
+  lq_symv(V, Sx[0], Sx[1], Sx[2], VSx);
+  lq_symv(J, W[0], W[1], W[2], g);  // J W
+  const float trS = S[0] + S[1] + S[2], trV = V[0] + V[1] + V[2];
+  const float xSx = fmaf(x[0], Sx[0], fmaf(x[1], Sx[1], x[2] * Sx[2]));
+  const float xVx = fmaf(x[0], Vx[0], fmaf(x[1], Vx[1], x[2] * Vx[2]));
+  const float SxVx = fmaf(Sx[0], Vx[0], fmaf(Sx[1], Vx[1], Sx[2] * Vx[2]));
+  const float SdV = fmaf(S[0], V[0], fmaf(S[1], V[1], fmaf(S[2], V[2],
+                    2.0f * fmaf(S[3], V[3], fmaf(S[4], V[4], S[5] * V[5])))));
+  const float Wx = fmaf(W[0], x[0], fmaf(W[1], x[1], W[2] * x[2]));
+  const float f2 = f[0], f3 = f[1], f4 = f[2], f5 = f[3];
+  const float kx = fmaf(-945.0f * f5, xSx * xVx,
+                        fmaf(105.0f * f4, fmaf(trS, xVx, fmaf(trV, xSx, 4.0f * SxVx)),
+                             -15.0f * f3 * fmaf(trS, trV, 2.0f * SdV)));
+  const float c4a = 105.0f * f4 * xVx, c4b = 105.0f * f4 * xSx, c3 = -7.5f * f3;  // the 0.5 folded in
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    float v = fmaf(0.5f * kx, x[d], fmaf(c4a, Sx[d], c4b * Vx[d]));
+    v = fmaf(c3, fmaf(4.0f, VSx[d] + SVx[d], fmaf(2.0f * trV, Sx[d], 2.0f * trS * Vx[d])), v);
+    g[d] += v;
+  }
+  const float c1 = fmaf(-7.5f * Wx, f3, fmaf(52.5f * xVx, f4, -7.5f * trV * f3));
+  const float c2 = fmaf(1.5f * Wx, f2, fmaf(-7.5f * xVx, f3, 1.5f * trV * f2));
+  const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+  for (int e = 0; e < 6; e++) {
+    const int i = ii[e], j = jj[e];
+    float v = fmaf(c1 * x[i], x[j], 1.5f * f2 * fmaf(W[i], x[j], x[i] * W[j]));
+    v = fmaf(-15.0f * f3, fmaf(Vx[i], x[j], x[i] * Vx[j]), v);
+    v = fmaf(3.0f * f2, V[e], v);
+    G[e] = i == j ? v + c2 : v;
+  }
+}
+
+// Per-warp shared state of the linearized quadrupole during one group's walk:
+// the queue of accepted nodes waiting for their one-per-group evaluation (one
+// node per lane when 32 have gathered), each lane's running sums of a_q and
+// J over the nodes it evaluated, and the group's constants.
+struct LinQueue {
+  int node[32];
+  float acc[9][32];  // [a_q (3), J (6)][lane]
+  float grp[16];     // c (3), r_g^2, W (3), V (6)
+};
+
+// Group centre and squared half diagonal, IEEE operations in the oracle's
+// order (group_centre in oracle/sbh_oracle.c), so both take the same
+// linearization decisions.
+__device__ __forceinline__ void lq_group_centre(const float* gmin, const float* gmax, float* c4) {
+  float hd[3];
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    c4[d] = __fmul_rn(0.5f, __fadd_rn(gmin[d], gmax[d]));
+    hd[d] = __fmul_rn(0.5f, __fsub_rn(gmax[d], gmin[d]));
+  }
+  c4[3] = __fadd_rn(__fadd_rn(__fmul_rn(hd[0], hd[0]), __fmul_rn(hd[1], hd[1])), __fmul_rn(hd[2], hd[2]));
+}
+
+// Whether an accepted quadrupole node is linearized (warp-uniform).
+__device__ __forceinline__ bool lq_linear(const float* c4, const float4& cell, float k2) {
+  const float dx = __fsub_rn(c4[0], cell.x), dy = __fsub_rn(c4[1], cell.y), dz = __fsub_rn(c4[2], cell.z);
+  const float R2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+  return c4[3] <= __fmul_rn(k2, R2);
+}
+
+// Sum over the warp, result in every lane.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Evaluates the queued nodes, one per lane (lanes < cnt): adds a_q and J to
+// the lane's sums and, when node_adj is given, the node's dL/dX and dL/dS.
+__device__ __forceinline__ void lq_flush(const NodeRec* __restrict__ nodes, LinQueue* lq, int cnt, float eps2,
+                                         float* __restrict__ node_adj, int lane) {
+  __syncwarp();
+  if (lane < cnt) {
+    const int k = lq->node[lane];
+    const NodeRec* nd = nodes + k;
+    const float4 A = __ldg(&nd->com), Qd = __ldg(&nd->quad), X2 = __ldg(&nd->quad2);
+    const float x[3] = {lq->grp[0] - A.x, lq->grp[1] - A.y, lq->grp[2] - A.z};
+    const float S[6] = {Qd.x, Qd.y, Qd.z, Qd.w, X2.x, X2.y};
+    float a[3], J[6], f[4];
+    lq_field(x, S, eps2, a, J, f);
+#pragma unroll
+    for (int c = 0; c < 3; c++) lq->acc[c][lane] += a[c];
+#pragma unroll
+    for (int c = 0; c < 6; c++) lq->acc[3 + c][lane] += J[c];
+    if (node_adj) {
+      float g[3], G[6];
+      lq_node_adjoint(x, S, J, f, &lq->grp[4], &lq->grp[7], g, G);
+      float* na = node_adj + static_cast<int64_t>(k) * kNodeAdj;
+#pragma unroll
+      for (int c = 0; c < 3; c++) atomicAdd(&na[c], -g[c]);
+#pragma unroll
+      for (int c = 0; c < 6; c++) atomicAdd(&na[4 + c], G[c]);
+    }
+  }
+  __syncwarp();
 }
 
 // The walks are compiled three times: four targets per lane (groups of up
@@ -875,7 +1042,7 @@ void carve(C& c, int64_t n, int nseg, int S, bool normals, bool adjoint, Layout&
   L.cap = cap;
   L.meta = c.template take<uint32_t>(8);
   L.gbins = c.template take<uint32_t>(kGroupBins);
-  L.counters = c.template take<unsigned long long>(4);
+  L.counters = c.template take<unsigned long long>(kCounters);
   L.boxes = c.template take<SegBox>(nseg);
   L.bb = c.template take<uint32_t>(6 * nseg);
   L.seg_off = c.template take<int64_t>(nseg + 1);
@@ -1042,7 +1209,7 @@ int sbh_native_build(cudaStream_t stream, const float* points, const float* mass
   uint32_t* status = static_cast<uint32_t*>(workspace);
   cudaError_t e = cudaMemsetAsync(status, 0, 64, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(L.meta, 0, 8 * sizeof(uint32_t), stream);
-  if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, 4 * sizeof(unsigned long long), stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(L.counters, 0, kCounters * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   // system offsets (device copy, or [0, n] for one system)
   if (num_systems > 1) {
@@ -1216,6 +1383,7 @@ int check_params(const sbh_native_params* p) {
   if (p->prune_radius < 0.0f) return invalid("prune_radius must be >= 0");
   if (p->prune_radius > 0.0f && !(p->cutoff > 0.0f)) return invalid("prune_radius needs an erfc cutoff (cutoff > 0)");
   if (!(p->quadrupole_radius >= 0.0f)) return invalid("quadrupole_radius must be >= 0");
+  if (!(p->quadrupole_linear >= 0.0f)) return invalid("quadrupole_linear must be >= 0");
   return SBH_OK;
 }
 
@@ -1232,14 +1400,16 @@ WalkParams walk_params(const sbh_native_params* p) {
                     p->prune_radius * p->prune_radius,
                     qr > 0.0f ? qr * qr : 0.0f,
                     static_cast<float>(0.5 / c),
-                    static_cast<float>(1.0 / (2.0 * 1.7724538509055160 * c * c * c))};
+                    static_cast<float>(1.0 / (2.0 * 1.7724538509055160 * c * c * c)),
+                    p->quadrupole && p->quadrupole_linear > 0.0f ? p->quadrupole_linear * p->quadrupole_linear
+                                                                  : 0.0f};
 }
 
 // Recounts the interactions of the last force or adjoint walk (same tree,
 // parameters and target range) into the counters, once per walk.
 int refresh_counts(cudaStream_t stream, const void* ws, const Header& h, const Layout& L) {
   if (h.last_walk != 1 || h.counts_fresh) return SBH_OK;
-  cudaError_t e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
+  cudaError_t e = cudaMemsetAsync(L.counters, 0, kCounters * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   const sbh_native_params& p = h.last_params;
   Header hr = h;
@@ -1453,7 +1623,7 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   const uint32_t* qperm = which == 0 ? v0 : v1;
   query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
-  e = cudaMemsetAsync(L.counters, 0, 3 * sizeof(unsigned long long), stream);
+  e = cudaMemsetAsync(L.counters, 0, kCounters * sizeof(unsigned long long), stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1), 0, INT64_MAX};
   e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, tpl2::wn_walk_kernel, tree_view(L), G, beta, out,
@@ -1491,11 +1661,25 @@ int sbh_native_quadrupole_count(cudaStream_t stream, const void* workspace, size
   if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
   if (!far_quadrupole) return invalid("far_quadrupole must be non-null");
   if (int rc = refresh_counts(stream, workspace, h, L)) return rc;
-  unsigned long long c = 0;
-  cudaError_t e = cudaMemcpyAsync(&c, L.counters + 2, sizeof(c), cudaMemcpyDeviceToHost, stream);
+  unsigned long long c[2] = {0, 0};
+  cudaError_t e = cudaMemcpyAsync(c, L.counters + 2, sizeof(c), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
-  *far_quadrupole = c;
+  *far_quadrupole = c[0] + c[1];
+  return SBH_OK;
+}
+
+int sbh_native_far_counts(cudaStream_t stream, const void* workspace, size_t workspace_bytes, uint64_t* out3) {
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!out3) return invalid("out3 must be non-null");
+  if (int rc = refresh_counts(stream, workspace, h, L)) return rc;
+  unsigned long long c[3] = {0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(c, L.counters + 2, sizeof(c), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  for (int i = 0; i < 3; i++) out3[i] = c[i];
   return SBH_OK;
 }
 

@@ -38,6 +38,9 @@ constexpr int kQueryGroup = SBH_QUERY_GROUP;  // targets per group of external q
 static_assert(kQueryGroup <= kGroupTwoSlots, "query groups are walked by the two-slot kernels");
 constexpr int kNodeAdj = 12;    // per-node adjoint floats: A_X(3) A_M(1) G(6) pad(2)
 constexpr int kPartAdj = 4;     // per-particle adjoint floats: dx(3) dm(1)
+// interaction counters of the count-only walk: far, near (per target), far with the exact
+// quadrupole, far with the linearized quadrupole (per target), linearized (group, node) pairs
+constexpr int kCounters = 8;
 
 }  // namespace nt
 }  // namespace sbh

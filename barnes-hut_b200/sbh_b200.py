@@ -146,6 +146,7 @@ _SIGS = {
     "sbh_native_stats": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_quadrupole_count": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_set_group_size": ([_c_p, _c_p, _c_sz, _c_i], _c_i),
+    "sbh_native_far_counts": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_set_target_range": ([_c_p, _c_p, _c_sz, _c_i64, _c_i64], _c_i),
     "sbh_mesh_sample_workspace_bytes": ([_c_i64], _c_sz),
     "sbh_mesh_vertex_workspace_bytes": ([_c_i64], _c_sz),
@@ -161,15 +162,25 @@ class NativeParams(ctypes.Structure):
 
     _fields_ = [("beta", ctypes.c_float), ("softening", ctypes.c_float), ("cutoff", ctypes.c_float),
                 ("quadrupole", ctypes.c_int), ("periodic", ctypes.c_int), ("box_length", ctypes.c_float),
-                ("prune_radius", ctypes.c_float), ("quadrupole_radius", ctypes.c_float)]
+                ("prune_radius", ctypes.c_float), ("quadrupole_radius", ctypes.c_float),
+                ("quadrupole_linear", ctypes.c_float)]
 
 
 # Accepted nodes closer to a target group than this many opening radii take
-# the quadrupole, farther ones the monopole alone. On Plummer spheres at
-# beta = 2 it keeps the quadrupole on about half of the far interactions and
-# raises the force error from 1.8e-5 to 2.9e-5 (N = 2^20, rel-L2 against the
-# FP64 direct sum). 0 gives every accepted node the quadrupole.
-QUADRUPOLE_RADIUS = 1.6
+# the quadrupole, farther ones the monopole alone (0: every accepted node
+# takes it). With the once-per-group linearized form below the quadrupole of a
+# distant node costs little, so every accepted node keeps it.
+QUADRUPOLE_RADIUS = 0.0
+
+# Accepted quadrupole nodes with r_g <= QUADRUPOLE_LINEAR |c - cell centre|
+# (c the group box centre, r_g its half diagonal) take the quadrupole to first
+# order about c, evaluated once per group instead of once per target
+# (sbh_native_params.quadrupole_linear; 0: every quadrupole is exact). On the
+# bench workload (8 Plummer spheres of 2^20, beta 2, groups of 128) 95% of the
+# far interactions are linearized at 0.5; the adjoint walk went from 365 ms
+# (exact quadrupole within 1.6 opening radii) to 324 ms at the same force error
+# against the FP64 direct sum (2.5e-5).
+QUADRUPOLE_LINEAR = 0.5
 
 _lib_handle = None
 _lib_lock = threading.Lock()
@@ -1013,19 +1024,24 @@ class NativeTree:
 
     @staticmethod
     def params(beta=2.0, softening=1e-3, cutoff=0.0, quadrupole=True, periodic=False, box_length=1.0,
-               prune_radius=0.0, quadrupole_radius=QUADRUPOLE_RADIUS) -> NativeParams:
+               prune_radius=0.0, quadrupole_radius=QUADRUPOLE_RADIUS,
+               quadrupole_linear=QUADRUPOLE_LINEAR) -> NativeParams:
         return NativeParams(float(beta), float(softening), float(cutoff), int(bool(quadrupole)), int(bool(periodic)),
-                            float(box_length), float(prune_radius), float(quadrupole_radius))
+                            float(box_length), float(prune_radius), float(quadrupole_radius),
+                            float(quadrupole_linear))
 
     def force(self, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0, quadrupole: bool = True,
               periodic: bool = False, box_length: float = 1.0, prune_radius: float = 0.0,
-              quadrupole_radius: float = QUADRUPOLE_RADIUS, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+              quadrupole_radius: float = QUADRUPOLE_RADIUS, quadrupole_linear: float = QUADRUPOLE_LINEAR,
+              out: Optional[torch.Tensor] = None) -> torch.Tensor:
         """Softened self-gravity. periodic: minimum image in a cube of side
         box_length (monopole far field); cutoff > 0: the erfc short-range
         split; prune_radius > 0: skip cells beyond it (TreePM short range);
         quadrupole_radius: the quadrupole only within that many opening radii
-        of the group (0: everywhere)."""
-        prm = self.params(beta, softening, cutoff, quadrupole, periodic, box_length, prune_radius, quadrupole_radius)
+        of the group (0: everywhere); quadrupole_linear: kappa of the
+        once-per-group first-order quadrupole (0: exact everywhere)."""
+        prm = self.params(beta, softening, cutoff, quadrupole, periodic, box_length, prune_radius, quadrupole_radius,
+                          quadrupole_linear)
         out = out if out is not None else torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
         _check(lib().sbh_native_force(_stream_ptr(self.device), ctypes.byref(prm), _p(out), _p(self.ws),
                                       self.ws.numel()), "native_force")
@@ -1033,9 +1049,11 @@ class NativeTree:
 
     def force_vjp(self, cotangent, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,
                   quadrupole: bool = True, periodic: bool = False, box_length: float = 1.0,
-                  prune_radius: float = 0.0, quadrupole_radius: float = QUADRUPOLE_RADIUS, want_force: bool = True):
+                  prune_radius: float = 0.0, quadrupole_radius: float = QUADRUPOLE_RADIUS,
+                  quadrupole_linear: float = QUADRUPOLE_LINEAR, want_force: bool = True):
         """(force or None, d/d points, d/d masses) of sum(cotangent * force)."""
-        prm = self.params(beta, softening, cutoff, quadrupole, periodic, box_length, prune_radius, quadrupole_radius)
+        prm = self.params(beta, softening, cutoff, quadrupole, periodic, box_length, prune_radius, quadrupole_radius,
+                          quadrupole_linear)
         cot = _f32(cotangent, self.device)
         if cot.shape != (self.n, 3):
             raise ValueError("cotangent must have shape (N, 3)")
@@ -1084,8 +1102,12 @@ class NativeTree:
         fq = ctypes.c_uint64(0)
         _check(lib().sbh_native_quadrupole_count(_stream_ptr(self.device), _p(self.ws), self.ws.numel(),
                                                   ctypes.byref(fq)), "native_quadrupole_count")
+        fc = (ctypes.c_uint64 * 3)()
+        _check(lib().sbh_native_far_counts(_stream_ptr(self.device), _p(self.ws), self.ws.numel(), fc),
+               "native_far_counts")
         return dict(nodes=int(out[0]), groups=int(out[1]), far=int(out[2]), near=int(out[3]),
-                    far_quadrupole=int(fq.value))
+                    far_quadrupole=int(fq.value), far_quadrupole_exact=int(fc[0]),
+                    far_quadrupole_linear=int(fc[1]), linear_pairs=int(fc[2]))
 
     def export(self):
         """(sorted keys u64, permutation, node records (nn x 80 bytes)) as CPU numpy arrays."""

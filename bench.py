@@ -139,14 +139,78 @@ def cpu_reference_eval_time(points, masses, sample: int, threads: int):
     tree = O.RefTree3D(points, masses, variant=0)  # Tree3D<8,1>: leaf size 8
     t_build = time.perf_counter() - t0
     t0 = time.perf_counter()
-    tree.eval(q, BETA, O.REF_K_SOFT_FORCE, eps=EPS, threads=threads)
+    _, counts = tree.eval(q, BETA, O.REF_K_SOFT_FORCE, eps=EPS, threads=threads)
     t_force = time.perf_counter() - t0
     t0 = time.perf_counter()
     tree.eval(q, BETA, O.REF_K_SOFT_FORCE_VJP, eps=EPS, cot=cot, threads=threads)
     t_vjp = time.perf_counter() - t0
     scale = n / q.shape[0]
+    # num_contribs of evaluateBarnesHut_stackless (include/barnes_hut.h:29,45,50): the interactions each
+    # query takes under the reference's own per-target opening rule
     return t_build + (t_force + t_vjp) * scale, dict(build_s=t_build, force_sample_s=t_force, vjp_sample_s=t_vjp,
-                                                     sample_queries=int(q.shape[0]))
+                                                     sample_queries=int(q.shape[0]),
+                                                     interactions_per_query=float(np.mean(counts)))
+
+
+def reference_gpu_plugin_time(points, masses, cot):
+    """The reference's own GPU plugin (its src/sbh_ffi.cu, unmodified, built
+    for sm_100a into oracle/_ref/libsbh_ref_gpu.so) on this GPU, through its
+    handlers in the order of the reference's custom_vjp recompute flow
+    (python/jax_sbh_ffi.py:1804-1891): octree8 build at depth 7 (corners =
+    data min/max -+ 1e-3), softened force, rebuild, softened query-side VJP,
+    all N queries, "no cutoff" = 1e6 box lengths, pruning off. One warm-up
+    evaluation on 4,096 queries loads the module; one full evaluation is
+    timed with CUDA events (it includes the handlers' own cudaMalloc, frees
+    and stream synchronisations)."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import sbh_oracle as O
+
+    L = O.refgpu()
+    dev = torch.device("cuda", 0)
+    n = points.shape[0]
+    depth = 7
+    total = O.octree8_total_nodes(depth)
+    P = torch.as_tensor(points, device=dev)
+    M = torch.as_tensor(masses, device=dev)
+    C = torch.as_tensor(cot, device=dev)
+    Z = torch.zeros_like(P)
+    MN = torch.as_tensor(points.min(0) - np.float32(1e-3), device=dev)
+    MX = torch.as_tensor(points.max(0) + np.float32(1e-3), device=dev)
+    leaf = torch.empty(n * 32, dtype=torch.uint8, device=dev)
+    node = torch.empty(total * 104, dtype=torch.uint8, device=dev)
+    con = torch.empty(total * 32, dtype=torch.uint8, device=dev)
+    f = torch.empty((n, 3), device=dev)
+    g = torch.empty((n, 3), device=dev)
+    cut = 1e6 * float((points.max(0) - points.min(0)).max())
+    s = torch.cuda.current_stream().cuda_stream
+
+    def evaluate(nq):
+        O.refgpu_check(L.ref_build_octree8(s, P.data_ptr(), Z.data_ptr(), M.data_ptr(), n, MN.data_ptr(),
+                                           MX.data_ptr(), leaf.data_ptr(), leaf.numel(), node.data_ptr(), node.numel(),
+                                           con.data_ptr(), con.numel(), depth))
+        O.refgpu_check(L.ref_bh_force_octree8_soft(s, leaf.data_ptr(), leaf.numel(), node.data_ptr(), node.numel(),
+                                                   P.data_ptr(), nq, f.data_ptr(), BETA, EPS, cut, 0, 4.0, 0, 1.0,
+                                                   256))
+        O.refgpu_check(L.ref_build_octree8(s, P.data_ptr(), Z.data_ptr(), M.data_ptr(), n, MN.data_ptr(),
+                                           MX.data_ptr(), leaf.data_ptr(), leaf.numel(), node.data_ptr(), node.numel(),
+                                           con.data_ptr(), con.numel(), depth))
+        O.refgpu_check(L.ref_bh_force_octree8_soft_vjp(s, leaf.data_ptr(), leaf.numel(), node.data_ptr(),
+                                                       node.numel(), P.data_ptr(), nq, C.data_ptr(), g.data_ptr(),
+                                                       BETA, EPS, cut, 0, 4.0, 0, 1.0, 256))
+
+    evaluate(4096)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    evaluate(n)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return dict(ms_per_eval=ms, evals_per_s=1000.0 / ms, n=n, max_depth=depth,
+                what="the reference's unmodified GPU plugin: octree8 build, softened force, rebuild, softened "
+                     "query-side VJP of all N queries (its custom_vjp recompute flow)")
 
 
 def run_reference(args):
@@ -176,6 +240,14 @@ def run_reference(args):
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "detail": info,
     }
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            cot = np.random.default_rng(5).normal(size=p.shape).astype(np.float32)
+            line["reference_gpu_plugin"] = reference_gpu_plugin_time(p, m, cot)
+    except (ImportError, OSError, RuntimeError) as e:  # plugin not built here: the CPU line stands alone
+        line["reference_gpu_plugin"] = {"unavailable": str(e).splitlines()[0][:200]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -720,7 +792,7 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    total_ms, walk_ms = 0.0, 0.0
+    total_ms, walk_ms, build_ms = 0.0, 0.0, 0.0
     marks = []
     for _ in range(args.steps):
         flush.zero_()
@@ -732,6 +804,7 @@ def run_ours(args):
     for a, b, c, d in marks:
         total_ms += a.elapsed_time(d)
         walk_ms += b.elapsed_time(c)
+        build_ms += a.elapsed_time(b)
     clocks = sampler.stop()
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
@@ -863,9 +936,13 @@ def run_ours(args):
 
     # roofline of the dominant kernel (the adjoint walk)
     walk_s = walk_ms / args.steps * 1e-3
-    flops_walk = adjoint_walk_flops(st)
+    flops_walk = adjoint_walk_flops(st, n * K)
     fp32_peak = measure_fp32_peak(B, torch, dev)
     traffic = WALK_DRAM_BYTES_PER_PARTICLE * n * K
+    # the build: HBM-bound, algorithmic bytes per build of K systems
+    build_s = build_ms / args.steps * 1e-3
+    build_bytes = K * n * BUILD_ALG_BYTES_PER_PARTICLE + st["nodes"] * BUILD_ALG_BYTES_PER_NODE
+    hbm_peak, hbm_source = hbm_peak_gbs()
 
     extras = {}
     if not args.no_extras:
@@ -884,12 +961,24 @@ def run_ours(args):
 
     if rank == 0:
         cpu = None
+        ref_rule = None
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             t_eval, info = cpu_reference_eval_time(systems[0][0], systems[0][1], args.cpu_sample, threads)
             cpu = {"value": 1.0 / t_eval, "unit": "evals/s", "cores": threads, "kind": "reference",
                    "sample": (f"reference Tree3D<8,1> build of all {n} points + force and query-side VJP of "
                               f"{info['sample_queries']} sampled particles (beta 2), extrapolated to all")}
+            # the walk's flops by the convention of 20 flop per interaction (GPU Gems 3 ch. 31), the VJP
+            # counted as twice the force, with the interactions the reference's per-target rule takes
+            inter = info["interactions_per_query"] * n * K
+            flops_ref = REF_FLOPS_PER_INTERACTION * (1 + REF_VJP_FACTOR) * inter
+            ref_rule = {"flops_per_interaction": REF_FLOPS_PER_INTERACTION, "vjp_factor": REF_VJP_FACTOR,
+                        "interactions_per_step": inter,
+                        "interactions_per_query": info["interactions_per_query"],
+                        "achieved": flops_ref / walk_s / 1e12, "frac": flops_ref / walk_s / 1e12 / fp32_peak,
+                        "counted_by": (f"num_contribs of the reference's CPU evaluateBarnesHut_stackless on "
+                                       f"Tree3D<8,1> (leaf 8, beta 2) over {info['sample_queries']} sampled "
+                                       "queries of system 0")}
         launches = args.steps * (build_launches(K) + WALK_LAUNCHES + FINALIZE_LAUNCHES)
         plain_eps = 1000.0 / plain_ms
         line = {
@@ -897,7 +986,10 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer spheres, a=1, r<10a)",
             "config": {"workload": workload(n, K), "n": n, "systems_per_gpu": K, "beta": BETA, "theta": 1.0 / BETA,
-                       "softening": EPS, "leaf_size": LEAF, "far_field": f"monopole, + quadrupole within {B.QUADRUPOLE_RADIUS} opening radii of the group",
+                       "softening": EPS, "leaf_size": LEAF,
+                       "far_field": (f"monopole at every target + quadrupole of every accepted node, taken to first "
+                                     f"order about the group centre (once per group) where r_g <= "
+                                     f"{B.QUADRUPOLE_LINEAR} |c - cell centre|, exact at every target elsewhere"),
                        "vjp": "positions and masses",
                        "batched": f"{K} systems in one forest: one build, one walk, one finalize per step",
                        "l2": "flushed between steps (256 MB write, outside the timed events)",
@@ -914,7 +1006,23 @@ def run_ours(args):
                          "peak": fp32_peak, "unit": "TFLOP/s", "frac": flops_walk / walk_s / 1e12 / fp32_peak,
                          "peak_source": "measured in this run: the faster of sbh_probe_fp32 and sbh_probe_fp32x2 (FMA chains, scalar and packed)",
                          "traffic": traffic, "walk_ms": walk_s * 1e3,
-                         "interactions": {"far": st["far"], "far_quadrupole": st["far_quadrupole"], "near": st["near"]}},
+                         "interactions": {"far": st["far"], "far_quadrupole_exact": st["far_quadrupole_exact"],
+                                          "far_quadrupole_linear": st["far_quadrupole_linear"],
+                                          "linear_pairs": st["linear_pairs"], "near": st["near"]},
+                         "flops_counted_as": "per operation of the walk's own formulas (an FMA as 2): per target "
+                                             "200 per far node with the exact quadrupole, 45 with the monopole "
+                                             "(linearized nodes included), 55 per near pair; 370 per linearized "
+                                             "(group, node) pair and 33 per target for the group expansion",
+                         "reference_convention": ref_rule,
+                         "build": {"bound": "hbm", "achieved": build_bytes / build_s / 1e9, "peak": hbm_peak,
+                                   "unit": "GB/s", "frac": build_bytes / build_s / 1e9 / hbm_peak,
+                                   "peak_source": hbm_source, "algorithmic_bytes": build_bytes,
+                                   "build_ms": build_s * 1e3,
+                                   "traffic": (None if BUILD_DRAM_BYTES_PER_PARTICLE is None
+                                               else BUILD_DRAM_BYTES_PER_PARTICLE * n * K),
+                                   "bytes_counted_as": "per particle 16 read (position, mass) + 20 written "
+                                                       "(sorted position and mass, permutation); per node 80 "
+                                                       "written"}},
             "cpu_baseline": cpu,
             "e2e": {"value": world * K * 1000.0 / e_ms, "unit": "evals/s",
                     "h2d_bytes_per_step": int(K * n * 28), "d2h_bytes_per_step": int(K * n * 28),
@@ -959,17 +1067,53 @@ WALK_LAUNCHES = 2
 WALK_DRAM_BYTES_PER_PARTICLE = 150.9
 FINALIZE_LAUNCHES = 5
 
-# FP32 flops per interaction of the adjoint walk (force + adjoint, counted
-# from adjoint_walk_kernel, an FMA as 2): far node with the quadrupole, far
-# node with the monopole alone, near pair.
+# FP32 flops of the adjoint walk (force + adjoint, counted from
+# adjoint_walk_kernel and lq_field / lq_node_adjoint, an FMA as 2): per target
+# and far node with the exact quadrupole, per target and far node with the
+# monopole (the linearized nodes' monopole included), per near pair; per
+# (group, node) pair with the linearized quadrupole (field, Jacobian and node
+# adjoint, once per group), and per target the group expansion applied at the
+# end (force and query-side gradient).
 ADJ_FLOPS_FAR_QUAD = 200
 ADJ_FLOPS_FAR_MONO = 45
 ADJ_FLOPS_NEAR = 55
+ADJ_FLOPS_LINEAR_PAIR = 370
+ADJ_FLOPS_LINEAR_APPLY = 33
 
 
-def adjoint_walk_flops(st) -> float:
-    fq = st["far_quadrupole"]
-    return ADJ_FLOPS_FAR_QUAD * fq + ADJ_FLOPS_FAR_MONO * (st["far"] - fq) + ADJ_FLOPS_NEAR * st["near"]
+# The roofline convention of the benchmark definition: 20 flop per
+# interaction (Nyland, Harris and Prins, GPU Gems 3 ch. 31), the VJP counted
+# as twice the force, interactions as the reference's per-target rule counts
+# them.
+REF_FLOPS_PER_INTERACTION = 20
+REF_VJP_FACTOR = 2
+
+# Algorithmic bytes of one native build: per particle the position and mass
+# read (16) and the sorted position and mass plus the permutation written
+# (16 + 4); per node one 80-byte record written.
+BUILD_ALG_BYTES_PER_PARTICLE = 16 + 20
+BUILD_ALG_BYTES_PER_NODE = 80
+
+# DRAM bytes (read + write) of one forest build per particle, summed over the
+# build's kernels from one ncu capture of the bench's 8 x 2^20 Plummer forest.
+BUILD_DRAM_BYTES_PER_PARTICLE = None
+
+
+def hbm_peak_gbs():
+    """The measured copy bandwidth of MEASURED_PEAKS.json, else the pool's
+    earlier measurement."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, STREAM-style copy)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback (6.65 TB/s, an earlier copy measurement on this pool)"
+
+
+def adjoint_walk_flops(st, n_targets) -> float:
+    fq = st["far_quadrupole_exact"]
+    lin = ADJ_FLOPS_LINEAR_PAIR * st["linear_pairs"] + (ADJ_FLOPS_LINEAR_APPLY * n_targets if st["linear_pairs"] else 0)
+    return ADJ_FLOPS_FAR_QUAD * fq + ADJ_FLOPS_FAR_MONO * (st["far"] - fq) + ADJ_FLOPS_NEAR * st["near"] + lin
 
 
 def main():

@@ -377,6 +377,12 @@ typedef struct sbh_native_params {
                               closer to the group box than quadrupole_radius opening radii
                               (beta * diagonal), the monopole alone beyond; 0: for every
                               accepted node */
+  float quadrupole_linear; /* with quadrupole = 1: kappa > 0 takes the quadrupole of an accepted node
+                              to first order about the group box centre c, a_q(c - X) + J(c - X)
+                              (x - c), instead of at every target, when the group's half diagonal
+                              r_g satisfies r_g^2 <= kappa^2 |c - cell centre|^2. The monopole is
+                              still evaluated at every target. Such a node costs one evaluation per
+                              group instead of one per target; 0: every quadrupole is exact */
 } sbh_native_params;
 
 /* Most targets one group holds (one warp walks a group). */
@@ -475,9 +481,16 @@ int sbh_native_stats(cudaStream_t stream, const void* workspace, size_t workspac
                      uint64_t* out4);
 
 /* Synchronises; *far_quadrupole = the far interactions (per target) of the
- * last force or adjoint walk on this workspace that took the quadrupole. */
+ * last force or adjoint walk on this workspace that took the quadrupole,
+ * exact or linearized. */
 int sbh_native_quadrupole_count(cudaStream_t stream, const void* workspace, size_t workspace_bytes,
                                 uint64_t* far_quadrupole);
+
+/* Synchronises; out3 = {far interactions per target with the exact
+ * quadrupole, far interactions per target with the linearized quadrupole,
+ * (group, node) pairs of the linearized ones} of the last force or adjoint
+ * walk on this workspace. A linearized pair is evaluated once per group. */
+int sbh_native_far_counts(cudaStream_t stream, const void* workspace, size_t workspace_bytes, uint64_t* out3);
 
 /* Synchronises; copies sorted keys (n x u64), the permutation (n x u32,
  * sorted slot -> input index) and the 80-byte node records to device buffers

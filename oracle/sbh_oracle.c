@@ -759,6 +759,7 @@ typedef struct {
   int32_t* near_idx; /* near-field leaf node ids */
   int64_t* gstart;
   int64_t* gend;
+  float* gcen; /* per group: centre (3) and squared half diagonal of its box (float) */
 } NativeTree;
 
 static void cell_geometry(const NativeTree* t, int64_t nd, uint64_t key) {
@@ -815,6 +816,7 @@ void orc_native_free(void* h) {
   free(t->near_idx);
   free(t->gstart);
   free(t->gend);
+  free(t->gcen);
   free(t);
 }
 
@@ -1029,6 +1031,35 @@ static int native_quad_order(float d2, float rc2) {
   return !(g_orc_quad_g > 0.0f) || d2 < g_orc_quad_g * rc2;
 }
 
+static float g_orc_quad_lin2 = 0.0f; /* kappa^2 in float, as the CUDA walk holds it */
+void orc_native_set_quad_linear(float kappa) { g_orc_quad_lin2 = kappa > 0.0f ? kappa * kappa : 0.0f; }
+
+/* Far-entry flags of the plan (NativeTree.far_quad). */
+#define QUAD_NONE 0
+#define QUAD_EXACT 1
+#define QUAD_LINEAR 2
+
+/* Group centre c = (gmin + gmax) / 2 and squared half diagonal rg2 of a
+ * group box, in float with one rounding per operation (the CUDA walk's
+ * order); the quadrupole of an accepted node is linearized about c when
+ * rg2 <= kappa^2 |c - cell centre|^2. */
+static void group_centre(const float* gmin, const float* gmax, float* c4) {
+  float hd[3];
+  for (int d = 0; d < 3; d++) {
+    c4[d] = 0.5f * (gmin[d] + gmax[d]);
+    hd[d] = 0.5f * (gmax[d] - gmin[d]);
+  }
+  c4[3] = (hd[0] * hd[0] + hd[1] * hd[1]) + hd[2] * hd[2];
+}
+
+static int quad_linear(const float* c4, const float* cell) {
+  if (!(g_orc_quad_lin2 > 0.0f)) return 0;
+  float dx = c4[0] - cell[0], dy = c4[1] - cell[1], dz = c4[2] - cell[2];
+  float R2 = (dx * dx + dy * dy) + dz * dz;
+  return c4[3] <= g_orc_quad_lin2 * R2;
+}
+
+
 /*
  * Target groups cut from the tree. For every node holding more than G
  * particles its children are taken in order; each maximal run of
@@ -1091,6 +1122,7 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
   t->group_size = group_size;
   free(t->gstart);
   free(t->gend);
+  free(t->gcen);
   t->gstart = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
   t->gend = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
   int64_t ng;
@@ -1104,6 +1136,7 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
     }
   }
   t->ngroups = ng;
+  t->gcen = (float*)malloc(sizeof(float) * 4 * (ng > 0 ? ng : 1));
   double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
   native_moments(t, pts, masses, mom);
   float fbeta = (float)beta;
@@ -1125,6 +1158,7 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
         gmin[d] = fminf(gmin[d], v);
         gmax[d] = fmaxf(gmax[d], v);
       }
+    group_centre(gmin, gmax, &t->gcen[4 * g]);
     int64_t k = 0, cnt_int = 0;
     while (k < t->nn) {
       float X[3], M, C[3];
@@ -1142,7 +1176,8 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
           t->far_idx = (int32_t*)realloc(t->far_idx, sizeof(int32_t) * fcap);
           t->far_quad = (uint8_t*)realloc(t->far_quad, fcap);
         }
-        t->far_quad[nf] = (uint8_t)native_quad_order(d2, rc2);
+        t->far_quad[nf] = (uint8_t)(!native_quad_order(d2, rc2) ? QUAD_NONE
+                                    : quad_linear(&t->gcen[4 * g], C) ? QUAD_LINEAR : QUAD_EXACT);
         t->far_idx[nf++] = (int32_t)k;
         cnt_int += 1;
         k = t->skip[k];
@@ -1166,6 +1201,79 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
   return total;
 }
 
+/* The quadrupole field a_q(x) of quad_force and its Jacobian J = da_q/dx
+ * (symmetric: a_q is the gradient of 0.5 S : grad grad h^{-1/2}),
+ * with h = |x|^2 + eps^2 + 1e-12, tau = 1.5 tr S:
+ *   J = h^{-5/2} (3 S + tau I) - 15 h^{-7/2} (S x x^T + x x^T S)
+ *       - 5 tau h^{-7/2} x x^T - 7.5 (x^T S x) h^{-7/2} I + 52.5 (x^T S x) h^{-9/2} x x^T.
+ * J packed (xx, yy, zz, xy, xz, yz). */
+static void quad_field_jacobian(const double* x, const double* S, double eps, double* a, double* J) {
+  double h = x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + eps * eps + 1e-12;
+  double ih = 1.0 / h, ir = 1.0 / sqrt(h);
+  double ir5 = ir * ih * ih, ir7 = ir5 * ih, ir9 = ir7 * ih;
+  double Sx[3];
+  sym_mul(S, x, Sx);
+  double tau = 1.5 * (S[0] + S[1] + S[2]);
+  double xSx = x[0] * Sx[0] + x[1] * Sx[1] + x[2] * Sx[2];
+  for (int d = 0; d < 3; d++) a[d] = ir5 * (3.0 * Sx[d] + tau * x[d]) - 7.5 * xSx * ir7 * x[d];
+  static const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+  for (int e = 0; e < 6; e++) {
+    int i = ii[e], j = jj[e];
+    double dij = i == j ? 1.0 : 0.0;
+    J[e] = ir5 * (3.0 * S[e] + tau * dij) - 15.0 * ir7 * (Sx[i] * x[j] + x[i] * Sx[j]) - 5.0 * tau * ir7 * x[i] * x[j] -
+           7.5 * xSx * ir7 * dij + 52.5 * xSx * ir9 * x[i] * x[j];
+  }
+}
+
+/* Accepted nodes whose quadrupole is taken to first order about the group
+ * box centre c instead of at every target: those with r_g <= kappa |c - X|
+ * (r_g the half diagonal of the group box, X the node's COM);
+ * a_q(x) ~ a_q(c - X) + J(c - X) (x - c). kappa <= 0: never. */
+/* The node side of one linearized quadrupole for a group with cotangent sum
+ * W = sum_t w_t and V = sym sum_t w_t (x_t - c)^T (packed xx, yy, zz, xy, xz,
+ * yz): L = W . a_q(x) + V : J(x) with x = c - X. Returns g = dL/dx (so
+ * dL/dX = -g) and G = dL/dS (the symmetric-gradient convention of quad_vjp).
+ * With h = |x|^2 + eps^2 + 1e-12 and f_n = h^{-(2n+1)/2}:
+ *   G = c1 x x^T + 1.5 f2 (W x^T + x W^T) - 15 f3 (Vx x^T + x (Vx)^T) + c2 I + 3 f2 V,
+ *     c1 = -7.5 (W.x) f3 + 52.5 (x.Vx) f4 - 7.5 tr(V) f3, c2 = 1.5 (W.x) f2 - 7.5 (x.Vx) f3 + 1.5 tr(V) f2;
+ *   g = J W + 0.5 [ -945 f5 (x.Sx)(x.Vx) x
+ *         + 105 f4 ((tr S (x.Vx) + tr V (x.Sx) + 4 Sx.Vx) x + 2 (x.Vx) Sx + 2 (x.Sx) Vx)
+ *         - 15 f3 ((tr S tr V + 2 S:V) x + 4 V Sx + 4 S Vx + 2 tr V Sx + 2 tr S Vx) ]
+ * (contractions of the third to fifth derivatives of h^{-1/2}). */
+static void quad_linear_node_adjoint(const double* x, const double* S, double eps, const double* W, const double* V,
+                                     double* g, double* G) {
+  double a[3], J[6];
+  quad_field_jacobian(x, S, eps, a, J);
+  double h = x[0] * x[0] + x[1] * x[1] + x[2] * x[2] + eps * eps + 1e-12;
+  double ih = 1.0 / h, ir = 1.0 / sqrt(h);
+  double f2 = ir * ih * ih, f3 = f2 * ih, f4 = f3 * ih, f5 = f4 * ih;
+  double Sx[3], Vx[3], SVx[3], VSx[3], JW[3];
+  sym_mul(S, x, Sx);
+  sym_mul(V, x, Vx);
+  sym_mul(S, Vx, SVx);
+  sym_mul(V, Sx, VSx);
+  sym_mul(J, W, JW);
+  double trS = S[0] + S[1] + S[2], trV = V[0] + V[1] + V[2];
+  double xSx = x[0] * Sx[0] + x[1] * Sx[1] + x[2] * Sx[2];
+  double xVx = x[0] * Vx[0] + x[1] * Vx[1] + x[2] * Vx[2];
+  double SxVx = Sx[0] * Vx[0] + Sx[1] * Vx[1] + Sx[2] * Vx[2];
+  double SdV = S[0] * V[0] + S[1] * V[1] + S[2] * V[2] + 2.0 * (S[3] * V[3] + S[4] * V[4] + S[5] * V[5]);
+  double Wx = W[0] * x[0] + W[1] * x[1] + W[2] * x[2];
+  double kx = -945.0 * f5 * xSx * xVx + 105.0 * f4 * (trS * xVx + trV * xSx + 4.0 * SxVx) -
+              15.0 * f3 * (trS * trV + 2.0 * SdV);
+  for (int d = 0; d < 3; d++)
+    g[d] = JW[d] + 0.5 * (kx * x[d] + 210.0 * f4 * (xVx * Sx[d] + xSx * Vx[d]) -
+                          15.0 * f3 * (4.0 * VSx[d] + 4.0 * SVx[d] + 2.0 * trV * Sx[d] + 2.0 * trS * Vx[d]));
+  double c1 = -7.5 * Wx * f3 + 52.5 * xVx * f4 - 7.5 * trV * f3;
+  double c2 = 1.5 * Wx * f2 - 7.5 * xVx * f3 + 1.5 * trV * f2;
+  static const int ii[6] = {0, 1, 2, 0, 0, 1}, jj[6] = {0, 1, 2, 1, 2, 2};
+  for (int e = 0; e < 6; e++) {
+    int i = ii[e], j = jj[e];
+    G[e] = c1 * x[i] * x[j] + 1.5 * f2 * (W[i] * x[j] + x[i] * W[j]) - 15.0 * f3 * (Vx[i] * x[j] + x[i] * Vx[j]) +
+           (i == j ? c2 : 0.0) + 3.0 * f2 * V[e];
+  }
+}
+
 /*
  * Evaluate the planned sums with the given (possibly perturbed) positions
  * and masses: topology, sorted order and decisions stay frozen, node
@@ -1184,6 +1292,7 @@ void orc_native_eval(void* h, const float* pts, const float* masses, double eps,
 #pragma omp parallel for schedule(dynamic, 8) reduction(+ : L)
   for (int64_t g = 0; g < t->ngroups; g++) {
     int64_t s0 = t->gstart[g], s1 = t->gend[g];
+    const double gc[3] = {t->gcen[4 * g], t->gcen[4 * g + 1], t->gcen[4 * g + 2]};
     for (int64_t i = s0; i < s1; i++) {
       int64_t qi = t->perm[i];
       double q[3] = {pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]};
@@ -1194,7 +1303,16 @@ void orc_native_eval(void* h, const float* pts, const float* masses, double eps,
         double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
         native_mi(r);
         soft_force_pair(r, o[0], &sp, acc);
-        if (quad && t->far_quad[e]) quad_force(r, o + 4, eps, acc);
+        if (quad && t->far_quad[e] == QUAD_EXACT) {
+          quad_force(r, o + 4, eps, acc);
+        } else if (quad && t->far_quad[e] == QUAD_LINEAR) {
+          /* first order about the (frozen) group centre */
+          double rc[3] = {gc[0] - o[1], gc[1] - o[2], gc[2] - o[3]};
+          double a[3], J[6], dl[3] = {q[0] - gc[0], q[1] - gc[1], q[2] - gc[2]}, Jd[3];
+          quad_field_jacobian(rc, o + 4, eps, a, J);
+          sym_mul(J, dl, Jd);
+          for (int d = 0; d < 3; d++) acc[d] += a[d] + Jd[d];
+        }
       }
       for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
         int32_t k = t->near_idx[e];
@@ -1243,6 +1361,32 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
   memset(dm, 0, sizeof(double) * n);
   for (int64_t g = 0; g < t->ngroups; g++) {
     int64_t s0 = t->gstart[g], s1 = t->gend[g];
+    const double gc[3] = {t->gcen[4 * g], t->gcen[4 * g + 1], t->gcen[4 * g + 2]};
+    /* linearized quadrupoles: the group's cotangent sums W = sum w, V = sym sum w (x - c)^T; per node
+     * dL/dX = -g, dL/dS = G (quad_linear_node_adjoint); each target's query side takes J w */
+    double W[3] = {0, 0, 0}, V[6] = {0, 0, 0, 0, 0, 0};
+    for (int64_t i = s0; i < s1; i++) {
+      int64_t qi = t->perm[i];
+      double wi[3] = {w[3 * qi], w[3 * qi + 1], w[3 * qi + 2]};
+      double dl[3] = {pts[3 * qi] - gc[0], pts[3 * qi + 1] - gc[1], pts[3 * qi + 2] - gc[2]};
+      for (int d = 0; d < 3; d++) W[d] += wi[d];
+      V[0] += wi[0] * dl[0];
+      V[1] += wi[1] * dl[1];
+      V[2] += wi[2] * dl[2];
+      V[3] += 0.5 * (wi[0] * dl[1] + wi[1] * dl[0]);
+      V[4] += 0.5 * (wi[0] * dl[2] + wi[2] * dl[0]);
+      V[5] += 0.5 * (wi[1] * dl[2] + wi[2] * dl[1]);
+    }
+    for (int64_t e = t->far_off[g]; quad && e < t->far_off[g + 1]; e++) {
+      if (t->far_quad[e] != QUAD_LINEAR) continue;
+      int32_t k = t->far_idx[e];
+      const double* o = &mom[MOM * k];
+      double rc[3] = {gc[0] - o[1], gc[1] - o[2], gc[2] - o[3]};
+      double gl[3], Gl[6];
+      quad_linear_node_adjoint(rc, o + 4, eps, W, V, gl, Gl);
+      for (int d = 0; d < 3; d++) AX[MOM * k + 1 + d] -= gl[d];
+      for (int c = 0; c < 6; c++) AX[MOM * k + 4 + c] += Gl[c];
+    }
     for (int64_t i = s0; i < s1; i++) {
       int64_t qi = t->perm[i];
       double q[3] = {pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]};
@@ -1256,7 +1400,13 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
         double jt[3] = {0, 0, 0}, f[3] = {0, 0, 0};
         soft_force_pair_vjp(r, o[0], wi, &sp, jt);
         soft_force_pair(r, 1.0, &sp, f);
-        if (quad && t->far_quad[e]) quad_vjp(r, o + 4, wi, eps, jt, &AX[MOM * k + 4]);
+        if (quad && t->far_quad[e] == QUAD_EXACT) quad_vjp(r, o + 4, wi, eps, jt, &AX[MOM * k + 4]);
+        if (quad && t->far_quad[e] == QUAD_LINEAR) {
+          double rc[3] = {gc[0] - o[1], gc[1] - o[2], gc[2] - o[3]}, a[3], J[6], Jw[3];
+          quad_field_jacobian(rc, o + 4, eps, a, J);
+          sym_mul(J, wi, Jw);
+          for (int d = 0; d < 3; d++) gq[d] += Jw[d];  /* the node side is added per group above */
+        }
         for (int d = 0; d < 3; d++) {
           gq[d] += jt[d];
           AX[MOM * k + 1 + d] -= jt[d];
@@ -1313,10 +1463,25 @@ int64_t orc_native_quadrupole_interactions(void* h) {
   int64_t total = 0;
   for (int64_t g = 0; g < t->ngroups; g++) {
     int64_t c = 0;
-    for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) c += t->far_quad[e];
+    for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) c += t->far_quad[e] != QUAD_NONE;
     total += c * (t->gend[g] - t->gstart[g]);
   }
   return total;
+}
+
+/* Far interactions (per target) of the plan with the linearized quadrupole,
+ * and the (group, node) pairs they come from. */
+void orc_native_linear_quadrupole_counts(void* h, int64_t* per_target, int64_t* pairs) {
+  NativeTree* t = (NativeTree*)h;
+  int64_t pt = 0, pr = 0;
+  for (int64_t g = 0; g < t->ngroups; g++) {
+    int64_t c = 0;
+    for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) c += t->far_quad[e] == QUAD_LINEAR;
+    pr += c;
+    pt += c * (t->gend[g] - t->gstart[g]);
+  }
+  *per_target = pt;
+  *pairs = pr;
 }
 
 void orc_native_plan_stats(void* h, int64_t* ngroups, int64_t* nfar, int64_t* nnear) {
@@ -1398,6 +1563,22 @@ static inline void far_term(const double* r, double M, const double* S, int use_
   const double tr = S[0] + S[1] + S[2];
   const double xSx = r[0] * Sx[0] + r[1] * Sx[1] + r[2] * Sx[2];
   for (int d = 0; d < 3; d++) acc[d] += c * r[d] + ir5 * (3.0 * Sx[d] + 1.5 * tr * r[d]) - 7.5 * xSx * ir5 * ih * r[d];
+}
+
+/* The field of one planned far entry at q: the monopole, plus the exact
+ * quadrupole (QUAD_EXACT) or its first-order expansion about the frozen group
+ * centre gc (QUAD_LINEAR). */
+static inline void plan_far_term(const double* q, const double* o, int flag, const double* gc, const SoftParams* sp,
+                                 double* acc) {
+  double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
+  far_term(r, o[0], o + 4, flag == QUAD_EXACT, sp, acc);
+  if (flag == QUAD_LINEAR) {
+    double rc[3] = {gc[0] - o[1], gc[1] - o[2], gc[2] - o[3]}, a[3], J[6], Jd[3];
+    double dl[3] = {q[0] - gc[0], q[1] - gc[1], q[2] - gc[2]};
+    quad_field_jacobian(rc, o + 4, sp->eps, a, J);
+    sym_mul(J, dl, Jd);
+    for (int d = 0; d < 3; d++) acc[d] += a[d] + Jd[d];
+  }
 }
 
 void orc_native_fd(void* h, const float* pts, const float* masses, const float* w, double eps, int quad,
@@ -1515,13 +1696,13 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
       int ai = -1;
       for (int a = 0; a < na; a++)
         if (anc[a] == K) ai = a;
-      const int uq = quad && t->far_quad[e];
+      const int uq = quad ? t->far_quad[e] : QUAD_NONE;
+      const double gck[3] = {t->gcen[4 * gk], t->gcen[4 * gk + 1], t->gcen[4 * gk + 2]};
       for (int c = 0; c < 4; c++) {
         double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
         for (int p = 0; p < 2; p++) {
           const double* o = ai >= 0 ? pm[ai][c][p] : &mom[MOM * K];
-          double r[3] = {xp[c][p][0] - o[1], xp[c][p][1] - o[2], xp[c][p][2] - o[3]};
-          far_term(r, o[0], o + 4, uq, &sp, f[p]);
+          plan_far_term(xp[c][p], o, uq, gck, &sp, f[p]);
         }
         D4[c] += wk[0] * (f[0][0] - f[1][0]) + wk[1] * (f[0][1] - f[1][1]) + wk[2] * (f[0][2] - f[1][2]);
       }
@@ -1562,17 +1743,14 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
       const int32_t A = anc[a];
       for (int64_t e = foff[A]; e < foff[A + 1]; e++) {
         const int64_t g = fgrp[e];
-        const int uq = quad && fq[e];
+        const int uq = quad ? fq[e] : QUAD_NONE;
+        const double gcg[3] = {t->gcen[4 * g], t->gcen[4 * g + 1], t->gcen[4 * g + 2]};
         for (int64_t s = t->gstart[g]; s < t->gend[g]; s++) {
           if (s == sk) continue; /* target k's row is term (1) */
           const double* ws = &sw[3 * s];
           for (int c = 0; c < 4; c++) {
             double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
-            for (int p = 0; p < 2; p++) {
-              const double* o = pm[a][c][p];
-              double r[3] = {sx[3 * s] - o[1], sx[3 * s + 1] - o[2], sx[3 * s + 2] - o[3]};
-              far_term(r, o[0], o + 4, uq, &sp, f[p]);
-            }
+            for (int p = 0; p < 2; p++) plan_far_term(&sx[3 * s], pm[a][c][p], uq, gcg, &sp, f[p]);
             D4[c] += ws[0] * (f[0][0] - f[1][0]) + ws[1] * (f[0][1] - f[1][1]) + ws[2] * (f[0][2] - f[1][2]);
           }
         }

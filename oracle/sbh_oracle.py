@@ -100,6 +100,8 @@ def _orc() -> ctypes.CDLL:
         lib.orc_native_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_d, _c_i, _c_p, _c_p]
         lib.orc_native_plan_stats.argtypes = [_c_p, _c_p, _c_p, _c_p]
         lib.orc_native_fd.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_i, _c_p, _c_i64, _c_d, _c_d, _c_p, _c_p]
+        lib.orc_native_set_quad_linear.argtypes = [_c_f]
+        lib.orc_native_linear_quadrupole_counts.argtypes = [_c_p, _c_p, _c_p]
         lib._typed = True
     return lib
 
@@ -248,6 +250,13 @@ class NativeTree:
         """Far interactions (per target) of the plan that take the quadrupole."""
         return int(self._lib.orc_native_quadrupole_interactions(self._h))
 
+    def linear_quadrupole_counts(self):
+        """(far interactions per target with the linearized quadrupole, the
+        (group, node) pairs they come from) of the recorded plan."""
+        a, b = _c_i64(), _c_i64()
+        self._lib.orc_native_linear_quadrupole_counts(self._h, ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
     def plan_stats(self):
         a, b, c = _c_i64(), _c_i64(), _c_i64()
         self._lib.orc_native_plan_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
@@ -299,6 +308,24 @@ class native_periodic:
 
     def __exit__(self, *exc):
         _orc().orc_native_set_periodic(0, 1.0, 0.0)
+        return False
+
+
+class native_quadrupole_linear:
+    """Context: accepted quadrupole nodes with r_g^2 <= kappa^2 |c - cell centre|^2
+    (group box centre c, half diagonal r_g) take the quadrupole to first
+    order about c (the CUDA walk's quadrupole_linear); 0 restores the exact
+    form everywhere. Plans recorded inside keep their flags."""
+
+    def __init__(self, kappa: float):
+        self.kappa = kappa
+
+    def __enter__(self):
+        _orc().orc_native_set_quad_linear(self.kappa)
+        return self
+
+    def __exit__(self, *exc):
+        _orc().orc_native_set_quad_linear(0.0)
         return False
 
 

@@ -177,7 +177,7 @@ def test_config3_gradient_vs_fp64_finite_differences_at_2e20(cuda, plummer_1m):
     gx, gm, gq = gx.cpu().numpy()[idx], gm.cpu().numpy()[idx], gq.cpu().numpy()[idx]
     st = t.stats()
     T = O.NativeTree(p, m, leaf_size=16)
-    with O.native_quadrupole_radius(B.QUADRUPOLE_RADIUS):
+    with O.native_quadrupole_radius(B.QUADRUPOLE_RADIUS), O.native_quadrupole_linear(B.QUADRUPOLE_LINEAR):
         count = T.plan(BETA, G)
     assert count == st["far"] + st["near"], "the GPU walk and the oracle took different plans"
     # h = 1e-4 central differences carry an O(h^2) truncation error of about

@@ -53,19 +53,26 @@ def test_native_tree_bit_exact_vs_oracle(cuda, dist, leaf):
     np.testing.assert_allclose(nd["com"][:, 3].sum() >= 0, True)
 
 
-@pytest.mark.parametrize("quad,qradius", [(True, 0.0), (True, 1.6), (False, 0.0)])
-def test_native_force_matches_oracle_same_plan(cuda, quad, qradius):
+@pytest.mark.parametrize("quad,qradius,linear", [(True, 0.0, 0.0), (True, 1.6, 0.0), (False, 0.0, 0.0),
+                                                 (True, 0.0, 0.5), (True, 1.6, 0.35)])
+def test_native_force_matches_oracle_same_plan(cuda, quad, qradius, linear):
     """qradius 0: every accepted node takes the quadrupole; 1.6: only those
-    within 1.6 opening radii of the group (the default)."""
+    within 1.6 opening radii of the group. linear > 0: the quadrupoles of
+    nodes far from the group (r_g <= linear |c - cell centre|) are taken to
+    first order about the group centre, once per group."""
     p, m = W.plummer(30000, seed=5)
     t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=False)
-    f = t.force(beta=2.0, softening=1e-3, quadrupole=quad, quadrupole_radius=qradius).cpu().numpy()
+    f = t.force(beta=2.0, softening=1e-3, quadrupole=quad, quadrupole_radius=qradius,
+                quadrupole_linear=linear).cpu().numpy()
     st = t.stats()
     T = O.NativeTree(p, m, leaf_size=16)
-    with O.native_quadrupole_radius(qradius):
+    with O.native_quadrupole_radius(qradius), O.native_quadrupole_linear(linear):
         inter = T.plan(2.0, B.native_group_size())
     want, _ = T.force(1e-3, quad=quad)
     assert rel_l2(f, want) < 1e-5
+    lin_target, lin_pairs = T.linear_quadrupole_counts()
+    assert st["far_quadrupole_linear"] == lin_target and st["linear_pairs"] == lin_pairs
+    assert (lin_pairs > 0) == (linear > 0)
     # same node-packed target groups
     assert st["groups"] == T.plan_stats()[0]
     # same opening decisions up to ulp-level ties
@@ -85,25 +92,31 @@ def test_native_force_accuracy_vs_fp64_direct(cuda):
     idx = np.random.default_rng(0).choice(p.shape[0], 4096, replace=False)
     want = O.direct_force_soft(p, m, p[idx], 1e-3)
     err = {}
-    for q in (0.0, B.QUADRUPOLE_RADIUS):
-        f = t.force(beta=2.0, softening=1e-3, quadrupole=True, quadrupole_radius=q).cpu().numpy()
-        err[q] = rel_l2(f[idx], want)
+    # exact quadrupole everywhere; the default (every accepted node, linearized where far from the group);
+    # exact quadrupole within 1.6 opening radii, monopole beyond; monopole only
+    for name, kw in (("exact", dict(quadrupole_radius=0.0, quadrupole_linear=0.0)), ("default", {}),
+                     ("radius", dict(quadrupole_radius=1.6, quadrupole_linear=0.0))):
+        f = t.force(beta=2.0, softening=1e-3, quadrupole=True, **kw).cpu().numpy()
+        err[name] = rel_l2(f[idx], want)
     f = t.force(beta=2.0, softening=1e-3, quadrupole=False).cpu().numpy()
     err["mono"] = rel_l2(f[idx], want)
-    assert err[0.0] < err[B.QUADRUPOLE_RADIUS] < err["mono"]
-    assert err[B.QUADRUPOLE_RADIUS] < 8e-5
+    assert err["exact"] < err["default"] < err["mono"]
+    assert err["exact"] < err["radius"] < err["mono"]
+    assert err["default"] < 8e-5
 
 
-@pytest.mark.parametrize("quad,qradius", [(True, 0.0), (True, 1.6), (False, 0.0)])
-def test_native_adjoint_matches_oracle(cuda, quad, qradius):
+@pytest.mark.parametrize("quad,qradius,linear", [(True, 0.0, 0.0), (True, 1.6, 0.0), (False, 0.0, 0.0),
+                                                 (True, 0.0, 0.5), (True, 1.6, 0.35)])
+def test_native_adjoint_matches_oracle(cuda, quad, qradius, linear):
     rng = np.random.default_rng(7)
     p, m = W.plummer(20000, seed=7)
     m = (m * rng.uniform(0.5, 1.5, m.shape)).astype(np.float32)
     w = rng.normal(size=p.shape).astype(np.float32)
     t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True)
-    f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=quad, quadrupole_radius=qradius)
+    f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=quad, quadrupole_radius=qradius,
+                            quadrupole_linear=linear)
     T = O.NativeTree(p, m, leaf_size=16)
-    with O.native_quadrupole_radius(qradius):
+    with O.native_quadrupole_radius(qradius), O.native_quadrupole_linear(linear):
         T.plan(2.0, B.native_group_size())
     want_f, _ = T.force(1e-3, quad=quad)
     dx, dm = T.adjoint(w, 1e-3, quad=quad)
@@ -313,17 +326,20 @@ def test_native_target_ranges_sum_to_full(cuda, world):
 def test_native_two_and_three_slot_kernels_match_oracle(cuda, group_size):
     """Groups of at most 64 run on the two-targets-per-lane walks, of 65 to
     96 on the three-per-lane walks: forces and the full adjoint with the
-    quadrupole (radius 1.6) against the oracle's plan with the same group
-    size, on a clustered and a uniform system."""
+    default quadrupole (every accepted node, linearized about the group
+    centre where the group is small against its distance) against the
+    oracle's plan with the same group size, on a clustered and a uniform
+    system."""
     rng = np.random.default_rng(61)
     for p, m in (W.plummer(20000, seed=62), W.uniform_cube(15000, seed=63)):
         w = rng.normal(size=p.shape).astype(np.float32)
         t = B.NativeTree().build(p, m, leaf_size=16, with_adjoint=True, group_size=group_size)
-        f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=True, quadrupole_radius=1.6)
-        f2 = t.force(beta=2.0, softening=1e-3, quadrupole=True, quadrupole_radius=1.6).cpu().numpy()
+        f, gx, gm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole=True)
+        f2 = t.force(beta=2.0, softening=1e-3, quadrupole=True).cpu().numpy()
         st = t.stats()
+        assert st["linear_pairs"] > 0
         T = O.NativeTree(p, m, leaf_size=16)
-        with O.native_quadrupole_radius(1.6):
+        with O.native_quadrupole_radius(B.QUADRUPOLE_RADIUS), O.native_quadrupole_linear(B.QUADRUPOLE_LINEAR):
             inter = T.plan(2.0, group_size)
         want_f, _ = T.force(1e-3, quad=True)
         dx, dm = T.adjoint(w, 1e-3, quad=True)

@@ -128,3 +128,34 @@ def test_native_adjoint_approximates_exact_gradient():
     ex, em = O.direct_full_adjoint(p, m, w, 1e-3)
     assert rel_l2(dx, ex) < 1e-3
     assert rel_l2(dm, em) < 1e-3
+
+
+def test_native_linearized_quadrupole_adjoint_matches_finite_differences():
+    """With the quadrupole of distant nodes taken to first order about the
+    group centre (frozen with the plan), the oracle's adjoint -- the query
+    side J w, and per (group, node) dL/dX and dL/dS of W . a_q + V : J --
+    equals Richardson-extrapolated central differences of the same frozen
+    plan, and agrees with full-loss differences of the evaluator."""
+    rng = np.random.default_rng(16)
+    p, m = W.plummer(2000, seed=16)
+    m = (m * rng.uniform(0.5, 1.5, m.shape)).astype(np.float32)
+    w = rng.normal(size=p.shape).astype(np.float32)
+    eps = 1e-2
+    T = O.NativeTree(p, m, leaf_size=8)
+    with O.native_quadrupole_linear(0.5):
+        T.plan(2.0, 32)
+    lin_target, lin_pairs = T.linear_quadrupole_counts()
+    assert 0 < lin_target < T.quadrupole_interactions() and lin_pairs > 0
+    dx, dm = T.adjoint(w, eps, quad=True)
+    idx = rng.choice(p.shape[0], 30, replace=False)
+    fx, fm = T.finite_differences(w, eps, idx, hx=1e-4, hm_rel=1e-4, quad=True)
+    fx2, fm2 = T.finite_differences(w, eps, idx, hx=5e-5, hm_rel=5e-5, quad=True)
+    assert rel_l2(dx[idx], (4 * fx2 - fx) / 3) < 1e-8
+    assert rel_l2(dm[idx], (4 * fm2 - fm) / 3) < 1e-8
+    k, h = idx[0], 1e-3
+    pp = p.astype(np.float64)
+    pp[k, 2] += h
+    lp = T.force(eps, points=pp.astype(np.float32), masses=m, w=w, quad=True)[1]
+    pp[k, 2] -= 2 * h
+    lm = T.force(eps, points=pp.astype(np.float32), masses=m, w=w, quad=True)[1]
+    assert abs((lp - lm) / (2 * h) - dx[k, 2]) <= 2e-3 * (abs(dx[k, 2]) + 1.0)
