@@ -744,6 +744,50 @@ __device__ __forceinline__ void lq_node_adjoint(const float* x, const float* S, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Node tiles staged in shared memory. The walks visit nodes in pre-order, so
+// after an opened node the next one is its neighbour in memory, and an
+// accepted node with a small subtree skips only a few records. A warp stages
+// the opening data (topology, COM, cell) of 32 consecutive nodes at once, one
+// node per lane, with cp.async (16 bytes a copy, cached in L2 only), and
+// walks from shared memory until the pre-order index leaves the tile. One L2
+// round trip then serves every visit inside the tile, where each visit used
+// to wait on its own loads. When a visit's successor lies outside the tile,
+// the next tile's copy starts before the visit's terms are evaluated and is
+// waited for only after them, so the copy overlaps the arithmetic.
+constexpr int kTile = 32;
+struct NodeTile {
+  int4 topo[kTile];
+  float4 com[kTile];
+  float4 cell[kTile];
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// Starts staging nodes [base, min(base + kTile, end)) into the warp's tile.
+// Every lane calls it (warp-uniform) after it has read what it needs from
+// the previous tile; stage_wait() completes the copy for all lanes.
+__device__ __forceinline__ void stage_tile_async(const NodeRec* __restrict__ nodes, int base, int end,
+                                                 NodeTile* tile, int lane) {
+  __syncwarp();  // every lane has finished reading the previous tile
+  const int k = base + lane;
+  if (k < end) {
+    const NodeRec* nd = nodes + k;
+    cp_async16(&tile->topo[lane], &nd->topo);
+    cp_async16(&tile->com[lane], &nd->com);
+    cp_async16(&tile->cell[lane], &nd->cell);
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void stage_wait() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncwarp();
+}
+
 // Per-warp shared state of the linearized quadrupole during one group's walk:
 // the queue of accepted nodes waiting for their one-per-group evaluation (one
 // node per lane when 32 have gathered), each lane's running sums of a_q and
