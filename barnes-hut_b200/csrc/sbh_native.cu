@@ -978,6 +978,68 @@ __global__ void adjoint_combine_kernel(const float4* __restrict__ sp, const uint
   }
 }
 
+// Winding-number node adjoints -> difference arrays over each node's
+// particle range: dL/dX / M (3), (dL/dX . Xc) / M (1), dL/dN (3), with Xc the
+// COM relative to the system's box centre (single-system trees).
+__global__ void wn_node_push_kernel(const NodeRec* __restrict__ nodes, const uint32_t* __restrict__ nn_ptr,
+                                    const float* __restrict__ node_adj, const SegBox* __restrict__ boxes,
+                                    DVec<14>* __restrict__ D) {
+  const uint32_t nn = *nn_ptr;
+  const SegBox b = boxes[0];
+  const double half = 0.5 * static_cast<double>(b.span);
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nn; k += gridDim.x * blockDim.x) {
+    const float* a = node_adj + static_cast<int64_t>(k) * kNodeAdj;
+    bool any = false;
+    for (int c = 0; c < 7; c++) any |= a[c] != 0.0f;
+    if (!any) continue;
+    const NodeRec r = nodes[k];
+    const double M = r.com.w;
+    if (M == 0.0) continue;
+    const double X[3] = {static_cast<double>(r.com.x) - (static_cast<double>(b.lo[0]) + half),
+                         static_cast<double>(r.com.y) - (static_cast<double>(b.lo[1]) + half),
+                         static_cast<double>(r.com.z) - (static_cast<double>(b.lo[2]) + half)};
+    double val[7];
+    for (int c = 0; c < 3; c++) val[c] = a[c] / M;
+    val[3] = (a[0] * X[0] + a[1] * X[1] + a[2] * X[2]) / M;
+    for (int c = 0; c < 3; c++) val[4 + c] = a[4 + c];
+    for (int c = 0; c < 7; c++) {
+      atomicAdd(&D[r.topo.x].v[c], val[c]);
+      atomicAdd(&D[r.topo.y].v[c], -val[c]);
+    }
+  }
+}
+
+// Per sorted source: the direct terms plus the node terms through
+// X = sum m p / M and sum m n (inclusive prefix of D = exclusive prefix at i + 1),
+// written in input order.
+__global__ void wn_combine_kernel(const float4* __restrict__ sp, const float4* __restrict__ sn,
+                                  const uint32_t* __restrict__ perm, const SegBox* __restrict__ boxes, int64_t n,
+                                  const float* __restrict__ part_adj, const float* __restrict__ part_dn,
+                                  const DVec<14>* __restrict__ C, float* __restrict__ dp, float* __restrict__ dn,
+                                  float* __restrict__ dm) {
+  const SegBox b = boxes[0];
+  const double half = 0.5 * static_cast<double>(b.span);
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float4 p = sp[i], nr = sn[i];
+    const double x[3] = {static_cast<double>(p.x) - (static_cast<double>(b.lo[0]) + half),
+                         static_cast<double>(p.y) - (static_cast<double>(b.lo[1]) + half),
+                         static_cast<double>(p.z) - (static_cast<double>(b.lo[2]) + half)};
+    const DVec<14>& c = C[i + 1];
+    const double m = p.w;
+    const uint32_t o = perm[i];
+    const double nn3[3] = {nr.x, nr.y, nr.z};
+    for (int d = 0; d < 3; d++) {
+      dp[3 * static_cast<int64_t>(o) + d] =
+          static_cast<float>(static_cast<double>(part_adj[kPartAdj * i + d]) + m * c.v[d]);
+      dn[3 * static_cast<int64_t>(o) + d] = static_cast<float>(static_cast<double>(part_dn[3 * i + d]) + m * c.v[4 + d]);
+    }
+    const double q = x[0] * c.v[0] + x[1] * c.v[1] + x[2] * c.v[2] - c.v[3] + nn3[0] * c.v[4] + nn3[1] * c.v[5] +
+                     nn3[2] * c.v[6];
+    dm[o] = static_cast<float>(static_cast<double>(part_adj[kPartAdj * i + 3]) + q);
+  }
+}
+
 // The query-side gradient of the last adjoint walk (sorted order) in input order.
 __global__ void query_side_kernel(const uint32_t* __restrict__ perm, int64_t n, const float* __restrict__ gq,
                                   float* __restrict__ out) {
@@ -1675,6 +1737,72 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   remember_walk(workspace, 2, nullptr);
   return check_launch("sbh_native_winding_number");
+}
+
+int sbh_native_winding_number_vjp(cudaStream_t stream, float beta, const float* queries, int64_t nq,
+                                  const float* cotangent, float* out, float* grad_queries, float* grad_points,
+                                  float* grad_normals, float* grad_masses, void* workspace, size_t workspace_bytes,
+                                  void* query_workspace, size_t query_workspace_bytes) {
+  if (!(beta > 0.0f)) return invalid("beta must be > 0");
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!h.normals) return invalid("the tree was built without normals");
+  if (!h.adjoint) return invalid("the tree was built without adjoint scratch (with_adjoint = 0)");
+  if (h.nseg != 1) return invalid("query evaluation needs a single-system tree");
+  if (nq < 0 || nq >= (1ll << 31)) return invalid("number of queries must be in [0, 2^31)");
+  if (h.n > 0 && (!grad_points || !grad_normals || !grad_masses))
+    return invalid("grad_points, grad_normals and grad_masses must be non-null");
+  if (nq > 0 && (!queries || !cotangent || !grad_queries))
+    return invalid("queries, cotangent and grad_queries must be non-null");
+  size_t need = sbh_native_query_workspace_bytes(nq);
+  if (nq > 0 && (!query_workspace || query_workspace_bytes < need))
+    return fail(SBH_ERR_WORKSPACE, "query workspace too small: need " + std::to_string(need) + " bytes");
+  const int64_t n = h.n;
+  cudaError_t e = cudaSuccess;
+  if (n > 0) {
+    e = cudaMemsetAsync(L.part_adj, 0, n * kPartAdj * sizeof(float), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.gq, 0, n * 3 * sizeof(float), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(L.D, 0, (n + 1) * sizeof(DVec<14>), stream);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
+  }
+  if (nq > 0 && n == 0) {
+    e = cudaMemsetAsync(grad_queries, 0, nq * 3 * sizeof(float), stream);
+    if (e == cudaSuccess && out) e = cudaMemsetAsync(out, 0, nq * sizeof(float), stream);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  }
+  if (nq > 0 && n > 0) {
+    Carver c(query_workspace, query_workspace_bytes);
+    uint32_t* qmeta = c.take<uint32_t>(8);
+    uint64_t* k0 = c.take<uint64_t>(nq);
+    uint64_t* k1 = c.take<uint64_t>(nq);
+    uint32_t* v0 = c.take<uint32_t>(nq);
+    uint32_t* v1 = c.take<uint32_t>(nq);
+    uint32_t* hist = c.take<uint32_t>(radix_hist_elems(nq));
+    uint32_t* stmp = c.take<uint32_t>(scan_tiles(radix_hist_elems(nq)));
+    float4* tp = c.take<float4>(nq);
+    int4* groups = c.take<int4>(nq / kQueryGroup + 1);
+    query_keys_kernel<<<gs(nq), 256, 0, stream>>>(queries, nq, L.boxes, k0);
+    int which = 0;
+    e = radix_sort<uint64_t>(stream, k0, v0, k1, v1, nq, 63, false, hist, stmp, &which);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    const uint32_t* qperm = which == 0 ? v0 : v1;
+    query_gather_kernel<<<gs(nq), 256, 0, stream>>>(queries, qperm, nq, tp, groups, qmeta);
+    WalkTargets G{tp, qperm, groups, qmeta, 0, qmeta + 2, static_cast<uint32_t>(nq / kQueryGroup + 1), 0, INT64_MAX};
+    e = launch_walk(stream, qmeta + 2, nq / kQueryGroup + 1, tpl2::wn_adjoint_walk_kernel, tree_view(L), G, beta,
+                    cotangent, out, grad_queries, L.node_adj, L.part_adj, L.gq);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  }
+  if (n > 0) {
+    wn_node_push_kernel<<<gs(L.cap), 256, 0, stream>>>(L.nodes, L.meta, L.node_adj, L.boxes, L.D);
+    e = exclusive_scan<DVec<14>>(stream, ArrayLoad<DVec<14>>{L.D}, n + 1, L.D, L.dtmp, false);
+    if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+    wn_combine_kernel<<<gs(n), 256, 0, stream>>>(L.sp, L.sn, L.v0, L.boxes, n, L.part_adj, L.gq, L.D, grad_points,
+                                                 grad_normals, grad_masses);
+  }
+  remember_walk(workspace, 2, nullptr);
+  return check_launch("sbh_native_winding_number_vjp");
 }
 
 // Synchronises the stream and reports [node count, group count, far

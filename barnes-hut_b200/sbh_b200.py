@@ -143,6 +143,8 @@ _SIGS = {
     "sbh_native_adjoint_query_side": ([_c_p, _c_p, _c_p, _c_sz], _c_i),
     "sbh_native_query_workspace_bytes": ([_c_i64], _c_sz),
     "sbh_native_winding_number": ([_c_p, _c_f, _c_p, _c_i64, _c_p, _c_p, _c_sz, _c_p, _c_sz], _c_i),
+    "sbh_native_winding_number_vjp": ([_c_p, _c_f, _c_p, _c_i64, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_sz, _c_p,
+                                       _c_sz], _c_i),
     "sbh_native_stats": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_quadrupole_count": ([_c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_set_group_size": ([_c_p, _c_p, _c_sz, _c_i], _c_i),
@@ -1095,6 +1097,30 @@ class NativeTree:
                "native_winding_number")
         return out
 
+    def winding_number_vjp(self, queries, cotangent, *, beta: float = 2.0, want_value: bool = False):
+        """(w or None, dL/dqueries (M, 3), dL/dpoints (N, 3), dL/dnormals
+        (N, 3), dL/dmasses (N,)) of L = sum_i u_i w(q_i) for the cotangent u
+        (M,); the tree must be built with normals and with_adjoint."""
+        q = _f32(queries, self.device)
+        u = _f32(cotangent, self.device)
+        if q.ndim != 2 or q.shape[1] != 3:
+            raise ValueError("queries must be (M, 3)")
+        if u.shape != (q.shape[0],):
+            raise ValueError("cotangent must have shape (M,)")
+        need = int(lib().sbh_native_query_workspace_bytes(q.shape[0]))
+        if self.qws is None or self.qws.numel() < need:
+            self.qws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
+        w = torch.empty(q.shape[0], dtype=torch.float32, device=self.device) if want_value else None
+        gq = torch.empty((q.shape[0], 3), dtype=torch.float32, device=self.device)
+        gp = torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
+        gn = torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
+        gm = torch.empty(self.n, dtype=torch.float32, device=self.device)
+        _check(lib().sbh_native_winding_number_vjp(_stream_ptr(self.device), float(beta), _p(q), q.shape[0], _p(u),
+                                                   _p(w), _p(gq), _p(gp), _p(gn), _p(gm), _p(self.ws),
+                                                   self.ws.numel(), _p(self.qws), self.qws.numel()),
+               "native_winding_number_vjp")
+        return w, gq, gp, gn, gm
+
     def stats(self) -> dict:
         out = (ctypes.c_uint64 * 4)()
         rc = lib().sbh_native_stats(_stream_ptr(self.device), _p(self.ws), self.ws.numel(), out)
@@ -1158,6 +1184,37 @@ class _NativeGravity(torch.autograd.Function):
 # groups of 128 or 96 suit clustered systems, 64 near-uniform ones; leaves of
 # 12 to 20 cost about the same on Plummer spheres.
 AUTOTUNE_CANDIDATES = ((16, 128), (16, 96), (16, 64), (24, 64))
+
+
+class _NativeWindingNumber(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, points, normals, masses, queries, cfg):
+        beta, leaf = cfg
+        t = NativeTree().build(points.detach(), masses.detach(), normals=normals.detach(), leaf_size=leaf,
+                               with_adjoint=False)
+        ctx.save_for_backward(points, normals, masses, queries)
+        ctx.cfg = cfg
+        return t.winding_number(queries.detach(), beta=beta)
+
+    @staticmethod
+    def backward(ctx, cot):
+        points, normals, masses, queries = ctx.saved_tensors
+        beta, leaf = ctx.cfg
+        t = NativeTree().build(points.detach(), masses.detach(), normals=normals.detach(), leaf_size=leaf,
+                               with_adjoint=True)
+        _, gq, gp, gn, gm = t.winding_number_vjp(queries.detach(), cot.contiguous(), beta=beta)
+        return gp, gn, gm, gq, None
+
+
+def native_winding_number(points, normals, masses, queries, *, beta: float = 2.0, leaf_size: int = 16):
+    """Generalized winding number of oriented points (points, normals,
+    masses = area weights) at the queries, on the native tree; differentiable
+    with respect to all four through the analytic adjoint walk (the tree is
+    rebuilt in the backward pass, opening decisions recomputed)."""
+    dev = _device()
+    points, normals, masses, queries = (x if isinstance(x, torch.Tensor) else _f32(x, dev)
+                                        for x in (points, normals, masses, queries))
+    return _NativeWindingNumber.apply(points, normals, masses, queries, (float(beta), int(leaf_size)))
 
 
 def autotune_native(points, masses, system_offsets=None, *, normals=None, adjoint: bool = True,

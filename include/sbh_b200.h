@@ -472,6 +472,20 @@ int sbh_native_winding_number(cudaStream_t stream, float beta, const float* quer
                               float* out, void* workspace, size_t workspace_bytes,
                               void* query_workspace, size_t query_workspace_bytes);
 
+/* Adjoint of sbh_native_winding_number: with cotangent u (nq floats) and
+ * L = sum_i u_i w(q_i), writes dL/dq (grad_queries, nq x 3, input order) and
+ * dL/d(points, normals, masses) of the sources (n x 3, n x 3, n, input
+ * order), and w itself to out when out is non-null. The tree must be built
+ * with normals and with_adjoint. Same plan as the forward (opening decisions
+ * recomputed, not stored); the far field of a node is (sum m n) . (X - q) K,
+ * so its adjoints reach the sources through X = sum m p / M and sum m n. No
+ * reference counterpart: the reference's winding number (signedSolidAngle,
+ * include/kernel.h:73-80; src/sbh_gpu.cu:53-187) has no derivative. */
+int sbh_native_winding_number_vjp(cudaStream_t stream, float beta, const float* queries, int64_t nq,
+                                  const float* cotangent, float* out, float* grad_queries, float* grad_points,
+                                  float* grad_normals, float* grad_masses, void* workspace, size_t workspace_bytes,
+                                  void* query_workspace, size_t query_workspace_bytes);
+
 /* Synchronises; out4 = {nodes, target groups, far interactions, near
  * interactions} of the last build / evaluation on this workspace. The walks
  * themselves carry no counters: after a force or adjoint walk the counts

@@ -760,6 +760,11 @@ typedef struct {
   int64_t* gstart;
   int64_t* gend;
   float* gcen; /* per group: centre (3) and squared half diagonal of its box (float) */
+  /* winding-number plan over external queries (orc_native_wn_plan) */
+  int64_t wn_nq, wn_ngroups;
+  int64_t* wn_qperm; /* sorted query -> input index */
+  int64_t *wn_far_off, *wn_near_off;
+  int32_t *wn_far_idx, *wn_near_idx;
 } NativeTree;
 
 static void cell_geometry(const NativeTree* t, int64_t nd, uint64_t key) {
@@ -817,6 +822,11 @@ void orc_native_free(void* h) {
   free(t->gstart);
   free(t->gend);
   free(t->gcen);
+  free(t->wn_qperm);
+  free(t->wn_far_off);
+  free(t->wn_near_off);
+  free(t->wn_far_idx);
+  free(t->wn_near_idx);
   free(t);
 }
 
@@ -1771,5 +1781,241 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
   free(sm);
   free(sw);
   free(sx);
+  free(mom);
+}
+
+/*
+ * Winding number of external queries on the native tree, as the CUDA
+ * sbh_native_winding_number walks it (a single-system tree built with
+ * normals): the queries are sorted by the 63-bit Morton key of their position
+ * in the tree's box (clamped to it, IEEE double quantisation), stably by
+ * index, and cut into groups of 32 consecutive sorted queries; each group's
+ * box takes the opening test of the gravity walk (no quadrupole, no prune).
+ * Accepted nodes contribute (sum_p m_p n_p) . (X - q) K(|X - q|) with X the
+ * node's COM, near sources m n . (p - q) K(|p - q|), K(r) = 1 / (4 pi (r^3 +
+ * 1e-5)) (signedSolidAngle, include/kernel.h:73-80). Sums in double.
+ */
+#define WN_GROUP 32
+#define WN_K4PI 0.07957747154594767
+
+static double wn_kernel_d(double r2) {
+  double r = sqrt(r2);
+  return WN_K4PI / (r2 * r + 1e-5);
+}
+
+int64_t orc_native_wn_plan(void* h, const float* pts, const float* masses, const float* queries, int64_t nq,
+                           double beta) {
+  NativeTree* t = (NativeTree*)h;
+  free(t->wn_qperm);
+  free(t->wn_far_off);
+  free(t->wn_near_off);
+  free(t->wn_far_idx);
+  free(t->wn_near_idx);
+  t->wn_nq = nq;
+  double scale = 2097152.0 / (double)t->span;
+  uint64_t* kv = (uint64_t*)malloc(sizeof(uint64_t) * 2 * (nq > 0 ? nq : 1));
+  for (int64_t i = 0; i < nq; i++) {
+    uint64_t key = 0;
+    for (int d = 0; d < 3; d++) {
+      double tq = ((double)queries[3 * i + d] - (double)t->lo[d]) * scale;
+      double f = floor(tq);
+      uint64_t qv = !(f >= 0.0) ? 0 : (f > 2097151.0 ? 2097151u : (uint64_t)f);
+      for (int b = 0; b < 21; b++) key |= ((qv >> b) & 1ull) << (3 * b + d);
+    }
+    kv[2 * i] = key;
+    kv[2 * i + 1] = (uint64_t)i;
+  }
+  qsort(kv, (size_t)nq, 2 * sizeof(uint64_t), cmp_key_idx);
+  t->wn_qperm = (int64_t*)malloc(sizeof(int64_t) * (nq > 0 ? nq : 1));
+  for (int64_t i = 0; i < nq; i++) t->wn_qperm[i] = (int64_t)kv[2 * i + 1];
+  free(kv);
+  int64_t ng = (nq + WN_GROUP - 1) / WN_GROUP;
+  t->wn_ngroups = ng;
+  double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
+  native_moments(t, pts, masses, mom);
+  float fbeta = (float)beta;
+  int64_t fcap = 1 << 16, ncap = 1 << 16, nf = 0, nr = 0, total = 0;
+  t->wn_far_idx = (int32_t*)malloc(sizeof(int32_t) * fcap);
+  t->wn_near_idx = (int32_t*)malloc(sizeof(int32_t) * ncap);
+  t->wn_far_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
+  t->wn_near_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
+  for (int64_t g = 0; g < ng; g++) {
+    t->wn_far_off[g] = nf;
+    t->wn_near_off[g] = nr;
+    int64_t s0 = g * WN_GROUP, s1 = s0 + WN_GROUP < nq ? s0 + WN_GROUP : nq;
+    float gmin[3] = {INFINITY, INFINITY, INFINITY}, gmax[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = s0; i < s1; i++)
+      for (int d = 0; d < 3; d++) {
+        float v = queries[3 * t->wn_qperm[i] + d];
+        gmin[d] = fminf(gmin[d], v);
+        gmax[d] = fmaxf(gmax[d], v);
+      }
+    int64_t k = 0, cnt = 0;
+    while (k < t->nn) {
+      float X[3], M, C[3];
+      com_float(mom, k, X, &M);
+      native_cell(t, k, gmin, gmax, C);
+      if (M == 0.0f) {
+        k = t->skip[k];
+        continue;
+      }
+      int is_leaf = (k + 1 >= t->nn) || (t->skip[k] == k + 1);
+      float d2, rc2;
+      if (native_accept(t, k, C, gmin, gmax, fbeta, &d2, &rc2)) {
+        if (nf == fcap) t->wn_far_idx = (int32_t*)realloc(t->wn_far_idx, sizeof(int32_t) * (fcap *= 2));
+        t->wn_far_idx[nf++] = (int32_t)k;
+        cnt += 1;
+        k = t->skip[k];
+      } else if (is_leaf) {
+        if (nr == ncap) t->wn_near_idx = (int32_t*)realloc(t->wn_near_idx, sizeof(int32_t) * (ncap *= 2));
+        t->wn_near_idx[nr++] = (int32_t)k;
+        cnt += t->end[k] - t->start[k];
+        k = t->skip[k];
+      } else {
+        k = k + 1;
+      }
+    }
+    total += cnt * (s1 - s0);
+  }
+  t->wn_far_off[ng] = nf;
+  t->wn_near_off[ng] = nr;
+  free(mom);
+  return total;
+}
+
+/* node sums of m n (nn x 3) in double, by prefix sums over the sorted order */
+static double* wn_node_normals(const NativeTree* t, const float* normals, const float* masses) {
+  double* P = (double*)calloc(((size_t)t->n + 1) * 3, sizeof(double));
+  for (int64_t i = 0; i < t->n; i++) {
+    int64_t s = t->perm[i];
+    for (int d = 0; d < 3; d++) P[3 * (i + 1) + d] = P[3 * i + d] + (double)masses[s] * normals[3 * s + d];
+  }
+  double* Nm = (double*)malloc(sizeof(double) * 3 * (t->nn > 0 ? t->nn : 1));
+  for (int64_t k = 0; k < t->nn; k++)
+    for (int d = 0; d < 3; d++) Nm[3 * k + d] = P[3 * t->end[k] + d] - P[3 * t->start[k] + d];
+  free(P);
+  return Nm;
+}
+
+/* out[i] = winding number at query i (input order) with the recorded plan */
+void orc_native_wn_eval(void* h, const float* pts, const float* normals, const float* masses, const float* queries,
+                        double* out) {
+  NativeTree* t = (NativeTree*)h;
+  double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
+  native_moments(t, pts, masses, mom);
+  double* Nm = wn_node_normals(t, normals, masses);
+#pragma omp parallel for schedule(dynamic, 8)
+  for (int64_t g = 0; g < t->wn_ngroups; g++) {
+    int64_t s0 = g * WN_GROUP, s1 = s0 + WN_GROUP < t->wn_nq ? s0 + WN_GROUP : t->wn_nq;
+    for (int64_t i = s0; i < s1; i++) {
+      int64_t qi = t->wn_qperm[i];
+      double q[3] = {queries[3 * qi], queries[3 * qi + 1], queries[3 * qi + 2]};
+      double acc = 0.0;
+      for (int64_t e = t->wn_far_off[g]; e < t->wn_far_off[g + 1]; e++) {
+        int32_t k = t->wn_far_idx[e];
+        const double* o = &mom[MOM * k];
+        double d[3] = {o[1] - q[0], o[2] - q[1], o[3] - q[2]};
+        acc += (Nm[3 * k] * d[0] + Nm[3 * k + 1] * d[1] + Nm[3 * k + 2] * d[2]) *
+               wn_kernel_d(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      }
+      for (int64_t e = t->wn_near_off[g]; e < t->wn_near_off[g + 1]; e++) {
+        int32_t k = t->wn_near_idx[e];
+        for (int32_t j = t->start[k]; j < t->end[k]; j++) {
+          int64_t sj = t->perm[j];
+          double d[3] = {pts[3 * sj] - q[0], pts[3 * sj + 1] - q[1], pts[3 * sj + 2] - q[2]};
+          acc += masses[sj] * (normals[3 * sj] * d[0] + normals[3 * sj + 1] * d[1] + normals[3 * sj + 2] * d[2]) *
+                 wn_kernel_d(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        }
+      }
+      out[qi] = acc;
+    }
+  }
+  free(Nm);
+  free(mom);
+}
+
+/*
+ * Adjoint of orc_native_wn_eval's L = sum_i u_i w(q_i) with the plan frozen.
+ * For one term f = a . d K(r), d = p - q, r = |d| (a = m n for a source, the
+ * node's sum m n for a far node, p its COM): df/dd = a K - 3 (a . d) r K^2 d / k4pi
+ * (K' = -3 r^2 K^2 / k4pi for K = k4pi / (r^3 + 1e-5)), df/dq = -df/dd, df/dp =
+ * df/dd, df/da = d K. A source takes dp += u df/dd, dn += u m d K,
+ * dm += u (n . d) K; a node's dL/dX = sum u df/dd and dL/d(sum m n) = sum u d K
+ * reach its particles through X = sum m p / M and sum m n:
+ * dp += (m / M) dL/dX, dn += m dL/dN, dm += dL/dX . (p - X) / M + n . dL/dN.
+ * dq: nq x 3 (input order), dp, dn: n x 3, dm: n.
+ */
+void orc_native_wn_adjoint(void* h, const float* pts, const float* normals, const float* masses,
+                           const float* queries, const float* u, double* dq, double* dp, double* dn, double* dm) {
+  NativeTree* t = (NativeTree*)h;
+  int64_t n = t->n;
+  double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
+  native_moments(t, pts, masses, mom);
+  double* Nm = wn_node_normals(t, normals, masses);
+  double* A = (double*)calloc((size_t)(t->nn > 0 ? t->nn : 1) * 6, sizeof(double)); /* dL/dX, dL/dN */
+  memset(dq, 0, sizeof(double) * 3 * t->wn_nq);
+  memset(dp, 0, sizeof(double) * 3 * n);
+  memset(dn, 0, sizeof(double) * 3 * n);
+  memset(dm, 0, sizeof(double) * n);
+  for (int64_t g = 0; g < t->wn_ngroups; g++) {
+    int64_t s0 = g * WN_GROUP, s1 = s0 + WN_GROUP < t->wn_nq ? s0 + WN_GROUP : t->wn_nq;
+    for (int64_t i = s0; i < s1; i++) {
+      int64_t qi = t->wn_qperm[i];
+      double q[3] = {queries[3 * qi], queries[3 * qi + 1], queries[3 * qi + 2]};
+      double ui = u[qi];
+      for (int64_t e = t->wn_far_off[g]; e < t->wn_far_off[g + 1]; e++) {
+        int32_t k = t->wn_far_idx[e];
+        const double* o = &mom[MOM * k];
+        double d[3] = {o[1] - q[0], o[2] - q[1], o[3] - q[2]};
+        double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], r = sqrt(r2), K = wn_kernel_d(r2);
+        double ad = Nm[3 * k] * d[0] + Nm[3 * k + 1] * d[1] + Nm[3 * k + 2] * d[2];
+        for (int c = 0; c < 3; c++) {
+          double g1 = Nm[3 * k + c] * K - 3.0 * ad * r * K * K * d[c] / WN_K4PI;
+          dq[3 * qi + c] -= ui * g1;
+          A[6 * k + c] += ui * g1;
+          A[6 * k + 3 + c] += ui * d[c] * K;
+        }
+      }
+      for (int64_t e = t->wn_near_off[g]; e < t->wn_near_off[g + 1]; e++) {
+        int32_t k = t->wn_near_idx[e];
+        for (int32_t j = t->start[k]; j < t->end[k]; j++) {
+          int64_t sj = t->perm[j];
+          double d[3] = {pts[3 * sj] - q[0], pts[3 * sj + 1] - q[1], pts[3 * sj + 2] - q[2]};
+          double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], r = sqrt(r2), K = wn_kernel_d(r2);
+          double mj = masses[sj];
+          double nd = normals[3 * sj] * d[0] + normals[3 * sj + 1] * d[1] + normals[3 * sj + 2] * d[2];
+          for (int c = 0; c < 3; c++) {
+            double g1 = mj * (normals[3 * sj + c] * K - 3.0 * nd * r * K * K * d[c] / WN_K4PI);
+            dq[3 * qi + c] -= ui * g1;
+            dp[3 * sj + c] += ui * g1;
+            dn[3 * sj + c] += ui * mj * d[c] * K;
+          }
+          dm[sj] += ui * nd * K;
+        }
+      }
+    }
+  }
+  for (int64_t k = 0; k < t->nn; k++) {
+    const double* o = &mom[MOM * k];
+    double M = o[0];
+    if (M == 0.0) continue;
+    const double* a = &A[6 * k];
+    int any = 0;
+    for (int c = 0; c < 6; c++) any |= a[c] != 0.0;
+    if (!any) continue;
+    for (int32_t j = t->start[k]; j < t->end[k]; j++) {
+      int64_t sj = t->perm[j];
+      double mj = masses[sj];
+      double y[3] = {(double)pts[3 * sj] - o[1], (double)pts[3 * sj + 1] - o[2], (double)pts[3 * sj + 2] - o[3]};
+      for (int c = 0; c < 3; c++) {
+        dp[3 * sj + c] += mj / M * a[c];
+        dn[3 * sj + c] += mj * a[3 + c];
+      }
+      dm[sj] += (a[0] * y[0] + a[1] * y[1] + a[2] * y[2]) / M + normals[3 * sj] * a[3] + normals[3 * sj + 1] * a[4] +
+                normals[3 * sj + 2] * a[5];
+    }
+  }
+  free(A);
+  free(Nm);
   free(mom);
 }

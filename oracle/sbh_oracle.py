@@ -102,6 +102,10 @@ def _orc() -> ctypes.CDLL:
         lib.orc_native_fd.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_d, _c_i, _c_p, _c_i64, _c_d, _c_d, _c_p, _c_p]
         lib.orc_native_set_quad_linear.argtypes = [_c_f]
         lib.orc_native_linear_quadrupole_counts.argtypes = [_c_p, _c_p, _c_p]
+        lib.orc_native_wn_plan.restype = _c_i64
+        lib.orc_native_wn_plan.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d]
+        lib.orc_native_wn_eval.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p]
+        lib.orc_native_wn_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]
         lib._typed = True
     return lib
 
@@ -256,6 +260,32 @@ class NativeTree:
         a, b = _c_i64(), _c_i64()
         self._lib.orc_native_linear_quadrupole_counts(self._h, ctypes.byref(a), ctypes.byref(b))
         return a.value, b.value
+
+    def wn_plan(self, queries, beta) -> int:
+        """Record the winding-number plan of external queries (the CUDA
+        walk's query groups of 32); returns the interaction count."""
+        self.queries = _f32(queries)
+        return int(self._lib.orc_native_wn_plan(self._h, _ptr(self.points), _ptr(self.masses), _ptr(self.queries),
+                                                self.queries.shape[0], float(beta)))
+
+    def wn_eval(self, normals, points=None, masses=None, queries=None):
+        """Winding number at the planned queries (float64), for possibly
+        perturbed points, normals, masses and queries (plan frozen)."""
+        p = self.points if points is None else _f32(points)
+        m = self.masses if masses is None else _f32(masses)
+        q = self.queries if queries is None else _f32(queries)
+        out = np.zeros(q.shape[0], np.float64)
+        self._lib.orc_native_wn_eval(self._h, _ptr(p), _ptr(_f32(normals)), _ptr(m), _ptr(q), _ptr(out))
+        return out
+
+    def wn_adjoint(self, normals, u):
+        """(dq, dp, dn, dm) of sum_i u_i w(q_i) with the plan frozen (float64)."""
+        nq, n = self.queries.shape[0], self.points.shape[0]
+        dq, dp, dn = np.zeros((nq, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        dm = np.zeros(n)
+        self._lib.orc_native_wn_adjoint(self._h, _ptr(self.points), _ptr(_f32(normals)), _ptr(self.masses),
+                                        _ptr(self.queries), _ptr(_f32(u)), _ptr(dq), _ptr(dp), _ptr(dn), _ptr(dm))
+        return dq, dp, dn, dm
 
     def plan_stats(self):
         a, b, c = _c_i64(), _c_i64(), _c_i64()

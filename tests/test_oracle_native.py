@@ -159,3 +159,38 @@ def test_native_linearized_quadrupole_adjoint_matches_finite_differences():
     pp[k, 2] -= 2 * h
     lm = T.force(eps, points=pp.astype(np.float32), masses=m, w=w, quad=True)[1]
     assert abs((lp - lm) / (2 * h) - dx[k, 2]) <= 2e-3 * (abs(dx[k, 2]) + 1.0)
+
+
+def test_native_winding_number_adjoint_matches_finite_differences():
+    """The oracle's winding-number plan (queries in Morton order, groups of 32)
+    equals the direct sum in its direct limit, and its adjoint with respect to
+    queries, source positions, normals and weights matches central
+    differences of the frozen-plan evaluation."""
+    p, nrm, m = W.ellipsoid_surface(3000, seed=3)
+    rng = np.random.default_rng(1)
+    q = rng.uniform(-1.5, 1.5, (200, 3)).astype(np.float32)
+    u = rng.normal(size=200).astype(np.float32)
+    T = O.NativeTree(p, m, leaf_size=8)
+    T.wn_plan(q, 1e30)
+    assert np.abs(T.wn_eval(nrm) - O.direct_winding_number(p, nrm, m, q)).max() < 1e-10
+    T.wn_plan(q, 2.0)
+    dq, dp, dn, dm = T.wn_adjoint(nrm, u)
+    p64, n64, q64, m64 = (a.astype(np.float64) for a in (p, nrm, q, m))
+
+    def loss(pp=p64, nn=n64, mm=m64, qq=q64):
+        # float64 inputs are rounded to float32 by the evaluator: steps are kept well above that
+        return float(np.dot(u, T.wn_eval(nn.astype(np.float32), points=pp.astype(np.float32),
+                                         masses=mm.astype(np.float32), queries=qq.astype(np.float32))))
+
+    h = 1e-3
+    for i in (3, 50):
+        for c in range(3):
+            a = q64.copy(); a[i, c] += h; lp = loss(qq=a); a[i, c] -= 2 * h; lm = loss(qq=a)
+            assert abs((lp - lm) / (2 * h) - dq[i, c]) <= 2e-3 * (abs(dq[i, c]) + 1e-3)
+    for j in (7, 1200):
+        a = p64.copy(); a[j, 0] += h; lp = loss(pp=a); a[j, 0] -= 2 * h; lm = loss(pp=a)
+        assert abs((lp - lm) / (2 * h) - dp[j, 0]) <= 2e-3 * (abs(dp[j, 0]) + 1e-3)
+        a = n64.copy(); a[j, 1] += h; lp = loss(nn=a); a[j, 1] -= 2 * h; lm = loss(nn=a)
+        assert abs((lp - lm) / (2 * h) - dn[j, 1]) <= 2e-3 * (abs(dn[j, 1]) + 1e-3)
+        a = m64.copy(); hm = 1e-2 * m64[j]; a[j] += hm; lp = loss(mm=a); a[j] -= 2 * hm; lm = loss(mm=a)
+        assert abs((lp - lm) / (2 * hm) - dm[j]) <= 2e-3 * (abs(dm[j]) + 1e-3)
