@@ -347,23 +347,24 @@ def forest_measurement(B, torch, dev, rank, world, flush):
 
 def stochastic_measurement(B, torch, P0, M0, idx, ref, flush):
     """Config 2a, stochastic variant: the reference's stochastic octree8
-    estimator (MLPCV, src/sbh_ffi.cu:2146-2291) on the 2^20-particle Plummer
-    system, depth-7 tree, at a sample of 65,536 queries (the first 1,024 of
-    them the accuracy subset). The reference has no "nodes per query" knob;
-    one and 32 particle paths per depth-3 subdomain (samples_per_subdomain)
-    are measured. Classic octree8 BH on the same queries beside it."""
-    rng = np.random.default_rng(17)
-    others = rng.choice(P0.shape[0], 65536 - idx.numel(), replace=False)
-    qidx = torch.cat([idx, torch.tensor(others, device=P0.device)])
-    Q = P0[qidx].contiguous()
+    estimator (MLPCV, src/sbh_ffi.cu:2146-2291) at all 2^20 particles of the
+    Plummer system, depth-7 tree; the error against the FP64 direct sum on
+    the 1,024-target accuracy subset. The reference has no "nodes per query"
+    knob: samples_per_subdomain draws that many particle paths in each of the
+    (up to 512) depth-3 subdomains of a query, and each path evaluates the 8
+    children of every node it descends through. 32 paths per subdomain is
+    the configuration's "32 samples"; 1 path per subdomain is the fewest the
+    estimator allows. Classic octree8 BH on the same queries beside it."""
+    Q = P0.contiguous()
     Z = torch.zeros_like(P0)
     span = float((P0.max(0).values - P0.min(0).values).max())
     leaf, node = B.build_octree8_buffers(P0, Z, M0, max_depth=7)
     kw = dict(beta=BETA, softening_scale=EPS, cutoff_scale=1e6 * span, prune_enabled=False)
 
-    def timed(fn):
-        fn()
-        torch.cuda.synchronize()
+    def timed(fn, warm):
+        if warm:
+            fn()
+            torch.cuda.synchronize()
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -372,15 +373,16 @@ def stochastic_measurement(B, torch, P0, M0, idx, ref, flush):
         torch.cuda.synchronize()
         return out, e0.elapsed_time(e1)
 
-    k = idx.numel()
-    rel = lambda f: float(torch.linalg.norm(f[:k].double() - ref) / torch.linalg.norm(ref))  # noqa: E731
-    out = dict(queries=int(Q.shape[0]), max_depth=7)
+    rel = lambda f: float(torch.linalg.norm(f[idx].double() - ref) / torch.linalg.norm(ref))  # noqa: E731
+    out = dict(queries=int(Q.shape[0]), max_depth=7,
+               mapping=("samples_per_subdomain = particle paths per depth-3 subdomain (the reference has no "
+                        "nodes-per-query knob); s32 is the configuration's 32 samples"))
     for sps in (1, 32):
         st, st_ms = timed(lambda: B.softened_stochastic_barnes_hut_force_octree8(  # noqa: B023
-            leaf, node, Q, samples_per_subdomain=sps, seed=3, **kw))
+            leaf, node, Q, samples_per_subdomain=sps, seed=3, **kw), warm=sps == 1)
         out[f"stochastic_s{sps}"] = dict(ms=st_ms, queries_per_s=Q.shape[0] / (st_ms * 1e-3),
                                          rel_l2_vs_fp64_direct=rel(st))
-    cl, cl_ms = timed(lambda: B.softened_barnes_hut_force_octree8(leaf, node, Q, **kw))
+    cl, cl_ms = timed(lambda: B.softened_barnes_hut_force_octree8(leaf, node, Q, **kw), warm=True)
     out["classic"] = dict(ms=cl_ms, queries_per_s=Q.shape[0] / (cl_ms * 1e-3), rel_l2_vs_fp64_direct=rel(cl))
     return out
 
@@ -451,6 +453,34 @@ def winding_measurement(B, torch, dev, flush):
     ms = tot / 3
     err_in = float((out[inside] - 1.0).abs().mean())
     err_out = float(out[~inside].abs().mean())
+    # against the FP64 direct sum (signedSolidAngle) at 1,024 of the queries
+    sub = np.random.default_rng(9).choice(q.shape[0], 1024, replace=False)
+    Qs = Q[sub].double()
+    P64, N64, M64 = P.double(), N.double(), M.double()
+    ref64 = torch.zeros(1024, dtype=torch.float64, device=dev)
+    for a in range(0, 1024, 32):
+        d = P64[None, :, :] - Qs[a:a + 32, None, :]
+        r = torch.linalg.norm(d, dim=2)
+        ref64[a:a + 32] = ((M64[None, :] * (d * N64[None, :, :]).sum(2)) / (4.0 * np.pi * (r ** 3 + 1e-5))).sum(1)
+    rel64 = float(torch.linalg.norm(out[sub].double() - ref64) / torch.linalg.norm(ref64))
+    del P64, N64, M64
+    # the adjoint with respect to queries, source positions, normals and weights (one walk + finalize)
+    vtree = B.NativeTree(dev).build(P, M, normals=N, leaf_size=LEAF, with_adjoint=True)
+    U = torch.tensor(np.random.default_rng(4).normal(size=q.shape[0]).astype(np.float32), device=dev)
+
+    def vstep():
+        vtree.build(P, M, normals=N, leaf_size=LEAF, with_adjoint=True)
+        return vtree.winding_number_vjp(Q, U, beta=BETA, want_value=True)
+
+    vstep()
+    torch.cuda.synchronize()
+    flush.zero_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    vstep()
+    e1.record()
+    torch.cuda.synchronize()
+    vjp_ms = e0.elapsed_time(e1)
     # the reference's algorithm on this GPU: its adaptive Tree3D<1,3> (leaf size 1, built here on the
     # device with the reference CPU builder's bytes) and its warp-vote traversal (src/sbh_gpu.cu)
     def ref_step():
@@ -467,7 +497,10 @@ def winding_measurement(B, torch, dev, flush):
     torch.cuda.synchronize()
     ref_ms = e0.elapsed_time(e1)
     return dict(sources=262144, queries=1048576, ms=ms, queries_per_s=1048576 / (ms * 1e-3),
-                mean_abs_err_inside=err_in, mean_abs_err_outside=err_out,
+                mean_abs_err_inside=err_in, mean_abs_err_outside=err_out, rel_l2_vs_fp64_direct=rel64,
+                fp64_subset=1024,
+                vjp_ms=vjp_ms, vjp_what=("build + winding number and its adjoint with respect to queries, source "
+                                         "positions, normals and weights (one walk + finalize)"),
                 reference_algorithm_ms=ref_ms, speedup_vs_reference_algorithm=ref_ms / ms,
                 reference_algorithm_mean_abs_err_inside=float((rout[inside] - 1.0).abs().mean()),
                 reference_algorithm_mean_abs_err_outside=float(rout[~inside].abs().mean()),
@@ -1060,11 +1093,11 @@ WALK_LAUNCHES = 2
 
 # DRAM bytes (read + write) of one adjoint walk per particle, from one ncu
 # capture (dram__bytes_read.sum + dram__bytes_write.sum) of the packed walk
-# (four targets per lane) over 4 Plummer systems of 262,144 particles at
-# quadrupole radius 1.6: 124.39 MB + 33.80 MB for 1,048,576 particles. The walk's DRAM traffic is
-# its L2 misses on the tree, the particles and the adjoint arrays, which grow
-# with the particle count.
-WALK_DRAM_BYTES_PER_PARTICLE = 150.9
+# (four targets per lane, node tiles, linearized quadrupoles) over 4 Plummer
+# systems of 262,144 particles: 127.01 MB + 39.26 MB for 1,048,576 particles.
+# The walk's DRAM traffic is its L2 misses on the tree, the particles and the
+# adjoint arrays, which grow with the particle count.
+WALK_DRAM_BYTES_PER_PARTICLE = 158.6
 FINALIZE_LAUNCHES = 5
 
 # FP32 flops of the adjoint walk (force + adjoint, counted from
@@ -1095,8 +1128,9 @@ BUILD_ALG_BYTES_PER_PARTICLE = 16 + 20
 BUILD_ALG_BYTES_PER_NODE = 80
 
 # DRAM bytes (read + write) of one forest build per particle, summed over the
-# build's kernels from one ncu capture of the bench's 8 x 2^20 Plummer forest.
-BUILD_DRAM_BYTES_PER_PARTICLE = None
+# build's 69 kernels from one ncu capture of the bench's 8 x 2^20 Plummer
+# forest (4,911.9 MB read + 1,900.0 MB written).
+BUILD_DRAM_BYTES_PER_PARTICLE = 812.0
 
 
 def hbm_peak_gbs():
