@@ -31,8 +31,4 @@ __device__ __forceinline__ float2 vsplat<float2>(float s) {
   return make_float2(s, s);
 }
 
-// e += the sum of x's components (one value for a scalar slot, two for a pair).
-__device__ __forceinline__ void vacc(float& e, float x) { e = __fadd_rn(e, x); }
-__device__ __forceinline__ void vacc(float& e, float2 x) { e = __fadd_rn(e, __fadd_rn(x.x, x.y)); }
-
 }  // namespace sbh
