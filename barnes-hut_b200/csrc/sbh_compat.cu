@@ -495,6 +495,101 @@ __global__ void __launch_bounds__(256)
   out[3 * qi + 2] = az;
 }
 
+// Warp-cooperative form of o8_bh_kernel, for queries taken in Morton order
+// (32 neighbouring queries per warp). The warp walks one DFS stack in shared
+// memory whose entries carry the lanes that still descend at that node, and
+// each lane takes its own prune and opening decisions, exactly as its thread
+// does in o8_bh_kernel: a node is pushed (children in the same order) when
+// some lane opens it, with that set of lanes. A lane's nodes thus come off
+// the stack in the order of its own per-thread DFS, so it adds the same terms
+// in the same order and every output row equals o8_bh_kernel's bit for bit;
+// node records and leaf particles are read once per warp instead of once per
+// thread, and the lanes at a leaf loop over its particles together.
+constexpr int kO8WarpsPerBlock = 4;
+struct O8StackEntry {
+  int node;
+  uint32_t lanes;
+};
+
+template <int KERNEL>
+__global__ void __launch_bounds__(32 * kO8WarpsPerBlock)
+    o8_bh_warp_kernel(const Leaf3* __restrict__ leaf, const OctreeNode8* __restrict__ nodes,
+                      const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq, float beta,
+                      Soft s, int prune_on, float r_cut_sq, Periodic per, float* __restrict__ out, uint32_t* status,
+                      O8Bounds bd, const uint32_t* __restrict__ order) {
+  __shared__ O8StackEntry stacks[kO8WarpsPerBlock][kO8Stack];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  O8StackEntry* stack = stacks[warp];
+  const int64_t ti = (static_cast<int64_t>(blockIdx.x) * kO8WarpsPerBlock + warp) * 32 + lane;
+  const bool valid = ti < nq;
+  const uint32_t live = __ballot_sync(0xffffffffu, valid);
+  if (live == 0) return;  // warp-uniform
+  const int64_t qi = valid ? static_cast<int64_t>(order[ti]) : 0;
+  float qx = 0.f, qy = 0.f, qz = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+  if (valid) {
+    qx = queries[3 * qi];
+    qy = queries[3 * qi + 1];
+    qz = queries[3 * qi + 2];
+    if (KERNEL == O8_SOFT_VJP || KERNEL == O8_GRAV_GRAD_VJP) {
+      gx = cot[3 * qi];
+      gy = cot[3 * qi + 1];
+      gz = cot[3 * qi + 2];
+    }
+  }
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  if (lane == 0) stack[0] = O8StackEntry{0, live};
+  __syncwarp();
+  int top = 1;  // warp-uniform
+  bool overflow = false;
+  uint32_t visits = 0;  // bounded as in o8_bh_kernel
+  while (top > 0) {
+    if (++visits > bd.num_nodes) {
+      if (lane == 0) raise_status(status, SBH_DEV_ITER_LIMIT);
+      break;
+    }
+    const O8StackEntry en = stack[--top];
+    __syncwarp();  // every lane has read the entry before it is overwritten
+    const int idx = en.node;
+    if (o8_mass(nodes, idx) == 0.0f) continue;
+    const OctreeNode8& nd = nodes[idx];
+    bool act = (en.lanes >> lane) & 1u;
+    if (KERNEL != O8_GRAV_GRAD && KERNEL != O8_GRAV_GRAD_VJP)
+      act = act && !o8_prune(nd, qx, qy, qz, prune_on, r_cut_sq, per);
+    const bool far = act && o8_far(nd, qx, qy, qz, beta, per);
+    if (far) {
+      if (nd.is_leaf) {
+        o8_leaf_sum<KERNEL>(leaf, nd.start, o8_leaf_end(nd.start, nd.end, bd, status), qx, qy, qz, gx, gy, gz, s,
+                            per, ax, ay, az);
+      } else {
+        o8_pair<KERNEL>(qx, qy, qz, nd.contrib.pos[0], nd.contrib.pos[1], nd.contrib.pos[2], nd.contrib.mass, gx,
+                        gy, gz, s, per, ax, ay, az);
+      }
+    }
+    const uint32_t open = __ballot_sync(0xffffffffu, act && !far);
+    if (open) {
+      const uint8_t mask = nd.child_mask;
+      for (int c = 0; c < 8; c++) {
+        if (mask & (1u << c)) {
+          if (!o8_node_ok(nd.child[c], bd, status)) continue;
+          if (top < kO8Stack) {
+            if (lane == 0) stack[top] = O8StackEntry{static_cast<int>(nd.child[c]), open};
+            top++;
+          } else {
+            overflow = true;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+  if (overflow && lane == 0) raise_status(status, SBH_DEV_STACK_OVERFLOW);
+  if (valid) {
+    out[3 * qi] = ax;
+    out[3 * qi + 1] = ay;
+    out[3 * qi + 2] = az;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // octree8 stochastic BH, the multi-level prefix control variate
 // (src/sbh_ffi.cu:2146-2442). Same curand calls as the reference, so a
@@ -901,6 +996,29 @@ static int o8_launch_bh(int kernel, cudaStream_t stream, const void* leaf, size_
   int orc = SBH_OK;
   const uint32_t* order = o8_query_order(stream, N, queries, nq, workspace, workspace_bytes, &orc);
   if (orc != SBH_OK) return orc;
+  if (order) {  // Morton-ordered queries: one warp walks 32 neighbours together
+    const unsigned gw = grid_for(nq, 32 * kO8WarpsPerBlock);
+    const unsigned tw = 32 * kO8WarpsPerBlock;
+    switch (kernel) {
+      case O8_GRAV_GRAD:
+        o8_bh_warp_kernel<O8_GRAV_GRAD><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out,
+                                                               status, bd, order);
+        break;
+      case O8_SOFT:
+        o8_bh_warp_kernel<O8_SOFT><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per,
+                                                          out, status, bd, order);
+        break;
+      case O8_GRAV_GRAD_VJP:
+        o8_bh_warp_kernel<O8_GRAV_GRAD_VJP><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out,
+                                                                   status, bd, order);
+        break;
+      default:
+        o8_bh_warp_kernel<O8_SOFT_VJP><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq,
+                                                              per, out, status, bd, order);
+        break;
+    }
+    return check_launch("barnes_hut_force_octree8");
+  }
   unsigned g = grid_for(nq, 256);
   switch (kernel) {
     case O8_GRAV_GRAD:

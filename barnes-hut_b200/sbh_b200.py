@@ -483,8 +483,9 @@ def _status_after(ws, what, check_status):
 
 
 def _octree8_ws_bytes(nq: int) -> int:
-    """Workspace with room to take the queries in Morton order (the results
-    do not depend on the order; the per-thread traversal diverges less)."""
+    """Workspace with room to take the queries in Morton order, which lets a
+    warp walk 32 neighbouring queries down one shared stack (the results do
+    not depend on the order)."""
     return int(lib().sbh_traversal_ordered_workspace_bytes(int(nq)))
 
 

@@ -228,10 +228,12 @@ size_t sbh_traversal_workspace_bytes(void);
 
 /* Workspace with which the per-query octree8 traversals (classic, softened,
  * their VJPs and the stochastic ones) of nq queries take the queries in
- * Morton order of their positions: a warp's threads then walk nearby paths.
- * Every query's result is the same in either order (each query is
- * traversed on its own, its curand streams seeded by its own index); with a
- * smaller workspace, or below 4,096 queries, they run in input order. */
+ * Morton order of their positions: a warp's threads then walk nearby paths,
+ * and the deterministic ones walk them down one stack per warp, reading each
+ * node once for the lanes that reach it. Every query's result is the same in
+ * either order (each query takes its own decisions in its own order, its
+ * curand streams seeded by its own index); with a smaller workspace, or
+ * below 4,096 queries, they run in input order, one thread per query. */
 size_t sbh_traversal_ordered_workspace_bytes(int64_t nq);
 
 /* ---------------------------------------------------------------------- */
