@@ -43,4 +43,4 @@ def test_kernels_on_reference_buffers(cuda, case):
                               (v, g[case + f"_stoch_s{seed}_soft{soft}_vjp"])):
                 got = got.cpu().numpy()
                 row = np.linalg.norm(got - want, axis=1) / np.maximum(np.linalg.norm(want, axis=1), 1e-30)
-                assert (row < 1e-4).mean() > 0.99
+                assert row.max() < 1e-4  # every row on the reference's sampled paths

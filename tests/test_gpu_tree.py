@@ -158,7 +158,8 @@ def test_tree_mlpcv_fixed_seed_matches_reference(cuda, dim):
         got = B._stochastic_tree_call(kernel, leaf, node, contrib, q, 2, 5, 0.0, 1.0, False, 1.0, 64).cpu().numpy()
         want = out.cpu().numpy()
         row = np.abs(got - want).reshape(256, -1).max(1) / np.maximum(np.abs(want).reshape(256, -1).max(1), 1e-30)
-        assert (row < 1e-4).mean() > 0.99
+        # same curand streams: every row on the reference's sampled paths
+        assert row.max() < 1e-4, f"{int((row >= 1e-4).sum())} rows differ, worst {row.max():.2e}"
 
 
 def test_node3_winding_number_and_direct_limit(cuda):
@@ -303,5 +304,9 @@ def test_sbh_gpu_module_evaluations_match_reference(cuda, dim):
         torch.cuda.synchronize()
         got, _ = getattr(B, f"multi_level_prefix_control_variate_{name}")(leaf, node, contrib, q, 2)
         want = out.cpu().numpy()
-        row = np.abs(got.cpu().numpy() - want) / np.maximum(np.abs(want), 1e-30)
-        assert (row < 1e-4).mean() > 0.99
+        # same curand streams: every row on the reference's sampled paths; the
+        # error is relative, with values near zero (a winding number far
+        # outside) measured against 1% of the outputs' RMS
+        rms = float(np.sqrt(np.mean(want.astype(np.float64) ** 2)))
+        row = np.abs(got.cpu().numpy() - want) / np.maximum(np.abs(want), 1e-2 * rms)
+        assert row.max() < 1e-4, f"{int((row >= 1e-4).sum())} rows differ, worst {row.max():.2e}"
