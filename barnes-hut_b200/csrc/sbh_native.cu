@@ -905,6 +905,8 @@ constexpr int kAdjointWalkMinBlocks = 4;
    : (PERV) ? ((CUTV) ? NS::KERNEL<false, true, true> : NS::KERNEL<false, false, true>)       \
             : ((CUTV) ? NS::KERNEL<false, true, false> : NS::KERNEL<false, false, false>))
 
+#include "sbh_native_stochastic.inc"
+
 // Node adjoints -> difference arrays over each node's particle range. Per
 // node (coordinates relative to the system's box centre c0, Xc = X - c0):
 //   V_X = A_X / M, V_Q = A_M - A_X . Xc / M, G, G Xc, Xc^T G Xc   (14 values)
@@ -1676,6 +1678,42 @@ int sbh_native_force_vjp(cudaStream_t stream, const sbh_native_params* params, c
   if (!grad_points || !grad_masses) return invalid("gradient outputs must be non-null");
   if (int rc = sbh_native_adjoint_walk(stream, params, cotangent, force_out, workspace, workspace_bytes)) return rc;
   return sbh_native_adjoint_finalize(stream, grad_points, grad_masses, workspace, workspace_bytes);
+}
+
+int sbh_native_stochastic_force(cudaStream_t stream, const sbh_native_params* params, float beta_coarse,
+                                int samples, uint64_t seed, float* force_out, void* workspace,
+                                size_t workspace_bytes) {
+  if (int rc = check_params(params)) return rc;
+  if (params->cutoff > 0.0f || params->periodic || params->prune_radius > 0.0f)
+    return invalid("the stochastic estimator serves Plummer-softened free-space gravity (no cutoff, periodic box "
+                   "or prune radius)");
+  if (!(beta_coarse > 0.0f) || beta_coarse > params->beta) return invalid("beta_coarse must be in (0, beta]");
+  if (samples < 1 || samples > kStochMaxSamples)
+    return invalid("samples must be in [1, " + std::to_string(kStochMaxSamples) + "]");
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (h.n == 0) return SBH_OK;
+  if (!force_out) return invalid("force_out must be non-null");
+  if (partial_range(h)) return invalid("the stochastic estimator needs the full target range");
+  // coarse part: the force walk at beta_coarse, quadrupole at every accepted node
+  WalkParams wp = walk_params(params);
+  wp.beta = beta_coarse;
+  wp.quad_g = 0.0f;
+  wp.quad_lin = 0.0f;
+  const int64_t mg = h.n + h.nseg;
+  auto k = h.group_size > kGroupThreeSlots ? tpl4::force_walk_kernel<true, false, false>
+           : h.group_size > kGroupTwoSlots ? tpl3::force_walk_kernel<true, false, false>
+                                           : tpl2::force_walk_kernel<true, false, false>;
+  const WalkTree T = tree_view(L);
+  const WalkTargets G = self_targets(L, h);
+  cudaError_t e = launch_walk(stream, L.work, mg, k, T, G, wp, force_out);
+  if (e == cudaSuccess)
+    e = launch_walk(stream, L.work, mg, stoch_group_kernel, T, G, beta_coarse, params->beta, wp.eps2, samples, seed,
+                    force_out);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  remember_walk(workspace, 0, nullptr);
+  return check_launch("sbh_native_stochastic_force");
 }
 
 size_t sbh_native_query_workspace_bytes(int64_t nq) {

@@ -156,6 +156,7 @@ _SIGS = {
     "sbh_sample_mesh_surface": ([_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_i64, _c_u64, _c_p, _c_p, _c_p, _c_p, _c_sz],
                                 _c_i),
     "sbh_native_export": ([_c_p, _c_p, _c_sz, _c_p, _c_p, _c_p, _c_sz, _c_p], _c_i),
+    "sbh_native_stochastic_force": ([_c_p, _c_p, _c_f, _c_i, ctypes.c_uint64, _c_p, _c_p, _c_sz], _c_i),
 }
 
 
@@ -1048,6 +1049,21 @@ class NativeTree:
         out = out if out is not None else torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
         _check(lib().sbh_native_force(_stream_ptr(self.device), ctypes.byref(prm), _p(out), _p(self.ws),
                                       self.ws.numel()), "native_force")
+        return out
+
+    def stochastic_force(self, *, beta: float = 2.0, beta_coarse: float = 1.0, samples: int = 32, seed: int = 0,
+                         softening: float = 1e-3, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Stochastic Barnes-Hut self-gravity (Plummer softening): the group
+        walk at beta_coarse plus, per target group, `samples` nodes of its
+        coarse cut drawn in proportion to their octupole size and refined
+        to beta (sbh_native_stochastic_force). Its expectation is
+        force(beta=beta, quadrupole_radius=0, quadrupole_linear=0); the
+        draws depend on the seed and each group's first input index."""
+        prm = self.params(beta, softening, 0.0, True, False, 1.0, 0.0, 0.0, 0.0)
+        out = out if out is not None else torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
+        _check(lib().sbh_native_stochastic_force(_stream_ptr(self.device), ctypes.byref(prm), float(beta_coarse),
+                                                 int(samples), ctypes.c_uint64(int(seed) & (2 ** 64 - 1)), _p(out),
+                                                 _p(self.ws), self.ws.numel()), "native_stochastic_force")
         return out
 
     def force_vjp(self, cotangent, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,

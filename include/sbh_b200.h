@@ -435,6 +435,27 @@ int sbh_native_build(cudaStream_t stream, const float* points, const float* mass
 int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float* force_out,
                      void* workspace, size_t workspace_bytes);
 
+/* Stochastic Barnes-Hut self-gravity on the tree in `workspace`
+ * (Plummer softening, free space: params->cutoff <= 0, no periodic box or
+ * prune radius; params->beta is the refined opening beta_f, params'
+ * quadrupole settings are not used). force_out (n x 3, input order) = the
+ * group walk at beta_coarse (monopole + quadrupole everywhere) plus, per
+ * target group, `samples` (1..1024) nodes of the group's coarse cut drawn
+ * by stratified sampling in proportion to M r_g^3 / r^5 (r from the group
+ * box centre; zero where the box clears beta_f cell diagonals), each adding
+ * (group walk of the node's subtree at beta_f - the node's quadrupole) /
+ * (samples * probability) at the group's targets. Its expectation is the
+ * group walk at beta_f with the quadrupole at every accepted node
+ * (sbh_native_force with quadrupole_radius = quadrupole_linear = 0); the
+ * draws depend on the seed and the group's first input index only. The
+ * stochastic counterpart of the reference's stochastic octree8 traversal
+ * (src/sbh_ffi.cu:2146-2291) on this library's tree: `samples` is the
+ * number of tree nodes drawn per query. Needs the full target range and
+ * allocates nothing. */
+int sbh_native_stochastic_force(cudaStream_t stream, const sbh_native_params* params, float beta_coarse,
+                                int samples, uint64_t seed, float* force_out, void* workspace,
+                                size_t workspace_bytes);
+
 /* One traversal computing the force (optional force_out) and the full
  * adjoint of L = sum_i w_i . a_i: grad_points (n x 3) and grad_masses (n),
  * exact for the evaluated approximation (query side, direct sources, and the

@@ -2019,3 +2019,317 @@ void orc_native_wn_adjoint(void* h, const float* pts, const float* normals, cons
   free(Nm);
   free(mom);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Native stochastic Barnes-Hut (the CUDA sbh_native_stochastic_force)        */
+/* ------------------------------------------------------------------------ */
+/*
+ * The estimator, per target group (groups cut from the tree as in
+ * native_node_groups), on the GPU's own node records:
+ *   1. coarse part: the group walk at beta_c (a node is accepted when the
+ *      group box clears beta_c diagonals of its cell centre); accepted
+ *      nodes add their monopole + quadrupole about the COM at every target,
+ *      the leaves reached add their particles directly;
+ *   2. weights: an accepted node n gets w_n = M r_g^3 / r^5 (r_g^2 = tr S / M,
+ *      r^2 = |c - COM|^2 + eps^2 with c the group box centre: the size of the
+ *      octupole the quadrupole leaves out), or 0 when the group box already
+ *      clears beta_f diagonals of the cell (there the refined walk below is
+ *      the node's own quadrupole);
+ *   3. K stratified draws u_k = (k + U_k) W / K, W = sum w_n, each picking
+ *      the node whose interval [running sum before n, after n) holds u_k,
+ *      U_k uniform from (seed, input index of the group's first target, k);
+ *      the group's targets share the draws;
+ *   4. a node drawn c times adds c W / (K len_n) (R_n - F_n) at every target,
+ *      R_n the group walk of n's subtree at beta_f and F_n the node's
+ *      monopole + quadrupole, len_n its interval's length.
+ * E[estimate] = coarse part + sum over w_n > 0 of (R_n - F_n) = the group walk
+ * at beta_f with the quadrupole at every accepted node. Weights, running sums
+ * and draws are computed in float with the CUDA kernel's operation order
+ * (IEEE +, *, /, sqrt, no contraction), so the same nodes are drawn; forces
+ * are summed in double.
+ */
+typedef struct {
+  float com[4], cell[4], quad[4], quad2[4];
+  int32_t topo[4];
+} OrcNodeRec;
+
+#define ORC_LEAF_FLAG 0x100
+
+/* SplitMix64's output function (Steele, Lea and Flood, "Fast splittable
+ * pseudorandom number generators", OOPSLA 2014) on a Weyl sequence indexed by
+ * (index, draw): 24 bits -> a float in [0, 1). */
+static float orc_stoch_uniform(uint64_t seed, uint64_t idx, int k) {
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull * (idx * 64u + (uint64_t)k + 1u);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (float)(z >> 40) * 0x1p-24f;
+}
+
+static int stoch_accept(const float* cell, const float* lo, const float* hi, float beta) {
+  float rc = cell[3] * beta;
+  float tt[3];
+  for (int d = 0; d < 3; d++) {
+    float a = lo[d] - cell[d], b = cell[d] - hi[d];
+    float m = a > b ? a : b;
+    tt[d] = m > 0.0f ? m : 0.0f;
+  }
+  float d2 = tt[0] * tt[0] + tt[1] * tt[1] + tt[2] * tt[2];
+  return d2 > rc * rc;
+}
+
+/* w_n for the group with box [lo, hi] and centre c */
+static float stoch_weight(const OrcNodeRec* nd, const float* lo, const float* hi, const float* c, float beta_f,
+                          float eps2) {
+  if (stoch_accept(nd->cell, lo, hi, beta_f)) return 0.0f;
+  float trS = (nd->quad[0] + nd->quad[1]) + nd->quad[2];
+  trS = trS > 0.0f ? trS : 0.0f;
+  float dx = c[0] - nd->com[0], dy = c[1] - nd->com[1], dz = c[2] - nd->com[2];
+  float r2 = ((dx * dx + dy * dy) + dz * dz) + eps2;
+  float num = trS * sqrtf(trS / nd->com[3]);
+  float den = (r2 * r2) * sqrtf(r2);
+  return num / den;
+}
+
+/* monopole + quadrupole of node c at q, h = |r|^2 + eps2 */
+static void stoch_node_far(const OrcNodeRec* c, const float* q, double eps2, double* acc) {
+  double r[3] = {(double)q[0] - c->com[0], (double)q[1] - c->com[1], (double)q[2] - c->com[2]};
+  double h = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + eps2;
+  double ih = 1.0 / h, ir = 1.0 / sqrt(h);
+  double ir3 = ir * ih, ir5 = ir3 * ih;
+  double S[6] = {c->quad[0], c->quad[1], c->quad[2], c->quad[3], c->quad2[0], c->quad2[1]};
+  double Sx[3];
+  sym_mul(S, r, Sx);
+  double tr = S[0] + S[1] + S[2];
+  double xSx = r[0] * Sx[0] + r[1] * Sx[1] + r[2] * Sx[2];
+  double M = c->com[3];
+  for (int d = 0; d < 3; d++)
+    acc[d] += -M * ir3 * r[d] + ir5 * (3.0 * Sx[d] + 1.5 * tr * r[d]) - 7.5 * xSx * ir5 * ih * r[d];
+}
+
+static void stoch_direct(const float* sp, int32_t s0, int32_t s1, const float* q, double eps2, double* acc) {
+  for (int32_t j = s0; j < s1; j++) {
+    double r[3] = {(double)q[0] - sp[4 * j], (double)q[1] - sp[4 * j + 1], (double)q[2] - sp[4 * j + 2]};
+    double h = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + eps2;
+    double c = -(double)sp[4 * j + 3] / (h * sqrt(h));
+    for (int d = 0; d < 3; d++) acc[d] += c * r[d];
+  }
+}
+
+/* R_n(q) - F_n(q): the group walk of node n0's subtree at beta_f (n0 itself
+ * is opened: its weight is positive only when the box does not clear it)
+ * minus n0's monopole + quadrupole, at target q. */
+static void stoch_correction(const OrcNodeRec* N, const float* sp, int32_t n0, const float* lo, const float* hi,
+                             const float* q, float beta_f, double eps2, double* d3) {
+  double R[3] = {0, 0, 0}, F[3] = {0, 0, 0};
+  const OrcNodeRec* nd = &N[n0];
+  if (nd->topo[3] & ORC_LEAF_FLAG) {
+    stoch_direct(sp, nd->topo[0], nd->topo[1], q, eps2, R);
+  } else {
+    for (int32_t k = n0 + 1; k < nd->topo[2];) {
+      const OrcNodeRec* c = &N[k];
+      if (c->com[3] == 0.0f) {
+        k = c->topo[2];
+      } else if (stoch_accept(c->cell, lo, hi, beta_f)) {
+        stoch_node_far(c, q, eps2, R);
+        k = c->topo[2];
+      } else if (c->topo[3] & ORC_LEAF_FLAG) {
+        stoch_direct(sp, c->topo[0], c->topo[1], q, eps2, R);
+        k = c->topo[2];
+      } else {
+        k = k + 1;
+      }
+    }
+  }
+  stoch_node_far(nd, q, eps2, F);
+  for (int d = 0; d < 3; d++) d3[d] = R[d] - F[d];
+}
+
+/*
+ * n targets = the sorted sources sp (n x 4: x, y, z, m), perm: sorted ->
+ * input index, nodes: nn records of 80 bytes (the GPU export). out (the
+ * estimate) and expect (its expectation, the group walk at beta_f), n x 3 in
+ * input order; either may be NULL. Returns the number of subtree walks
+ * (distinct drawn nodes) over all groups.
+ */
+int64_t orc_native_stochastic(const float* sp, const uint32_t* perm, int64_t n, const void* nodes, int64_t nn,
+                              int group_size, float beta_c, float beta_f, float eps2, int K, uint64_t seed,
+                              double* out, double* expect) {
+  const OrcNodeRec* N = (const OrcNodeRec*)nodes;
+  NativeTree t;
+  memset(&t, 0, sizeof(t));
+  t.n = n;
+  t.nn = nn;
+  size_t cap = nn > 0 ? (size_t)nn : 1;
+  t.start = (int32_t*)malloc(sizeof(int32_t) * cap);
+  t.end = (int32_t*)malloc(sizeof(int32_t) * cap);
+  t.skip = (int32_t*)malloc(sizeof(int32_t) * cap);
+  t.level = (int8_t*)malloc(cap);
+  for (int64_t k = 0; k < nn; k++) {
+    t.start[k] = N[k].topo[0];
+    t.end[k] = N[k].topo[1];
+    t.skip[k] = N[k].topo[2];
+    t.level[k] = (int8_t)(N[k].topo[3] & 0xff);
+  }
+  int64_t* gs = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
+  int64_t* ge = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
+  int64_t ng = native_node_groups(&t, group_size, gs, ge);
+  double de2 = (double)eps2;
+  int64_t walks = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : walks)
+  for (int64_t g = 0; g < ng; g++) {
+    int64_t s0 = gs[g], s1 = ge[g], m = s1 - s0;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = s0; i < s1; i++)
+      for (int d = 0; d < 3; d++) {
+        lo[d] = fminf(lo[d], sp[4 * i + d]);
+        hi[d] = fmaxf(hi[d], sp[4 * i + d]);
+      }
+    float c4[4];
+    group_centre(lo, hi, c4);
+    int64_t r0 = 0, r1 = nn; /* the root whose particles hold the group */
+    for (int64_t k = 0; k < nn; k = N[k].topo[2]) {
+      if (N[k].topo[0] <= s0 && s0 < N[k].topo[1]) {
+        r0 = k;
+        r1 = N[k].topo[2];
+        break;
+      }
+    }
+    double* fc = (double*)calloc((size_t)m * 3, sizeof(double));
+    double* ex = (double*)calloc((size_t)m * 3, sizeof(double));
+    double* co = (double*)calloc((size_t)m * 3, sizeof(double));
+    float W = 0.0f;
+    /* pass 1: coarse part, W, the expectation of the correction */
+    for (int64_t k = r0; k < r1;) {
+      const OrcNodeRec* c = &N[k];
+      int leaf = (c->topo[3] & ORC_LEAF_FLAG) != 0;
+      if (c->com[3] == 0.0f) {
+        k = c->topo[2];
+      } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
+        float w = stoch_weight(c, lo, hi, c4, beta_f, eps2);
+        W = W + w;
+        for (int64_t i = s0; i < s1; i++) {
+          const float q[3] = {sp[4 * i], sp[4 * i + 1], sp[4 * i + 2]};
+          stoch_node_far(c, q, de2, &fc[3 * (i - s0)]);
+          if (w > 0.0f && expect) {
+            double d3[3];
+            stoch_correction(N, sp, (int32_t)k, lo, hi, q, beta_f, de2, d3);
+            for (int d = 0; d < 3; d++) ex[3 * (i - s0) + d] += d3[d];
+          }
+        }
+        k = c->topo[2];
+      } else if (leaf) {
+        for (int64_t i = s0; i < s1; i++) {
+          const float q[3] = {sp[4 * i], sp[4 * i + 1], sp[4 * i + 2]};
+          stoch_direct(sp, c->topo[0], c->topo[1], q, de2, &fc[3 * (i - s0)]);
+        }
+        k = c->topo[2];
+      } else {
+        k = k + 1;
+      }
+    }
+    /* pass 2: the K stratified draws, shared by the group's targets */
+    if (W > 0.0f) {
+      const uint64_t gi = perm[s0];
+      float P = 0.0f, step = W / (float)K;
+      int kk = 0;
+      float u = ((float)kk + orc_stoch_uniform(seed, gi, kk)) * step;
+      int32_t last = -1;
+      float last_scale = 0.0f;
+      for (int64_t k = r0; k < r1 && kk < K;) {
+        const OrcNodeRec* c = &N[k];
+        int leaf = (c->topo[3] & ORC_LEAF_FLAG) != 0;
+        if (c->com[3] == 0.0f) {
+          k = c->topo[2];
+        } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
+          float w = stoch_weight(c, lo, hi, c4, beta_f, eps2);
+          float Pn = P + w;
+          if (Pn > P) { /* a weight that rounding absorbed has an empty interval */
+            float scale = W / ((float)K * (Pn - P));
+            int cnt = 0;
+            last = (int32_t)k;
+            last_scale = scale;
+            while (kk < K && u < Pn) {
+              cnt++;
+              kk++;
+              if (kk < K) u = ((float)kk + orc_stoch_uniform(seed, gi, kk)) * step;
+            }
+            if (cnt > 0) {
+              float sc = (float)cnt * scale;
+              walks++;
+              for (int64_t i = s0; i < s1; i++) {
+                const float q[3] = {sp[4 * i], sp[4 * i + 1], sp[4 * i + 2]};
+                double d3[3];
+                stoch_correction(N, sp, (int32_t)k, lo, hi, q, beta_f, de2, d3);
+                for (int d = 0; d < 3; d++) co[3 * (i - s0) + d] += d3[d] * (double)sc;
+              }
+            }
+          }
+          P = Pn;
+          k = c->topo[2];
+        } else if (leaf) {
+          k = c->topo[2];
+        } else {
+          k = k + 1;
+        }
+      }
+      /* draws at the top end that rounding left past the last interval */
+      if (kk < K && last >= 0) {
+        float sc = (float)(K - kk) * last_scale;
+        walks++;
+        for (int64_t i = s0; i < s1; i++) {
+          const float q[3] = {sp[4 * i], sp[4 * i + 1], sp[4 * i + 2]};
+          double d3[3];
+          stoch_correction(N, sp, last, lo, hi, q, beta_f, de2, d3);
+          for (int d = 0; d < 3; d++) co[3 * (i - s0) + d] += d3[d] * (double)sc;
+        }
+      }
+    }
+    for (int64_t i = s0; i < s1; i++) {
+      const uint64_t oi = perm[i];
+      for (int d = 0; d < 3; d++) {
+        if (out) out[3 * oi + d] = fc[3 * (i - s0) + d] + co[3 * (i - s0) + d];
+        if (expect) expect[3 * oi + d] = fc[3 * (i - s0) + d] + ex[3 * (i - s0) + d];
+      }
+    }
+    free(fc);
+    free(ex);
+    free(co);
+  }
+  free(gs);
+  free(ge);
+  free(t.start);
+  free(t.end);
+  free(t.skip);
+  free(t.level);
+  return walks;
+}
+
+/* Node records in the GPU's 80-byte layout from the oracle's tree (float
+ * COM and second moments of the double sums; cell centre and diagonal
+ * side * sqrt(3); topology with the leaf flag), for CPU-side runs of
+ * orc_native_stochastic. */
+void orc_native_records(void* h, const float* pts, const float* masses, void* out) {
+  NativeTree* t = (NativeTree*)h;
+  double* mom = (double*)malloc(sizeof(double) * MOM * (t->nn > 0 ? t->nn : 1));
+  native_moments(t, pts, masses, mom);
+  OrcNodeRec* R = (OrcNodeRec*)out;
+  for (int64_t k = 0; k < t->nn; k++) {
+    const double* o = &mom[MOM * k];
+    OrcNodeRec r;
+    memset(&r, 0, sizeof(r));
+    for (int d = 0; d < 3; d++) r.com[d] = (float)o[1 + d];
+    r.com[3] = (float)o[0];
+    for (int d = 0; d < 3; d++) r.cell[d] = t->center[3 * k + d];
+    r.cell[3] = t->side[k] * 1.7320508f;
+    for (int c = 0; c < 4; c++) r.quad[c] = (float)o[4 + c];
+    r.quad2[0] = (float)o[8];
+    r.quad2[1] = (float)o[9];
+    r.topo[0] = t->start[k];
+    r.topo[1] = t->end[k];
+    r.topo[2] = t->skip[k];
+    r.topo[3] = (int32_t)t->level[k] | (native_is_leaf(t, k) ? ORC_LEAF_FLAG : 0);
+    R[k] = r;
+  }
+  free(mom);
+}

@@ -106,6 +106,10 @@ def _orc() -> ctypes.CDLL:
         lib.orc_native_wn_plan.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_i64, _c_d]
         lib.orc_native_wn_eval.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p]
         lib.orc_native_wn_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]
+        lib.orc_native_records.argtypes = [_c_p, _c_p, _c_p, _c_p]
+        lib.orc_native_stochastic.restype = _c_i64
+        lib.orc_native_stochastic.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_i, _c_f, _c_f, _c_f, _c_i,
+                                              ctypes.c_uint64, _c_p, _c_p]
         lib._typed = True
     return lib
 
@@ -286,6 +290,18 @@ class NativeTree:
         self._lib.orc_native_wn_adjoint(self._h, _ptr(self.points), _ptr(_f32(normals)), _ptr(self.masses),
                                         _ptr(self.queries), _ptr(_f32(u)), _ptr(dq), _ptr(dp), _ptr(dn), _ptr(dm))
         return dq, dp, dn, dm
+
+    def node_records(self) -> np.ndarray:
+        """Node records in the GPU's layout (nn x 80 bytes) from this tree."""
+        out = np.zeros((self.num_nodes, 80), np.uint8)
+        self._lib.orc_native_records(self._h, _ptr(self.points), _ptr(self.masses), _ptr(out))
+        return out
+
+    def sorted_sources(self):
+        """(sorted sources (n x 4: x, y, z, m), permutation sorted -> input)."""
+        perm = self.arrays()["perm"]
+        sp = np.concatenate([self.points[perm], self.masses[perm, None]], axis=1)
+        return np.ascontiguousarray(sp, np.float32), perm.astype(np.uint32)
 
     def plan_stats(self):
         a, b, c = _c_i64(), _c_i64(), _c_i64()
@@ -706,3 +722,23 @@ def mesh_vertex_sources(V, F):
     good = ln > 0
     nrm[good] = nsum[good] / ln[good, None]
     return nrm, mass
+
+
+def native_stochastic(sorted_sources, perm, node_records, *, group_size=128, beta_coarse=1.0, beta=2.0,
+                      softening=1e-3, samples=32, seed=0, expectation=True):
+    """The native stochastic Barnes-Hut estimator restated (orc_native_stochastic)
+    on given node records (the GPU export, or NativeTree.node_records()).
+    Returns (estimate, expectation or None, subtree walks), the first two
+    float64 n x 3 in input order. softening enters as eps^2 + 1e-12 in
+    float, as the CUDA walk holds it."""
+    sp = _f32(sorted_sources)
+    pm = np.ascontiguousarray(np.asarray(perm, np.uint32))
+    nodes = np.ascontiguousarray(np.asarray(node_records, np.uint8))
+    n, nn = sp.shape[0], nodes.size // 80
+    eps2 = np.float32(np.float32(softening) * np.float32(softening) + np.float32(1e-12))
+    out = np.zeros((n, 3), np.float64)
+    ex = np.zeros((n, 3), np.float64) if expectation else None
+    walks = _orc().orc_native_stochastic(_ptr(sp), _ptr(pm), n, _ptr(nodes), nn, int(group_size), float(beta_coarse),
+                                         float(beta), float(eps2), int(samples), ctypes.c_uint64(int(seed)),
+                                         _ptr(out), _ptr(ex))
+    return out, ex, int(walks)

@@ -1,0 +1,109 @@
+"""GPU: the native stochastic Barnes-Hut estimator (sbh_native_stochastic_force)
+against the oracle's restatement (orc_native_stochastic) run on the GPU's own
+exported tree: at a fixed seed both draw the same nodes, so every row agrees
+within FP32 tolerance; over seeds the mean converges to the expectation, the
+force walk at beta with the quadrupole everywhere (on the GPU, and the
+oracle's), within its standard error; and the error against the FP64 direct
+sum at 32 drawn nodes per query is bounded."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+import sbh_b200 as B
+import sbh_oracle as O
+import sbh_workloads as W
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _tree(n, seed=3, leaf=16):
+    p, m = W.plummer(n, seed=seed)
+    t = B.NativeTree().build(p, m, leaf_size=leaf)
+    _, perm, rec = t.export()
+    sp = np.ascontiguousarray(np.concatenate([p[perm], m[perm, None]], axis=1), np.float32)
+    return p, m, t, sp, perm, rec
+
+
+@pytest.mark.parametrize("bc,K", [(1.0, 32), (1.5, 32), (1.0, 1), (0.75, 7)])
+def test_fixed_seed_matches_oracle(cuda, bc, K):
+    p, m, t, sp, perm, rec = _tree(20000)
+    got = t.stochastic_force(beta=2.0, beta_coarse=bc, samples=K, seed=11, softening=1e-3).cpu().numpy()
+    want, ex, walks = O.native_stochastic(sp, perm, rec, group_size=B.native_group_size(), beta_coarse=bc, beta=2.0,
+                                          softening=1e-3, samples=K, seed=11)
+    assert walks > 0
+    # same draws: the rows differ by FP32 rounding of the coarse part and of
+    # each drawn node's (refined - quadrupole) difference times its weight
+    assert rel_l2(got, want) < 3e-5
+    row = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
+    assert row.max() < 2e-3, f"worst row {row.max():.2e}"
+    # and the estimate is not its expectation (the draws do something)
+    assert rel_l2(want, ex) > 1e-6
+
+
+def test_unbiased_over_seeds(cuda):
+    p, m, t, sp, perm, rec = _tree(8000, seed=4)
+    S, K = 64, 4
+    runs = np.stack([t.stochastic_force(beta_coarse=1.0, samples=K, seed=1000 + s).cpu().numpy().astype(np.float64)
+                     for s in range(S)])
+    _, ex, _ = O.native_stochastic(sp, perm, rec, group_size=B.native_group_size(), beta_coarse=1.0, samples=K,
+                                   seed=0)
+    # the expectation is the force walk at beta = 2 with the quadrupole everywhere
+    walk = t.force(beta=2.0, softening=1e-3, quadrupole_radius=0.0, quadrupole_linear=0.0).cpu().numpy()
+    assert rel_l2(walk, ex) < 1e-5
+    mean, sd = runs.mean(0), runs.std(0, ddof=1)
+    scale = np.linalg.norm(ex, axis=1, keepdims=True) * np.ones((1, 3))
+    noisy = sd > 1e-4 * scale  # components where sampling noise dominates FP32 rounding
+    assert noisy.mean() > 0.5
+    # rows of one group share their draws, so z-scores of one group are
+    # correlated; their mean square still has expectation 63 / 61
+    z = (mean - ex)[noisy] / (sd[noisy] / np.sqrt(S))
+    assert 0.7 < float(np.mean(z * z)) < 1.4, float(np.mean(z * z))
+    assert float(np.mean(np.abs(z) > 5.0)) < 2e-3
+    # rows without spread are deterministic and equal the expectation
+    quiet = ~noisy
+    assert np.all(np.abs(mean - ex)[quiet] <= 1e-4 * scale[quiet] + 1e-7)
+    # the mean over 64 seeds is 8x closer to the walk than one estimate
+    assert rel_l2(mean, walk) < 0.25 * rel_l2(runs[0], walk)
+
+
+def test_accuracy_vs_fp64_direct(cuda):
+    n = 1 << 17
+    p, m = W.plummer(n, seed=5)
+    t = B.NativeTree().build(p, m)
+    idx = np.random.default_rng(6).choice(n, 1024, replace=False)
+    ref = O.direct_force_soft(p, m, p[idx], 1e-3)
+    # 32 drawn nodes per query (CPU restatement at 5e4 particles: 8.1e-4 and 1.8e-4)
+    est = t.stochastic_force(samples=32, beta_coarse=1.0, seed=1).cpu().numpy()
+    assert rel_l2(est[idx], ref) < 2.5e-3
+    est = t.stochastic_force(samples=32, beta_coarse=1.5, seed=1).cpu().numpy()
+    assert rel_l2(est[idx], ref) < 6e-4
+
+
+def test_determinism_and_validation(cuda):
+    p, m, t, sp, perm, rec = _tree(3000, seed=7)
+    a = t.stochastic_force(seed=5)
+    b = t.stochastic_force(seed=5)
+    c = t.stochastic_force(seed=6)
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert not torch.equal(a, c)
+    # beta_coarse = beta: every weight is zero, the estimate is the force walk
+    d = t.stochastic_force(beta_coarse=2.0, seed=5)
+    e = t.stochastic_force(beta_coarse=2.0, seed=9)
+    f = t.force(beta=2.0, quadrupole_radius=0.0, quadrupole_linear=0.0)
+    assert torch.equal(d, e) and torch.equal(d, f)
+    with pytest.raises(ValueError):
+        t.stochastic_force(beta_coarse=2.5)  # coarser than beta is required
+    for k in (0, 1025):
+        with pytest.raises(ValueError):
+            t.stochastic_force(samples=k)
+    L = B.lib()
+    prm = t.params(2.0, 1e-3, 0.5, False)  # an erfc cutoff: not served
+    out = torch.empty((t.n, 3), device=cuda)
+    s = torch.cuda.current_stream(cuda).cuda_stream
+    assert L.sbh_native_stochastic_force(s, ctypes.byref(prm), 1.0, 8, ctypes.c_uint64(1), out.data_ptr(),
+                                         t.ws.data_ptr(), t.ws.numel()) != 0
+    assert "free-space" in B.last_error()

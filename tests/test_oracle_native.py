@@ -194,3 +194,30 @@ def test_native_winding_number_adjoint_matches_finite_differences():
         assert abs((lp - lm) / (2 * h) - dn[j, 1]) <= 2e-3 * (abs(dn[j, 1]) + 1e-3)
         a = m64.copy(); hm = 1e-2 * m64[j]; a[j] += hm; lp = loss(mm=a); a[j] -= 2 * hm; lm = loss(mm=a)
         assert abs((lp - lm) / (2 * hm) - dm[j]) <= 2e-3 * (abs(dm[j]) + 1e-3)
+
+
+def test_stochastic_restatement_unbiased_and_accurate():
+    """The stochastic estimator's restatement on the oracle's own tree: the
+    mean over seeds converges to its expectation (the group walk at beta =
+    2), which meets the FP64 direct sum; 32 drawn nodes per query stay
+    within the error the coarse opening leaves to sample."""
+    n = 6000
+    p, m = W.plummer(n, seed=8)
+    T = O.NativeTree(p, m, leaf_size=16)
+    rec = T.node_records()
+    sp, perm = T.sorted_sources()
+    runs, ex = [], None
+    for s in range(24):
+        est, e, walks = O.native_stochastic(sp, perm, rec, beta_coarse=1.0, samples=4, seed=s, expectation=ex is None)
+        ex = e if ex is None else ex
+        assert walks > 0
+        runs.append(est)
+    runs = np.stack(runs)
+    err_one = rel_l2(runs[0], ex)
+    err_mean = rel_l2(runs.mean(0), ex)
+    assert err_mean < 0.35 * err_one  # ~1 / sqrt(24) = 0.2 for an unbiased estimator
+    idx = np.arange(0, n, 7)
+    ref = O.direct_force_soft(p, m, p[idx], 1e-3)
+    assert rel_l2(ex[idx], ref) < 1e-4
+    est, _, _ = O.native_stochastic(sp, perm, rec, beta_coarse=1.0, samples=32, seed=1, expectation=False)
+    assert rel_l2(est[idx], ref) < 2e-3
