@@ -1696,21 +1696,9 @@ int sbh_native_stochastic_force(cudaStream_t stream, const sbh_native_params* pa
   if (h.n == 0) return SBH_OK;
   if (!force_out) return invalid("force_out must be non-null");
   if (partial_range(h)) return invalid("the stochastic estimator needs the full target range");
-  // coarse part: the force walk at beta_coarse, quadrupole at every accepted node
-  WalkParams wp = walk_params(params);
-  wp.beta = beta_coarse;
-  wp.quad_g = 0.0f;
-  wp.quad_lin = 0.0f;
-  const int64_t mg = h.n + h.nseg;
-  auto k = h.group_size > kGroupThreeSlots ? tpl4::force_walk_kernel<true, false, false>
-           : h.group_size > kGroupTwoSlots ? tpl3::force_walk_kernel<true, false, false>
-                                           : tpl2::force_walk_kernel<true, false, false>;
-  const WalkTree T = tree_view(L);
-  const WalkTargets G = self_targets(L, h);
-  cudaError_t e = launch_walk(stream, L.work, mg, k, T, G, wp, force_out);
-  if (e == cudaSuccess)
-    e = launch_walk(stream, L.work, mg, stoch_group_kernel, T, G, beta_coarse, params->beta, wp.eps2, samples, seed,
-                    force_out);
+  const WalkParams wp = walk_params(params);
+  cudaError_t e = launch_walk(stream, L.work, h.n + h.nseg, stoch_group_kernel, tree_view(L), self_targets(L, h),
+                              beta_coarse, params->beta, wp.eps2, samples, seed, force_out);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   remember_walk(workspace, 0, nullptr);
   return check_launch("sbh_native_stochastic_force");

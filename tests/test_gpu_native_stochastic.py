@@ -91,10 +91,12 @@ def test_determinism_and_validation(cuda):
     assert torch.equal(a, b)
     assert not torch.equal(a, c)
     # beta_coarse = beta: every weight is zero, the estimate is the force walk
+    # (the same terms, summed in another order)
     d = t.stochastic_force(beta_coarse=2.0, seed=5)
     e = t.stochastic_force(beta_coarse=2.0, seed=9)
     f = t.force(beta=2.0, quadrupole_radius=0.0, quadrupole_linear=0.0)
-    assert torch.equal(d, e) and torch.equal(d, f)
+    assert torch.equal(d, e)
+    assert rel_l2(d.cpu().numpy(), f.cpu().numpy()) < 1e-6
     with pytest.raises(ValueError):
         t.stochastic_force(beta_coarse=2.5)  # coarser than beta is required
     for k in (0, 1025):
