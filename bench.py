@@ -53,6 +53,10 @@ def workload(n: int, systems: int) -> str:
     return f"plummer_n{n}_eps1e-3_theta0.5_force_plus_full_vjp_{systems}_systems_per_step"
 
 
+EXTRAS = ("octree8_plain", "forest", "sharded_single_system", "winding_number", "winding_number_mesh",
+          "treepm_short_range", "stochastic_octree8", "direct_sum", "trajectory")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -65,6 +69,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the octree8, forest, winding-number, stochastic and trajectory measurements")
+    ap.add_argument("--extra", action="append", default=None, choices=EXTRAS,
+                    help="run only the named extra measurements (repeatable; default: all)")
     return ap.parse_args()
 
 
@@ -384,6 +390,22 @@ def stochastic_measurement(B, torch, P0, M0, idx, ref, flush):
                                          rel_l2_vs_fp64_direct=rel(st))
     cl, cl_ms = timed(lambda: B.softened_barnes_hut_force_octree8(leaf, node, Q, **kw), warm=True)
     out["classic"] = dict(ms=cl_ms, queries_per_s=Q.shape[0] / (cl_ms * 1e-3), rel_l2_vs_fp64_direct=rel(cl))
+    # the native stochastic estimator (sbh_native_stochastic_force): the group
+    # walk at beta_coarse plus 32 drawn tree nodes per query refined to beta = 2
+    tree = B.NativeTree().build(P0, M0)
+    nat = dict(samples=32, what=("group walk at beta_coarse + 32 tree nodes per query (shared by a target group) "
+                                 "drawn by octupole size and refined to beta 2; unbiased for the beta-2 force walk"))
+    for bc in (1.0, 1.25, 1.5):
+        st, st_ms = timed(lambda: tree.stochastic_force(beta=BETA, beta_coarse=bc, samples=32, seed=3,  # noqa: B023
+                                                        softening=EPS), warm=True)
+        nat[f"beta_coarse_{bc}"] = dict(ms=st_ms, queries_per_s=Q.shape[0] / (st_ms * 1e-3),
+                                        rel_l2_vs_fp64_direct=rel(st))
+    wk, wk_ms = timed(lambda: tree.force(beta=BETA, softening=EPS, quadrupole_radius=0.0, quadrupole_linear=0.0),
+                      warm=True)
+    nat["force_walk_beta_2"] = dict(ms=wk_ms, rel_l2_vs_fp64_direct=rel(wk),
+                                    what="the estimator's expectation: force walk at beta 2, quadrupole everywhere")
+    tree.release()
+    out["native"] = nat
     return out
 
 
@@ -979,18 +1001,26 @@ def run_ours(args):
 
     extras = {}
     if not args.no_extras:
-        if world == 1:
+        want = set(args.extra) if args.extra else set(EXTRAS)
+        if world == 1 and "octree8_plain" in want:
             extras["octree8_plain"] = octree8_plain_measurement(B, torch, P0, M0, W0, idx, ref, flush)
-        extras["forest"] = forest_measurement(B, torch, dev, rank, world, flush)
-        if world > 1:
+        if "forest" in want:  # every rank takes part (a collective-free shard of the systems)
+            extras["forest"] = forest_measurement(B, torch, dev, rank, world, flush)
+        if world > 1 and "sharded_single_system" in want:
             extras["sharded_single_system"] = sharded_measurement(B, torch, dev, rank, world, n)
         if world == 1:
-            extras["winding_number"] = winding_measurement(B, torch, dev, flush)
-            extras["winding_number_mesh"] = winding_mesh_measurement(B, torch, dev, flush)
-            extras["treepm_short_range"] = treepm_measurement(B, torch, dev, flush)
-            extras["stochastic_octree8"] = stochastic_measurement(B, torch, P0, M0, idx, ref, flush)
-            extras["direct_sum"] = direct_measurement(B, torch, P0, M0, W0, flush)
-            extras["trajectory"] = trajectory_measurement(torch, dev, flush)
+            if "winding_number" in want:
+                extras["winding_number"] = winding_measurement(B, torch, dev, flush)
+            if "winding_number_mesh" in want:
+                extras["winding_number_mesh"] = winding_mesh_measurement(B, torch, dev, flush)
+            if "treepm_short_range" in want:
+                extras["treepm_short_range"] = treepm_measurement(B, torch, dev, flush)
+            if "stochastic_octree8" in want:
+                extras["stochastic_octree8"] = stochastic_measurement(B, torch, P0, M0, idx, ref, flush)
+            if "direct_sum" in want:
+                extras["direct_sum"] = direct_measurement(B, torch, P0, M0, W0, flush)
+            if "trajectory" in want:
+                extras["trajectory"] = trajectory_measurement(torch, dev, flush)
 
     if rank == 0:
         cpu = None
