@@ -1704,6 +1704,41 @@ int sbh_native_stochastic_force(cudaStream_t stream, const sbh_native_params* pa
   return check_launch("sbh_native_stochastic_force");
 }
 
+int sbh_native_stochastic_force_vjp(cudaStream_t stream, const sbh_native_params* params, float beta_coarse,
+                                    int samples, uint64_t seed, const float* cotangent, float* force_out,
+                                    float* grad_points, float* grad_masses, void* workspace,
+                                    size_t workspace_bytes) {
+  if (int rc = check_params(params)) return rc;
+  if (params->cutoff > 0.0f || params->periodic || params->prune_radius > 0.0f)
+    return invalid("the stochastic estimator serves Plummer-softened free-space gravity (no cutoff, periodic box "
+                   "or prune radius)");
+  if (!(beta_coarse > 0.0f) || beta_coarse > params->beta) return invalid("beta_coarse must be in (0, beta]");
+  if (samples < 1 || samples > kStochMaxSamples)
+    return invalid("samples must be in [1, " + std::to_string(kStochMaxSamples) + "]");
+  Header h;
+  Layout L;
+  if (int rc = lookup(workspace, workspace_bytes, h, L)) return rc;
+  if (!h.adjoint) return invalid("the tree was built without adjoint scratch (with_adjoint = 0)");
+  if (h.n == 0) return SBH_OK;
+  if (!cotangent) return invalid("cotangent must be non-null");
+  if (!grad_points || !grad_masses) return invalid("gradient outputs must be non-null");
+  if (partial_range(h)) return invalid("the stochastic estimator needs the full target range");
+  if (force_out) {  // the estimate itself: the same draws
+    if (int rc = sbh_native_stochastic_force(stream, params, beta_coarse, samples, seed, force_out, workspace,
+                                             workspace_bytes))
+      return rc;
+  }
+  cudaError_t e = cudaMemsetAsync(L.part_adj, 0, h.n * kPartAdj * sizeof(float), stream);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
+  const WalkParams wp = walk_params(params);
+  e = launch_walk(stream, L.work, h.n + h.nseg, stoch_adjoint_kernel, tree_view(L), self_targets(L, h), beta_coarse,
+                  params->beta, wp.eps2, samples, seed, cotangent, L.gq, L.node_adj, L.part_adj);
+  if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
+  remember_walk(workspace, 0, nullptr);
+  return sbh_native_adjoint_finalize(stream, grad_points, grad_masses, workspace, workspace_bytes);
+}
+
 size_t sbh_native_query_workspace_bytes(int64_t nq) {
   if (nq < 0) return 0;
   Sizer s;

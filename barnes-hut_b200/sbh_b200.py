@@ -157,6 +157,8 @@ _SIGS = {
                                 _c_i),
     "sbh_native_export": ([_c_p, _c_p, _c_sz, _c_p, _c_p, _c_p, _c_sz, _c_p], _c_i),
     "sbh_native_stochastic_force": ([_c_p, _c_p, _c_f, _c_i, ctypes.c_uint64, _c_p, _c_p, _c_sz], _c_i),
+    "sbh_native_stochastic_force_vjp": ([_c_p, _c_p, _c_f, _c_i, ctypes.c_uint64, _c_p, _c_p, _c_p, _c_p, _c_p,
+                                         _c_sz], _c_i),
 }
 
 
@@ -1066,6 +1068,24 @@ class NativeTree:
                                                  _p(self.ws), self.ws.numel()), "native_stochastic_force")
         return out
 
+    def stochastic_force_vjp(self, cotangent, *, beta: float = 2.0, beta_coarse: float = 1.0, samples: int = 32,
+                             seed: int = 0, softening: float = 1e-3, want_force: bool = True):
+        """(estimate or None, d/d points, d/d masses) of sum(cotangent *
+        stochastic_force(...)) at the same seed, the draws held fixed
+        (sbh_native_stochastic_force_vjp; the tree built with_adjoint)."""
+        prm = self.params(beta, softening, 0.0, True, False, 1.0, 0.0, 0.0, 0.0)
+        cot = _f32(cotangent, self.device)
+        if cot.shape != (self.n, 3):
+            raise ValueError("cotangent must have shape (N, 3)")
+        f = torch.empty((self.n, 3), dtype=torch.float32, device=self.device) if want_force else None
+        gx = torch.empty((self.n, 3), dtype=torch.float32, device=self.device)
+        gm = torch.empty(self.n, dtype=torch.float32, device=self.device)
+        _check(lib().sbh_native_stochastic_force_vjp(_stream_ptr(self.device), ctypes.byref(prm), float(beta_coarse),
+                                                     int(samples), ctypes.c_uint64(int(seed) & (2 ** 64 - 1)),
+                                                     _p(cot), _p(f), _p(gx), _p(gm), _p(self.ws), self.ws.numel()),
+               "native_stochastic_force_vjp")
+        return f, gx, gm
+
     def force_vjp(self, cotangent, *, beta: float = 2.0, softening: float = 1e-3, cutoff: float = 0.0,
                   quadrupole: bool = True, periodic: bool = False, box_length: float = 1.0,
                   prune_radius: float = 0.0, quadrupole_radius: float = QUADRUPOLE_RADIUS,
@@ -1282,6 +1302,45 @@ def native_force_recompute_vjp(points, masses, *, beta: float = 2.0, softening: 
     masses = masses if isinstance(masses, torch.Tensor) else _f32(masses, dev)
     return _NativeGravity.apply(points, masses, (float(beta), float(softening), float(cutoff), int(leaf_size),
                                                  bool(quadrupole)))
+
+
+class _NativeStochasticGravity(torch.autograd.Function):
+    """The native stochastic estimator with its adjoint: forward builds the
+    tree and draws (seeded); backward rebuilds the tree from the saved inputs
+    and runs the adjoint of the same draws (held fixed)."""
+
+    @staticmethod
+    def forward(ctx, points, masses, cfg):
+        beta, beta_c, samples, seed, soft, leaf = cfg
+        ctx.save_for_backward(points, masses)
+        ctx.cfg = cfg
+        t = NativeTree().build(points.detach(), masses.detach(), leaf_size=leaf, with_adjoint=False)
+        return t.stochastic_force(beta=beta, beta_coarse=beta_c, samples=samples, seed=seed, softening=soft)
+
+    @staticmethod
+    def backward(ctx, cot):
+        points, masses = ctx.saved_tensors
+        beta, beta_c, samples, seed, soft, leaf = ctx.cfg
+        t = NativeTree().build(points.detach(), masses.detach(), leaf_size=leaf, with_adjoint=True)
+        _, gx, gm = t.stochastic_force_vjp(cot.contiguous(), beta=beta, beta_coarse=beta_c, samples=samples,
+                                           seed=seed, softening=soft, want_force=False)
+        return gx, gm, None
+
+
+def native_stochastic_force(points, masses, *, beta: float = 2.0, beta_coarse: float = 1.0, samples: int = 32,
+                            seed: int = 0, softening: float = 1e-3, leaf_size: int = 16) -> torch.Tensor:
+    """Differentiable stochastic Barnes-Hut self-gravity on the native tree
+    (NativeTree.stochastic_force; gradients w.r.t. points and masses with
+    the draws of `seed` held fixed)."""
+    if not 0 < beta_coarse <= beta:
+        raise ValueError("beta_coarse must be in (0, beta]")
+    if softening < 0:
+        raise ValueError("softening must be >= 0")
+    dev = _device()
+    points = points if isinstance(points, torch.Tensor) else _f32(points, dev)
+    masses = masses if isinstance(masses, torch.Tensor) else _f32(masses, dev)
+    return _NativeStochasticGravity.apply(points, masses, (float(beta), float(beta_coarse), int(samples), int(seed),
+                                                           float(softening), int(leaf_size)))
 
 
 # ---------------------------------------------------------------------------

@@ -400,6 +400,15 @@ def stochastic_measurement(B, torch, P0, M0, idx, ref, flush):
                                                         softening=EPS), warm=True)
         nat[f"beta_coarse_{bc}"] = dict(ms=st_ms, queries_per_s=Q.shape[0] / (st_ms * 1e-3),
                                         rel_l2_vs_fp64_direct=rel(st))
+    W0s = torch.randn_like(P0)
+    for bc in (1.0, 1.5):
+        _, vj_ms = timed(lambda: tree.stochastic_force_vjp(W0s, beta=BETA, beta_coarse=bc, samples=32,  # noqa: B023
+                                                          seed=3, softening=EPS, want_force=False), warm=True)
+        nat[f"beta_coarse_{bc}"]["vjp_ms"] = vj_ms
+    nat["vjp_what"] = ("gradients w.r.t. all positions and masses of sum(w . estimate), the draws held fixed "
+                       "(one adjoint walk + finalize)")
+    _, cv_ms = timed(lambda: tree.force_vjp(W0s, beta=BETA, softening=EPS, want_force=False), warm=True)
+    nat["force_walk_vjp_ms"] = cv_ms
     wk, wk_ms = timed(lambda: tree.force(beta=BETA, softening=EPS, quadrupole_radius=0.0, quadrupole_linear=0.0),
                       warm=True)
     nat["force_walk_beta_2"] = dict(ms=wk_ms, rel_l2_vs_fp64_direct=rel(wk),

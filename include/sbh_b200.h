@@ -456,6 +456,17 @@ int sbh_native_stochastic_force(cudaStream_t stream, const sbh_native_params* pa
                                 int samples, uint64_t seed, float* force_out, void* workspace,
                                 size_t workspace_bytes);
 
+/* The adjoint of sbh_native_stochastic_force's estimate at the same seed,
+ * with the draws held fixed (as the reference's stochastic VJPs hold their
+ * paths, src/sbh_ffi.cu:2293-2442): grad_points (n x 3) and grad_masses (n)
+ * of L = sum_i w_i . a_i, input order, with respect to every particle's
+ * position and mass (the tree built with_adjoint). force_out (optional)
+ * receives the estimate. */
+int sbh_native_stochastic_force_vjp(cudaStream_t stream, const sbh_native_params* params, float beta_coarse,
+                                    int samples, uint64_t seed, const float* cotangent, float* force_out,
+                                    float* grad_points, float* grad_masses, void* workspace,
+                                    size_t workspace_bytes);
+
 /* One traversal computing the force (optional force_out) and the full
  * adjoint of L = sum_i w_i . a_i: grad_points (n x 3) and grad_masses (n),
  * exact for the evaluated approximation (query side, direct sources, and the

@@ -755,6 +755,8 @@ typedef struct {
   int64_t* far_off; /* ngroups + 1 */
   int32_t* far_idx;
   uint8_t* far_quad; /* per far entry: 1 when the node takes the quadrupole */
+  double* far_coef;  /* per far entry: the term's coefficient (NULL: 1), set by orc_native_stochastic_plan */
+  double* near_coef; /* per near entry: the leaf's coefficient (NULL: 1) */
   int64_t* near_off;
   int32_t* near_idx; /* near-field leaf node ids */
   int64_t* gstart;
@@ -817,6 +819,8 @@ void orc_native_free(void* h) {
   free(t->far_off);
   free(t->far_idx);
   free(t->far_quad);
+  free(t->far_coef);
+  free(t->near_coef);
   free(t->near_off);
   free(t->near_idx);
   free(t->gstart);
@@ -1127,6 +1131,9 @@ int64_t orc_native_plan(void* h, const float* pts, const float* masses, double b
   free(t->far_off);
   free(t->far_idx);
   free(t->far_quad);
+  free(t->far_coef);
+  free(t->near_coef);
+  t->far_coef = t->near_coef = NULL;
   free(t->near_off);
   free(t->near_idx);
   t->group_size = group_size;
@@ -1311,27 +1318,33 @@ void orc_native_eval(void* h, const float* pts, const float* masses, double eps,
         int32_t k = t->far_idx[e];
         const double* o = &mom[MOM * k];
         double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
+        double tm[3] = {0, 0, 0};
         native_mi(r);
-        soft_force_pair(r, o[0], &sp, acc);
+        soft_force_pair(r, o[0], &sp, tm);
         if (quad && t->far_quad[e] == QUAD_EXACT) {
-          quad_force(r, o + 4, eps, acc);
+          quad_force(r, o + 4, eps, tm);
         } else if (quad && t->far_quad[e] == QUAD_LINEAR) {
           /* first order about the (frozen) group centre */
           double rc[3] = {gc[0] - o[1], gc[1] - o[2], gc[2] - o[3]};
           double a[3], J[6], dl[3] = {q[0] - gc[0], q[1] - gc[1], q[2] - gc[2]}, Jd[3];
           quad_field_jacobian(rc, o + 4, eps, a, J);
           sym_mul(J, dl, Jd);
-          for (int d = 0; d < 3; d++) acc[d] += a[d] + Jd[d];
+          for (int d = 0; d < 3; d++) tm[d] += a[d] + Jd[d];
         }
+        const double cf = t->far_coef ? t->far_coef[e] : 1.0;
+        for (int d = 0; d < 3; d++) acc[d] += cf * tm[d];
       }
       for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
         int32_t k = t->near_idx[e];
+        double tm[3] = {0, 0, 0};
         for (int32_t j = t->start[k]; j < t->end[k]; j++) {
           int64_t sj = t->perm[j];
           double r[3] = {q[0] - pts[3 * sj], q[1] - pts[3 * sj + 1], q[2] - pts[3 * sj + 2]};
           native_mi(r);
-          soft_force_pair(r, masses[sj], &sp, acc);
+          soft_force_pair(r, masses[sj], &sp, tm);
         }
+        const double cf = t->near_coef ? t->near_coef[e] : 1.0;
+        for (int d = 0; d < 3; d++) acc[d] += cf * tm[d];
       }
       if (out_force) {
         out_force[3 * qi] = acc[0];
@@ -1400,7 +1413,7 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
     for (int64_t i = s0; i < s1; i++) {
       int64_t qi = t->perm[i];
       double q[3] = {pts[3 * qi], pts[3 * qi + 1], pts[3 * qi + 2]};
-      double wi[3] = {w[3 * qi], w[3 * qi + 1], w[3 * qi + 2]};
+      const double wt[3] = {w[3 * qi], w[3 * qi + 1], w[3 * qi + 2]};
       double gq[3] = {0, 0, 0};
       for (int64_t e = t->far_off[g]; e < t->far_off[g + 1]; e++) {
         int32_t k = t->far_idx[e];
@@ -1408,6 +1421,9 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
         double r[3] = {q[0] - o[1], q[1] - o[2], q[2] - o[3]};
         native_mi(r);
         double jt[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+        /* a term with coefficient c: every adjoint is linear in the cotangent, so it takes c w */
+        const double cf = t->far_coef ? t->far_coef[e] : 1.0;
+        const double wi[3] = {cf * wt[0], cf * wt[1], cf * wt[2]};
         soft_force_pair_vjp(r, o[0], wi, &sp, jt);
         soft_force_pair(r, 1.0, &sp, f);
         if (quad && t->far_quad[e] == QUAD_EXACT) quad_vjp(r, o + 4, wi, eps, jt, &AX[MOM * k + 4]);
@@ -1425,6 +1441,8 @@ void orc_native_adjoint(void* h, const float* pts, const float* masses, const fl
       }
       for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
         int32_t k = t->near_idx[e];
+        const double cf = t->near_coef ? t->near_coef[e] : 1.0;
+        const double wi[3] = {cf * wt[0], cf * wt[1], cf * wt[2]};
         for (int32_t j = t->start[k]; j < t->end[k]; j++) {
           int64_t sj = t->perm[j];
           double r[3] = {q[0] - pts[3 * sj], q[1] - pts[3 * sj + 1], q[2] - pts[3 * sj + 2]};
@@ -1637,7 +1655,9 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
   }
   int32_t* fgrp = (int32_t*)malloc(sizeof(int32_t) * (foff[nn] > 0 ? foff[nn] : 1));
   uint8_t* fq = (uint8_t*)malloc(foff[nn] > 0 ? foff[nn] : 1);
+  double* fcf = (double*)malloc(sizeof(double) * (foff[nn] > 0 ? foff[nn] : 1));
   int32_t* ngrp = (int32_t*)malloc(sizeof(int32_t) * (noff[nn] > 0 ? noff[nn] : 1));
+  double* ncf = (double*)malloc(sizeof(double) * (noff[nn] > 0 ? noff[nn] : 1));
   int64_t* fcur = (int64_t*)malloc(sizeof(int64_t) * (nn > 0 ? nn : 1));
   int64_t* ncur = (int64_t*)malloc(sizeof(int64_t) * (nn > 0 ? nn : 1));
   memcpy(fcur, foff, sizeof(int64_t) * nn);
@@ -1647,11 +1667,14 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
       int32_t k = t->far_idx[e];
       if (!mark[k]) continue;
       fgrp[fcur[k]] = (int32_t)g;
+      fcf[fcur[k]] = t->far_coef ? t->far_coef[e] : 1.0;
       fq[fcur[k]++] = t->far_quad[e];
     }
     for (int64_t e = t->near_off[g]; e < t->near_off[g + 1]; e++) {
       int32_t k = t->near_idx[e];
-      if (mark[k]) ngrp[ncur[k]++] = (int32_t)g;
+      if (!mark[k]) continue;
+      ncf[ncur[k]] = t->near_coef ? t->near_coef[e] : 1.0;
+      ngrp[ncur[k]++] = (int32_t)g;
     }
   }
   free(fcur);
@@ -1708,17 +1731,19 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
         if (anc[a] == K) ai = a;
       const int uq = quad ? t->far_quad[e] : QUAD_NONE;
       const double gck[3] = {t->gcen[4 * gk], t->gcen[4 * gk + 1], t->gcen[4 * gk + 2]};
+      const double cf = t->far_coef ? t->far_coef[e] : 1.0;
       for (int c = 0; c < 4; c++) {
         double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
         for (int p = 0; p < 2; p++) {
           const double* o = ai >= 0 ? pm[ai][c][p] : &mom[MOM * K];
           plan_far_term(xp[c][p], o, uq, gck, &sp, f[p]);
         }
-        D4[c] += wk[0] * (f[0][0] - f[1][0]) + wk[1] * (f[0][1] - f[1][1]) + wk[2] * (f[0][2] - f[1][2]);
+        D4[c] += cf * (wk[0] * (f[0][0] - f[1][0]) + wk[1] * (f[0][1] - f[1][1]) + wk[2] * (f[0][2] - f[1][2]));
       }
     }
     for (int64_t e = t->near_off[gk]; e < t->near_off[gk + 1]; e++) {
       const int32_t K = t->near_idx[e];
+      const double cf = t->near_coef ? t->near_coef[e] : 1.0;
       for (int64_t s = t->start[K]; s < t->end[K]; s++) {
         if (s == sk) continue; /* the self pair is zero on both sides */
         for (int c = 0; c < 3; c++) {
@@ -1727,7 +1752,7 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
             double r[3] = {xp[c][p][0] - sx[3 * s], xp[c][p][1] - sx[3 * s + 1], xp[c][p][2] - sx[3 * s + 2]};
             far_term(r, sm[s], NULL, 0, &sp, f[p]);
           }
-          D4[c] += wk[0] * (f[0][0] - f[1][0]) + wk[1] * (f[0][1] - f[1][1]) + wk[2] * (f[0][2] - f[1][2]);
+          D4[c] += cf * (wk[0] * (f[0][0] - f[1][0]) + wk[1] * (f[0][1] - f[1][1]) + wk[2] * (f[0][2] - f[1][2]));
         }
       }
     }
@@ -1735,6 +1760,7 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
     const int32_t leafk = anc[na - 1];
     for (int64_t e = noff[leafk]; e < noff[leafk + 1]; e++) {
       const int64_t g = ngrp[e];
+      const double cf = ncf[e];
       for (int64_t s = t->gstart[g]; s < t->gend[g]; s++) {
         if (s == sk) continue;
         const double* ws = &sw[3 * s];
@@ -1744,7 +1770,7 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
             double r[3] = {sx[3 * s] - xp[c][p][0], sx[3 * s + 1] - xp[c][p][1], sx[3 * s + 2] - xp[c][p][2]};
             far_term(r, mp[c][p], NULL, 0, &sp, f[p]);
           }
-          D4[c] += ws[0] * (f[0][0] - f[1][0]) + ws[1] * (f[0][1] - f[1][1]) + ws[2] * (f[0][2] - f[1][2]);
+          D4[c] += cf * (ws[0] * (f[0][0] - f[1][0]) + ws[1] * (f[0][1] - f[1][1]) + ws[2] * (f[0][2] - f[1][2]));
         }
       }
     }
@@ -1753,6 +1779,7 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
       const int32_t A = anc[a];
       for (int64_t e = foff[A]; e < foff[A + 1]; e++) {
         const int64_t g = fgrp[e];
+        const double cf = fcf[e];
         const int uq = quad ? fq[e] : QUAD_NONE;
         const double gcg[3] = {t->gcen[4 * g], t->gcen[4 * g + 1], t->gcen[4 * g + 2]};
         for (int64_t s = t->gstart[g]; s < t->gend[g]; s++) {
@@ -1761,7 +1788,7 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
           for (int c = 0; c < 4; c++) {
             double f[2][3] = {{0, 0, 0}, {0, 0, 0}};
             for (int p = 0; p < 2; p++) plan_far_term(&sx[3 * s], pm[a][c][p], uq, gcg, &sp, f[p]);
-            D4[c] += ws[0] * (f[0][0] - f[1][0]) + ws[1] * (f[0][1] - f[1][1]) + ws[2] * (f[0][2] - f[1][2]);
+            D4[c] += cf * (ws[0] * (f[0][0] - f[1][0]) + ws[1] * (f[0][1] - f[1][1]) + ws[2] * (f[0][2] - f[1][2]));
           }
         }
       }
@@ -1772,7 +1799,9 @@ void orc_native_fd(void* h, const float* pts, const float* masses, const float* 
   }
   free(fgrp);
   free(fq);
+  free(fcf);
   free(ngrp);
+  free(ncf);
   free(foff);
   free(noff);
   free(mark);
@@ -2332,4 +2361,176 @@ void orc_native_records(void* h, const float* pts, const float* masses, void* ou
     R[k] = r;
   }
   free(mom);
+}
+
+/*
+ * The stochastic estimator of orc_native_stochastic as a frozen plan of the
+ * tree `h` (built on the same points: its topology is the GPU's), for
+ * orc_native_eval, orc_native_adjoint and orc_native_fd with quad = 1:
+ * per group, far entries (node, exact quadrupole, coefficient) and near
+ * entries (leaf, coefficient). The decisions and draws are taken on the given
+ * node records (the GPU export) exactly as orc_native_stochastic takes them:
+ *   coarse cut: accepted nodes (+1), leaves reached (+1);
+ *   a node n drawn c times with interval scale s: its quadrupole (-c s) and
+ *   the group walk of its subtree at beta_f (accepted nodes and leaves, +c s).
+ * The adjoint of this plan is the VJP of the estimate with the draws held
+ * fixed. Returns the number of far + near entries.
+ */
+typedef struct {
+  int64_t nf, nr, fcap, ncap;
+  int32_t *fi, *ni;
+  double *fc, *nc;
+} StochPlan;
+
+static void sp_far(StochPlan* P, int32_t k, double c) {
+  if (P->nf == P->fcap) {
+    P->fcap = P->fcap ? 2 * P->fcap : 1024;
+    P->fi = (int32_t*)realloc(P->fi, sizeof(int32_t) * P->fcap);
+    P->fc = (double*)realloc(P->fc, sizeof(double) * P->fcap);
+  }
+  P->fi[P->nf] = k;
+  P->fc[P->nf++] = c;
+}
+
+static void sp_near(StochPlan* P, int32_t k, double c) {
+  if (P->nr == P->ncap) {
+    P->ncap = P->ncap ? 2 * P->ncap : 1024;
+    P->ni = (int32_t*)realloc(P->ni, sizeof(int32_t) * P->ncap);
+    P->nc = (double*)realloc(P->nc, sizeof(double) * P->ncap);
+  }
+  P->ni[P->nr] = k;
+  P->nc[P->nr++] = c;
+}
+
+/* the entries of sc (R_n - F_n) for a group with box [lo, hi] */
+static void sp_refine(StochPlan* P, const OrcNodeRec* N, int32_t n0, double sc, const float* lo, const float* hi,
+                      float beta_f) {
+  sp_far(P, n0, -sc);
+  const OrcNodeRec* nd = &N[n0];
+  if (nd->topo[3] & ORC_LEAF_FLAG) {
+    sp_near(P, n0, sc);
+    return;
+  }
+  for (int32_t k = n0 + 1; k < nd->topo[2];) {
+    const OrcNodeRec* c = &N[k];
+    if (c->com[3] == 0.0f) {
+      k = c->topo[2];
+    } else if (stoch_accept(c->cell, lo, hi, beta_f)) {
+      sp_far(P, k, sc);
+      k = c->topo[2];
+    } else if (c->topo[3] & ORC_LEAF_FLAG) {
+      sp_near(P, k, sc);
+      k = c->topo[2];
+    } else {
+      k = k + 1;
+    }
+  }
+}
+
+int64_t orc_native_stochastic_plan(void* h, const float* pts, const void* nodes, int group_size, float beta_c,
+                                   float beta_f, float eps2, int K, uint64_t seed) {
+  NativeTree* t = (NativeTree*)h;
+  const OrcNodeRec* N = (const OrcNodeRec*)nodes;
+  const int64_t n = t->n, nn = t->nn;
+  free(t->far_off);
+  free(t->far_idx);
+  free(t->far_quad);
+  free(t->far_coef);
+  free(t->near_off);
+  free(t->near_idx);
+  free(t->near_coef);
+  free(t->gstart);
+  free(t->gend);
+  free(t->gcen);
+  t->group_size = group_size;
+  t->gstart = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
+  t->gend = (int64_t*)malloc(sizeof(int64_t) * (n + 2));
+  const int64_t ng = native_node_groups(t, group_size, t->gstart, t->gend);
+  t->ngroups = ng;
+  t->gcen = (float*)malloc(sizeof(float) * 4 * (ng > 0 ? ng : 1));
+  t->far_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
+  t->near_off = (int64_t*)malloc(sizeof(int64_t) * (ng + 1));
+  StochPlan P;
+  memset(&P, 0, sizeof(P));
+  for (int64_t g = 0; g < ng; g++) {
+    t->far_off[g] = P.nf;
+    t->near_off[g] = P.nr;
+    const int64_t s0 = t->gstart[g], s1 = t->gend[g];
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = s0; i < s1; i++)
+      for (int d = 0; d < 3; d++) {
+        lo[d] = fminf(lo[d], pts[3 * t->perm[i] + d]);
+        hi[d] = fmaxf(hi[d], pts[3 * t->perm[i] + d]);
+      }
+    float* c4 = &t->gcen[4 * g];
+    group_centre(lo, hi, c4);
+    int64_t r0 = 0, r1 = nn;
+    for (int64_t k = 0; k < nn; k = N[k].topo[2]) {
+      if (N[k].topo[0] <= s0 && s0 < N[k].topo[1]) {
+        r0 = k;
+        r1 = N[k].topo[2];
+        break;
+      }
+    }
+    float W = 0.0f;
+    for (int64_t k = r0; k < r1;) {
+      const OrcNodeRec* c = &N[k];
+      if (c->com[3] == 0.0f) {
+        k = c->topo[2];
+      } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
+        sp_far(&P, (int32_t)k, 1.0);
+        W = W + stoch_weight(c, lo, hi, c4, beta_f, eps2);
+        k = c->topo[2];
+      } else if (c->topo[3] & ORC_LEAF_FLAG) {
+        sp_near(&P, (int32_t)k, 1.0);
+        k = c->topo[2];
+      } else {
+        k = k + 1;
+      }
+    }
+    if (W > 0.0f) {
+      const uint64_t gi = t->perm[s0];
+      float Pr = 0.0f, step = W / (float)K;
+      int kk = 0;
+      float u = ((float)kk + orc_stoch_uniform(seed, gi, kk)) * step;
+      int32_t last = -1;
+      float last_scale = 0.0f;
+      for (int64_t k = r0; k < r1 && kk < K;) {
+        const OrcNodeRec* c = &N[k];
+        if (c->com[3] == 0.0f) {
+          k = c->topo[2];
+        } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
+          float Pn = Pr + stoch_weight(c, lo, hi, c4, beta_f, eps2);
+          if (Pn > Pr) {
+            float scale = W / ((float)K * (Pn - Pr));
+            int cnt = 0;
+            last = (int32_t)k;
+            last_scale = scale;
+            while (kk < K && u < Pn) {
+              cnt++;
+              kk++;
+              if (kk < K) u = ((float)kk + orc_stoch_uniform(seed, gi, kk)) * step;
+            }
+            if (cnt > 0) sp_refine(&P, N, (int32_t)k, (double)((float)cnt * scale), lo, hi, beta_f);
+          }
+          Pr = Pn;
+          k = c->topo[2];
+        } else if (c->topo[3] & ORC_LEAF_FLAG) {
+          k = c->topo[2];
+        } else {
+          k = k + 1;
+        }
+      }
+      if (kk < K && last >= 0) sp_refine(&P, N, last, (double)((float)(K - kk) * last_scale), lo, hi, beta_f);
+    }
+  }
+  t->far_off[ng] = P.nf;
+  t->near_off[ng] = P.nr;
+  t->far_idx = P.fi ? P.fi : (int32_t*)malloc(sizeof(int32_t));
+  t->far_coef = P.fc ? P.fc : (double*)malloc(sizeof(double));
+  t->near_idx = P.ni ? P.ni : (int32_t*)malloc(sizeof(int32_t));
+  t->near_coef = P.nc ? P.nc : (double*)malloc(sizeof(double));
+  t->far_quad = (uint8_t*)malloc(P.nf > 0 ? (size_t)P.nf : 1);
+  memset(t->far_quad, QUAD_EXACT, P.nf > 0 ? (size_t)P.nf : 1);
+  return P.nf + P.nr;
 }

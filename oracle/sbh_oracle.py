@@ -107,6 +107,8 @@ def _orc() -> ctypes.CDLL:
         lib.orc_native_wn_eval.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p]
         lib.orc_native_wn_adjoint.argtypes = [_c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p, _c_p]
         lib.orc_native_records.argtypes = [_c_p, _c_p, _c_p, _c_p]
+        lib.orc_native_stochastic_plan.restype = _c_i64
+        lib.orc_native_stochastic_plan.argtypes = [_c_p, _c_p, _c_p, _c_i, _c_f, _c_f, _c_f, _c_i, ctypes.c_uint64]
         lib.orc_native_stochastic.restype = _c_i64
         lib.orc_native_stochastic.argtypes = [_c_p, _c_p, _c_i64, _c_p, _c_i64, _c_i, _c_f, _c_f, _c_f, _c_i,
                                               ctypes.c_uint64, _c_p, _c_p]
@@ -296,6 +298,19 @@ class NativeTree:
         out = np.zeros((self.num_nodes, 80), np.uint8)
         self._lib.orc_native_records(self._h, _ptr(self.points), _ptr(self.masses), _ptr(out))
         return out
+
+    def stochastic_plan(self, node_records, *, group_size=128, beta_coarse=1.0, beta=2.0, softening=1e-3,
+                        samples=32, seed=0) -> int:
+        """Record the native stochastic estimator's terms at this seed as the
+        plan (orc_native_stochastic_plan: coefficients per term, decisions
+        and draws taken on node_records, the GPU export); force(quad=True),
+        adjoint(quad=True) and finite_differences(quad=True) then evaluate
+        the estimate and its VJP with the draws held fixed."""
+        nodes = np.ascontiguousarray(np.asarray(node_records, np.uint8))
+        eps2 = np.float32(np.float32(softening) * np.float32(softening) + np.float32(1e-12))
+        return int(self._lib.orc_native_stochastic_plan(self._h, _ptr(self.points), _ptr(nodes), int(group_size),
+                                                        float(beta_coarse), float(beta), float(eps2), int(samples),
+                                                        ctypes.c_uint64(int(seed))))
 
     def sorted_sources(self):
         """(sorted sources (n x 4: x, y, z, m), permutation sorted -> input)."""

@@ -109,3 +109,50 @@ def test_determinism_and_validation(cuda):
     assert L.sbh_native_stochastic_force(s, ctypes.byref(prm), 1.0, 8, ctypes.c_uint64(1), out.data_ptr(),
                                          t.ws.data_ptr(), t.ws.numel()) != 0
     assert "free-space" in B.last_error()
+
+
+@pytest.mark.parametrize("bc,K", [(1.0, 8), (1.5, 32)])
+def test_vjp_matches_oracle_plan_adjoint(cuda, bc, K):
+    """The adjoint of the estimate with the draws held fixed: gradients with
+    respect to every position and mass against the oracle's adjoint of the
+    same terms (orc_native_stochastic_plan on the GPU's node records, FP64)."""
+    p, m, t, sp, perm, rec = _tree(20000, seed=12)
+    w = np.random.default_rng(13).normal(size=p.shape).astype(np.float32)
+    f, gx, gm = t.stochastic_force_vjp(w, beta=2.0, beta_coarse=bc, samples=K, seed=5, softening=1e-3)
+    est = t.stochastic_force(beta=2.0, beta_coarse=bc, samples=K, seed=5, softening=1e-3)
+    torch.cuda.synchronize()
+    assert torch.equal(f, est)  # the same draws
+    T = O.NativeTree(p, m, leaf_size=16)
+    assert T.stochastic_plan(rec, group_size=B.native_group_size(), beta_coarse=bc, beta=2.0, softening=1e-3,
+                             samples=K, seed=5) > 0
+    dx, dm = T.adjoint(w, 1e-3, quad=True)
+    assert rel_l2(gx.cpu().numpy(), dx) < 1e-4
+    assert rel_l2(gm.cpu().numpy(), dm) < 1e-4
+    # the drawn terms matter: the classic walk's adjoint is farther away
+    _, cx, cm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole_radius=0.0, quadrupole_linear=0.0)
+    assert rel_l2(cx.cpu().numpy(), dx) > 3 * rel_l2(gx.cpu().numpy(), dx)
+
+
+def test_vjp_at_beta_coarse_equal_beta_is_the_force_walk_adjoint(cuda):
+    p, m, t, sp, perm, rec = _tree(8000, seed=14)
+    w = np.random.default_rng(15).normal(size=p.shape).astype(np.float32)
+    _, gx, gm = t.stochastic_force_vjp(w, beta_coarse=2.0, seed=3, want_force=False)
+    _, cx, cm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole_radius=0.0, quadrupole_linear=0.0)
+    assert rel_l2(gx.cpu().numpy(), cx.cpu().numpy()) < 1e-5
+    assert rel_l2(gm.cpu().numpy(), cm.cpu().numpy()) < 1e-5
+
+
+def test_autograd_matches_the_entry_point(cuda):
+    p, m = W.plummer(6000, seed=16)
+    P = torch.tensor(p, device=cuda, requires_grad=True)
+    M = torch.tensor(m, device=cuda, requires_grad=True)
+    f = B.native_stochastic_force(P, M, beta_coarse=1.0, samples=16, seed=9)
+    w = torch.randn_like(f)
+    (f * w).sum().backward()
+    t = B.NativeTree().build(p, m)
+    f2, gx, gm = t.stochastic_force_vjp(w, beta_coarse=1.0, samples=16, seed=9)
+    torch.cuda.synchronize()
+    assert torch.equal(f.detach(), f2)
+    # the node-side and source-side sums are float atomics: equal up to their order
+    assert rel_l2(P.grad.cpu().numpy(), gx.cpu().numpy()) < 1e-5
+    assert rel_l2(M.grad.cpu().numpy(), gm.cpu().numpy()) < 1e-5

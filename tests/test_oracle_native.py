@@ -221,3 +221,29 @@ def test_stochastic_restatement_unbiased_and_accurate():
     assert rel_l2(ex[idx], ref) < 1e-4
     est, _, _ = O.native_stochastic(sp, perm, rec, beta_coarse=1.0, samples=32, seed=1, expectation=False)
     assert rel_l2(est[idx], ref) < 2e-3
+
+
+def test_stochastic_plan_adjoint_matches_finite_differences():
+    """The stochastic estimate as a frozen plan with per-term coefficients
+    (orc_native_stochastic_plan): its value equals the restatement's
+    estimate, and its adjoint (the VJP with the draws held fixed) matches
+    FP64 central differences of the same frozen plan, for positions and
+    masses."""
+    n = 3000
+    p, m = W.plummer(n, seed=9)
+    T = O.NativeTree(p, m, leaf_size=16)
+    rec = T.node_records()
+    sp, perm = T.sorted_sources()
+    est, _, _ = O.native_stochastic(sp, perm, rec, beta_coarse=1.0, samples=8, seed=4, expectation=False)
+    assert T.stochastic_plan(rec, beta_coarse=1.0, samples=8, seed=4) > 0
+    val, _ = T.force(1e-3, quad=True)
+    # the plan sums the same terms with the double moments instead of the float records
+    assert rel_l2(val, est) < 1e-5
+    w = np.random.default_rng(10).normal(size=(n, 3)).astype(np.float32)
+    dx, dm = T.adjoint(w, 1e-3, quad=True)
+    idx = np.random.default_rng(11).choice(n, 40, replace=False)
+    fx1, fm1 = T.finite_differences(w, 1e-3, idx, hx=1e-4, hm_rel=1e-4, quad=True)
+    fx2, fm2 = T.finite_differences(w, 1e-3, idx, hx=5e-5, hm_rel=5e-5, quad=True)
+    fx, fm = (4 * fx2 - fx1) / 3, (4 * fm2 - fm1) / 3  # Richardson
+    assert rel_l2(dx[idx], fx) < 1e-5
+    assert rel_l2(dm[idx], fm) < 1e-5
