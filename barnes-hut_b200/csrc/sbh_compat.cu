@@ -505,22 +505,26 @@ __global__ void __launch_bounds__(256)
 // in the same order and every output row equals o8_bh_kernel's bit for bit;
 // node records and leaf particles are read once per warp instead of once per
 // thread, and the lanes at a leaf loop over its particles together.
-constexpr int kO8WarpsPerBlock = 4;
+// The block holds blockDim.x / 32 warps (the caller's `threads`, the
+// reference's launch parameter, in whole warps) and each warp a stack of
+// STACK entries in dynamic shared memory: 64 for a dense octree8 of depth
+// <= 9 (a DFS of depth d holds at most 7 d + 1 entries), otherwise the
+// reference's 128.
 struct O8StackEntry {
   int node;
   uint32_t lanes;
 };
 
-template <int KERNEL>
-__global__ void __launch_bounds__(32 * kO8WarpsPerBlock)
+template <int KERNEL, int STACK>
+__global__ void __launch_bounds__(1024)
     o8_bh_warp_kernel(const Leaf3* __restrict__ leaf, const OctreeNode8* __restrict__ nodes,
                       const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq, float beta,
                       Soft s, int prune_on, float r_cut_sq, Periodic per, float* __restrict__ out, uint32_t* status,
                       O8Bounds bd, const uint32_t* __restrict__ order) {
-  __shared__ O8StackEntry stacks[kO8WarpsPerBlock][kO8Stack];
+  extern __shared__ O8StackEntry o8_stacks[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  O8StackEntry* stack = stacks[warp];
-  const int64_t ti = (static_cast<int64_t>(blockIdx.x) * kO8WarpsPerBlock + warp) * 32 + lane;
+  O8StackEntry* stack = o8_stacks + warp * STACK;
+  const int64_t ti = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp) * 32 + lane;
   const bool valid = ti < nq;
   const uint32_t live = __ballot_sync(0xffffffffu, valid);
   if (live == 0) return;  // warp-uniform
@@ -571,7 +575,7 @@ __global__ void __launch_bounds__(32 * kO8WarpsPerBlock)
       for (int c = 0; c < 8; c++) {
         if (mask & (1u << c)) {
           if (!o8_node_ok(nd.child[c], bd, status)) continue;
-          if (top < kO8Stack) {
+          if (top < STACK) {
             if (lane == 0) stack[top] = O8StackEntry{static_cast<int>(nd.child[c]), open};
             top++;
           } else {
@@ -875,6 +879,43 @@ static const uint32_t* o8_query_order(cudaStream_t stream, const OctreeNode8* no
   return which == 0 ? v0 : v1;
 }
 
+// Whether the buffer is a dense octree8 of depth <= 9 ((8^(d+1) - 1) / 7
+// nodes), whose DFS never holds more than 64 stack entries.
+static bool o8_small_stack(uint32_t num_nodes) {
+  uint64_t total = 1, level = 1;
+  for (int d = 0; d <= 9; d++) {
+    if (total == num_nodes) return true;
+    level *= 8;
+    total += level;
+  }
+  return false;
+}
+
+template <int STACK>
+static void o8_launch_warp(int kernel, unsigned grid, unsigned block, size_t smem, cudaStream_t stream,
+                           const Leaf3* L, const OctreeNode8* N, const float* queries, const float* cot, int64_t nq,
+                           float beta, Soft s, int prune_on, float r_cut_sq, Periodic per, float* out,
+                           uint32_t* status, O8Bounds bd, const uint32_t* order) {
+  switch (kernel) {
+    case O8_GRAV_GRAD:
+      o8_bh_warp_kernel<O8_GRAV_GRAD, STACK><<<grid, block, smem, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f,
+                                                                           per, out, status, bd, order);
+      break;
+    case O8_SOFT:
+      o8_bh_warp_kernel<O8_SOFT, STACK><<<grid, block, smem, stream>>>(L, N, queries, cot, nq, beta, s, prune_on,
+                                                                      r_cut_sq, per, out, status, bd, order);
+      break;
+    case O8_GRAV_GRAD_VJP:
+      o8_bh_warp_kernel<O8_GRAV_GRAD_VJP, STACK><<<grid, block, smem, stream>>>(L, N, queries, cot, nq, beta, s, 0,
+                                                                               0.f, per, out, status, bd, order);
+      break;
+    default:
+      o8_bh_warp_kernel<O8_SOFT_VJP, STACK><<<grid, block, smem, stream>>>(L, N, queries, cot, nq, beta, s, prune_on,
+                                                                          r_cut_sq, per, out, status, bd, order);
+      break;
+  }
+}
+
 extern "C" {
 
 int sbh_bruteforce_gravity(cudaStream_t stream, const float* points, const float* masses, int64_t n, int dim,
@@ -997,25 +1038,17 @@ static int o8_launch_bh(int kernel, cudaStream_t stream, const void* leaf, size_
   const uint32_t* order = o8_query_order(stream, N, queries, nq, workspace, workspace_bytes, &orc);
   if (orc != SBH_OK) return orc;
   if (order) {  // Morton-ordered queries: one warp walks 32 neighbours together
-    const unsigned gw = grid_for(nq, 32 * kO8WarpsPerBlock);
-    const unsigned tw = 32 * kO8WarpsPerBlock;
-    switch (kernel) {
-      case O8_GRAV_GRAD:
-        o8_bh_warp_kernel<O8_GRAV_GRAD><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out,
-                                                               status, bd, order);
-        break;
-      case O8_SOFT:
-        o8_bh_warp_kernel<O8_SOFT><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per,
-                                                          out, status, bd, order);
-        break;
-      case O8_GRAV_GRAD_VJP:
-        o8_bh_warp_kernel<O8_GRAV_GRAD_VJP><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, 0, 0.f, per, out,
-                                                                   status, bd, order);
-        break;
-      default:
-        o8_bh_warp_kernel<O8_SOFT_VJP><<<gw, tw, 0, stream>>>(L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq,
-                                                              per, out, status, bd, order);
-        break;
+    const int warps = threads >= 64 ? (threads < 1024 ? threads / 32 : 32) : 1;
+    const unsigned tw = 32u * static_cast<unsigned>(warps);
+    const unsigned gw = grid_for(nq, static_cast<int>(tw));
+    if (o8_small_stack(bd.num_nodes)) {
+      const size_t sm = static_cast<size_t>(warps) * 64 * sizeof(O8StackEntry);
+      o8_launch_warp<64>(kernel, gw, tw, sm, stream, L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per, out,
+                         status, bd, order);
+    } else {
+      const size_t sm = static_cast<size_t>(warps) * kO8Stack * sizeof(O8StackEntry);
+      o8_launch_warp<kO8Stack>(kernel, gw, tw, sm, stream, L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per,
+                               out, status, bd, order);
     }
     return check_launch("barnes_hut_force_octree8");
   }

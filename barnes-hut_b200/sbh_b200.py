@@ -1217,6 +1217,36 @@ class _NativeGravity(torch.autograd.Function):
         return gx, gm, None
 
 
+# Candidate block sizes of autotune_octree8 (warps of 32 Morton-ordered
+# queries per block in the warp-cooperative octree8 traversals).
+AUTOTUNE_OCTREE8_THREADS = (64, 128, 256, 512)
+
+
+def autotune_octree8(leaf_bytes, node_bytes, queries, *, candidates=AUTOTUNE_OCTREE8_THREADS, reps: int = 2,
+                     **soft_kwargs) -> dict:
+    """Picks the octree8 traversals' block size for this tree and these
+    queries: times softened_barnes_hut_force_octree8 (soft_kwargs as its
+    keywords) at each candidate `threads` and returns the fastest. The
+    warp-cooperative traversal walks 32 Morton-ordered queries per warp with
+    threads / 32 warps per block; its per-warp shared-memory stack holds 64
+    entries for a dense octree8 of depth <= 9 and 128 otherwise. Results do
+    not depend on the block size."""
+    dev = _device()
+    leaf, node, q = _u8(leaf_bytes, dev), _u8(node_bytes, dev), _f32(queries, dev)
+    trials = []
+    for th in candidates:
+        softened_barnes_hut_force_octree8(leaf, node, q, threads=int(th), **soft_kwargs)  # warm-up
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            softened_barnes_hut_force_octree8(leaf, node, q, threads=int(th), **soft_kwargs)
+        b.record()
+        torch.cuda.synchronize(dev)
+        trials.append((a.elapsed_time(b) / reps, int(th)))
+    ms, th = min(trials)
+    return dict(threads=th, ms=ms, trials=[dict(threads=t_, ms=m_) for m_, t_ in trials])
+
+
 # Candidate (leaf size, most targets per group) pairs of autotune_native:
 # groups of 128 or 96 suit clustered systems, 64 near-uniform ones; leaves of
 # 12 to 20 cost about the same on Plummer spheres.

@@ -785,8 +785,12 @@ def octree8_plain_measurement(B, torch, P0, M0, W0, idx, ref, flush):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
+    # the block size of the warp-cooperative traversal (warps of 32 Morton-ordered queries per block)
+    leaf, node = B.build_octree8_buffers(P0, Z, M0, max_depth=7)
+    tuned = B.autotune_octree8(leaf, node, P0, **kw)
     return dict(ms_per_eval=ms, evals_per_s=1000.0 / ms, rel_l2_vs_fp64_direct=rel, max_depth=7,
-                note="query-side VJP only (the reference's VJP has no source or mass terms)")
+                note="query-side VJP only (the reference's VJP has no source or mass terms)",
+                threads=256, force_threads_autotuned=tuned)
 
 
 def run_ours(args):

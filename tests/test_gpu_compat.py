@@ -394,6 +394,33 @@ def test_octree8_large_build_and_force_sanity(cuda):
     assert rel_l2(got, want) < 5e-3  # octree8's geometric-centre criterion (reference README: ~1e-2)
 
 
+def test_octree8_block_size_changes_no_result(cuda):
+    """The warp-cooperative traversal with 1 to 32 warps per block (the
+    caller's `threads`) gives the same rows bit for bit, and so does the
+    one-thread-per-query kernel (a workspace without room for the order);
+    the autotuner picks one of its candidates."""
+    p, m = W.plummer(30000, seed=43)
+    leaf, node = B.build_octree8_buffers(p, np.zeros_like(p), m, p.min(0) - 1e-3, p.max(0) + 1e-3, max_depth=6)
+    q = p[:20000]
+    kw = dict(beta=2.0, softening_scale=1e-2, cutoff_scale=0.5, prune_enabled=True, prune_r_cut_mult=4.0)
+    outs = [B.softened_barnes_hut_force_octree8(leaf, node, q, threads=th, **kw) for th in (32, 96, 256, 1024)]
+    torch.cuda.synchronize()
+    for o in outs[1:]:
+        assert torch.equal(outs[0], o)
+    L = B.lib()
+    Q = torch.tensor(q, device=cuda)
+    ws = torch.empty(int(L.sbh_traversal_workspace_bytes()), dtype=torch.uint8, device=cuda)
+    out = torch.empty_like(Q)
+    assert L.sbh_barnes_hut_force_octree8_soft(torch.cuda.current_stream(cuda).cuda_stream, leaf.data_ptr(),
+                                               leaf.numel(), node.data_ptr(), node.numel(), Q.data_ptr(), Q.shape[0],
+                                               out.data_ptr(), 2.0, 1e-2, 0.5, 1, 4.0, 0, 1.0, 256, ws.data_ptr(),
+                                               ws.numel()) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0], out)
+    tuned = B.autotune_octree8(leaf, node, q, **kw)
+    assert tuned["threads"] in B.AUTOTUNE_OCTREE8_THREADS and len(tuned["trials"]) == 4
+
+
 def test_octree8_query_order_changes_no_result(cuda):
     """With the ordered workspace the per-query octree8 traversals take the
     queries in Morton order; every output row must equal the input-order
