@@ -156,3 +156,34 @@ def test_autograd_matches_the_entry_point(cuda):
     # the node-side and source-side sums are float atomics: equal up to their order
     assert rel_l2(P.grad.cpu().numpy(), gx.cpu().numpy()) < 1e-5
     assert rel_l2(M.grad.cpu().numpy(), gm.cpu().numpy()) < 1e-5
+
+
+def test_forest_and_tiny_systems_match_oracle(cuda):
+    """A forest of systems of 3,000, 17, 12,000 and 1 particles in one launch:
+    every group walks its own system's tree, draws by its own first input
+    index, and equals the oracle's restatement on the exported records; at
+    beta_coarse = beta the adjoint is the force walk's."""
+    systems = [W.plummer(n, seed=20 + i) for i, n in enumerate((3000, 17, 12000, 1))]
+    pts = np.concatenate([s[0] + np.float32(50.0 * i) for i, s in enumerate(systems)])
+    ms = np.concatenate([s[1] for s in systems])
+    offs = np.cumsum([0] + [s[0].shape[0] for s in systems])
+    t = B.NativeTree().build(pts, ms, system_offsets=offs, leaf_size=16)
+    _, perm, rec = t.export()
+    sp = np.ascontiguousarray(np.concatenate([pts[perm], ms[perm, None]], axis=1), np.float32)
+    got = t.stochastic_force(beta_coarse=1.0, samples=16, seed=2).cpu().numpy()
+    want, ex, walks = O.native_stochastic(sp, perm, rec, group_size=B.native_group_size(), beta_coarse=1.0,
+                                          samples=16, seed=2)
+    assert walks > 0 and np.isfinite(got).all()
+    assert rel_l2(got, want) < 3e-5
+    for i in range(len(systems)):  # per system too (the 1-particle system feels no force)
+        a, b = offs[i], offs[i + 1]
+        if np.abs(want[a:b]).max() > 0:
+            assert rel_l2(got[a:b], want[a:b]) < 1e-4
+        else:
+            assert np.abs(got[a:b]).max() == 0
+    w = np.random.default_rng(21).normal(size=pts.shape).astype(np.float32)
+    _, gx, gm = t.stochastic_force_vjp(w, beta_coarse=2.0, want_force=False)
+    _, cx, cm = t.force_vjp(w, beta=2.0, softening=1e-3, quadrupole_radius=0.0, quadrupole_linear=0.0,
+                            want_force=False)
+    assert rel_l2(gx.cpu().numpy(), cx.cpu().numpy()) < 1e-5
+    assert rel_l2(gm.cpu().numpy(), cm.cpu().numpy()) < 1e-5
