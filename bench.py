@@ -345,7 +345,18 @@ def forest_measurement(B, torch, dev, rank, world, flush):
     t_batched = timed(batched, 3)
     t_graph = timed(g.replay, 3)
     del g
+    # accuracy of the graph's forces: 512 targets of the largest and of the smallest system against
+    # the FP64 direct sum over their own system
+    acc = {}
+    sizes_mine = [s_[0].shape[0] for s_ in mine]
+    for tag, si in (("largest", int(np.argmax(sizes_mine))), ("smallest", int(np.argmin(sizes_mine)))):
+        o0, o1 = int(offs[si]), int(offs[si + 1])
+        sub = torch.tensor(np.random.default_rng(7).choice(o1 - o0, min(512, o1 - o0), replace=False), device=dev)
+        ref = fp64_direct_subset(pts[o0:o1], ms[o0:o1], sub, EPS)
+        acc[tag] = dict(particles=o1 - o0, rel_l2_vs_fp64_direct=float(
+            torch.linalg.norm(F[o0:o1][sub].double() - ref) / torch.linalg.norm(ref)))
     return dict(systems=int(b - a), particles=int(n), plain_ms=t_plain, batched_ms=t_batched, graph_ms=t_graph,
+                accuracy=acc,
                 batched_over_plain=t_plain / t_graph,
                 particle_evals_per_s_graph=n / (t_graph * 1e-3), particle_evals_per_s_plain=n / (t_plain * 1e-3),
                 autotuned=dict(leaf_size=leaf, group_size=group, trials=tune["trials"]))
