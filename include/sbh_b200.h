@@ -442,7 +442,7 @@ int sbh_native_force(cudaStream_t stream, const sbh_native_params* params, float
  * group walk at beta_coarse (monopole + quadrupole everywhere) plus, per
  * target group, `samples` (1..1024) nodes of the group's coarse cut drawn
  * by stratified sampling in proportion to M r_g^3 / r^5 (r from the group
- * box centre; zero where the box clears beta_f cell diagonals), each adding
+ * box to the node's COM; zero where the box clears beta_f cell diagonals), each adding
  * (group walk of the node's subtree at beta_f - the node's quadrupole) /
  * (samples * probability) at the group's targets. Its expectation is the
  * group walk at beta_f with the quadrupole at every accepted node

@@ -2060,8 +2060,8 @@ void orc_native_wn_adjoint(void* h, const float* pts, const float* normals, cons
  *      nodes add their monopole + quadrupole about the COM at every target,
  *      the leaves reached add their particles directly;
  *   2. weights: an accepted node n gets w_n = M r_g^3 / r^5 (r_g^2 = tr S / M,
- *      r^2 = |c - COM|^2 + eps^2 with c the group box centre: the size of the
- *      octupole the quadrupole leaves out), or 0 when the group box already
+ *      r^2 = dist(group box, COM)^2 + eps^2: the size of the octupole the
+ *      quadrupole leaves out at the box's nearest point), or 0 when the group box already
  *      clears beta_f diagonals of the cell (there the refined walk below is
  *      the node's own quadrupole);
  *   3. K stratified draws u_k = (k + U_k) W / K, W = sum w_n, each picking
@@ -2107,14 +2107,18 @@ static int stoch_accept(const float* cell, const float* lo, const float* hi, flo
   return d2 > rc * rc;
 }
 
-/* w_n for the group with box [lo, hi] and centre c */
-static float stoch_weight(const OrcNodeRec* nd, const float* lo, const float* hi, const float* c, float beta_f,
-                          float eps2) {
+/* w_n for the group with box [lo, hi]: r is the distance from the box to the COM */
+static float stoch_weight(const OrcNodeRec* nd, const float* lo, const float* hi, float beta_f, float eps2) {
   if (stoch_accept(nd->cell, lo, hi, beta_f)) return 0.0f;
   float trS = (nd->quad[0] + nd->quad[1]) + nd->quad[2];
   trS = trS > 0.0f ? trS : 0.0f;
-  float dx = c[0] - nd->com[0], dy = c[1] - nd->com[1], dz = c[2] - nd->com[2];
-  float r2 = ((dx * dx + dy * dy) + dz * dz) + eps2;
+  float t3[3];
+  for (int d = 0; d < 3; d++) {
+    float a = lo[d] - nd->com[d], b = nd->com[d] - hi[d];
+    float m = a > b ? a : b;
+    t3[d] = m > 0.0f ? m : 0.0f;
+  }
+  float r2 = ((t3[0] * t3[0] + t3[1] * t3[1]) + t3[2] * t3[2]) + eps2;
   float num = trS * sqrtf(trS / nd->com[3]);
   float den = (r2 * r2) * sqrtf(r2);
   return num / den;
@@ -2214,8 +2218,6 @@ int64_t orc_native_stochastic(const float* sp, const uint32_t* perm, int64_t n, 
         lo[d] = fminf(lo[d], sp[4 * i + d]);
         hi[d] = fmaxf(hi[d], sp[4 * i + d]);
       }
-    float c4[4];
-    group_centre(lo, hi, c4);
     int64_t r0 = 0, r1 = nn; /* the root whose particles hold the group */
     for (int64_t k = 0; k < nn; k = N[k].topo[2]) {
       if (N[k].topo[0] <= s0 && s0 < N[k].topo[1]) {
@@ -2235,7 +2237,7 @@ int64_t orc_native_stochastic(const float* sp, const uint32_t* perm, int64_t n, 
       if (c->com[3] == 0.0f) {
         k = c->topo[2];
       } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
-        float w = stoch_weight(c, lo, hi, c4, beta_f, eps2);
+        float w = stoch_weight(c, lo, hi, beta_f, eps2);
         W = W + w;
         for (int64_t i = s0; i < s1; i++) {
           const float q[3] = {sp[4 * i], sp[4 * i + 1], sp[4 * i + 2]};
@@ -2271,7 +2273,7 @@ int64_t orc_native_stochastic(const float* sp, const uint32_t* perm, int64_t n, 
         if (c->com[3] == 0.0f) {
           k = c->topo[2];
         } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
-          float w = stoch_weight(c, lo, hi, c4, beta_f, eps2);
+          float w = stoch_weight(c, lo, hi, beta_f, eps2);
           float Pn = P + w;
           if (Pn > P) { /* a weight that rounding absorbed has an empty interval */
             float scale = W / ((float)K * (Pn - P));
@@ -2479,7 +2481,7 @@ int64_t orc_native_stochastic_plan(void* h, const float* pts, const void* nodes,
         k = c->topo[2];
       } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
         sp_far(&P, (int32_t)k, 1.0);
-        W = W + stoch_weight(c, lo, hi, c4, beta_f, eps2);
+        W = W + stoch_weight(c, lo, hi, beta_f, eps2);
         k = c->topo[2];
       } else if (c->topo[3] & ORC_LEAF_FLAG) {
         sp_near(&P, (int32_t)k, 1.0);
@@ -2500,7 +2502,7 @@ int64_t orc_native_stochastic_plan(void* h, const float* pts, const void* nodes,
         if (c->com[3] == 0.0f) {
           k = c->topo[2];
         } else if (stoch_accept(c->cell, lo, hi, beta_c)) {
-          float Pn = Pr + stoch_weight(c, lo, hi, c4, beta_f, eps2);
+          float Pn = Pr + stoch_weight(c, lo, hi, beta_f, eps2);
           if (Pn > Pr) {
             float scale = W / ((float)K * (Pn - Pr));
             int cnt = 0;
