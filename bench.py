@@ -53,8 +53,8 @@ def workload(n: int, systems: int) -> str:
     return f"plummer_n{n}_eps1e-3_theta0.5_force_plus_full_vjp_{systems}_systems_per_step"
 
 
-EXTRAS = ("octree8_plain", "forest", "sharded_single_system", "winding_number", "winding_number_mesh",
-          "treepm_short_range", "stochastic_octree8", "direct_sum", "trajectory")
+EXTRAS = ("octree8_plain", "opening_sweep", "forest", "sharded_single_system", "winding_number",
+          "winding_number_mesh", "treepm_short_range", "stochastic_octree8", "direct_sum", "trajectory")
 
 
 def parse():
@@ -274,6 +274,30 @@ def fp64_direct_subset(points_d, masses_d, idx, eps):
         r2 = (d * d).sum(-1)
         c = -m[None, :] * (r2 + eps * eps + 1e-12) ** -1.5
         out[a:a + 64] = (c[..., None] * d).sum(1)
+    return out
+
+
+def opening_sweep_measurement(B, torch, P0, M0, W0, idx, ref, flush):
+    """How much of the walk the accuracy bar needs: one 2^20 system's fused
+    force + full adjoint (the step's kernel, same settings) at openings beta
+    = 1/theta from the configuration's 2 down to 1.25, with the force's
+    rel-L2 against the FP64 direct sum on the accuracy subset. The headline
+    stays at theta = 0.5; this only states the headroom."""
+    tree = B.NativeTree().build(P0, M0)
+    out = dict(what="build once; force + full adjoint per beta (CUDA events, L2 flushed)", points=[])
+    for beta in (2.0, 1.75, 1.5, 1.25):
+        f, _, _ = tree.force_vjp(W0, beta=beta, softening=EPS)
+        torch.cuda.synchronize()
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tree.force_vjp(W0, beta=beta, softening=EPS)
+        e1.record()
+        torch.cuda.synchronize()
+        rel = float(torch.linalg.norm(f[idx].double() - ref) / torch.linalg.norm(ref))
+        out["points"].append(dict(beta=beta, theta=1.0 / beta, force_vjp_ms=e0.elapsed_time(e1),
+                                  rel_l2_vs_fp64_direct=rel))
+    tree.release()
     return out
 
 
@@ -1028,6 +1052,8 @@ def run_ours(args):
         want = set(args.extra) if args.extra else set(EXTRAS)
         if world == 1 and "octree8_plain" in want:
             extras["octree8_plain"] = octree8_plain_measurement(B, torch, P0, M0, W0, idx, ref, flush)
+        if world == 1 and "opening_sweep" in want:
+            extras["opening_sweep"] = opening_sweep_measurement(B, torch, P0, M0, W0, idx, ref, flush)
         if "forest" in want:  # every rank takes part (a collective-free shard of the systems)
             extras["forest"] = forest_measurement(B, torch, dev, rank, world, flush)
         if world > 1 and "sharded_single_system" in want:
