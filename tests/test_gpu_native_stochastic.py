@@ -187,3 +187,24 @@ def test_forest_and_tiny_systems_match_oracle(cuda):
                             want_force=False)
     assert rel_l2(gx.cpu().numpy(), cx.cpu().numpy()) < 1e-5
     assert rel_l2(gm.cpu().numpy(), cm.cpu().numpy()) < 1e-5
+
+
+def test_empty_and_coincident_points(cuda):
+    """An empty tree gives empty outputs; a cloud with 600 copies of three
+    points (nodes whose particles coincide have r_g = 0 and weight 0, and
+    leaves beyond the leaf size) still equals the oracle's restatement."""
+    t = B.NativeTree().build(np.zeros((0, 3), np.float32), np.zeros(0, np.float32))
+    assert t.stochastic_force().shape == (0, 3)
+    f, gx, gm = t.stochastic_force_vjp(np.zeros((0, 3), np.float32))
+    assert f.shape == (0, 3) and gx.shape == (0, 3) and gm.shape == (0,)
+    p, _ = W.uniform_cube(2000, seed=31)
+    p = np.concatenate([p, np.repeat(p[:3], 200, axis=0)]).astype(np.float32)
+    m = np.full(p.shape[0], 1.0 / p.shape[0], np.float32)
+    t = B.NativeTree().build(p, m, leaf_size=16)
+    _, perm, rec = t.export()
+    sp = np.ascontiguousarray(np.concatenate([p[perm], m[perm, None]], axis=1), np.float32)
+    got = t.stochastic_force(beta_coarse=1.0, samples=32, seed=4).cpu().numpy()
+    want, _, _ = O.native_stochastic(sp, perm, rec, group_size=B.native_group_size(), beta_coarse=1.0, samples=32,
+                                     seed=4)
+    assert np.isfinite(got).all()
+    assert rel_l2(got, want) < 3e-5
