@@ -215,8 +215,8 @@ void orc_direct_force_soft_vjp(const float* pts, const float* masses, int64_t n,
  *   dL/dx_k = sum_j J(x_k - x_j) (m_j w_k - m_k w_j)       (J = d phi/dr, symmetric, even)
  *   dL/dm_k = sum_i w_i . phi(x_i - x_k)
  * A subset of k can be requested (idx); out_dx is (nk, 3), out_dm is (nk,).
- * This is the exact adjoint the north star's "gradient w.r.t. positions and
- * masses" asks for; the reference itself only has the query-side term.
+ * This is the exact gradient with respect to positions and masses; the
+ * reference itself only has the query-side term.
  */
 void orc_direct_full_adjoint(const float* pts, const float* masses, int64_t n,
                              const float* w, double eps, double cutoff, const int64_t* idx,

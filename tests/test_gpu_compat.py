@@ -7,7 +7,8 @@ compares it with
   * the CPU oracle (oracle/sbh_oracle.c), which evaluates the same algorithm
     with float decisions and double sums.
 Tolerances: integer/byte fields bit-exact; float sums within 1e-5 relative
-L2 (the north star's classic-BH tolerance) unless stated otherwise.
+L2 (the classic-BH parity tolerance against the reference's kernels) unless
+stated otherwise.
 """
 import numpy as np
 import pytest
