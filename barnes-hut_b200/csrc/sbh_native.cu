@@ -767,6 +767,45 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
+// Bulk copies (the TMA unit's non-tensor cp.async.bulk, no multicast) into
+// shared memory, completed on an mbarrier. The waits are bounded: a copy
+// that never completes makes the wait return false, and the caller flags
+// the workspace's status word and stops instead of spinning.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// Issued by one lane: orders the warp's earlier reads of the destination
+// (generic proxy) before the copy's writes (async proxy), arms the barrier
+// for `bytes` and starts the copy. dst, src and bytes are multiples of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  for (int i = 0; i < (1 << 22); i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Starts staging nodes [base, min(base + kTile, end)) into the warp's tile.
 // Every lane calls it (warp-uniform) after it has read what it needs from
 // the previous tile; stage_wait() completes the copy for all lanes.
@@ -1308,6 +1347,8 @@ int sbh_native_build(cudaStream_t stream, const float* points, const float* mass
   if (leaf_size < 1 || leaf_size > 32) return invalid("leaf_size must be in [1, 32]");
   if (n > 0 && (!points || !masses)) return invalid("points and masses must be non-null");
   if (!workspace) return fail(SBH_ERR_WORKSPACE, "workspace is null");
+  // the node records are read with 16-byte vector loads and bulk copies
+  if (reinterpret_cast<uintptr_t>(workspace) % 16 != 0) return invalid("workspace must be 16-byte aligned");
   size_t need = sbh_native_workspace_bytes(n, num_systems, leaf_size, normals != nullptr, with_adjoint);
   if (workspace_bytes < need)
     return fail(SBH_ERR_WORKSPACE, "workspace too small: need " + std::to_string(need) + " bytes");
@@ -1697,8 +1738,11 @@ int sbh_native_stochastic_force(cudaStream_t stream, const sbh_native_params* pa
   if (!force_out) return invalid("force_out must be non-null");
   if (partial_range(h)) return invalid("the stochastic estimator needs the full target range");
   const WalkParams wp = walk_params(params);
-  cudaError_t e = launch_walk(stream, L.work, h.n + h.nseg, stoch_group_kernel, tree_view(L), self_targets(L, h),
-                              beta_coarse, params->beta, wp.eps2, samples, seed, force_out);
+  uint32_t* status = static_cast<uint32_t*>(workspace);  // SBH_DEV_ITER_LIMIT if a tile copy never completes
+  cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
+  if (e == cudaSuccess)
+    e = launch_walk(stream, L.work, h.n + h.nseg, stoch_group_kernel, tree_view(L), self_targets(L, h), beta_coarse,
+                    params->beta, wp.eps2, samples, seed, force_out, status);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   remember_walk(workspace, 0, nullptr);
   return check_launch("sbh_native_stochastic_force");
@@ -1732,8 +1776,12 @@ int sbh_native_stochastic_force_vjp(cudaStream_t stream, const sbh_native_params
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   zero_node_adj_kernel<<<gs(L.cap * kNodeAdj), 256, 0, stream>>>(L.node_adj, L.meta);
   const WalkParams wp = walk_params(params);
-  e = launch_walk(stream, L.work, h.n + h.nseg, stoch_adjoint_kernel, tree_view(L), self_targets(L, h), beta_coarse,
-                  params->beta, wp.eps2, samples, seed, cotangent, L.gq, L.node_adj, L.part_adj);
+  uint32_t* status = static_cast<uint32_t*>(workspace);
+  if (!force_out) e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);  // else the forward cleared it
+  if (e == cudaSuccess)
+    e = launch_walk(stream, L.work, h.n + h.nseg, stoch_adjoint_kernel, tree_view(L), self_targets(L, h),
+                    beta_coarse, params->beta, wp.eps2, samples, seed, cotangent, L.gq, L.node_adj, L.part_adj,
+                    status);
   if (e != cudaSuccess) return fail(SBH_ERR_CUDA, cudaGetErrorString(e));
   remember_walk(workspace, 0, nullptr);
   return sbh_native_adjoint_finalize(stream, grad_points, grad_masses, workspace, workspace_bytes);
