@@ -424,7 +424,8 @@ size_t sbh_native_workspace_bytes(int64_t n, int num_systems, int leaf_size, int
  * (n x 3, optional: winding number). system_offsets: device int64 array of
  * num_systems + 1 offsets into the concatenated inputs (NULL for one system).
  * leaf_size in [1, 32]. with_adjoint reserves the scratch of
- * sbh_native_force_vjp. Later calls on the same workspace evaluate this tree. */
+ * sbh_native_force_vjp. Later calls on the same workspace evaluate this tree.
+ * The workspace must be 16-byte aligned (cudaMalloc's is). */
 int sbh_native_build(cudaStream_t stream, const float* points, const float* masses,
                      const float* normals, int64_t n, const int64_t* system_offsets,
                      int num_systems, int leaf_size, int with_adjoint, void* workspace,
