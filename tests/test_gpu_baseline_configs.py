@@ -21,6 +21,12 @@
   gradient; and the query-side term against the FP64 direct query-side VJP,
   beside the reference's octree8 VJP on the same targets.
 
+* Config 2b's sources: the winding number of 262,144 oriented points on the
+  ellipsoid (1, 0.7, 0.5) on the native tree, at 65,536 of the
+  configuration's uniform queries: value and full adjoint against the
+  oracle's float64 evaluation of the same plan, value against the FP64
+  direct sum.
+
 Each test prints the figures it checks (pytest -s shows them).
 """
 import numpy as np
@@ -216,3 +222,26 @@ def test_config3_gradient_vs_fp64_finite_differences_at_2e20(cuda, plummer_1m):
     assert e_x1 < 1e-2
     assert a_x < 1e-3 and a_m < 3e-3
     assert e_q < 1e-4
+
+
+def test_config2b_winding_number_parity_at_size(cuda):
+    pts, nrm, wgt = W.ellipsoid_surface(262144, seed=2)
+    q = W.uniform_box_queries(1048576, seed=3)
+    q = np.ascontiguousarray(q[np.random.default_rng(4).choice(q.shape[0], 65536, replace=False)])
+    u = np.random.default_rng(5).normal(size=q.shape[0]).astype(np.float32)
+    t = B.NativeTree().build(pts, wgt, normals=nrm, leaf_size=16, with_adjoint=True)
+    w, gq, gp, gn, gm = t.winding_number_vjp(q, u, beta=2.0, want_value=True)
+    T = O.NativeTree(pts, wgt, leaf_size=16)
+    T.wn_plan(q, 2.0)
+    want_w = T.wn_eval(nrm)
+    dq, dp, dn, dm = T.wn_adjoint(nrm, u)
+    errs = dict(value=rel_l2(w.cpu().numpy(), want_w), dq=rel_l2(gq.cpu().numpy(), dq),
+                dp=rel_l2(gp.cpu().numpy(), dp), dn=rel_l2(gn.cpu().numpy(), dn), dm=rel_l2(gm.cpu().numpy(), dm))
+    sub = np.arange(0, q.shape[0], 64)
+    direct = O.direct_winding_number(pts, nrm, wgt, q[sub])
+    errs["vs_fp64_direct"] = rel_l2(w.cpu().numpy()[sub], direct)
+    print("config 2b parity at 262,144 sources / 65,536 queries:", errs)
+    assert errs["value"] < 1e-5
+    for k in ("dq", "dp", "dn", "dm"):
+        assert errs[k] < 1e-4
+    assert errs["vs_fp64_direct"] < 5e-3
