@@ -10,7 +10,10 @@
     quantisation puts in another cell than the IEEE oracle is reported;
   - the softened force and its VJP at 4,096 of the particles against the
     reference's kernels (src/sbh_ffi.cu:1995-2042, 2092-2144) on the same
-    buffers, within 1e-5 relative L2.
+    buffers, within 1e-5 relative L2;
+  - the stochastic estimator and its VJP (32 paths per subdomain, fixed
+    seed, src/sbh_ffi.cu:2146-2442) at the same queries: every row within
+    1e-4 of the reference's.
 * Config 1: N = 10,000 uniform in the unit cube, eps = 1e-3, theta = 0.5,
   leaf size 8: the native tree and the octree8 path against the FP64 direct
   sum, the reference's CPU Tree3D<8,1> beside them.
@@ -143,6 +146,29 @@ def test_octree8_depth7_build_and_traversals_at_2e20_match_reference(cuda, plumm
     print(f"[octree8 2^20 depth 7, 4096 queries] force vs reference kernel {ef:.2e}, VJP {ev:.2e}")
     assert ef < 1e-5
     assert ev < 1e-5
+
+    # the stochastic estimator (MLPCV, 32 paths per subdomain: config 2a's "32 samples") and its VJP at
+    # the same queries, same seed: the same curand streams, so every row on the reference's paths
+    sf = torch.zeros((nq, 3), device=cuda)
+    O.refgpu_check(L.ref_stochastic_bh_force_octree8(_S(), 1, lp, lb_, np_, nb, Q.data_ptr(), nq, sf.data_ptr(), 32, 7,
+                                                     BETA, EPS, cut, 0, 4.0, 0, 1.0, 256))
+    sv = torch.zeros((nq, 3), device=cuda)
+    O.refgpu_check(L.ref_stochastic_bh_force_octree8_vjp(_S(), 1, lp, lb_, np_, nb, Q.data_ptr(), nq, C.data_ptr(),
+                                                         sv.data_ptr(), 32, 7, BETA, EPS, cut, 0, 4.0, 0, 1.0, 256))
+    skw = dict(samples_per_subdomain=32, seed=7, beta=BETA, softening_scale=EPS, cutoff_scale=cut,
+               prune_enabled=False, check_status=True)
+    gf = B.softened_stochastic_barnes_hut_force_octree8(leaf, node, q, **skw)
+    gv = B.softened_stochastic_barnes_hut_force_octree8_vjp(leaf, node, q, cot, **skw)
+    torch.cuda.synchronize()
+    for tag, got, want in (("force", gf, sf), ("VJP", gv, sv)):
+        g_, w_ = got.cpu().numpy(), want.cpu().numpy()
+        # rows relative to their own norm, floored at 1% of the rows' RMS norm (a row that nearly
+        # cancels would otherwise inflate its FP32 rounding; a different path is an O(1) error)
+        nrm_ = np.linalg.norm(w_.astype(np.float64), axis=1)
+        row = np.linalg.norm(g_ - w_, axis=1) / np.maximum(nrm_, 1e-2 * np.sqrt(np.mean(nrm_ ** 2)))
+        print(f"[stochastic octree8 2^20 depth 7, 4096 queries, 32 paths] {tag}: worst row {row.max():.2e}, "
+              f"rel-L2 {rel_l2(g_, w_):.2e}")
+        assert row.max() < 1e-4
 
 
 def test_config1_uniform_10k_accuracy_vs_fp64_direct(cuda):
