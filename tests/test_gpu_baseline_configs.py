@@ -24,6 +24,10 @@
   gradient; and the query-side term against the FP64 direct query-side VJP,
   beside the reference's octree8 VJP on the same targets.
 
+* Config 4 at its size (256 Plummer systems, N log-uniform in [1e3, 2e5],
+  11.6M particles): the forest's force walk in one launch equals each
+  system walked on its own; the fused force + adjoint of the forest equals
+  the separate systems' for the largest and the smallest system.
 * Config 2b's sources: the winding number of 262,144 oriented points on the
   ellipsoid (1, 0.7, 0.5) on the native tree, at 65,536 of the
   configuration's uniform queries: value and full adjoint against the
@@ -271,3 +275,36 @@ def test_config2b_winding_number_parity_at_size(cuda):
     for k in ("dq", "dp", "dn", "dm"):
         assert errs[k] < 1e-4
     assert errs["vs_fp64_direct"] < 5e-3
+
+
+def test_config4_forest_equals_separate_systems_at_size(cuda):
+    systems, sizes = W.forest(256, 1000, 200000, seed=0)
+    pts = torch.tensor(np.concatenate([s_[0] for s_ in systems]), device=cuda)
+    ms = torch.tensor(np.concatenate([s_[1] for s_ in systems]), device=cuda)
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    w = torch.randn(pts.shape, device=cuda, generator=torch.Generator(device=cuda).manual_seed(6))
+    forest = B.NativeTree().build(pts, ms, system_offsets=offs, leaf_size=16)
+    f_all = forest.force(beta=BETA, softening=EPS)
+    _, gx_all, gm_all = forest.force_vjp(w, beta=BETA, softening=EPS, want_force=False)
+    tree = B.NativeTree()
+    worst = 0.0
+    for i in range(len(systems)):
+        a, b = int(offs[i]), int(offs[i + 1])
+        tree.build(pts[a:b], ms[a:b], leaf_size=16)
+        fi = tree.force(beta=BETA, softening=EPS)
+        # same tree and groups; node moments differ in the last bits because the forest's FP64
+        # prefix sums also carry the earlier systems
+        worst = max(worst, rel_l2(f_all[a:b].cpu().numpy(), fi.cpu().numpy()))
+    checked = []
+    for i in (int(np.argmax(sizes)), int(np.argmin(sizes))):
+        a, b = int(offs[i]), int(offs[i + 1])
+        tree.build(pts[a:b], ms[a:b], leaf_size=16)
+        _, gxi, gmi = tree.force_vjp(w[a:b], beta=BETA, softening=EPS, want_force=False)
+        checked.append((rel_l2(gx_all[a:b].cpu().numpy(), gxi.cpu().numpy()),
+                        rel_l2(gm_all[a:b].cpu().numpy(), gmi.cpu().numpy())))
+    print(f"config 4 forest ({int(offs[-1])} particles, 256 systems): worst system force {worst:.2e}; "
+          f"adjoint (positions, masses) largest {checked[0][0]:.2e} {checked[0][1]:.2e}, "
+          f"smallest {checked[1][0]:.2e} {checked[1][1]:.2e}")
+    assert worst < 1e-6
+    for gx_err, gm_err in checked:
+        assert gx_err < 1e-5 and gm_err < 1e-5
