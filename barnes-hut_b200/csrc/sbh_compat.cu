@@ -503,17 +503,25 @@ __global__ void __launch_bounds__(256)
 // some lane opens it, with that set of lanes. A lane's nodes thus come off
 // the stack in the order of its own per-thread DFS, so it adds the same terms
 // in the same order and every output row equals o8_bh_kernel's bit for bit;
-// node records and leaf particles are read once per warp instead of once per
-// thread, and the lanes at a leaf loop over its particles together.
+// node records are read once per warp instead of once per thread. At a leaf
+// the warp copies the particles in chunks of 32 (one coalesced load per lane)
+// into a per-warp buffer in shared memory, and the summing lanes read them
+// from there in the leaf's order.
 // The block holds blockDim.x / 32 warps (the caller's `threads`, the
-// reference's launch parameter, in whole warps) and each warp a stack of
-// STACK entries in dynamic shared memory: 64 for a dense octree8 of depth
-// <= 9 (a DFS of depth d holds at most 7 d + 1 entries), otherwise the
-// reference's 128.
+// reference's launch parameter, in whole warps). Its dynamic shared memory
+// holds each warp's leaf buffer (32 x 16 B), then each warp's stack of STACK
+// entries: 64 for a dense octree8 of depth <= 9 (a DFS of depth d holds at
+// most 7 d + 1 entries), otherwise the reference's 128.
 struct O8StackEntry {
   int node;
   uint32_t lanes;
 };
+
+constexpr int kO8LeafChunk = 32;
+
+__host__ __device__ constexpr size_t o8_warp_smem(int warps, int stack) {
+  return static_cast<size_t>(warps) * (kO8LeafChunk * sizeof(float4) + stack * sizeof(O8StackEntry));
+}
 
 template <int KERNEL, int STACK>
 __global__ void __launch_bounds__(1024)
@@ -521,9 +529,10 @@ __global__ void __launch_bounds__(1024)
                       const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq, float beta,
                       Soft s, int prune_on, float r_cut_sq, Periodic per, float* __restrict__ out, uint32_t* status,
                       O8Bounds bd, const uint32_t* __restrict__ order) {
-  extern __shared__ O8StackEntry o8_stacks[];
+  extern __shared__ float4 o8_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  O8StackEntry* stack = o8_stacks + warp * STACK;
+  float4* chunk = o8_smem + warp * kO8LeafChunk;
+  O8StackEntry* stack = reinterpret_cast<O8StackEntry*>(o8_smem + (blockDim.x >> 5) * kO8LeafChunk) + warp * STACK;
   const int64_t ti = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp) * 32 + lane;
   const bool valid = ti < nq;
   const uint32_t live = __ballot_sync(0xffffffffu, valid);
@@ -560,14 +569,30 @@ __global__ void __launch_bounds__(1024)
     if (KERNEL != O8_GRAV_GRAD && KERNEL != O8_GRAV_GRAD_VJP)
       act = act && !o8_prune(nd, qx, qy, qz, prune_on, r_cut_sq, per);
     const bool far = act && o8_far(nd, qx, qy, qz, beta, per);
-    if (far) {
-      if (nd.is_leaf) {
-        o8_leaf_sum<KERNEL>(leaf, nd.start, o8_leaf_end(nd.start, nd.end, bd, status), qx, qy, qz, gx, gy, gz, s,
-                            per, ax, ay, az);
-      } else {
-        o8_pair<KERNEL>(qx, qy, qz, nd.contrib.pos[0], nd.contrib.pos[1], nd.contrib.pos[2], nd.contrib.mass, gx,
-                        gy, gz, s, per, ax, ay, az);
+    if (nd.is_leaf) {  // warp-uniform: every lane reads the same node
+      if (__ballot_sync(0xffffffffu, far)) {
+        const uint32_t start = nd.start, end = o8_leaf_end(start, nd.end, bd, status);
+        for (uint32_t c = start; c < end; c += kO8LeafChunk) {
+          const uint32_t i = c + lane;
+          if (i < end) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(leaf + i));
+            chunk[lane] = make_float4(a.x, a.y, a.z, __ldg(&leaf[i].mass));
+          }
+          __syncwarp();
+          const int cnt = end - c < kO8LeafChunk ? static_cast<int>(end - c) : kO8LeafChunk;
+          if (far) {
+#pragma unroll 4
+            for (int j = 0; j < cnt; j++) {
+              const float4 p = chunk[j];
+              o8_pair<KERNEL>(qx, qy, qz, p.x, p.y, p.z, p.w, gx, gy, gz, s, per, ax, ay, az);
+            }
+          }
+          __syncwarp();  // the chunk is read before the next one overwrites it
+        }
       }
+    } else if (far) {
+      o8_pair<KERNEL>(qx, qy, qz, nd.contrib.pos[0], nd.contrib.pos[1], nd.contrib.pos[2], nd.contrib.mass, gx, gy,
+                      gz, s, per, ax, ay, az);
     }
     const uint32_t open = __ballot_sync(0xffffffffu, act && !far);
     if (open) {
@@ -1042,11 +1067,11 @@ static int o8_launch_bh(int kernel, cudaStream_t stream, const void* leaf, size_
     const unsigned tw = 32u * static_cast<unsigned>(warps);
     const unsigned gw = grid_for(nq, static_cast<int>(tw));
     if (o8_small_stack(bd.num_nodes)) {
-      const size_t sm = static_cast<size_t>(warps) * 64 * sizeof(O8StackEntry);
+      const size_t sm = o8_warp_smem(warps, 64);
       o8_launch_warp<64>(kernel, gw, tw, sm, stream, L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per, out,
                          status, bd, order);
     } else {
-      const size_t sm = static_cast<size_t>(warps) * kO8Stack * sizeof(O8StackEntry);
+      const size_t sm = o8_warp_smem(warps, kO8Stack);
       o8_launch_warp<kO8Stack>(kernel, gw, tw, sm, stream, L, N, queries, cot, nq, beta, s, prune_on, r_cut_sq, per,
                                out, status, bd, order);
     }
