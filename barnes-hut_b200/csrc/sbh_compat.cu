@@ -373,10 +373,162 @@ __device__ __forceinline__ bool o8_prune(const OctreeNode8& nd, float qx, float 
 
 enum O8Kernel { O8_GRAV_GRAD = 0, O8_SOFT = 1, O8_SOFT_VJP = 2, O8_GRAV_GRAD_VJP = 3 };
 
+// Softened pair terms in one fixed order of single-rounding operations
+// (flush-to-zero, as the rest of this file under fast math), written once for
+// a scalar pair and once for two pairs packed into FFMA2 / FADD2 / FMUL2
+// (sm_100 f32x2). Both forms round every component the same way, so the
+// traversal that sums a leaf two particles at a time and the one that sums
+// it one at a time add bit-identical terms. The accumulation into the
+// query's sum stays scalar and in the leaf's order.
+struct F2 {
+  unsigned long long v;
+};
+
+__device__ __forceinline__ F2 f2_pack(float a, float b) {
+  F2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(F2 x, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v));
+}
+__device__ __forceinline__ float o8_add(float a, float b) {
+  float d;
+  asm("add.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
+}
+__device__ __forceinline__ float o8_sub(float a, float b) {
+  float d;
+  asm("sub.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
+}
+__device__ __forceinline__ float o8_mul(float a, float b) {
+  float d;
+  asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
+}
+__device__ __forceinline__ float o8_fma(float a, float b, float c) {
+  float d;
+  asm("fma.rn.ftz.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ F2 o8_add(F2 a, F2 b) {
+  F2 d;
+  asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ F2 o8_sub(F2 a, F2 b) {
+  F2 d;
+  asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ F2 o8_mul(F2 a, F2 b) {
+  F2 d;
+  asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+  return d;
+}
+__device__ __forceinline__ F2 o8_fma(F2 a, F2 b, F2 c) {
+  F2 d;
+  asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return d;
+}
+__device__ __forceinline__ float o8_splat_like(float, float s) { return s; }
+__device__ __forceinline__ F2 o8_splat_like(F2, float s) { return f2_pack(s, s); }
+__device__ __forceinline__ float o8_rsqrt(float a) { return rsqrtf(a); }
+__device__ __forceinline__ F2 o8_rsqrt(F2 a) {
+  float x, y;
+  f2_unpack(a, x, y);
+  return f2_pack(rsqrtf(x), rsqrtf(y));
+}
+
+// Shared first steps of the softened pair: r^2 = (rx rx + ry ry) + rz rz as
+// two fused steps, h = (r^2 + eps^2) + 1e-12 and 1 / sqrt(h).
+template <typename V>
+__device__ __forceinline__ void o8_soft_head(V rx, V ry, V rz, V eps2, V& r2, V& ir) {
+  r2 = o8_fma(rz, rz, o8_fma(ry, ry, o8_mul(rx, rx)));
+  ir = o8_rsqrt(o8_add(o8_add(r2, eps2), o8_splat_like(eps2, 1e-12f)));
+}
+
+// Whether a pair lies in the att = 1 range (no cutoff, or r^2 + 1e-12 under
+// the unity radius): then its terms skip the erfc attenuation.
+__device__ __forceinline__ bool o8_unity(float r2, const Soft& s) {
+  return !(s.cutoff > 0.0f && o8_add(r2, 1e-12f) >= s.unity_r2);
+}
+
+// erfc attenuation of one pair outside the att = 1 range (soft_coeff's and
+// soft_vjp_accum's slow path): att, and the VJP's radial term cc.
+__device__ __forceinline__ void o8_soft_att(float r2, float ir3, const Soft& s, float& att, float& cc) {
+  float dist = sqrtf(o8_add(r2, 1e-12f));
+  float u = dist / (2.0f * s.cutoff);
+  float e = 1.0f;
+  att = 1.0f;
+  if (u >= kAttUnityU) {
+    e = expf(-(u * u));
+    att = erfcf(u) + (2.0f / 1.772453850905516f) * u * e;
+  }
+  cc = ir3 * dist * e / (2.0f * 1.772453850905516f * s.cutoff * s.cutoff * s.cutoff);
+}
+
+// Softened force of one pair, nm = -m: acc += c r with c = nm / h^{3/2}
+// (times att outside the att = 1 range).
+__device__ __forceinline__ void o8_soft_force(float rx, float ry, float rz, float nm, float eps2, const Soft& s,
+                                              float& ax, float& ay, float& az) {
+  float r2, ir;
+  o8_soft_head(rx, ry, rz, eps2, r2, ir);
+  const float ir3 = o8_mul(o8_mul(ir, ir), ir);
+  float c;
+  if (o8_unity(r2, s)) {
+    c = o8_mul(nm, ir3);
+  } else {
+    float att, cc;
+    o8_soft_att(r2, ir3, s, att, cc);
+    c = o8_mul(o8_mul(nm, att), ir3);
+  }
+  ax = o8_fma(c, rx, ax);
+  ay = o8_fma(c, ry, ay);
+  az = o8_fma(c, rz, az);
+}
+
+// Query-side VJP of one softened pair, nm = -m: acc += nm (lin g - rad r),
+// with lin = att / h^{3/2} and rad = (r . g) (3 att / h^{5/2} + cc); the
+// negated radial term is formed directly (rounding is symmetric in sign).
+__device__ __forceinline__ void o8_soft_vjp(float rx, float ry, float rz, float nm, float gx, float gy, float gz,
+                                            float eps2, const Soft& s, float& ax, float& ay, float& az) {
+  float r2, ir;
+  o8_soft_head(rx, ry, rz, eps2, r2, ir);
+  const float ir3 = o8_mul(o8_mul(ir, ir), ir);
+  const float ir5 = o8_mul(o8_mul(ir3, ir), ir);
+  const float rg = o8_fma(rz, gz, o8_fma(ry, gy, o8_mul(rx, gx)));
+  float lin, nrad;
+  if (o8_unity(r2, s)) {
+    lin = ir3;
+    nrad = o8_mul(rg, o8_mul(-3.0f, ir5));
+  } else {
+    float att, cc;
+    o8_soft_att(r2, ir3, s, att, cc);
+    lin = o8_mul(att, ir3);
+    nrad = o8_mul(rg, o8_sub(o8_mul(o8_mul(-3.0f, att), ir5), cc));
+  }
+  ax = o8_fma(nm, o8_fma(nrad, rx, o8_mul(lin, gx)), ax);
+  ay = o8_fma(nm, o8_fma(nrad, ry, o8_mul(lin, gy)), ay);
+  az = o8_fma(nm, o8_fma(nrad, rz, o8_mul(lin, gz)), az);
+}
+
 template <int KERNEL>
 __device__ __forceinline__ void o8_pair(float qx, float qy, float qz, float px, float py, float pz, float m,
                                         float gx, float gy, float gz, const Soft& s, const Periodic& per,
                                         float& ax, float& ay, float& az) {
+  if (KERNEL == O8_SOFT || KERNEL == O8_SOFT_VJP) {
+    const float rx = min_image_floor(o8_sub(qx, px), per);
+    const float ry = min_image_floor(o8_sub(qy, py), per);
+    const float rz = min_image_floor(o8_sub(qz, pz), per);
+    const float eps2 = o8_mul(s.eps, s.eps);
+    if (KERNEL == O8_SOFT)
+      o8_soft_force(rx, ry, rz, -m, eps2, s, ax, ay, az);
+    else
+      o8_soft_vjp(rx, ry, rz, -m, gx, gy, gz, eps2, s, ax, ay, az);
+    return;
+  }
   float rx = min_image_floor(qx - px, per);
   float ry = min_image_floor(qy - py, per);
   float rz = min_image_floor(qz - pz, per);
@@ -385,16 +537,136 @@ __device__ __forceinline__ void o8_pair(float qx, float qy, float qz, float px, 
     ax += c * rx;
     ay += c * ry;
     az += c * rz;
-  } else if (KERNEL == O8_SOFT) {
-    float c = soft_coeff(rx * rx + ry * ry + rz * rz, m, s);
-    ax += c * rx;
-    ay += c * ry;
-    az += c * rz;
-  } else if (KERNEL == O8_SOFT_VJP) {
-    soft_vjp_accum(rx, ry, rz, m, gx, gy, gz, s, ax, ay, az);
   } else {
     grav_grad_vjp_accum(rx, ry, rz, m, gx, gy, gz, ax, ay, az);
   }
+}
+
+// Two softened pairs without a periodic box, particles a then b: positions
+// X, Y, Z and negated masses NM packed (a, b). The pair terms are packed, and
+// each pair adds into the sums in order. With CHECK, a pair outside the
+// att = 1 range sends both through the scalar form; without it the caller
+// has shown that both pairs lie inside that range.
+template <int KERNEL, bool CHECK>
+__device__ __forceinline__ void o8_pair2(const F2& QX, const F2& QY, const F2& QZ, F2 X, F2 Y, F2 Z, F2 NM,
+                                         const F2& GX, const F2& GY, const F2& GZ, float eps2, const Soft& s,
+                                         float& ax, float& ay, float& az) {
+  const F2 rx = o8_sub(QX, X), ry = o8_sub(QY, Y), rz = o8_sub(QZ, Z);
+  F2 r2, ir;
+  o8_soft_head(rx, ry, rz, f2_pack(eps2, eps2), r2, ir);
+  float xa, xb, ya, yb, za, zb, ma, mb;
+  f2_unpack(rx, xa, xb);
+  f2_unpack(ry, ya, yb);
+  f2_unpack(rz, za, zb);
+  f2_unpack(NM, ma, mb);
+  if (CHECK) {
+    float r2a, r2b;
+    f2_unpack(r2, r2a, r2b);
+    if (!(o8_unity(r2a, s) && o8_unity(r2b, s))) {
+      float gx, gy, gz, dummy;
+      f2_unpack(GX, gx, dummy);
+      f2_unpack(GY, gy, dummy);
+      f2_unpack(GZ, gz, dummy);
+      if (KERNEL == O8_SOFT) {
+        o8_soft_force(xa, ya, za, ma, eps2, s, ax, ay, az);
+        o8_soft_force(xb, yb, zb, mb, eps2, s, ax, ay, az);
+      } else {
+        o8_soft_vjp(xa, ya, za, ma, gx, gy, gz, eps2, s, ax, ay, az);
+        o8_soft_vjp(xb, yb, zb, mb, gx, gy, gz, eps2, s, ax, ay, az);
+      }
+      return;
+    }
+  }
+  const F2 ir3 = o8_mul(o8_mul(ir, ir), ir);
+  if (KERNEL == O8_SOFT) {
+    float ca, cb;
+    f2_unpack(o8_mul(NM, ir3), ca, cb);
+    ax = o8_fma(ca, xa, ax);
+    ay = o8_fma(ca, ya, ay);
+    az = o8_fma(ca, za, az);
+    ax = o8_fma(cb, xb, ax);
+    ay = o8_fma(cb, yb, ay);
+    az = o8_fma(cb, zb, az);
+  } else {
+    const F2 ir5 = o8_mul(o8_mul(ir3, ir), ir);
+    const F2 rg = o8_fma(rz, GZ, o8_fma(ry, GY, o8_mul(rx, GX)));
+    const F2 nrad = o8_mul(rg, o8_mul(f2_pack(-3.0f, -3.0f), ir5));
+    float ta, tb;
+    f2_unpack(o8_fma(nrad, rx, o8_mul(ir3, GX)), ta, tb);
+    ax = o8_fma(ma, ta, ax);
+    ax = o8_fma(mb, tb, ax);
+    f2_unpack(o8_fma(nrad, ry, o8_mul(ir3, GY)), ta, tb);
+    ay = o8_fma(ma, ta, ay);
+    ay = o8_fma(mb, tb, ay);
+    f2_unpack(o8_fma(nrad, rz, o8_mul(ir3, GZ)), ta, tb);
+    az = o8_fma(ma, ta, az);
+    az = o8_fma(mb, tb, az);
+  }
+}
+
+// One warp's staging buffer for a leaf's particles: 32 positions and
+// negated masses, component by component, so that two or four consecutive
+// particles load into packed register pairs with one shared-memory read.
+constexpr int kO8LeafChunk = 32;
+
+struct __align__(16) O8Chunk {
+  float x[kO8LeafChunk], y[kO8LeafChunk], z[kO8LeafChunk], nm[kO8LeafChunk];
+};
+
+__device__ __forceinline__ F2 o8_ld2(const float* p) {
+  F2 r;
+  r.v = *reinterpret_cast<const unsigned long long*>(p);
+  return r;
+}
+
+// The softened terms of cnt staged particles for one query, in order.
+template <int KERNEL, bool CHECK>
+__device__ __forceinline__ void o8_chunk_sum(const O8Chunk& ch, int cnt, float qx, float qy, float qz, float gx,
+                                             float gy, float gz, const Soft& s, float& ax, float& ay, float& az) {
+  const F2 QX = f2_pack(qx, qx), QY = f2_pack(qy, qy), QZ = f2_pack(qz, qz);
+  const F2 GX = f2_pack(gx, gx), GY = f2_pack(gy, gy), GZ = f2_pack(gz, gz);
+  const float eps2 = o8_mul(s.eps, s.eps);
+  int j = 0;
+  for (; j + 3 < cnt; j += 4) {
+    const ulonglong2 X = *reinterpret_cast<const ulonglong2*>(&ch.x[j]);
+    const ulonglong2 Y = *reinterpret_cast<const ulonglong2*>(&ch.y[j]);
+    const ulonglong2 Z = *reinterpret_cast<const ulonglong2*>(&ch.z[j]);
+    const ulonglong2 M = *reinterpret_cast<const ulonglong2*>(&ch.nm[j]);
+    o8_pair2<KERNEL, CHECK>(QX, QY, QZ, F2{X.x}, F2{Y.x}, F2{Z.x}, F2{M.x}, GX, GY, GZ, eps2, s, ax, ay, az);
+    o8_pair2<KERNEL, CHECK>(QX, QY, QZ, F2{X.y}, F2{Y.y}, F2{Z.y}, F2{M.y}, GX, GY, GZ, eps2, s, ax, ay, az);
+  }
+  if (j + 1 < cnt) {
+    o8_pair2<KERNEL, CHECK>(QX, QY, QZ, o8_ld2(&ch.x[j]), o8_ld2(&ch.y[j]), o8_ld2(&ch.z[j]), o8_ld2(&ch.nm[j]),
+                            GX, GY, GZ, eps2, s, ax, ay, az);
+    j += 2;
+  }
+  if (j < cnt) {
+    const float rx = o8_sub(qx, ch.x[j]), ry = o8_sub(qy, ch.y[j]), rz = o8_sub(qz, ch.z[j]);
+    if (KERNEL == O8_SOFT)
+      o8_soft_force(rx, ry, rz, ch.nm[j], eps2, s, ax, ay, az);
+    else
+      o8_soft_vjp(rx, ry, rz, ch.nm[j], gx, gy, gz, eps2, s, ax, ay, az);
+  }
+}
+
+// Whether every pair of the query with a particle inside the cell (centre
+// c, half size h, as o8_in_cell tests it) lies in the att = 1 range: the
+// farthest corner's squared distance stays under the unity radius, with an
+// absolute slack per axis (1e-6 of the magnitudes involved) and a relative
+// margin (1e-4) far above the rounding of the differences and of r^2.
+__device__ __forceinline__ bool o8_cell_unity(float qx, float qy, float qz, const OctreeNode8& nd, const Soft& s) {
+  if (!(s.cutoff > 0.0f)) return true;
+  const float h = nd.half_size;
+  const float mx = fabsf(qx - nd.cx) + h + 1e-6f * (fabsf(qx) + fabsf(nd.cx) + h);
+  const float my = fabsf(qy - nd.cy) + h + 1e-6f * (fabsf(qy) + fabsf(nd.cy) + h);
+  const float mz = fabsf(qz - nd.cz) + h + 1e-6f * (fabsf(qz) + fabsf(nd.cz) + h);
+  const float R2 = mx * mx + my * my + mz * mz;
+  return R2 * 1.0001f + 1e-12f < s.unity_r2;
+}
+
+__device__ __forceinline__ bool o8_in_cell(float px, float py, float pz, const OctreeNode8& nd) {
+  const float h = nd.half_size;
+  return fabsf(px - nd.cx) <= h && fabsf(py - nd.cy) <= h && fabsf(pz - nd.cz) <= h;
 }
 
 template <int KERNEL>
@@ -517,10 +789,8 @@ struct O8StackEntry {
   uint32_t lanes;
 };
 
-constexpr int kO8LeafChunk = 32;
-
 __host__ __device__ constexpr size_t o8_warp_smem(int warps, int stack) {
-  return static_cast<size_t>(warps) * (kO8LeafChunk * sizeof(float4) + stack * sizeof(O8StackEntry));
+  return static_cast<size_t>(warps) * (sizeof(O8Chunk) + stack * sizeof(O8StackEntry));
 }
 
 template <int KERNEL, int STACK>
@@ -531,8 +801,9 @@ __global__ void __launch_bounds__(1024)
                       O8Bounds bd, const uint32_t* __restrict__ order) {
   extern __shared__ float4 o8_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float4* chunk = o8_smem + warp * kO8LeafChunk;
-  O8StackEntry* stack = reinterpret_cast<O8StackEntry*>(o8_smem + (blockDim.x >> 5) * kO8LeafChunk) + warp * STACK;
+  O8Chunk& chunk = reinterpret_cast<O8Chunk*>(o8_smem)[warp];
+  O8StackEntry* stack = reinterpret_cast<O8StackEntry*>(reinterpret_cast<O8Chunk*>(o8_smem) + (blockDim.x >> 5)) +
+                        warp * STACK;
   const int64_t ti = (static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + warp) * 32 + lane;
   const bool valid = ti < nq;
   const uint32_t live = __ballot_sync(0xffffffffu, valid);
@@ -572,19 +843,43 @@ __global__ void __launch_bounds__(1024)
     if (nd.is_leaf) {  // warp-uniform: every lane reads the same node
       if (__ballot_sync(0xffffffffu, far)) {
         const uint32_t start = nd.start, end = o8_leaf_end(start, nd.end, bd, status);
+        constexpr bool kSoft = KERNEL == O8_SOFT || KERNEL == O8_SOFT_VJP;
+        const bool q_unity = !far || o8_cell_unity(qx, qy, qz, nd, s);
+        // chunks of 32 particles, one per lane, the next one loaded while
+        // the current one is summed
+        float4 nxt = make_float4(0.f, 0.f, 0.f, 0.f);
+        float nxt_m = 0.f;
+        if (start + lane < end) {
+          nxt = __ldg(reinterpret_cast<const float4*>(leaf + start + lane));
+          nxt_m = __ldg(&leaf[start + lane].mass);
+        }
         for (uint32_t c = start; c < end; c += kO8LeafChunk) {
           const uint32_t i = c + lane;
+          bool in_cell = true;
           if (i < end) {
-            const float4 a = __ldg(reinterpret_cast<const float4*>(leaf + i));
-            chunk[lane] = make_float4(a.x, a.y, a.z, __ldg(&leaf[i].mass));
+            chunk.x[lane] = nxt.x;
+            chunk.y[lane] = nxt.y;
+            chunk.z[lane] = nxt.z;
+            chunk.nm[lane] = -nxt_m;
+            in_cell = o8_in_cell(nxt.x, nxt.y, nxt.z, nd);
           }
+          if (i + kO8LeafChunk < end) {
+            nxt = __ldg(reinterpret_cast<const float4*>(leaf + i + kO8LeafChunk));
+            nxt_m = __ldg(&leaf[i + kO8LeafChunk].mass);
+          }
+          const bool unity = __all_sync(0xffffffffu, in_cell && q_unity);
           __syncwarp();
           const int cnt = end - c < kO8LeafChunk ? static_cast<int>(end - c) : kO8LeafChunk;
           if (far) {
-#pragma unroll 4
-            for (int j = 0; j < cnt; j++) {
-              const float4 p = chunk[j];
-              o8_pair<KERNEL>(qx, qy, qz, p.x, p.y, p.z, p.w, gx, gy, gz, s, per, ax, ay, az);
+            if (kSoft && !per.on) {
+              if (unity)
+                o8_chunk_sum<KERNEL, false>(chunk, cnt, qx, qy, qz, gx, gy, gz, s, ax, ay, az);
+              else
+                o8_chunk_sum<KERNEL, true>(chunk, cnt, qx, qy, qz, gx, gy, gz, s, ax, ay, az);
+            } else {
+              for (int j = 0; j < cnt; j++)
+                o8_pair<KERNEL>(qx, qy, qz, chunk.x[j], chunk.y[j], chunk.z[j], -chunk.nm[j], gx, gy, gz, s, per,
+                                ax, ay, az);
             }
           }
           __syncwarp();  // the chunk is read before the next one overwrites it

@@ -459,6 +459,17 @@ def test_octree8_query_order_changes_no_result(cuda):
                                                               1, 4.0, 0, 1.0, 256, w, wb))
     both(lambda o, w, wb: L.sbh_barnes_hut_force_octree8_soft_vjp(s, lp, lb, np_, nb, Q.data_ptr(), nq, C.data_ptr(),
                                                                   o, 2.0, 1e-2, 0.5, 1, 4.0, 0, 1.0, 256, w, wb))
+    # The attenuation range against the depth-6 leaf cells (about 0.3 wide):
+    # no pair attenuated (the "no cutoff" convention of 1e6 box sizes); an
+    # att = 1 radius of cutoff / 256 = 0.5, which some leaves lie wholly
+    # inside and others straddle; and a periodic box (scalar pair form).
+    span = float((p.max(0) - p.min(0)).max())
+    for cut, per, box in ((1e6 * span, 0, 1.0), (128.0, 0, 1.0), (0.5, 1, 1.1 * span)):
+        both(lambda o, w, wb: L.sbh_barnes_hut_force_octree8_soft(s, lp, lb, np_, nb, Q.data_ptr(), nq, o, 2.0, 1e-2,
+                                                                  cut, 0, 4.0, per, box, 256, w, wb))
+        both(lambda o, w, wb: L.sbh_barnes_hut_force_octree8_soft_vjp(s, lp, lb, np_, nb, Q.data_ptr(), nq,
+                                                                      C.data_ptr(), o, 2.0, 1e-2, cut, 0, 4.0, per,
+                                                                      box, 256, w, wb))
     for soft in (0, 1):
         both(lambda o, w, wb: L.sbh_stochastic_bh_force_octree8(s, soft, lp, lb, np_, nb, Q.data_ptr(), nq, o, 2, 7,
                                                                 2.0, 1e-2, 0.5, 1, 4.0, 0, 1.0, 256, w, wb))
