@@ -669,12 +669,27 @@ __device__ __forceinline__ bool o8_in_cell(float px, float py, float pz, const O
   return fabsf(px - nd.cx) <= h && fabsf(py - nd.cy) <= h && fabsf(pz - nd.cz) <= h;
 }
 
+// One query's terms from leaf particles [start, end), in order; softened
+// pairs without a periodic box go two at a time through o8_pair2.
 template <int KERNEL>
 __device__ __forceinline__ void o8_leaf_sum(const Leaf3* __restrict__ leaf, uint32_t start, uint32_t end,
                                             float qx, float qy, float qz, float gx, float gy, float gz,
                                             const Soft& s, const Periodic& per, float& ax, float& ay,
                                             float& az) {
-  for (uint32_t i = start; i < end; i++) {
+  uint32_t i = start;
+  if ((KERNEL == O8_SOFT || KERNEL == O8_SOFT_VJP) && !per.on) {
+    const F2 QX = f2_pack(qx, qx), QY = f2_pack(qy, qy), QZ = f2_pack(qz, qz);
+    const F2 GX = f2_pack(gx, gx), GY = f2_pack(gy, gy), GZ = f2_pack(gz, gz);
+    const float eps2 = o8_mul(s.eps, s.eps);
+    for (; i + 1 < end; i += 2) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(leaf + i));
+      const float4 b = __ldg(reinterpret_cast<const float4*>(leaf + i + 1));
+      const float ma = __ldg(&leaf[i].mass), mb = __ldg(&leaf[i + 1].mass);
+      o8_pair2<KERNEL, true>(QX, QY, QZ, f2_pack(a.x, b.x), f2_pack(a.y, b.y), f2_pack(a.z, b.z), f2_pack(-ma, -mb),
+                             GX, GY, GZ, eps2, s, ax, ay, az);
+    }
+  }
+  for (; i < end; i++) {
     const float4* p = reinterpret_cast<const float4*>(leaf + i);
     float4 a = __ldg(p);
     float m = __ldg(&leaf[i].mass);
