@@ -669,6 +669,171 @@ __device__ __forceinline__ bool o8_in_cell(float px, float py, float pz, const O
   return fabsf(px - nd.cx) <= h && fabsf(py - nd.cy) <= h && fabsf(pz - nd.cz) <= h;
 }
 
+// Direct softened sums without a periodic box, two queries per thread (q
+// and q + blockDim.x of the block's 2 blockDim.x queries). Particles are
+// staged per tile already splatted ((x, x), (y, y), (z, z), (-m, -m)), so each
+// shared-memory read lands in a packed register pair. When every pair of the
+// tile with the block's queries lies in the att = 1 range (the farthest
+// corners of the two bounding boxes, with margins, inside the unity radius:
+// always so under the "no cutoff" convention), each particle meets both
+// queries in one pass of FFMA2 / FADD2 / FMUL2 in the fixed order of
+// o8_soft_force and o8_soft_vjp, with the tile sums packed too. Otherwise the
+// tile takes those scalar forms query by query. Both round every component
+// the same way. Each tile's sum joins the query's Kahan-compensated total,
+// as in direct_soft_kernel.
+struct __align__(16) DirectSplat {
+  F2 x, y, z, nm;
+};
+
+constexpr int kDirectWarps = kDirectThreads / 32;
+
+// Box of the block's values: v[0..2] minima, v[3..5] maxima over the warp,
+// then over the warps through part[kDirectWarps][8] (the caller syncs the
+// block between the two calls).
+__device__ __forceinline__ void direct_box_warp(float* v, float (*part)[8]) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      v[d] = fminf(v[d], __shfl_xor_sync(0xffffffffu, v[d], o));
+      v[3 + d] = fmaxf(v[3 + d], __shfl_xor_sync(0xffffffffu, v[3 + d], o));
+    }
+  if ((threadIdx.x & 31) == 0)
+    for (int d = 0; d < 6; d++) part[threadIdx.x >> 5][d] = v[d];
+}
+
+__device__ __forceinline__ void direct_box_block(float* v, const float (*part)[8]) {
+  for (int d = 0; d < 3; d++) {
+    v[d] = part[0][d];
+    v[3 + d] = part[0][3 + d];
+  }
+  for (int w = 1; w < kDirectWarps; w++)
+    for (int d = 0; d < 3; d++) {
+      v[d] = fminf(v[d], part[w][d]);
+      v[3 + d] = fmaxf(v[3 + d], part[w][3 + d]);
+    }
+}
+
+template <bool VJP>
+__global__ void __launch_bounds__(kDirectThreads, 4)
+    direct_soft2_kernel(const float* __restrict__ pts, const float* __restrict__ masses, int64_t n,
+                        const float* __restrict__ queries, const float* __restrict__ cot, int64_t nq,
+                        float* __restrict__ out, Soft s) {
+  __shared__ DirectSplat tile[kDirectThreads];
+  __shared__ float qpart[kDirectWarps][8], tpart[kDirectWarps][8];
+  const int64_t qa = static_cast<int64_t>(blockIdx.x) * (2 * kDirectThreads) + threadIdx.x;
+  const int64_t qb = qa + kDirectThreads;
+  float q[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}, g[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int64_t qi = t ? qb : qa;
+    if (qi < nq) {
+      for (int d = 0; d < 3; d++) {
+        q[t][d] = queries[3 * qi + d];
+        if (VJP) g[t][d] = cot[3 * qi + d];
+      }
+    }
+  }
+  float qbox[6];
+  for (int d = 0; d < 3; d++) {
+    qbox[d] = fminf(q[0][d], q[1][d]);
+    qbox[3 + d] = fmaxf(q[0][d], q[1][d]);
+  }
+  direct_box_warp(qbox, qpart);
+  const F2 QX = f2_pack(q[0][0], q[1][0]), QY = f2_pack(q[0][1], q[1][1]), QZ = f2_pack(q[0][2], q[1][2]);
+  const F2 GX = f2_pack(g[0][0], g[1][0]), GY = f2_pack(g[0][1], g[1][1]), GZ = f2_pack(g[0][2], g[1][2]);
+  const float eps2 = o8_mul(s.eps, s.eps);
+  const F2 EPS2 = f2_pack(eps2, eps2), M3 = f2_pack(-3.0f, -3.0f), ZERO = f2_pack(0.0f, 0.0f);
+  float sum[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}, comp[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+  for (int64_t base = 0; base < n; base += kDirectThreads) {
+    const int64_t j = base + threadIdx.x;
+    float px = 0.f, py = 0.f, pz = 0.f, pm = 0.f;
+    float tbox[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    if (j < n) {
+      px = pts[3 * j];
+      py = pts[3 * j + 1];
+      pz = pts[3 * j + 2];
+      pm = masses[j];
+      tbox[0] = tbox[3] = px;
+      tbox[1] = tbox[4] = py;
+      tbox[2] = tbox[5] = pz;
+    }
+    tile[threadIdx.x] = DirectSplat{f2_pack(px, px), f2_pack(py, py), f2_pack(pz, pz), f2_pack(-pm, -pm)};
+    direct_box_warp(tbox, tpart);
+    __syncthreads();
+    // the farthest corners of the query box and the tile box (block-uniform)
+    bool unity = !(s.cutoff > 0.0f);
+    if (!unity) {
+      float qb6[6], tb6[6], R2 = 0.0f;
+      direct_box_block(qb6, qpart);
+      direct_box_block(tb6, tpart);
+      for (int d = 0; d < 3; d++) {
+        const float span = fmaxf(fabsf(qb6[3 + d] - tb6[d]), fabsf(tb6[3 + d] - qb6[d]));
+        const float mag = fmaxf(fmaxf(fabsf(qb6[d]), fabsf(qb6[3 + d])), fmaxf(fabsf(tb6[d]), fabsf(tb6[3 + d])));
+        const float m = span + 1e-6f * mag;
+        R2 += m * m;
+      }
+      unity = R2 * 1.0001f + 1e-12f < s.unity_r2;
+    }
+    const int cnt = static_cast<int>(n - base < kDirectThreads ? n - base : kDirectThreads);
+    float a[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+    if (unity) {
+      F2 AX = ZERO, AY = ZERO, AZ = ZERO;
+#pragma unroll 4
+      for (int k = 0; k < cnt; k++) {
+        const DirectSplat p = tile[k];
+        const F2 rx = o8_sub(QX, p.x), ry = o8_sub(QY, p.y), rz = o8_sub(QZ, p.z);
+        F2 r2, ir;
+        o8_soft_head(rx, ry, rz, EPS2, r2, ir);
+        const F2 ir3 = o8_mul(o8_mul(ir, ir), ir);
+        if (!VJP) {
+          const F2 c = o8_mul(p.nm, ir3);
+          AX = o8_fma(c, rx, AX);
+          AY = o8_fma(c, ry, AY);
+          AZ = o8_fma(c, rz, AZ);
+        } else {
+          const F2 ir5 = o8_mul(o8_mul(ir3, ir), ir);
+          const F2 rg = o8_fma(rz, GZ, o8_fma(ry, GY, o8_mul(rx, GX)));
+          const F2 nrad = o8_mul(rg, o8_mul(M3, ir5));
+          AX = o8_fma(p.nm, o8_fma(nrad, rx, o8_mul(ir3, GX)), AX);
+          AY = o8_fma(p.nm, o8_fma(nrad, ry, o8_mul(ir3, GY)), AY);
+          AZ = o8_fma(p.nm, o8_fma(nrad, rz, o8_mul(ir3, GZ)), AZ);
+        }
+      }
+      f2_unpack(AX, a[0][0], a[1][0]);
+      f2_unpack(AY, a[0][1], a[1][1]);
+      f2_unpack(AZ, a[0][2], a[1][2]);
+    } else {
+      for (int k = 0; k < cnt; k++) {
+        const DirectSplat p = tile[k];
+        float x, y, z, nm, unused;
+        f2_unpack(p.x, x, unused);
+        f2_unpack(p.y, y, unused);
+        f2_unpack(p.z, z, unused);
+        f2_unpack(p.nm, nm, unused);
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          const float rx = o8_sub(q[t][0], x), ry = o8_sub(q[t][1], y), rz = o8_sub(q[t][2], z);
+          if (VJP)
+            o8_soft_vjp(rx, ry, rz, nm, g[t][0], g[t][1], g[t][2], eps2, s, a[t][0], a[t][1], a[t][2]);
+          else
+            o8_soft_force(rx, ry, rz, nm, eps2, s, a[t][0], a[t][1], a[t][2]);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; t++)
+      for (int d = 0; d < 3; d++) kahan_add(sum[t][d], comp[t][d], a[t][d]);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int64_t qi = t ? qb : qa;
+    if (qi < nq)
+      for (int d = 0; d < 3; d++) out[3 * qi + d] = sum[t][d];
+  }
+}
+
 // One query's terms from leaf particles [start, end), in order; softened
 // pairs without a periodic box go two at a time through o8_pair2.
 template <int KERNEL>
@@ -1295,10 +1460,13 @@ int sbh_direct_force_soft(cudaStream_t stream, const float* points, const float*
   if (int rc = check_threads(threads)) return rc;
   if (nq == 0) return SBH_OK;
   const bool per = periodic && box_length > 0.0f;
-  auto k = per ? direct_soft_kernel<0, true> : direct_soft_kernel<0, false>;
-  k<<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(points, masses, n, queries, nullptr, nq, out,
-                                                                 Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
-                                                                 Periodic{periodic, box_length});
+  const Soft soft{fmaxf(softening_scale, 0.0f), cutoff_scale};
+  if (per)
+    direct_soft_kernel<0, true><<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(
+        points, masses, n, queries, nullptr, nq, out, soft, Periodic{periodic, box_length});
+  else
+    direct_soft2_kernel<false><<<grid_for(nq, 2 * kDirectThreads), kDirectThreads, 0, stream>>>(
+        points, masses, n, queries, nullptr, nq, out, soft);
   return check_launch("direct_force_soft");
 }
 
@@ -1312,10 +1480,13 @@ int sbh_direct_force_soft_vjp(cudaStream_t stream, const float* points, const fl
   if (int rc = check_threads(threads)) return rc;
   if (nq == 0) return SBH_OK;
   const bool per = periodic && box_length > 0.0f;
-  auto k = per ? direct_soft_kernel<1, true> : direct_soft_kernel<1, false>;
-  k<<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(points, masses, n, queries, cotangent, nq, out,
-                                                                 Soft{fmaxf(softening_scale, 0.0f), cutoff_scale},
-                                                                 Periodic{periodic, box_length});
+  const Soft soft{fmaxf(softening_scale, 0.0f), cutoff_scale};
+  if (per)
+    direct_soft_kernel<1, true><<<grid_for(nq, kDirectThreads), kDirectThreads, 0, stream>>>(
+        points, masses, n, queries, cotangent, nq, out, soft, Periodic{periodic, box_length});
+  else
+    direct_soft2_kernel<true><<<grid_for(nq, 2 * kDirectThreads), kDirectThreads, 0, stream>>>(
+        points, masses, n, queries, cotangent, nq, out, soft);
   return check_launch("direct_force_soft_vjp");
 }
 
